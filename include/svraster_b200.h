@@ -1,0 +1,192 @@
+/*
+ * svraster_b200 -- C ABI of the B200 (sm_100a) sparse-voxel SDF rasterizer.
+ *
+ * Plain pointers, sizes and a CUDA stream (passed as void*); no framework types.  Every
+ * pointer argument is a DEVICE pointer unless its name ends in _host.  Every entry point
+ * returns 0 on success or a negative svr_status_t; svr_last_error() gives a message.
+ * Launches are asynchronous on `stream` unless noted.  Entry points that size their work
+ * from device data (svr_count_rendered, svr_valid_table_count) synchronise `stream`.
+ *
+ * The functions replace the native ops of the reference's `svraster_cuda._C` module
+ * (cuda/binding.cpp:28-56); each declaration names the reference function it stands for.
+ */
+#ifndef SVRASTER_B200_H
+#define SVRASTER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SVR_API __attribute__((visibility("default")))
+#else
+#define SVR_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    SVR_OK = 0,
+    SVR_ERR_ARG = -1,        /* bad argument (size, mode, null pointer)            */
+    SVR_ERR_CUDA = -2,       /* a CUDA runtime call failed                          */
+    SVR_ERR_CAPACITY = -3,   /* a caller-provided buffer is too small               */
+    SVR_ERR_DEVICE = -4,     /* a kernel reported an error through its status word  */
+    SVR_ERR_UNSUPPORTED = -5 /* mode not supported by this build                    */
+} svr_status_t;
+
+/* One camera.  A batch of views is an array of these; views are rendered into packed
+ * outputs where view v owns pixels [pix_offset, pix_offset + W*H) of every plane and
+ * tiles [tile_offset, tile_offset + tiles_x*tiles_y) of the tile arrays.
+ * Matches RasterSettings (cuda/svraster_cuda/renderer.py:16-41): w2c / c2w are row-major
+ * 4x4 float32 device matrices of which the first 3 rows are used; bg is 3 floats. */
+typedef struct {
+    int32_t width, height;
+    int32_t tiles_x, tiles_y;
+    int32_t tile_offset;
+    int32_t pad0;
+    int64_t pix_offset;
+    float tanfovx, tanfovy, cx, cy;
+    float near_plane;
+    float pad1;
+    const float* w2c;
+    const float* c2w;
+    const float* bg;
+} svr_view_t;
+
+/* Maximum number of views in one batched launch. */
+#define SVR_MAX_VIEWS 128
+#define SVR_TILE 16
+
+SVR_API const char* svr_last_error(void);
+SVR_API int svr_version(void);
+
+/* ---------------------------------------------------------------- preprocess
+ * Replaces _C.rasterize_preprocess (cuda/src/preprocess.cu:158-228).
+ * Per view v and voxel i writes n_dup[v*N + i] (int32) and the view's geometry state into
+ * geom_buffer (svr_geom_buffer_bytes(N * n_views) bytes, 256-aligned device memory). */
+SVR_API size_t svr_geom_buffer_bytes(int64_t n_items);
+SVR_API int svr_preprocess(const svr_view_t* views_host, int n_views, int N,
+                   const float* centers, const float* lengths, const uint8_t* is_leaf,
+                   const int64_t* octpaths,
+                   int32_t* out_n_dup, void* geom_buffer, void* stream);
+
+/* Read the per-voxel geometry fields back out of a geom buffer (for tests and
+ * reference-compatible debugging): n_dup u32[M], bboxes u32[M,2], quadrant bits u32[M]. */
+SVR_API int svr_unpack_geom(const void* geom_buffer, int64_t n_items, uint32_t* n_dup, uint32_t* bboxes,
+                    uint32_t* bits, void* stream);
+
+/* Prefix-sum the duplication counts and return the total number of (tile, voxel, octant)
+ * records R and the OR of the octree paths of every rendered voxel (used to trim the
+ * sort key).  Synchronises `stream` (the reference does the same, forward.cu:892-896). */
+SVR_API int svr_count_rendered(int64_t n_items, void* geom_buffer, int64_t* num_rendered_host,
+                       uint64_t* path_or_host, void* stream);
+
+/* ---------------------------------------------------------------- binning
+ * Replaces the duplicate/sort/range part of rasterize_voxels_procedure
+ * (cuda/src/forward.cu:749-829, 882-939): emits (tile | order-rank, octant | voxel) pairs,
+ * sorts them with a stable radix sort whose key is trimmed to the bits that can differ
+ * (order-equivalent to the reference's 64-bit key), and writes per-tile [start, end). */
+SVR_API size_t svr_binning_buffer_bytes(int64_t num_rendered, int total_tiles);
+SVR_API size_t svr_image_buffer_bytes(int64_t total_pixels, int total_tiles);
+SVR_API int svr_bin_and_sort(const svr_view_t* views_host, int n_views, int N, int64_t num_rendered,
+                     uint64_t path_or, const int64_t* octpaths, void* geom_buffer,
+                     void* binning_buffer, size_t binning_bytes, void* image_buffer, void* stream);
+
+/* Sorted per-tile values (octant << 29 | voxel id) and tile ranges, for tests. */
+SVR_API int svr_unpack_binning(const void* binning_buffer, int64_t num_rendered, int total_tiles,
+                       const void* image_buffer, int64_t total_pixels, uint32_t* vals,
+                       uint32_t* ranges, uint32_t* tile_last, uint32_t* n_contrib, void* stream);
+
+/* ---------------------------------------------------------------- render
+ * Replaces _C.rasterize_voxels (cuda/src/forward.cu:986-1096) for the SDF density mode.
+ * geos f32[N,8], rgbs f32[n_rgb_views*N, 3] (one block per view when n_rgb_views ==
+ * n_views, else shared), s_val f32[1] on the device.  Outputs are packed per view (see
+ * svr_view_t): color f32[3*P], depth f32[4*P] (may be NULL when !need_depth), normal
+ * f32[3*P] (NULL when !need_normal), T f32[P], max_w f32[N] (NULL unless tracking).
+ * n_samp in {1,2,3} (vox_geo_mode triinterp1 / triinterp / triinterp3). */
+SVR_API int svr_render_fwd(const svr_view_t* views_host, int n_views, int N, int64_t num_rendered,
+                   int n_samp, int need_depth, int need_normal,
+                   const float* centers, const float* lengths, const float* geos, const float* rgbs,
+                   int n_rgb_views, const float* s_val, void* geom_buffer, void* binning_buffer,
+                   void* image_buffer, float* out_color, float* out_depth, float* out_normal,
+                   float* out_T, float* max_w, void* stream);
+
+/* Replaces _C.rasterize_voxels_backward (cuda/src/backward.cu:986-1109), SDF density
+ * (always three sub-samples, backward.cu:944-946).  Accumulates into dL_dvox f32[N,12]
+ * ([8 corner SDF | 3 rgb | |dL/dalpha * alpha|], caller zeroes it; with n_rgb_views ==
+ * n_views the rgb gradient goes to drgbs f32[n_views*N,3] instead when non-NULL) and
+ * dL_ds f32[1].  gt_color f32[3*P] is read only when lambda_R_concen > 0. */
+SVR_API int svr_render_bwd(const svr_view_t* views_host, int n_views, int N, int64_t num_rendered,
+                   int need_depth, int need_normal, float lambda_R_concen, const float* gt_color,
+                   const float* s_val, void* binning_buffer, void* image_buffer,
+                   const float* out_T, const float* dL_dcolor, const float* dL_ddepth,
+                   const float* dL_dnormal, const float* dL_dT,
+                   float* dL_dvox, float* drgbs, float* dL_ds, void* stream);
+
+/* Device status word of the raster launches that used this image buffer (0 = clean;
+ * bit 1 wait timeout, bit 2 index out of range, bit 4 duplicate count mismatch).
+ * Synchronises `stream`.  Replaces the reference's __trap() sanity checks
+ * (preprocess.cu:141-146, forward.cu:796-801, backward.cu:126-137). */
+SVR_API int svr_read_status(const void* image_buffer, int64_t total_pixels, int total_tiles,
+                    uint32_t* status_host, void* stream);
+
+/* ---------------------------------------------------------------- per-voxel parameters
+ * Replace _C.gather_triinterp_geo_params[_bw] (cuda/src/geo_params_gather.cu:134-173). */
+SVR_API int svr_gather_geo(int64_t n_care, const int64_t* care_idx, const int64_t* vox_key,
+                   const float* grid_pts, float* geos, void* stream);
+SVR_API int svr_gather_geo_bw(int64_t n_care, const int64_t* care_idx, const int64_t* vox_key,
+                      const float* dL_dgeos, float* dL_dgrid, void* stream);
+
+/* Replace _C.sh_compute / _C.sh_compute_bw (cuda/src/sh_compute.cu:243-299).  n_idx == 0
+ * means all N voxels.  sh0 f32[N,3], shs f32[N,M-1,3]. */
+SVR_API int svr_sh_eval(int N, int64_t n_idx, const int64_t* idx, int degree, int M,
+                const float* centers, const float* cam_pos, const float* sh0, const float* shs,
+                float* rgbs, void* stream);
+SVR_API int svr_sh_eval_bw(int N, int64_t n_idx, const int64_t* idx, int degree, int M,
+                   const float* centers, const float* cam_pos, const float* dL_drgbs,
+                   float* dL_dsh0, float* dL_dshs, void* stream);
+
+/* ---------------------------------------------------------------- grid regularisers
+ * Replace _C.valid_gradient_table (cuda/src/utils.cu:362-408) + the key sort of
+ * src/utils/octree_utils.py:293-314.  Two calls sharing one workspace: count (synchronises;
+ * workspace >= svr_valid_table_workspace_bytes(N, 0)), then fill (workspace >=
+ * svr_valid_table_workspace_bytes(N, count)).  grid_mask is u8[res^3], res = 2^res_pow2. */
+SVR_API size_t svr_valid_table_workspace_bytes(int N, int64_t count);
+SVR_API int svr_valid_table_count(int N, const float* centers, const float* sizes,
+                          const float* scene_center, float inside_extent, int res_pow2,
+                          const uint8_t* is_leaf, void* workspace, int64_t* count_host,
+                          void* stream);
+SVR_API int svr_valid_table_fill(int N, const float* centers, const float* sizes,
+                         const float* scene_center, float inside_extent, int res_pow2,
+                         const uint8_t* is_leaf, int64_t count, void* workspace,
+                         uint8_t* grid_mask, int32_t* grid_keys, int32_t* grid2voxel,
+                         void* stream);
+
+/* Replace _C.laplacian_smoothness_bw (cuda/src/ls_compute.cu:111-153) and
+ * _C.grid_eikonal_bw (cuda/src/ge_compute.cu:119-160); accumulate into grid_grad f32[M].
+ * `seed` replaces the reference's clock64() seed so runs are reproducible; `status` is a
+ * device u32 that collects index errors (0 when clean). */
+SVR_API int svr_laplacian_bw(int G, int A, const int32_t* active, const int32_t* grid_keys,
+                     const int32_t* grid2voxel, int grid_res, const uint8_t* grid_mask,
+                     const float* voxel_coords, const float* voxel_sizes, int N,
+                     const int64_t* vox_key, const float* grid_pts, int M, float weight,
+                     float vox_size_inv, int seed, float* grid_grad, uint32_t* status,
+                     void* stream);
+SVR_API int svr_eikonal_bw(int G, int A, const int32_t* active, const int32_t* grid_keys,
+                   const int32_t* grid2voxel, int grid_res, const uint8_t* grid_mask,
+                   const float* voxel_coords, const float* voxel_sizes, int N,
+                   const int64_t* vox_key, const float* grid_pts, int M, float weight,
+                   float vox_size_inv, int seed, float* grid_grad, uint32_t* status,
+                   void* stream);
+
+/* ---------------------------------------------------------------- optimiser
+ * Replace _C.unbiased_adam_step / _C.biased_adam_step (cuda/src/adam_step.cu:106-159). */
+SVR_API int svr_adam_step(int64_t numel, int biased, int sparse, float* param, const float* grad,
+                  float* exp_avg, float* exp_avg_sq, double step, double lr, double beta1,
+                  double beta2, float eps, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,194 @@
+"""ctypes front-end of the C oracle (``svr_oracle.c``) -- TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` use
+this module, and only as a checker or a timed CPU baseline.  Everything takes and returns
+numpy arrays in the reference's layouts (see ``svr_oracle.c`` for the file:line map).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SO = {32: os.path.join(_HERE, "_build", "libsvr_oracle.so"), 64: os.path.join(_HERE, "_build", "libsvr_oracle64.so")}
+_libs = {}
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib(bits=32):
+    """The single-precision checker (bits=32) or the FP64 per-ray oracle (bits=64)."""
+    if bits not in _libs:
+        if not os.path.exists(_SO[bits]):
+            build()
+        L = C.CDLL(_SO[bits])
+        L.svo_num_rendered.restype = C.c_int64
+        L.svo_valid_table_count.restype = C.c_int64
+        _libs[bits] = L
+    return _libs[bits]
+
+
+def _r(x, bits):
+    return C.c_double(float(x)) if bits == 64 else C.c_float(float(x))
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def _f(x):
+    return C.c_float(float(x))
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def preprocess(cam, centers, lengths, is_leaf):
+    """cuda/src/preprocess.cu:36-154 -> (n_dup int32[N], bboxes uint32[N,2], bits uint32[N])."""
+    centers = _c(centers, np.float32); lengths = _c(lengths, np.float32).reshape(-1)
+    is_leaf = _c(is_leaf, np.uint8).reshape(-1)
+    N = len(lengths)
+    ndup = np.zeros(N, np.int32); bb = np.zeros((N, 2), np.uint32); bits = np.zeros(N, np.uint32)
+    lib().svo_preprocess(C.c_int(N), C.c_int(cam.width), C.c_int(cam.height), _f(cam.tanfovx), _f(cam.tanfovy),
+                         _f(cam.cx), _f(cam.cy), _p(_c(cam.w2c, np.float32)), _p(_c(cam.c2w, np.float32)),
+                         _f(cam.near), _p(centers), _p(lengths), _p(is_leaf), _p(ndup), _p(bb), _p(bits))
+    return ndup, bb, bits
+
+
+def binning(cam, octpath, ndup, bboxes, bits):
+    """forward.cu:749-829 + stable sort -> (keys uint64[R], vals uint32[R], ranges uint32[T,2])."""
+    ndup = _c(ndup, np.int32)
+    R = lib().svo_num_rendered(C.c_int(len(ndup)), _p(ndup))
+    gx, gy = (cam.width + 15) // 16, (cam.height + 15) // 16
+    keys = np.zeros(max(R, 1), np.uint64); vals = np.zeros(max(R, 1), np.uint32)
+    ranges = np.zeros((gx * gy, 2), np.uint32)
+    lib().svo_binning(C.c_int(len(ndup)), C.c_int(cam.width), C.c_int(cam.height), _p(_c(octpath, np.int64)),
+                      _p(ndup), _p(_c(bboxes, np.uint32)), _p(_c(bits, np.uint32)), _p(keys), _p(vals), _p(ranges))
+    return keys[:R], vals[:R], ranges
+
+
+def render_fwd(cam, bg, n_samp, need_depth, need_normal, ranges, vals, bboxes, centers, lengths, geos, rgbs,
+               s_val, track_max_w=False, bits=32):
+    """forward.cu:41-564 (SDF) -> dict of outputs in the reference layouts.  ``bits=64``
+    evaluates the same per-ray algorithm in double precision."""
+    W, H = cam.width, cam.height
+    dt = np.float64 if bits == 64 else np.float32
+    N = len(lengths.reshape(-1))
+    T_t = ((W + 15) // 16) * ((H + 15) // 16)
+    o = dict(color=np.zeros((3, H, W), dt), depth=np.zeros((4, H, W), dt),
+             normal=np.zeros((3, H, W), dt), T=np.zeros((1, H, W), dt),
+             max_w=np.zeros((N, 1), dt) if track_max_w else None,
+             tile_last=np.zeros(T_t, np.uint32), n_contrib=np.zeros(H * W, np.uint32))
+    vals = _c(vals, np.uint32)
+    lib(bits).svo_render_fwd(C.c_int(W), C.c_int(H), _f(cam.tanfovx), _f(cam.tanfovy), _f(cam.cx), _f(cam.cy),
+                             _p(_c(cam.c2w, np.float32)), _p(_c(bg, np.float32)), C.c_int(n_samp),
+                             C.c_int(int(need_depth)), C.c_int(int(need_normal)), _p(_c(ranges, np.uint32)),
+                             _p(vals if len(vals) else np.zeros(1, np.uint32)), _p(_c(bboxes, np.uint32)),
+                             _p(_c(centers, dt)), _p(_c(lengths, dt)), _p(_c(geos, dt)),
+                             _p(_c(rgbs, dt)), _r(s_val, bits), _p(o["color"]), _p(o["depth"]), _p(o["normal"]),
+                             _p(o["T"]), _p(o["max_w"]), _p(o["tile_last"]), _p(o["n_contrib"]))
+    return o
+
+
+def render_bwd(cam, bg, need_depth, need_normal, ranges, tile_last, vals, bboxes, centers, lengths, geos, rgbs,
+               s_val, out_T, n_contrib, dcolor, ddepth, dnormal, dT, lambda_R_concen=0.0, gt_color=None, bits=32):
+    """backward.cu:41-851 (SDF, n_samp=3) -> (dL_dvox [N,12], dL_ds float)."""
+    W, H = cam.width, cam.height
+    dt = np.float64 if bits == 64 else np.float32
+    N = len(lengths.reshape(-1))
+    dvox = np.zeros((N, 12), dt)
+    ds = np.zeros(1, dt)
+    vals = _c(vals, np.uint32)
+    gt = _c(gt_color, dt) if gt_color is not None else np.zeros(3 * H * W, dt)
+    lib(bits).svo_render_bwd(C.c_int(W), C.c_int(H), _f(cam.tanfovx), _f(cam.tanfovy), _f(cam.cx), _f(cam.cy),
+                             _p(_c(cam.c2w, np.float32)), _p(_c(bg, np.float32)), C.c_int(int(need_depth)),
+                             C.c_int(int(need_normal)), _p(_c(ranges, np.uint32)), _p(_c(tile_last, np.uint32)),
+                             _p(vals if len(vals) else np.zeros(1, np.uint32)), _p(_c(bboxes, np.uint32)),
+                             _p(_c(centers, dt)), _p(_c(lengths, dt)), _p(_c(geos, dt)),
+                             _p(_c(rgbs, dt)), _r(s_val, bits), _p(_c(out_T, dt)),
+                             _p(_c(n_contrib, np.uint32)), _p(_c(dcolor, dt)), _p(_c(ddepth, dt)),
+                             _p(_c(dnormal, dt)), _p(_c(dT, dt)), _r(lambda_R_concen, bits), _p(gt),
+                             _p(dvox), _p(ds))
+    return dvox, float(ds[0])
+
+
+def gather_geo(care_idx, vox_key, grid, n_vox):
+    geos = np.zeros((n_vox, 8), np.float32)
+    care_idx = _c(care_idx, np.int64)
+    lib().svo_gather_geo(C.c_int(len(care_idx)), _p(care_idx), _p(_c(vox_key, np.int64)),
+                         _p(_c(grid, np.float32)), _p(geos))
+    return geos
+
+
+def gather_geo_bw(care_idx, vox_key, dgeos, n_grid):
+    dgrid = np.zeros((n_grid, 1), np.float32)
+    care_idx = _c(care_idx, np.int64)
+    lib().svo_gather_geo_bw(C.c_int(len(care_idx)), _p(care_idx), _p(_c(vox_key, np.int64)),
+                            _p(_c(dgeos, np.float32)), _p(dgrid))
+    return dgrid
+
+
+def sh_eval(deg, idx, centers, cam_pos, sh0, shs):
+    N = len(centers); M = 1 + shs.shape[1]
+    idx = _c(idx if idx is not None else np.zeros(0, np.int64), np.int64)
+    rgbs = np.zeros((N, 3), np.float32)
+    lib().svo_sh_eval(C.c_int(N), C.c_int(len(idx)), _p(idx if len(idx) else np.zeros(1, np.int64)), C.c_int(deg),
+                      C.c_int(M), _p(_c(centers, np.float32)), _p(_c(cam_pos, np.float32)),
+                      _p(_c(sh0, np.float32)), _p(_c(shs, np.float32)), _p(rgbs))
+    return rgbs
+
+
+def sh_eval_bw(deg, idx, centers, cam_pos, drgbs, M):
+    N = len(centers)
+    idx = _c(idx if idx is not None else np.zeros(0, np.int64), np.int64)
+    dsh0 = np.zeros((N, 3), np.float32); dshs = np.zeros((N, M - 1, 3), np.float32)
+    lib().svo_sh_eval_bw(C.c_int(N), C.c_int(len(idx)), _p(idx if len(idx) else np.zeros(1, np.int64)),
+                         C.c_int(deg), C.c_int(M), _p(_c(centers, np.float32)), _p(_c(cam_pos, np.float32)),
+                         _p(_c(drgbs, np.float32)), _p(dsh0), _p(dshs))
+    return dsh0, dshs
+
+
+def valid_table(centers, sizes, scene_center, inside_extent, res_pow2, is_leaf):
+    centers = _c(centers, np.float32); sizes = _c(sizes, np.float32).reshape(-1)
+    sc = _c(scene_center, np.float32); leaf = _c(is_leaf, np.uint8).reshape(-1)
+    N = len(sizes)
+    G = lib().svo_valid_table_count(C.c_int(N), _p(centers), _p(sizes), _p(sc), _f(inside_extent),
+                                    C.c_int(res_pow2), _p(leaf))
+    res = 1 << res_pow2
+    mask = np.zeros(res ** 3, np.uint8)
+    keys = np.zeros(max(G, 1), np.int32); g2v = np.zeros(max(G, 1), np.int32)
+    lib().svo_valid_table(C.c_int(N), _p(centers), _p(sizes), _p(sc), _f(inside_extent), C.c_int(res_pow2),
+                          _p(leaf), _p(mask), _p(keys), _p(g2v))
+    return mask.astype(bool), keys[:G], g2v[:G]
+
+
+def _grid_loss(fn, grid, vox_key, coords, vsizes, res, mask, keys, g2v, active, weight, vox_size_inv, seed, grad):
+    grad = _c(grad, np.float32).copy()
+    active = _c(active, np.int32)
+    fn(C.c_int(len(keys)), C.c_int(len(active)), _p(active), _p(_c(keys, np.int32)), _p(_c(g2v, np.int32)),
+       C.c_int(res), _p(_c(mask, np.uint8)), _p(_c(coords, np.float32)), _p(_c(vsizes, np.float32)),
+       _p(_c(vox_key, np.int64)), _p(_c(grid, np.float32)), _f(weight), _f(vox_size_inv), C.c_int(seed), _p(grad))
+    return grad
+
+
+def laplacian_bw(*a, **k):
+    """ls_compute.cu:14-109 with an explicit seed."""
+    return _grid_loss(lib().svo_laplacian_bw, *a, **k)
+
+
+def eikonal_bw(*a, **k):
+    """ge_compute.cu:14-117 with an explicit seed."""
+    return _grid_loss(lib().svo_eikonal_bw, *a, **k)
+
+
+def adam(param, grad, m, v, step, lr, beta1, beta2, eps, biased=False, sparse=False):
+    p = _c(param, np.float32).copy(); m = _c(m, np.float32).copy(); v = _c(v, np.float32).copy()
+    lib().svo_adam(C.c_int(p.size), C.c_int(int(biased)), C.c_int(int(sparse)), _p(p), _p(_c(grad, np.float32)),
+                   _p(m), _p(v), C.c_double(step), C.c_double(lr), C.c_double(beta1), C.c_double(beta2), _f(eps))
+    return p, m, v

@@ -1,0 +1,132 @@
+"""ctypes binding of ``libsvraster_b200.so`` (the C ABI in ``include/svraster_b200.h``).
+
+Torch is used only for device memory and the current CUDA stream: every call passes raw
+device pointers and ``torch.cuda.current_stream().cuda_stream``.  There is no fallback:
+if the library is missing or cannot load, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsvraster_b200.so")
+
+SVR_MAX_VIEWS = 128
+TILE = 16
+
+
+class ViewDesc(C.Structure):
+    """Mirror of ``svr_view_t``."""
+    _fields_ = [
+        ("width", C.c_int32), ("height", C.c_int32),
+        ("tiles_x", C.c_int32), ("tiles_y", C.c_int32),
+        ("tile_offset", C.c_int32), ("pad0", C.c_int32),
+        ("pix_offset", C.c_int64),
+        ("tanfovx", C.c_float), ("tanfovy", C.c_float), ("cx", C.c_float), ("cy", C.c_float),
+        ("near_plane", C.c_float), ("pad1", C.c_float),
+        ("w2c", C.c_void_p), ("c2w", C.c_void_p), ("bg", C.c_void_p),
+    ]
+
+
+_P, _I, _I64, _U64, _F, _D, _SZ = C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.c_float, C.c_double, C.c_size_t
+
+_SIGS = {
+    "svr_last_error": (C.c_char_p, []),
+    "svr_version": (_I, []),
+    "svr_geom_buffer_bytes": (_SZ, [_I64]),
+    "svr_preprocess": (_I, [_P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
+    "svr_unpack_geom": (_I, [_P, _I64, _P, _P, _P, _P]),
+    "svr_count_rendered": (_I, [_I64, _P, C.POINTER(C.c_int64), C.POINTER(C.c_uint64), _P]),
+    "svr_binning_buffer_bytes": (_SZ, [_I64, _I]),
+    "svr_image_buffer_bytes": (_SZ, [_I64, _I]),
+    "svr_bin_and_sort": (_I, [_P, _I, _I, _I64, _U64, _P, _P, _P, _SZ, _P, _P]),
+    "svr_unpack_binning": (_I, [_P, _I64, _I, _P, _I64, _P, _P, _P, _P, _P]),
+    "svr_render_fwd": (_I, [_P, _I, _I, _I64, _I, _I, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P,
+                            _P, _P, _P, _P, _P, _P]),
+    "svr_render_bwd": (_I, [_P, _I, _I, _I64, _I, _I, _F, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                            _P, _P, _P, _P]),
+    "svr_read_status": (_I, [_P, _I64, _I, C.POINTER(C.c_uint32), _P]),
+    "svr_gather_geo": (_I, [_I64, _P, _P, _P, _P, _P]),
+    "svr_gather_geo_bw": (_I, [_I64, _P, _P, _P, _P, _P]),
+    "svr_sh_eval": (_I, [_I, _I64, _P, _I, _I, _P, _P, _P, _P, _P, _P]),
+    "svr_sh_eval_bw": (_I, [_I, _I64, _P, _I, _I, _P, _P, _P, _P, _P, _P]),
+    "svr_valid_table_workspace_bytes": (_SZ, [_I, _I64]),
+    "svr_valid_table_count": (_I, [_I, _P, _P, _P, _F, _I, _P, _P, C.POINTER(C.c_int64), _P]),
+    "svr_valid_table_fill": (_I, [_I, _P, _P, _P, _F, _I, _P, _I64, _P, _P, _P, _P, _P]),
+    "svr_laplacian_bw": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P]),
+    "svr_eikonal_bw": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P]),
+    "svr_adam_step": (_I, [_I64, _I, _I, _P, _P, _P, _P, _D, _D, _D, _D, _F, _P]),
+}
+
+_lib = None
+
+
+def load():
+    """Load the CUDA library once; raise if it is missing (there is no fallback path)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"svraster_b200: CUDA library not built ({LIB_PATH}); run svraster_b200/build.py")
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def exported_symbols():
+    return list(_SIGS)
+
+
+class SvrError(RuntimeError):
+    pass
+
+
+def check(rc: int, what: str):
+    if rc != 0:
+        msg = load().svr_last_error().decode(errors="replace")
+        raise SvrError(f"{what} failed (status {rc}): {msg}")
+
+
+def ptr(t):
+    """Device pointer of a tensor (None -> NULL)."""
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+def stream_ptr(device=None):
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def require_cuda(*tensors):
+    for t in tensors:
+        if t is not None and torch.is_tensor(t) and not t.is_cuda:
+            raise SvrError("svraster_b200 operates on CUDA tensors only")
+
+
+def make_views(cams):
+    """Build a ctypes array of ViewDesc from dicts with keys width, height, tanfovx, tanfovy,
+    cx, cy, near, w2c, c2w, bg (the last three device float32 tensors)."""
+    n = len(cams)
+    if n == 0 or n > SVR_MAX_VIEWS:
+        raise SvrError(f"view count must be in 1..{SVR_MAX_VIEWS}")
+    arr = (ViewDesc * n)()
+    tile_off, pix_off = 0, 0
+    for i, c in enumerate(cams):
+        v = arr[i]
+        v.width, v.height = int(c["width"]), int(c["height"])
+        v.tiles_x, v.tiles_y = (v.width + TILE - 1) // TILE, (v.height + TILE - 1) // TILE
+        v.tile_offset, v.pix_offset = tile_off, pix_off
+        v.tanfovx, v.tanfovy = float(c["tanfovx"]), float(c["tanfovy"])
+        v.cx, v.cy = float(c["cx"]), float(c["cy"])
+        v.near_plane = float(c.get("near", 0.02))
+        v.w2c, v.c2w, v.bg = ptr(c["w2c"]), ptr(c["c2w"]), ptr(c["bg"])
+        tile_off += v.tiles_x * v.tiles_y
+        pix_off += v.width * v.height
+    return arr, tile_off, pix_off

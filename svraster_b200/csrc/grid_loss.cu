@@ -1,0 +1,330 @@
+// Dense-grid registration and the parent-child / sibling smoothness adjoints.
+//
+// valid table: cuda/src/utils.cu:190-252 registers every voxel's cells of the virtual dense
+// grid through an atomic slot counter and sorts afterwards (src/utils/octree_utils.py:
+// 293-314).  Here the slots come from a prefix sum of per-voxel cell counts (deterministic,
+// no N*64 over-allocation) and a stable radix sort orders the (key, voxel) pairs.
+// Laplacian / grid-Eikonal adjoints: cuda/src/ls_compute.cu:14-109, ge_compute.cu:14-117
+// with the sample helpers of auxiliary.h:392-471.  The jitter seed is an argument.
+#include <string>
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include "svr_common.cuh"
+
+using namespace svr;
+
+int svr_fail(int code, const char* what);
+#define CUDA_TRY(x)                                                                      \
+    do {                                                                                 \
+        cudaError_t e_ = (x);                                                            \
+        if (e_ != cudaSuccess) return svr_fail(SVR_ERR_CUDA, cudaGetErrorString(e_));    \
+    } while (0)
+
+static inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+__device__ __forceinline__ bool voxel_cells(const float* center, float size, const float* scene_center, float ext,
+                                            int res, bool leaf, int lo[3], int hi[3]) {
+    const float cells = (size / ext) * res;
+    if ((!leaf) && ((cells > 1.5f) || (cells < 0.9f))) return false;
+    if ((leaf) && (cells < 0.9f)) return false;
+    float mn[3], mx[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { mn[d] = scene_center[d] - 0.5f * ext; mx[d] = scene_center[d] + 0.5f * ext; }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) if (center[d] < mn[d] || center[d] > mx[d]) return false;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float a = center[d] - 0.5f * size, b = center[d] + 0.5f * size;
+        lo[d] = int(roundf((a - mn[d]) / (mx[d] - mn[d]) * res));
+        hi[d] = int(roundf((b - mn[d]) / (mx[d] - mn[d]) * res));
+        // stay inside the dense grid (a voxel straddling the inside bound would otherwise
+        // register cells past the end of grid_mask)
+        lo[d] = max(0, min(res, lo[d]));
+        hi[d] = max(0, min(res, hi[d]));
+    }
+    return true;
+}
+
+__global__ void cell_count_kernel(int N, const float* __restrict__ centers, const float* __restrict__ sizes,
+                                  const float* __restrict__ sc, float ext, int res, const uint8_t* __restrict__ leaf,
+                                  uint32_t* __restrict__ counts)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int lo[3], hi[3];
+    uint32_t c = 0;
+    if (voxel_cells(centers + 3 * (size_t)i, sizes[i], sc, ext, res, leaf[i] != 0, lo, hi)) {
+        const int a = hi[0] - lo[0], b = hi[1] - lo[1], d = hi[2] - lo[2];
+        if (a > 0 && b > 0 && d > 0) c = (uint32_t)a * b * d;
+    }
+    counts[i] = c;
+}
+
+__global__ void cell_fill_kernel(int N, const float* __restrict__ centers, const float* __restrict__ sizes,
+                                 const float* __restrict__ sc, float ext, int res, const uint8_t* __restrict__ leaf,
+                                 const uint32_t* __restrict__ counts, const uint32_t* __restrict__ scan,
+                                 uint8_t* __restrict__ mask, int32_t* __restrict__ keys, int32_t* __restrict__ vox)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N || counts[i] == 0) return;
+    int lo[3], hi[3];
+    voxel_cells(centers + 3 * (size_t)i, sizes[i], sc, ext, res, leaf[i] != 0, lo, hi);
+    uint32_t off = scan[i] - counts[i];
+    for (int x = lo[0]; x < hi[0]; ++x)
+        for (int y = lo[1]; y < hi[1]; ++y)
+            for (int z = lo[2]; z < hi[2]; ++z) {
+                const int f = x + res * (y + res * z);
+                mask[f] = 1;
+                keys[off] = f;
+                vox[off] = i;
+                ++off;
+            }
+}
+
+struct TableWs {
+    size_t counts, scan, scan_tmp, scan_tmp_bytes, keys_in, vox_in, sort_tmp, sort_tmp_bytes, total;
+};
+static TableWs table_ws(int N, int64_t G) {
+    TableWs L{};
+    const int n = N > 0 ? N : 1;
+    const int g = G > 0 ? (int)G : 1;
+    size_t st = 0, rt = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, st, (const uint32_t*)nullptr, (uint32_t*)nullptr, n);
+    cub::DeviceRadixSort::SortPairs(nullptr, rt, (const int32_t*)nullptr, (int32_t*)nullptr,
+                                    (const int32_t*)nullptr, (int32_t*)nullptr, g);
+    size_t off = 0;
+    L.counts = off; off = align_up(off + 4 * (size_t)n, 256);
+    L.scan = off; off = align_up(off + 4 * (size_t)n, 256);
+    L.scan_tmp = off; L.scan_tmp_bytes = st; off = align_up(off + st, 256);
+    L.keys_in = off; off = align_up(off + 4 * (size_t)g, 256);
+    L.vox_in = off; off = align_up(off + 4 * (size_t)g, 256);
+    L.sort_tmp = off; L.sort_tmp_bytes = rt; off = align_up(off + rt, 256);
+    L.total = off;
+    return L;
+}
+
+extern "C" size_t svr_valid_table_workspace_bytes(int N, int64_t count) { return table_ws(N, count).total; }
+
+extern "C" int svr_valid_table_count(int N, const float* centers, const float* sizes, const float* scene_center,
+                                     float inside_extent, int res_pow2, const uint8_t* is_leaf, void* workspace,
+                                     int64_t* count_host, void* stream)
+{
+    if (res_pow2 < 1 || res_pow2 > 10) return svr_fail(SVR_ERR_ARG, "grid resolution must be 2^1..2^10");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (N <= 0) { *count_host = 0; return SVR_OK; }
+    TableWs L = table_ws(N, 0);
+    char* w = (char*)workspace;
+    const int res = 1 << res_pow2;
+    cell_count_kernel<<<(N + 255) / 256, 256, 0, st>>>(N, centers, sizes, scene_center, inside_extent, res, is_leaf,
+                                                      (uint32_t*)(w + L.counts));
+    CUDA_TRY(cudaGetLastError());
+    size_t tb = L.scan_tmp_bytes;
+    CUDA_TRY(cub::DeviceScan::InclusiveSum(w + L.scan_tmp, tb, (const uint32_t*)(w + L.counts),
+                                           (uint32_t*)(w + L.scan), N, st));
+    uint32_t total = 0;
+    CUDA_TRY(cudaMemcpyAsync(&total, w + L.scan + 4 * (size_t)(N - 1), 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    *count_host = total;
+    return SVR_OK;
+}
+
+extern "C" int svr_valid_table_fill(int N, const float* centers, const float* sizes, const float* scene_center,
+                                    float inside_extent, int res_pow2, const uint8_t* is_leaf, int64_t count,
+                                    void* workspace, uint8_t* grid_mask, int32_t* grid_keys, int32_t* grid2voxel,
+                                    void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    const int res = 1 << res_pow2;
+    CUDA_TRY(cudaMemsetAsync(grid_mask, 0, (size_t)res * res * res, st));
+    if (N <= 0 || count <= 0) return SVR_OK;
+    // counts / scan live at the same offsets for any G, so the count pass's results stay valid
+    TableWs L = table_ws(N, count);
+    char* w = (char*)workspace;
+    cell_fill_kernel<<<(N + 255) / 256, 256, 0, st>>>(N, centers, sizes, scene_center, inside_extent, res, is_leaf,
+                                                     (const uint32_t*)(w + L.counts), (const uint32_t*)(w + L.scan),
+                                                     grid_mask, (int32_t*)(w + L.keys_in), (int32_t*)(w + L.vox_in));
+    CUDA_TRY(cudaGetLastError());
+    int bits = 1;
+    while ((1ll << bits) < (long long)res * res * res) ++bits;
+    size_t tb = L.sort_tmp_bytes;
+    CUDA_TRY(cub::DeviceRadixSort::SortPairs(w + L.sort_tmp, tb, (const int32_t*)(w + L.keys_in), grid_keys,
+                                             (const int32_t*)(w + L.vox_in), grid2voxel, (int)count, 0, bits, st));
+    return SVR_OK;
+}
+
+// ------------------------------------------------------------------ smoothness adjoints
+__device__ __forceinline__ float hash_to_float(uint32_t x) {
+    x ^= x >> 17; x *= 0xed5ad4bbu; x ^= x >> 11; x *= 0xac4c1b51u; x ^= x >> 15; x *= 0x31848babu; x ^= x >> 14;
+    return (x & 0xFFFFFF) / float(0x1000000);
+}
+__device__ __forceinline__ float3 rand_vec(int tid, int seed) {
+    return f3(hash_to_float((uint32_t)(seed * 73856093 ^ tid * 3 + 0)),
+              hash_to_float((uint32_t)(seed * 19349663 ^ tid * 3 + 1)),
+              hash_to_float((uint32_t)(seed * 83492791 ^ tid * 3 + 2)));
+}
+__device__ __forceinline__ int find_key(const int32_t* keys, int n, int key) {
+    int l = 0, r = n - 1;
+    while (l <= r) {
+        const int m = (l + r) / 2;
+        const int k = keys[m];
+        if (k == key) return m;
+        if (k < key) l = m + 1; else r = m - 1;
+    }
+    return -1;
+}
+__device__ __forceinline__ bool neighbours_ok(int x, int y, int z, int res, const uint8_t* mask) {
+    if (x <= 0 || x >= res - 1 || y <= 0 || y >= res - 1 || z <= 0 || z >= res - 1) return false;
+    const int rr = res * res;
+    const int c = x + y * res + z * rr;
+    return mask[c + 1] && mask[c - 1] && mask[c + res] && mask[c - res] && mask[c + rr] && mask[c - rr];
+}
+
+struct SampleCtx {
+    int G, N, M, res;
+    const int32_t* keys;
+    const int32_t* g2v;
+    const float* coords;
+    const float* vsizes;
+    const int64_t* vox_key;
+    const float* grid;
+};
+
+// auxiliary.h:433-482: owner voxel of grid cell (x,y,z), clamped trilinear weights at the
+// jittered point, SDF value.  Returns the owner id or -1.
+__device__ __forceinline__ int sample_cell(const SampleCtx& c, int x, int y, int z, float3 rv, float w[8], float& sdf,
+                                           unsigned* status) {
+    sdf = 0.f;
+    const int id = find_key(c.keys, c.G, x + y * c.res + z * c.res * c.res);
+    if (id < 0) return -1;
+    const int v = c.g2v[id];
+    if (v < 0 || v >= c.N) { atomicOr(status, ERR_BAD_INDEX); return -1; }
+    const float3 pt = f3(x + rv.x, y + rv.y, z + rv.z);
+    const float3 base = f3(c.coords[3 * v], c.coords[3 * v + 1], c.coords[3 * v + 2]);
+    const float size = c.vsizes[v];
+    tri_weights((pt - base) / size, w);
+    float s = 0.f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        if (w[i] < 0) w[i] = 0;
+        if (w[i] > 1) w[i] = 1;
+        const int64_t p = c.vox_key[8 * (int64_t)v + i];
+        if (p < 0 || p >= c.M) { atomicOr(status, ERR_BAD_INDEX); return -1; }
+        s += c.grid[p] * w[i];
+    }
+    sdf = s;
+    return v;
+}
+__device__ __forceinline__ void scatter8(const SampleCtx& c, int v, const float* w, float d, float* grad) {
+    if (v < 0) return;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) atomicAdd(grad + c.vox_key[8 * (int64_t)v + i], d * w[i]);
+}
+
+__global__ void __launch_bounds__(256) laplacian_kernel(SampleCtx c, int A, const int32_t* __restrict__ active,
+                                                        const uint8_t* __restrict__ mask, float weight,
+                                                        float vox_size_inv, int seed, float* __restrict__ grad,
+                                                        unsigned* status)
+{
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= A) return;
+    const int a = active[tid];
+    if (a < 0 || a >= c.G) { atomicOr(status, ERR_BAD_INDEX); return; }
+    const int gk = c.keys[a];
+    const int res = c.res;
+    if (gk < 0 || gk >= res * res * res) { atomicOr(status, ERR_BAD_INDEX); return; }
+    const int x = gk % res, y = (gk / res) % res, z = gk / (res * res);
+    if (!mask[gk] || !neighbours_ok(x, y, z, res, mask)) return;
+    const float3 rv = rand_vec(tid, seed);
+    const int dx[6] = {+1, -1, 0, 0, 0, 0}, dy[6] = {0, 0, +1, -1, 0, 0}, dz[6] = {0, 0, 0, 0, +1, -1};
+    float w[7][8];
+    int vid[7];
+    float nb[6], center;
+    vid[0] = sample_cell(c, x, y, z, rv, w[0], center, status);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) vid[i + 1] = sample_cell(c, x + dx[i], y + dy[i], z + dz[i], rv, w[i + 1], nb[i], status);
+    const float lx = nb[0] + nb[1] - 2.0f * center;
+    const float ly = nb[2] + nb[3] - 2.0f * center;
+    const float lz = nb[4] + nb[5] - 2.0f * center;
+    const float lr = sqrtf(lx * lx + ly * ly + lz * lz + 1e-10f);
+    // ls_compute.cu:79-83 evaluates these in double (0.5 is a double literal there)
+    const float size = weight * 0.5 * vox_size_inv * vox_size_inv;
+    const float gx = 0.5 / lr * 2 * lx * size;
+    const float gy = 0.5 / lr * 2 * ly * size;
+    const float gz = 0.5 / lr * 2 * lz * size;
+    const float gc = -2.0f * (gx + gy + gz);
+    scatter8(c, vid[0], w[0], gc, grad);
+    scatter8(c, vid[1], w[1], gx, grad); scatter8(c, vid[2], w[2], gx, grad);
+    scatter8(c, vid[3], w[3], gy, grad); scatter8(c, vid[4], w[4], gy, grad);
+    scatter8(c, vid[5], w[5], gz, grad); scatter8(c, vid[6], w[6], gz, grad);
+}
+
+__global__ void __launch_bounds__(256) eikonal_kernel(SampleCtx c, int A, const int32_t* __restrict__ active,
+                                                      const uint8_t* __restrict__ mask, float weight,
+                                                      float vox_size_inv, int seed, float* __restrict__ grad,
+                                                      unsigned* status)
+{
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= A) return;
+    const int a = active[tid];
+    if (a < 0 || a >= c.G) { atomicOr(status, ERR_BAD_INDEX); return; }
+    const int gk = c.keys[a];
+    const int res = c.res;
+    if (gk < 0 || gk >= res * res * res) { atomicOr(status, ERR_BAD_INDEX); return; }
+    const int x = gk % res, y = (gk / res) % res, z = gk / (res * res);
+    if (!mask[gk] || !neighbours_ok(x, y, z, res, mask)) return;
+    const float3 rv = rand_vec(tid, seed);
+    const int dx[6] = {+1, -1, 0, 0, 0, 0}, dy[6] = {0, 0, +1, -1, 0, 0}, dz[6] = {0, 0, 0, 0, +1, -1};
+    float w[6][8];
+    int vid[6];
+    float s[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) vid[i] = sample_cell(c, x + dx[i], y + dy[i], z + dz[i], rv, w[i], s[i], status);
+    const float dxv = (s[0] - s[1]) * 0.5f, dyv = (s[2] - s[3]) * 0.5f, dzv = (s[4] - s[5]) * 0.5f;
+    const float gn = sqrtf(dxv * dxv + dyv * dyv + dzv * dzv + 1e-6f);
+    const float gw = gn * 0.5 * vox_size_inv;   // ge_compute.cu:93, double literal
+    const float dg = 2.0f * (gw - 1.0f) * weight;
+    const float ddx = dg * dxv / gn * 0.5f * vox_size_inv;
+    const float ddy = dg * dyv / gn * 0.5f * vox_size_inv;
+    const float ddz = dg * dzv / gn * 0.5f * vox_size_inv;
+    scatter8(c, vid[0], w[0], ddx, grad); scatter8(c, vid[1], w[1], -ddx, grad);
+    scatter8(c, vid[2], w[2], ddy, grad); scatter8(c, vid[3], w[3], -ddy, grad);
+    scatter8(c, vid[4], w[4], ddz, grad); scatter8(c, vid[5], w[5], -ddz, grad);
+}
+
+static int grid_loss(bool lap, int G, int A, const int32_t* active, const int32_t* keys, const int32_t* g2v, int res,
+                     const uint8_t* mask, const float* coords, const float* vsizes, int N, const int64_t* vox_key,
+                     const float* grid, int M, float weight, float vox_size_inv, int seed, float* grad,
+                     unsigned* status, void* stream)
+{
+    if (A <= 0) return SVR_OK;
+    if (!active || !keys || !g2v || !mask || !coords || !vsizes || !vox_key || !grid || !grad || !status)
+        return svr_fail(SVR_ERR_ARG, "grid loss: null argument");
+    SampleCtx c{G, N, M, res, keys, g2v, coords, vsizes, vox_key, grid};
+    cudaStream_t st = (cudaStream_t)stream;
+    if (lap) laplacian_kernel<<<(A + 255) / 256, 256, 0, st>>>(c, A, active, mask, weight, vox_size_inv, seed, grad, status);
+    else eikonal_kernel<<<(A + 255) / 256, 256, 0, st>>>(c, A, active, mask, weight, vox_size_inv, seed, grad, status);
+    CUDA_TRY(cudaGetLastError());
+    return SVR_OK;
+}
+
+extern "C" int svr_laplacian_bw(int G, int A, const int32_t* active, const int32_t* grid_keys, const int32_t* grid2voxel,
+                                int grid_res, const uint8_t* grid_mask, const float* voxel_coords,
+                                const float* voxel_sizes, int N, const int64_t* vox_key, const float* grid_pts, int M,
+                                float weight, float vox_size_inv, int seed, float* grid_grad, uint32_t* status,
+                                void* stream)
+{
+    return grid_loss(true, G, A, active, grid_keys, grid2voxel, grid_res, grid_mask, voxel_coords, voxel_sizes, N,
+                     vox_key, grid_pts, M, weight, vox_size_inv, seed, grid_grad, status, stream);
+}
+
+extern "C" int svr_eikonal_bw(int G, int A, const int32_t* active, const int32_t* grid_keys, const int32_t* grid2voxel,
+                              int grid_res, const uint8_t* grid_mask, const float* voxel_coords,
+                              const float* voxel_sizes, int N, const int64_t* vox_key, const float* grid_pts, int M,
+                              float weight, float vox_size_inv, int seed, float* grid_grad, uint32_t* status,
+                              void* stream)
+{
+    return grid_loss(false, G, A, active, grid_keys, grid2voxel, grid_res, grid_mask, voxel_coords, voxel_sizes, N,
+                     vox_key, grid_pts, M, weight, vox_size_inv, seed, grid_grad, status, stream);
+}

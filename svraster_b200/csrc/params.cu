@@ -1,0 +1,259 @@
+// Per-voxel parameter kernels: corner-SDF gather (+ adjoint), SH colour (+ adjoint), Adam.
+// Behaviour of cuda/src/geo_params_gather.cu, sh_compute.cu and adam_step.cu; all are
+// HBM-bound elementwise/gather work, mapped one thread per (voxel, corner) or per element
+// with 16-byte accesses where the layout allows.
+#include <cmath>
+#include <string>
+
+#include "svr_common.cuh"
+
+using namespace svr;
+
+int svr_fail(int code, const char* what);
+#define CUDA_TRY(x)                                                                      \
+    do {                                                                                 \
+        cudaError_t e_ = (x);                                                            \
+        if (e_ != cudaSuccess) return svr_fail(SVR_ERR_CUDA, cudaGetErrorString(e_));    \
+    } while (0)
+
+static inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// ------------------------------------------------------------------ gather
+// geo_params_gather.cu:22-46: geos[i, k] = grid[vox_key[i, k]] for i in care_idx.
+// Eight threads per voxel: the key reads and the geos writes are fully coalesced.
+__global__ void gather_geo_kernel(int64_t n_care, const int64_t* __restrict__ care_idx,
+                                  const int64_t* __restrict__ vox_key, const float* __restrict__ grid,
+                                  float* __restrict__ geos)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_care * 8) return;
+    const int64_t i = care_idx[t >> 3];
+    const int k = (int)(t & 7);
+    geos[8 * i + k] = __ldg(grid + vox_key[8 * i + k]);
+}
+
+// geo_params_gather.cu:48-72
+__global__ void gather_geo_bw_kernel(int64_t n_care, const int64_t* __restrict__ care_idx,
+                                     const int64_t* __restrict__ vox_key, const float* __restrict__ dgeos,
+                                     float* __restrict__ dgrid)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_care * 8) return;
+    const int64_t i = care_idx[t >> 3];
+    const int k = (int)(t & 7);
+    const float d = dgeos[8 * i + k];
+    if (d != 0.f) atomicAdd(dgrid + vox_key[8 * i + k], d);
+}
+
+extern "C" int svr_gather_geo(int64_t n_care, const int64_t* care_idx, const int64_t* vox_key,
+                              const float* grid_pts, float* geos, void* stream)
+{
+    if (n_care <= 0) return SVR_OK;
+    if (!care_idx || !vox_key || !grid_pts || !geos) return svr_fail(SVR_ERR_ARG, "gather: null argument");
+    gather_geo_kernel<<<nblk(n_care * 8, 256), 256, 0, (cudaStream_t)stream>>>(n_care, care_idx, vox_key, grid_pts, geos);
+    CUDA_TRY(cudaGetLastError());
+    return SVR_OK;
+}
+
+extern "C" int svr_gather_geo_bw(int64_t n_care, const int64_t* care_idx, const int64_t* vox_key,
+                                 const float* dgeos, float* dgrid, void* stream)
+{
+    if (n_care <= 0) return SVR_OK;
+    if (!care_idx || !vox_key || !dgeos || !dgrid) return svr_fail(SVR_ERR_ARG, "gather_bw: null argument");
+    gather_geo_bw_kernel<<<nblk(n_care * 8, 256), 256, 0, (cudaStream_t)stream>>>(n_care, care_idx, vox_key, dgeos, dgrid);
+    CUDA_TRY(cudaGetLastError());
+    return SVR_OK;
+}
+
+// ------------------------------------------------------------------ SH
+// sh_compute.cu:33-106 (forward) and :111-176 (adjoint; the clamp is not differentiated,
+// as in the reference).
+__constant__ float kSH_C2[5] = {1.0925484305920792f, -1.0925484305920792f, 0.31539156525252005f,
+                                -1.0925484305920792f, 0.5462742152960396f};
+__constant__ float kSH_C3[7] = {-0.5900435899266435f, 2.890611442640554f, -0.4570457994644658f,
+                                0.3731763325901154f, -0.4570457994644658f, 1.445305721320277f,
+                                -0.5900435899266435f};
+constexpr float SH_C0 = 0.28209479177387814f;
+constexpr float SH_C1 = 0.4886025119029199f;
+
+template <int DEG>
+__device__ __forceinline__ void sh_basis(float3 dir, float* B) {
+    const float x = dir.x, y = dir.y, z = dir.z;
+    B[0] = SH_C0;
+    if (DEG > 0) { B[1] = -SH_C1 * y; B[2] = SH_C1 * z; B[3] = -SH_C1 * x; }
+    if (DEG > 1) {
+        const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
+        B[4] = kSH_C2[0] * xy; B[5] = kSH_C2[1] * yz; B[6] = kSH_C2[2] * (2.0f * zz - xx - yy);
+        B[7] = kSH_C2[3] * xz; B[8] = kSH_C2[4] * (xx - yy);
+        if (DEG > 2) {
+            B[9] = kSH_C3[0] * y * (3.0f * xx - yy);
+            B[10] = kSH_C3[1] * xy * z;
+            B[11] = kSH_C3[2] * y * (4.0f * zz - xx - yy);
+            B[12] = kSH_C3[3] * z * (2.0f * zz - 3.0f * xx - 3.0f * yy);
+            B[13] = kSH_C3[4] * x * (4.0f * zz - xx - yy);
+            B[14] = kSH_C3[5] * z * (xx - yy);
+            B[15] = kSH_C3[6] * x * (xx - 3.0f * yy);
+        }
+    }
+}
+
+template <int DEG>
+__global__ void sh_eval_kernel(int N, int64_t n_idx, const int64_t* __restrict__ idx, int M,
+                               const float3* __restrict__ centers, const float3* __restrict__ cam_pos,
+                               const float3* __restrict__ sh0, const float3* __restrict__ shs,
+                               float3* __restrict__ rgbs)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t n = n_idx > 0 ? n_idx : N;
+    if (t >= n) return;
+    const int64_t i = n_idx > 0 ? idx[t] : t;
+    const float3 ro = *cam_pos;
+    float3 dir = centers[i] - ro;
+    dir = dir * rnorm3df(dir.x, dir.y, dir.z);
+    float B[16];
+    sh_basis<DEG>(dir, B);
+    const float3* sh = shs + i * (M - 1);
+    float3 res = B[0] * sh0[i];
+    constexpr int NB = (DEG + 1) * (DEG + 1);
+#pragma unroll
+    for (int k = 1; k < NB; ++k) res = res + B[k] * sh[k - 1];
+    res = res + 0.5f;
+    res.x *= (res.x > 0.0f);
+    res.y *= (res.y > 0.0f);
+    res.z *= (res.z > 0.0f);
+    rgbs[i] = res;
+}
+
+template <int DEG>
+__global__ void sh_eval_bw_kernel(int N, int64_t n_idx, const int64_t* __restrict__ idx, int M,
+                                  const float3* __restrict__ centers, const float3* __restrict__ cam_pos,
+                                  const float3* __restrict__ drgbs, float3* __restrict__ dsh0,
+                                  float3* __restrict__ dshs)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t n = n_idx > 0 ? n_idx : N;
+    if (t >= n) return;
+    const int64_t i = n_idx > 0 ? idx[t] : t;
+    const float3 ro = *cam_pos;
+    float3 dir = centers[i] - ro;
+    dir = dir * rnorm3df(dir.x, dir.y, dir.z);
+    float B[16];
+    sh_basis<DEG>(dir, B);
+    const float3 d = drgbs[i];
+    dsh0[i] = B[0] * d;
+    float3* o = dshs + i * (M - 1);
+    constexpr int NB = (DEG + 1) * (DEG + 1);
+#pragma unroll
+    for (int k = 1; k < NB; ++k) o[k - 1] = B[k] * d;
+}
+
+extern "C" int svr_sh_eval(int N, int64_t n_idx, const int64_t* idx, int degree, int M, const float* centers,
+                           const float* cam_pos, const float* sh0, const float* shs, float* rgbs, void* stream)
+{
+    if (degree < 0 || degree > 3 || M < (degree + 1) * (degree + 1)) return svr_fail(SVR_ERR_ARG, "sh degree");
+    const int64_t n = n_idx > 0 ? n_idx : N;
+    if (n <= 0) return SVR_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned g = nblk(n, 256);
+    const auto c = (const float3*)centers; const auto cp = (const float3*)cam_pos;
+    const auto s0 = (const float3*)sh0; const auto ss = (const float3*)shs; auto o = (float3*)rgbs;
+    switch (degree) {
+        case 0: sh_eval_kernel<0><<<g, 256, 0, st>>>(N, n_idx, idx, M, c, cp, s0, ss, o); break;
+        case 1: sh_eval_kernel<1><<<g, 256, 0, st>>>(N, n_idx, idx, M, c, cp, s0, ss, o); break;
+        case 2: sh_eval_kernel<2><<<g, 256, 0, st>>>(N, n_idx, idx, M, c, cp, s0, ss, o); break;
+        default: sh_eval_kernel<3><<<g, 256, 0, st>>>(N, n_idx, idx, M, c, cp, s0, ss, o); break;
+    }
+    CUDA_TRY(cudaGetLastError());
+    return SVR_OK;
+}
+
+extern "C" int svr_sh_eval_bw(int N, int64_t n_idx, const int64_t* idx, int degree, int M, const float* centers,
+                              const float* cam_pos, const float* drgbs, float* dsh0, float* dshs, void* stream)
+{
+    if (degree < 0 || degree > 3 || M < (degree + 1) * (degree + 1)) return svr_fail(SVR_ERR_ARG, "sh degree");
+    const int64_t n = n_idx > 0 ? n_idx : N;
+    if (n <= 0) return SVR_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned g = nblk(n, 256);
+    const auto c = (const float3*)centers; const auto cp = (const float3*)cam_pos;
+    const auto d = (const float3*)drgbs; auto o0 = (float3*)dsh0; auto o1 = (float3*)dshs;
+    switch (degree) {
+        case 0: sh_eval_bw_kernel<0><<<g, 256, 0, st>>>(N, n_idx, idx, M, c, cp, d, o0, o1); break;
+        case 1: sh_eval_bw_kernel<1><<<g, 256, 0, st>>>(N, n_idx, idx, M, c, cp, d, o0, o1); break;
+        case 2: sh_eval_bw_kernel<2><<<g, 256, 0, st>>>(N, n_idx, idx, M, c, cp, d, o0, o1); break;
+        default: sh_eval_bw_kernel<3><<<g, 256, 0, st>>>(N, n_idx, idx, M, c, cp, d, o0, o1); break;
+    }
+    CUDA_TRY(cudaGetLastError());
+    return SVR_OK;
+}
+
+// ------------------------------------------------------------------ Adam
+// adam_step.cu:21-104: lerp via two FMAs, bias corrections from the host in double.
+__device__ __forceinline__ float lerp_fma(float v0, float v1, float t) { return fmaf(t, v1, fmaf(-t, v0, v0)); }
+
+template <bool SPARSE, bool BIASED>
+__device__ __forceinline__ void adam_one(float& p, float g, float& m, float& v, float step_size, float b1, float b2,
+                                         float rbc2, float eps) {
+    if (SPARSE && g == 0.0f) return;
+    m = lerp_fma(g, m, b1);
+    v = lerp_fma(g * g, v, b2);
+    const float denom = BIASED ? sqrtf(v) + eps : fmaf(sqrtf(v), rbc2, eps);
+    p -= step_size * (m / denom);
+}
+
+template <bool SPARSE, bool BIASED>
+__global__ void adam_kernel(int64_t n, float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                            float* __restrict__ v, float step_size, float b1, float b2, float rbc2, float eps)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i4 = t * 4;
+    if (i4 + 3 < n) {
+        float4 P = reinterpret_cast<float4*>(p)[t];
+        const float4 G = reinterpret_cast<const float4*>(g)[t];
+        float4 Mv = reinterpret_cast<float4*>(m)[t];
+        float4 Vv = reinterpret_cast<float4*>(v)[t];
+        adam_one<SPARSE, BIASED>(P.x, G.x, Mv.x, Vv.x, step_size, b1, b2, rbc2, eps);
+        adam_one<SPARSE, BIASED>(P.y, G.y, Mv.y, Vv.y, step_size, b1, b2, rbc2, eps);
+        adam_one<SPARSE, BIASED>(P.z, G.z, Mv.z, Vv.z, step_size, b1, b2, rbc2, eps);
+        adam_one<SPARSE, BIASED>(P.w, G.w, Mv.w, Vv.w, step_size, b1, b2, rbc2, eps);
+        reinterpret_cast<float4*>(p)[t] = P;
+        reinterpret_cast<float4*>(m)[t] = Mv;
+        reinterpret_cast<float4*>(v)[t] = Vv;
+    } else {
+        for (int64_t i = i4; i < n; ++i) {
+            float P = p[i], Mv = m[i], Vv = v[i];
+            adam_one<SPARSE, BIASED>(P, g[i], Mv, Vv, step_size, b1, b2, rbc2, eps);
+            p[i] = P; m[i] = Mv; v[i] = Vv;
+        }
+    }
+}
+
+extern "C" int svr_adam_step(int64_t numel, int biased, int sparse, float* param, const float* grad, float* exp_avg,
+                             float* exp_avg_sq, double step, double lr, double beta1, double beta2, float eps,
+                             void* stream)
+{
+    if (numel <= 0) return SVR_OK;
+    if (!param || !grad || !exp_avg || !exp_avg_sq) return svr_fail(SVR_ERR_ARG, "adam: null argument");
+    const bool aligned = (((uintptr_t)param | (uintptr_t)grad | (uintptr_t)exp_avg | (uintptr_t)exp_avg_sq) & 15) == 0;
+    if (!aligned) return svr_fail(SVR_ERR_ARG, "adam: buffers must be 16-byte aligned");
+    float step_size, rbc2;
+    if (biased) { step_size = (float)lr; rbc2 = 1.f; }
+    else {
+        const double bc1 = 1.0 - std::pow(beta1, step);
+        const double bc2 = 1.0 - std::pow(beta2, step);
+        step_size = (float)(lr / bc1);
+        rbc2 = (float)(1.0 / std::sqrt(bc2));
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned g = nblk((numel + 3) / 4, 256);
+    const float b1 = (float)beta1, b2 = (float)beta2;
+    if (biased) {
+        if (sparse) adam_kernel<true, true><<<g, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
+        else adam_kernel<false, true><<<g, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
+    } else {
+        if (sparse) adam_kernel<true, false><<<g, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
+        else adam_kernel<false, false><<<g, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return SVR_OK;
+}

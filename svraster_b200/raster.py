@@ -1,0 +1,125 @@
+"""Host orchestration of the sm_100a rasterizer: buffers, stream, C-ABI calls.
+
+One object per render batch.  Views are described by dicts (see ``_lib.make_views``);
+a single view reproduces the reference's per-view ``_C.rasterize_preprocess`` /
+``_C.rasterize_voxels`` / ``_C.rasterize_voxels_backward`` (cuda/src/preprocess.cu:158-228,
+forward.cu:986-1096, backward.cu:986-1109) and several views run batched: one launch per
+stage for the whole batch, one sort over every view's records.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import _lib
+from ._lib import check, ptr, stream_ptr
+
+_u8 = torch.uint8
+
+
+def _empty_bytes(n, device):
+    return torch.empty(max(int(n), 16), dtype=_u8, device=device)
+
+
+class RasterState:
+    """Geometry / binning / image buffers of one batch of views (opaque byte tensors, like
+    the reference's geomBuffer / binningBuffer / imgBuffer)."""
+
+    def __init__(self, cams, n_vox, device):
+        self.cams = cams
+        self.views, self.total_tiles, self.total_pix = _lib.make_views(cams)
+        self.n_views = len(cams)
+        self.N = int(n_vox)
+        self.device = device
+        self.geom = None
+        self.binning = None
+        self.image = None
+        self.num_rendered = 0
+        self.path_or = 0
+
+    # -------------------------------------------------------------- preprocess
+    def preprocess(self, octpaths, centers, lengths, is_leaf):
+        L = _lib.load()
+        M = self.N * self.n_views
+        n_dup = torch.empty(M, dtype=torch.int32, device=self.device)
+        self.geom = _empty_bytes(L.svr_geom_buffer_bytes(M), self.device)
+        check(L.svr_preprocess(self.views, self.n_views, self.N, ptr(centers), ptr(lengths), ptr(is_leaf),
+                               ptr(octpaths), ptr(n_dup), ptr(self.geom), stream_ptr(self.device)),
+              "svr_preprocess")
+        return n_dup
+
+    # -------------------------------------------------------------- binning
+    def bin(self, octpaths):
+        L = _lib.load()
+        M = self.N * self.n_views
+        R, por = C.c_int64(0), C.c_uint64(0)
+        check(L.svr_count_rendered(M, ptr(self.geom), C.byref(R), C.byref(por), stream_ptr(self.device)),
+              "svr_count_rendered")
+        self.num_rendered, self.path_or = int(R.value), int(por.value)
+        nb = L.svr_binning_buffer_bytes(self.num_rendered, self.total_tiles)
+        self.binning = _empty_bytes(nb, self.device)
+        self.image = _empty_bytes(L.svr_image_buffer_bytes(self.total_pix, self.total_tiles), self.device)
+        check(L.svr_bin_and_sort(self.views, self.n_views, self.N, self.num_rendered, self.path_or, ptr(octpaths),
+                                 ptr(self.geom), ptr(self.binning), nb, ptr(self.image), stream_ptr(self.device)),
+              "svr_bin_and_sort")
+        return self.num_rendered
+
+    # -------------------------------------------------------------- render
+    def render(self, n_samp, need_depth, need_normal, centers, lengths, geos, rgbs, s_val, track_max_w=False,
+               rgb_per_view=False):
+        L = _lib.load()
+        P, dev = self.total_pix, self.device
+        color = torch.empty(3 * P, dtype=torch.float32, device=dev)
+        depth = torch.empty(4 * P, dtype=torch.float32, device=dev) if need_depth else None
+        normal = torch.empty(3 * P, dtype=torch.float32, device=dev) if need_normal else None
+        T = torch.empty(P, dtype=torch.float32, device=dev)
+        max_w = torch.zeros(self.N, dtype=torch.float32, device=dev) if track_max_w else None
+        check(L.svr_render_fwd(self.views, self.n_views, self.N, self.num_rendered, int(n_samp), int(need_depth),
+                               int(need_normal), ptr(centers), ptr(lengths), ptr(geos), ptr(rgbs),
+                               self.n_views if rgb_per_view else 1, ptr(s_val), ptr(self.geom), ptr(self.binning),
+                               ptr(self.image), ptr(color), ptr(depth), ptr(normal), ptr(T), ptr(max_w),
+                               stream_ptr(dev)), "svr_render_fwd")
+        return color, depth, normal, T, max_w
+
+    def render_backward(self, need_depth, need_normal, s_val, out_T, dcolor, ddepth, dnormal, dT,
+                        lambda_R_concen=0.0, gt_color=None, drgbs=None, dvox=None, ds=None):
+        L = _lib.load()
+        dev = self.device
+        if dvox is None:
+            dvox = torch.zeros(self.N, 12, dtype=torch.float32, device=dev)
+        if ds is None:
+            ds = torch.zeros(1, dtype=torch.float32, device=dev)
+        check(L.svr_render_bwd(self.views, self.n_views, self.N, self.num_rendered, int(need_depth),
+                               int(need_normal), float(lambda_R_concen), ptr(gt_color), ptr(s_val),
+                               ptr(self.binning), ptr(self.image), ptr(out_T), ptr(dcolor), ptr(ddepth),
+                               ptr(dnormal), ptr(dT), ptr(dvox), ptr(drgbs), ptr(ds), stream_ptr(dev)),
+              "svr_render_bwd")
+        return dvox, ds
+
+    # -------------------------------------------------------------- introspection (tests)
+    def status(self):
+        st = C.c_uint32(0)
+        check(_lib.load().svr_read_status(ptr(self.image), self.total_pix, self.total_tiles, C.byref(st),
+                                          stream_ptr(self.device)), "svr_read_status")
+        return int(st.value)
+
+    def geom_fields(self):
+        M = self.N * self.n_views
+        nd = torch.empty(M, dtype=torch.int32, device=self.device)
+        bb = torch.empty(M, 2, dtype=torch.int32, device=self.device)
+        bits = torch.empty(M, dtype=torch.int32, device=self.device)
+        check(_lib.load().svr_unpack_geom(ptr(self.geom), M, ptr(nd), ptr(bb), ptr(bits), stream_ptr(self.device)),
+              "svr_unpack_geom")
+        return nd, bb, bits
+
+    def binning_fields(self):
+        R = max(self.num_rendered, 1)
+        vals = torch.empty(R, dtype=torch.int32, device=self.device)
+        ranges = torch.empty(self.total_tiles, 2, dtype=torch.int32, device=self.device)
+        tl = torch.empty(self.total_tiles, dtype=torch.int32, device=self.device)
+        nc = torch.empty(self.total_pix, dtype=torch.int32, device=self.device)
+        check(_lib.load().svr_unpack_binning(ptr(self.binning), self.num_rendered, self.total_tiles, ptr(self.image),
+                                             self.total_pix, ptr(vals), ptr(ranges), ptr(tl), ptr(nc),
+                                             stream_ptr(self.device)), "svr_unpack_binning")
+        return vals[: self.num_rendered], ranges, tl, nc

@@ -1,0 +1,296 @@
+"""Seeded synthetic sparse-voxel scenes and pinhole cameras.
+
+The datasets the reference trains on are not available, so every workload here is
+a procedurally generated octree that follows the reference's own data layout:
+
+* ``octpath`` int64: 3 bits per level, level 1 in bits 45..47 (src/utils/octree_utils.py:13-22,
+  cuda/src/utils.cu:129-158).
+* voxel size ``scene_extent * 2**-level`` and centre ``scene_min + (ijk + 0.5) * size``
+  (octree_utils.py:51-60, 99-126).
+* grid points are the 8 corners of every voxel at level-16 integer resolution, merged by a
+  lexicographic unique; ``vox_key[N, 8]`` indexes them with corner order ``x<<2 | y<<1 | z``
+  (octree_utils.py:129-163, 203-222).
+
+Cameras follow ``src/cameras.py``: OpenCV axes (x right, y down, z forward), ``c2w`` /
+``w2c`` float32 4x4, ``tanfov = tan(fov / 2)``, principal point at the image centre.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+MAX_NUM_LEVELS = 16
+
+
+# ----------------------------------------------------------------------------- octree
+
+def ijk_to_octpath(ijk: np.ndarray, level: np.ndarray) -> np.ndarray:
+    """Octree path of voxels given integer coords at their own level (cuda/src/utils.cu:129-158)."""
+    ijk = ijk.astype(np.int64)
+    level = level.astype(np.int64).reshape(-1)
+    path = np.zeros(len(level), dtype=np.int64)
+    for l in range(MAX_NUM_LEVELS):
+        bits = ((ijk[:, 0] >> l) & 1) << 2 | ((ijk[:, 1] >> l) & 1) << 1 | ((ijk[:, 2] >> l) & 1)
+        path |= bits << (3 * l)
+    return path << (3 * (MAX_NUM_LEVELS - level))
+
+
+def octpath_to_ijk(path: np.ndarray, level: np.ndarray) -> np.ndarray:
+    """Inverse of :func:`ijk_to_octpath` (cuda/src/utils.cu:160-189)."""
+    level = level.astype(np.int64).reshape(-1)
+    p = path.astype(np.int64).reshape(-1) >> (3 * (MAX_NUM_LEVELS - level))
+    ijk = np.zeros((len(p), 3), dtype=np.int64)
+    for l in range(MAX_NUM_LEVELS):
+        b = p & 7
+        ijk[:, 0] |= ((b >> 2) & 1) << l
+        ijk[:, 1] |= ((b >> 1) & 1) << l
+        ijk[:, 2] |= (b & 1) << l
+        p = p >> 3
+    return ijk
+
+
+def build_grid_pts_link(ijk: np.ndarray, level: np.ndarray):
+    """Corner grid points shared between voxels (octree_utils.py:129-163, 203-222).
+
+    Returns ``(grid_pts_key int64[M,3], vox_key int64[N,8])`` with rows of
+    ``grid_pts_key`` in lexicographic (x, y, z) order, as ``unique(dim=0)`` gives.
+    """
+    shift = (MAX_NUM_LEVELS - level.astype(np.int64)).reshape(-1, 1, 1)
+    base = ijk.astype(np.int64).reshape(-1, 1, 3) << shift
+    octant = np.array([[(k >> 2) & 1, (k >> 1) & 1, k & 1] for k in range(8)], dtype=np.int64)
+    corners = base + (octant.reshape(1, 8, 3) << shift)          # [N, 8, 3], each < 2**16 + 1
+    flat = (corners[..., 0] << 34) | (corners[..., 1] << 17) | corners[..., 2]
+    uniq, inv = np.unique(flat.reshape(-1), return_inverse=True)
+    key = np.stack([uniq >> 34, (uniq >> 17) & ((1 << 17) - 1), uniq & ((1 << 17) - 1)], axis=1)
+    return key.astype(np.int64), inv.reshape(-1, 8).astype(np.int64)
+
+
+# ----------------------------------------------------------------------------- SDFs
+
+def sdf_sphere(p, r=0.5, c=(0.0, 0.0, 0.0)):
+    return np.linalg.norm(p - np.asarray(c, dtype=np.float64), axis=-1) - r
+
+
+def sdf_torus(p, R=0.35, r=0.12, c=(0.0, 0.0, 0.0)):
+    q = p - np.asarray(c, dtype=np.float64)
+    xz = np.sqrt(q[..., 0] ** 2 + q[..., 2] ** 2) - R
+    return np.sqrt(xz ** 2 + q[..., 1] ** 2) - r
+
+
+def sdf_spheres_torus(p):
+    """Union of 3 spheres and a torus with radii in [0.2, 0.5] (mid-size workload)."""
+    d = np.minimum(sdf_sphere(p, 0.5, (-0.3, 0.0, 0.0)), sdf_sphere(p, 0.3, (0.45, 0.3, 0.1)))
+    d = np.minimum(d, sdf_sphere(p, 0.2, (0.2, -0.5, 0.4)))
+    return np.minimum(d, sdf_torus(p, 0.45, 0.2, (0.1, 0.2, -0.35)))
+
+
+def make_bumpy_sphere(n_bumps=64, amp=0.05, r=0.5, width=0.25, seed=0):
+    rng = np.random.default_rng(seed)
+    dirs = rng.normal(size=(n_bumps, 3))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+
+    def f(p):
+        n = np.linalg.norm(p, axis=-1)
+        u = p / np.maximum(n, 1e-9)[..., None]
+        h = np.zeros(n.shape)
+        for d in dirs:
+            h += amp * np.exp(-np.sum((u - d) ** 2, axis=-1) / width ** 2)
+        return n - (r + h)
+    return f
+
+
+# ----------------------------------------------------------------------------- scene
+
+@dataclass
+class Scene:
+    octpath: np.ndarray          # int64 [N]
+    octlevel: np.ndarray         # int8  [N]
+    vox_center: np.ndarray       # f32   [N, 3]
+    vox_size: np.ndarray         # f32   [N, 1]
+    is_leaf: np.ndarray          # u8    [N]
+    vox_key: np.ndarray          # int64 [N, 8]
+    grid_pts_key: np.ndarray     # int64 [M, 3]
+    grid_pts_xyz: np.ndarray     # f32   [M, 3]
+    geo_grid_pts: np.ndarray     # f32   [M, 1]
+    sh0: np.ndarray              # f32   [N, 3]
+    shs: np.ndarray              # f32   [N, 15, 3]
+    log_s: float
+    scene_center: np.ndarray = field(default_factory=lambda: np.zeros(3, np.float32))
+    scene_extent: float = 2.0
+
+    @property
+    def n_vox(self):
+        return len(self.octpath)
+
+    @property
+    def s_val(self):
+        return float(np.exp(np.float32(self.log_s) * np.float32(10.0)))
+
+
+def build_scene(sdf, lv_min, lv_max, seed=0, scene_extent=2.0, band=2.0, keep=None,
+                kept_parent_frac=0.0, sh_degree=3):
+    """Recursively subdivide cells with ``|sdf(centre)| < band * size`` from ``lv_min`` to ``lv_max``.
+
+    Cells that are not subdivided stay as leaves when ``|sdf(centre)| < keep * size``
+    (``keep=None`` keeps all of them); the rest count as pruned empty space, the state a
+    trained scene reaches after the reference's max-weight pruning.
+
+    ``kept_parent_frac`` re-inserts that fraction of the parents of finest-level leaves as
+    non-leaf voxels, like the reference keeps deep parents on subdivision
+    (src/sparse_voxel_gears/adaptive.py:59-63); those are culled by the preprocess.
+    """
+    rng = np.random.default_rng(seed)
+    smin = -0.5 * scene_extent
+    n0 = 1 << lv_min
+    g = np.stack(np.meshgrid(np.arange(n0), np.arange(n0), np.arange(n0), indexing="ij"), -1).reshape(-1, 3)
+    cur_ijk, cur_lv = g.astype(np.int64), lv_min
+    leaf_ijk, leaf_lv, parents = [], [], []
+    while True:
+        size = scene_extent * 2.0 ** -cur_lv
+        c = smin + (cur_ijk + 0.5) * size
+        d = np.abs(sdf(c))
+        if cur_lv == lv_max:
+            kept = cur_ijk if keep is None else cur_ijk[d < keep * size]
+            leaf_ijk.append(kept); leaf_lv.append(np.full(len(kept), cur_lv))
+            break
+        near = d < band * size
+        stay = ~near if keep is None else (~near) & (d < keep * size)
+        leaf_ijk.append(cur_ijk[stay]); leaf_lv.append(np.full(int(stay.sum()), cur_lv))
+        sub = cur_ijk[near]
+        if cur_lv + 1 == lv_max and kept_parent_frac > 0 and len(sub):
+            pick = rng.random(len(sub)) < kept_parent_frac
+            parents.append(sub[pick])
+        octant = np.array([[(k >> 2) & 1, (k >> 1) & 1, k & 1] for k in range(8)], dtype=np.int64)
+        cur_ijk = ((sub[:, None, :] << 1) + octant[None]).reshape(-1, 3)
+        cur_lv += 1
+    ijk = np.concatenate(leaf_ijk)
+    lv = np.concatenate(leaf_lv).astype(np.int64)
+    leaf = np.ones(len(ijk), np.uint8)
+    if parents:
+        pij = np.concatenate(parents)
+        ijk = np.concatenate([ijk, pij]); lv = np.concatenate([lv, np.full(len(pij), lv_max - 1)])
+        leaf = np.concatenate([leaf, np.zeros(len(pij), np.uint8)])
+    # shuffle so voxel ids are not spatially ordered (as after many prune/subdivide rounds)
+    perm = rng.permutation(len(ijk))
+    ijk, lv, leaf = ijk[perm], lv[perm], leaf[perm]
+
+    size = (scene_extent * np.exp2(-lv.astype(np.float64))).astype(np.float32)
+    center = (smin + (ijk + 0.5) * size[:, None].astype(np.float64)).astype(np.float32)
+    octpath = ijk_to_octpath(ijk, lv)
+    gkey, vkey = build_grid_pts_link(ijk, lv)
+    finest = scene_extent * 2.0 ** -MAX_NUM_LEVELS
+    gxyz = (smin + gkey * finest).astype(np.float32)
+    h_min = scene_extent * 2.0 ** -lv_max
+    geo = sdf(gxyz.astype(np.float64)) + rng.normal(0.0, 0.01 * h_min, size=len(gxyz))
+    N = len(ijk)
+    sh0 = rng.uniform(-1.0, 1.0, size=(N, 3)).astype(np.float32)
+    n_rest = (sh_degree + 1) ** 2 - 1
+    shs = rng.normal(0.0, 0.05, size=(N, n_rest, 3)).astype(np.float32)
+    log_s = 0.1 * math.log(math.log(99.0) / h_min / 4.0)
+    return Scene(octpath=octpath, octlevel=lv.astype(np.int8), vox_center=center,
+                 vox_size=size.reshape(-1, 1), is_leaf=leaf, vox_key=vkey, grid_pts_key=gkey,
+                 grid_pts_xyz=gxyz, geo_grid_pts=geo.astype(np.float32).reshape(-1, 1),
+                 sh0=sh0, shs=shs, log_s=log_s, scene_extent=scene_extent)
+
+
+# ----------------------------------------------------------------------------- cameras
+
+@dataclass
+class Camera:
+    width: int
+    height: int
+    fovx: float
+    fovy: float
+    c2w: np.ndarray      # f32 [4, 4]
+    w2c: np.ndarray      # f32 [4, 4]
+    near: float = 0.02
+
+    @property
+    def tanfovx(self):
+        return math.tan(self.fovx * 0.5)
+
+    @property
+    def tanfovy(self):
+        return math.tan(self.fovy * 0.5)
+
+    @property
+    def cx(self):
+        return self.width * 0.5
+
+    @property
+    def cy(self):
+        return self.height * 0.5
+
+    @property
+    def position(self):
+        return self.c2w[:3, 3]
+
+    @property
+    def lookat(self):
+        return self.c2w[:3, 2]
+
+
+def look_at_camera(pos, width, height, fovx_deg=50.0, target=(0.0, 0.0, 0.0)):
+    pos = np.asarray(pos, np.float64)
+    f = np.asarray(target, np.float64) - pos
+    f /= np.linalg.norm(f)
+    up = np.array([0.0, 0.0, 1.0])
+    if abs(f @ up) > 0.99:
+        up = np.array([0.0, 1.0, 0.0])
+    right = np.cross(f, up); right /= np.linalg.norm(right)
+    down = np.cross(f, right)
+    c2w = np.eye(4)
+    c2w[:3, 0], c2w[:3, 1], c2w[:3, 2], c2w[:3, 3] = right, down, f, pos
+    w2c = np.linalg.inv(c2w)
+    fovx = math.radians(fovx_deg)
+    fovy = 2 * math.atan(math.tan(fovx / 2) * height / width)
+    # the reference inverts w2c in float32 on the device (src/cameras.py:146-149)
+    w2c32 = w2c.astype(np.float32)
+    c2w32 = np.linalg.inv(w2c32.astype(np.float64)).astype(np.float32)
+    return Camera(width, height, fovx, fovy, c2w32, w2c32)
+
+
+def ring_cameras(n, radius, width, height, fovx_deg=50.0, elev_deg=20.0, phase=0.0):
+    cams = []
+    for i in range(n):
+        az = phase + 2 * math.pi * i / n
+        el = math.radians(elev_deg)
+        p = radius * np.array([math.cos(az) * math.cos(el), math.sin(az) * math.cos(el), math.sin(el)])
+        cams.append(look_at_camera(p, width, height, fovx_deg))
+    return cams
+
+
+def fibonacci_cameras(n, radius, width, height, fovx_deg=50.0):
+    cams = []
+    ga = math.pi * (3.0 - math.sqrt(5.0))
+    for i in range(n):
+        z = 1 - 2 * (i + 0.5) / n
+        r = math.sqrt(max(0.0, 1 - z * z))
+        p = radius * np.array([math.cos(ga * i) * r, math.sin(ga * i) * r, z])
+        cams.append(look_at_camera(p, width, height, fovx_deg))
+    return cams
+
+
+# ----------------------------------------------------------------------------- workloads
+
+def scene_small(seed=0):
+    """Unit-sphere (r=0.5) scene at levels 5-7."""
+    return build_scene(lambda p: sdf_sphere(p, 0.5), 5, 7, seed=seed, band=1.0, keep=2.0,
+                       kept_parent_frac=0.05)
+
+
+def scene_mid(seed=0):
+    """3 spheres + torus at levels 6-10 (about a million voxels)."""
+    return build_scene(sdf_spheres_torus, 6, 10, seed=seed, band=0.35, keep=2.0, kept_parent_frac=0.02)
+
+
+def scene_batched(seed=0):
+    return build_scene(make_bumpy_sphere(seed=seed), 7, 11, seed=seed, band=0.5, keep=2.0)
+
+
+def scene_tiny(seed=0, lv_min=3, lv_max=5):
+    """A few thousand voxels; sized so the pure-C oracle finishes in well under a second."""
+    return build_scene(lambda p: sdf_sphere(p, 0.5), lv_min, lv_max, seed=seed, band=1.0, keep=3.0,
+                       kept_parent_frac=0.1)

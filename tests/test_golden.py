@@ -1,0 +1,151 @@
+"""Pin the oracle and the sm_100a library against golden vectors produced by the reference's
+own CUDA extension (tests/golden/make_golden.py, run on a B200).
+
+CPU tests check the C oracle against the goldens; GPU tests check the library.  Integer
+stages (duplicate counts, bboxes, octant bits, sorted record order, tile ranges, dense-grid
+table, Adam) must match bit for bit; floating-point outputs within the stated tolerances.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from tests.golden.cases import (ADAM_CASE, CASES, TABLE_CASE, build_adam_inputs, build_case_inputs,
+                                build_table_inputs, digest)
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    path = os.path.join(HERE, f"{name}.npz")
+    if not os.path.exists(path):
+        pytest.skip(f"golden fixture {name}.npz not generated yet")
+    return dict(np.load(path))
+
+
+def _check_inputs(g, inp):
+    assert str(g["digest"]) == digest(inp), "synthetic inputs changed; regenerate the golden fixtures"
+
+
+# Reference float32 vs our float32: identical expression shapes; only expf / rsqrtf ulps and
+# atomic summation order differ.
+IMG_RTOL, IMG_ATOL, BAD = 1e-4, 2e-5, 2e-3
+
+
+def _compare_render(res, g, cam):
+    H, W = cam.height, cam.width
+    from tests.helpers import assert_close
+    assert_close("color", res["color"].reshape(3, H, W), g["color"], IMG_RTOL, IMG_ATOL, BAD)
+    assert_close("T", res["T"].reshape(1, H, W), g["T"], IMG_RTOL, IMG_ATOL, BAD)
+    assert_close("depth", res["depth"].reshape(4, H, W), g["depth"], IMG_RTOL, 1e-4, BAD)
+    assert_close("normal", res["normal"].reshape(3, H, W), g["normal"], IMG_RTOL, 1e-4, BAD)
+    assert (np.asarray(res["n_contrib"]).reshape(-1) != g["n_contrib"]).mean() <= BAD
+
+
+def _compare_grads(dvox, ds, g, n_vox):
+    ref = np.zeros((n_vox, 12), np.float32)
+    ref[g["dvox_rows"]] = g["dvox"]
+    scale = np.abs(ref).max(0) + 1e-12
+    err = np.abs(np.asarray(dvox) - ref) / scale
+    assert np.quantile(err, 0.999) < 1e-3, np.quantile(err, 0.999)
+    assert abs(float(ds) - float(g["ds"][0])) <= 1e-3 * abs(float(g["ds"][0])) + 1e-3
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_oracle_matches_reference_goldens(name):
+    from oracle import oracle as O
+    g = load(name)
+    case = CASES[name]
+    inp = build_case_inputs(case)
+    _check_inputs(g, inp)
+    sc, cam, grads = inp["scene"], inp["cam"], inp["grads"]
+    nd, bb, bits = O.preprocess(cam, sc.vox_center, sc.vox_size, sc.is_leaf)
+    assert np.array_equal(nd, g["n_dup"])
+    assert np.array_equal(bb, g["bbox"])
+    assert np.array_equal(bits, g["bits"])
+    keys, vals, ranges = O.binning(cam, sc.octpath, nd, bb, bits)
+    assert int(g["num_rendered"]) == len(vals)
+    assert np.array_equal(keys, g["keys"])
+    assert np.array_equal(vals, g["vals"])
+    ne = g["ranges"][:, 1] > g["ranges"][:, 0]
+    assert np.array_equal(ranges[ne], g["ranges"][ne])
+    care = g["care"]
+    geos = O.gather_geo(care, sc.vox_key, sc.geo_grid_pts, sc.n_vox)
+    assert np.array_equal(geos[care], g["geos"])
+    rgbs = O.sh_eval(3, care, sc.vox_center, cam.position, sc.sh0, sc.shs)
+    np.testing.assert_allclose(rgbs[care], g["rgbs"], rtol=2e-6, atol=2e-6)
+    bg = np.asarray(case["bg"], np.float32)
+    n_samp = {3: 3, 2: 2, 1: 1}[case["vox_geo_mode"]]
+    f = O.render_fwd(cam, bg, n_samp, True, True, ranges, vals, bb, sc.vox_center, sc.vox_size, geos, rgbs,
+                     sc.s_val, track_max_w=True)
+    _compare_render(f, g, cam)
+    dvox, ds = O.render_bwd(cam, bg, True, True, ranges, g["tile_last"], vals, bb, sc.vox_center, sc.vox_size, geos,
+                            rgbs, sc.s_val, g["T"], g["n_contrib"], grads["color"], grads["depth"], grads["normal"],
+                            grads["T"], case["lambda_R_concen"], grads["gt"])
+    _compare_grads(dvox, ds, g, sc.n_vox)
+
+
+def test_oracle_table_and_smoothness_match_reference_goldens():
+    from oracle import oracle as O
+    g = load("table")
+    inp = build_table_inputs(TABLE_CASE)
+    _check_inputs(g, inp)
+    sc = inp["scene"]
+    mask, keys, g2v = O.valid_table(sc.vox_center, sc.vox_size, np.zeros(3), sc.scene_extent,
+                                    TABLE_CASE["res_pow2"], sc.is_leaf)
+    assert np.array_equal(mask, g["mask"])
+    assert np.array_equal(keys, g["keys"])
+    assert np.array_equal(g2v, g["g2v"])
+    res = 1 << TABLE_CASE["res_pow2"]
+    for name, fn in (("lap", O.laplacian_bw), ("eik", O.eikonal_bw)):
+        out = fn(sc.geo_grid_pts, sc.vox_key, inp["grid_voxel_coord"], inp["grid_voxel_size"], res, mask, keys, g2v,
+                 inp["active"], TABLE_CASE["weight"], TABLE_CASE["vox_size_inv"], int(g["seed"]),
+                 np.zeros((len(sc.geo_grid_pts), 1), np.float32)).reshape(-1)
+        scale = np.abs(g[name]).max() + 1e-20
+        assert np.abs(out - g[name]).max() <= 1e-4 * scale, name
+
+
+def test_oracle_adam_matches_reference_goldens():
+    from oracle import oracle as O
+    g = load("adam")
+    inp = build_adam_inputs(ADAM_CASE)
+    _check_inputs(g, inp)
+    c = ADAM_CASE
+    for biased in (False, True):
+        for sparse in (False, True):
+            k = f"{'b' if biased else 'u'}{'s' if sparse else 'd'}"
+            p, m, v = O.adam(inp["param"], inp["grad"], inp["m"], inp["v"], c["step"], c["lr"], c["beta1"],
+                             c["beta2"], c["eps"], biased=biased, sparse=sparse)
+            np.testing.assert_array_equal(p, g[k + "_p"])
+            np.testing.assert_array_equal(m, g[k + "_m"])
+            np.testing.assert_array_equal(v, g[k + "_v"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES))
+def test_library_matches_reference_goldens(name):
+    from tests.helpers import cuda_views
+    g = load(name)
+    case = CASES[name]
+    inp = build_case_inputs(case)
+    _check_inputs(g, inp)
+    sc, cam, grads = inp["scene"], inp["cam"], inp["grads"]
+    geos = np.zeros((sc.n_vox, 8), np.float32)
+    geos[g["care"]] = g["geos"]
+    rgbs = np.zeros((sc.n_vox, 3), np.float32)
+    rgbs[g["care"]] = g["rgbs"]
+    out = cuda_views(sc, [cam], geos, [rgbs], n_samp=case["vox_geo_mode"], bg=case["bg"], grads_list=[grads],
+                     lambda_R=case["lambda_R_concen"])
+    st = out["state"]
+    nd, bb, bits = [x.cpu().numpy().view(np.uint32) for x in st.geom_fields()]
+    assert np.array_equal(out["n_dup"].cpu().numpy(), g["n_dup"])
+    assert np.array_equal(bb.reshape(-1, 2), g["bbox"])
+    assert np.array_equal(bits, g["bits"])
+    vals, ranges, tl, nc = [x.cpu().numpy().view(np.uint32) for x in st.binning_fields()]
+    assert np.array_equal(vals, g["vals"]), "sorted record order differs from the reference"
+    ne = g["ranges"][:, 1] > g["ranges"][:, 0]
+    assert np.array_equal(ranges[ne], g["ranges"][ne])
+    res = {k: out[k].cpu().numpy() for k in ("color", "T", "depth", "normal")}
+    res["n_contrib"] = nc
+    _compare_render(res, g, cam)
+    _compare_grads(out["dvox"].cpu().numpy(), out["ds"].item(), g, sc.n_vox)
