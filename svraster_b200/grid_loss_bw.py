@@ -34,8 +34,9 @@ def _grid_loss(fn_name, grid_pts, vox_key, grid_voxel_coord, grid_voxel_size, gr
     sizes = grid_voxel_size.reshape(-1).to(torch.float32).contiguous()
     key = vox_key.to(torch.int64).contiguous()
     grid = grid_pts.detach().to(torch.float32).contiguous()
+    mask = grid_mask.contiguous()
     fn = getattr(_lib.load(), fn_name)
-    check(fn(keys.numel(), act.numel(), ptr(act), ptr(keys), ptr(g2v), int(grid_res), ptr(grid_mask.contiguous()),
+    check(fn(keys.numel(), act.numel(), ptr(act), ptr(keys), ptr(g2v), int(grid_res), ptr(mask),
              ptr(coords), ptr(sizes), key.shape[0], ptr(key), ptr(grid), grid.numel(), float(weight),
              float(vox_size_inv), _seed(seed), ptr(grid_pts_grad), ptr(status), stream_ptr(dev)), fn_name)
     return status

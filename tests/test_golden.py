@@ -61,8 +61,10 @@ def test_oracle_matches_reference_goldens(name):
     sc, cam, grads = inp["scene"], inp["cam"], inp["grads"]
     nd, bb, bits = O.preprocess(cam, sc.vox_center, sc.vox_size, sc.is_leaf)
     assert np.array_equal(nd, g["n_dup"])
-    assert np.array_equal(bb, g["bbox"])
-    assert np.array_equal(bits, g["bits"])
+    # the reference leaves bbox / octant bits of culled voxels unwritten (torch::empty)
+    r = nd > 0
+    assert np.array_equal(bb[r], g["bbox"][r])
+    assert np.array_equal(bits[r], g["bits"][r])
     keys, vals, ranges = O.binning(cam, sc.octpath, nd, bb, bits)
     assert int(g["num_rendered"]) == len(vals)
     assert np.array_equal(keys, g["keys"])
@@ -139,8 +141,9 @@ def test_library_matches_reference_goldens(name):
     st = out["state"]
     nd, bb, bits = [x.cpu().numpy().view(np.uint32) for x in st.geom_fields()]
     assert np.array_equal(out["n_dup"].cpu().numpy(), g["n_dup"])
-    assert np.array_equal(bb.reshape(-1, 2), g["bbox"])
-    assert np.array_equal(bits, g["bits"])
+    r = g["n_dup"] > 0
+    assert np.array_equal(bb.reshape(-1, 2)[r], g["bbox"][r])
+    assert np.array_equal(bits[r], g["bits"][r])
     vals, ranges, tl, nc = [x.cpu().numpy().view(np.uint32) for x in st.binning_fields()]
     assert np.array_equal(vals, g["vals"]), "sorted record order differs from the reference"
     ne = g["ranges"][:, 1] > g["ranges"][:, 0]

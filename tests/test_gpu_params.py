@@ -26,14 +26,16 @@ def test_gather_and_adjoint_bitexact():
     care = np.sort(rng.choice(sc.n_vox, sc.n_vox // 3, replace=False)).astype(np.int64)
     geos = torch.zeros(sc.n_vox, 8, device=dev)
     L = _lib.load()
-    check(L.svr_gather_geo(len(care), ptr(T(care, torch.int64)), ptr(T(sc.vox_key, torch.int64)),
-                           ptr(T(sc.geo_grid_pts)), ptr(geos), stream_ptr()), "gather")
+    # every tensor handed to the C ABI must outlive the call: bind them to names
+    care_t, key_t, grid_t = T(care, torch.int64), T(sc.vox_key, torch.int64), T(sc.geo_grid_pts)
+    check(L.svr_gather_geo(len(care), ptr(care_t), ptr(key_t), ptr(grid_t), ptr(geos), stream_ptr()), "gather")
     ref = O.gather_geo(care, sc.vox_key, sc.geo_grid_pts, sc.n_vox)
     assert np.array_equal(geos.cpu().numpy()[care], ref[care])
     dgeos = rng.normal(size=(sc.n_vox, 8)).astype(np.float32)
     dgrid = torch.zeros(len(sc.geo_grid_pts), 1, device=dev)
-    check(L.svr_gather_geo_bw(len(care), ptr(T(care, torch.int64)), ptr(T(sc.vox_key, torch.int64)), ptr(T(dgeos)),
-                              ptr(dgrid), stream_ptr()), "gather_bw")
+    dgeos_t = T(dgeos)
+    check(L.svr_gather_geo_bw(len(care), ptr(care_t), ptr(key_t), ptr(dgeos_t), ptr(dgrid), stream_ptr()),
+          "gather_bw")
     refg = O.gather_geo_bw(care, sc.vox_key, dgeos, len(sc.geo_grid_pts))
     np.testing.assert_allclose(dgrid.cpu().numpy(), refg, rtol=1e-5, atol=1e-5)
 
@@ -64,8 +66,8 @@ def test_adam_bitexact(biased, sparse, n):
     p, g = rng.normal(size=n).astype(np.float32), rng.normal(size=n).astype(np.float32)
     g[rng.random(n) < 0.3] = 0
     m, v = (0.1 * rng.normal(size=n)).astype(np.float32), np.abs(rng.normal(size=n)).astype(np.float32)
-    pt, mt, vt = T(p), T(m), T(v)
-    check(_lib.load().svr_adam_step(n, int(biased), int(sparse), ptr(pt), ptr(T(g)), ptr(mt), ptr(vt), 5.0, 0.01, 0.1,
+    pt, mt, vt, gt = T(p), T(m), T(v), T(g)
+    check(_lib.load().svr_adam_step(n, int(biased), int(sparse), ptr(pt), ptr(gt), ptr(mt), ptr(vt), 5.0, 0.01, 0.1,
                                     0.99, 1e-15, stream_ptr()), "adam")
     rp, rm, rv = O.adam(p, g, m, v, 5, 0.01, 0.1, 0.99, 1e-15, biased=biased, sparse=sparse)
     np.testing.assert_array_equal(pt.cpu().numpy(), rp)
