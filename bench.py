@@ -1,0 +1,380 @@
+"""Throughput benchmark of the sm_100a sparse-voxel SDF rasterizer training step.
+
+Workload (mid-size plain method): ~1.4M voxels at octree levels 6-10 around three spheres and
+a torus, SH degree 3, 8 views of 800x800 on a Fibonacci sphere of radius 3.  One step renders
+all 8 views forward and backward and runs the SDF regularisers and Adam (svraster_b200.step).
+
+  value : forward+backward Mrays/s of the batched step, inputs resident in HBM
+  e2e   : the same metric through the drop-in per-view API (svraster_b200.renderer with
+          autograd), upstream gradient planes copied from pinned host memory every step
+          and a scalar read back
+  roofline : the dominant kernel's algorithmic bytes / CUDA-event duration vs the measured
+          HBM copy bandwidth (MEASURED_PEAKS.json)
+  cpu_baseline : the CPU oracle (single thread) on one view of the same workload
+
+``--impl reference`` times the CPU restatement of the reference algorithm (the reference's
+only implementation of this path is CUDA) with all host threads on a bounded sample.
+Multi-GPU (torchrun): every rank renders its own 8 views (weak scaling) and the gradients are
+all-reduced over NCCL before Adam.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "mid-size: 3 spheres + torus, levels 6-10, SH deg 3, 8 views 800x800"
+N_VIEWS, W, H = 8, 800, 800
+
+
+def make_workload(rank=0):
+    from svraster_b200 import synthetic as S
+    scene = S.scene_mid(seed=0)
+    cams = S.fibonacci_cameras(N_VIEWS * max(1, rank + 1), 3.0, W, H, fovx_deg=50.0)[N_VIEWS * rank:N_VIEWS * (rank + 1)]
+    return scene, cams
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_traffic(kernel, workload):
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    e = d.get(kernel)
+    if not e or e.get("workload") != workload:
+        return None
+    return e.get("bytes_per_launch")
+
+
+# ----------------------------------------------------------------------------- our arm
+def run_ours(args, rank, world):
+    import torch
+    import torch.distributed as dist
+    from svraster_b200 import _lib
+    from svraster_b200.step import BatchedTrainStep
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    scene, cams = make_workload(rank)
+    step = BatchedTrainStep(scene, cams, device=dev, lambda_R_concen=0.1)
+    L = _lib.load()
+
+    # data parallel over views: the gradients are summed across ranks between the adjoints
+    # and Adam (the one exchange step of the path)
+    def allreduce_grads(grads):
+        for g in grads:
+            dist.all_reduce(g)
+    hook = allreduce_grads if world > 1 else None
+    for _ in range(args.warmup):
+        step.step(grad_hook=hook)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches0 = L.svr_kernel_launches()
+    step_events = []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clk:
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(args.steps):
+            step.step(time_render=True, grad_hook=hook)
+            step_events.append(step.ev)
+        ev1.record()
+        torch.cuda.synchronize()
+    launches = L.svr_kernel_launches() - launches0
+    fwd_ms = [e[0].elapsed_time(e[1]) for e in step_events]
+    bwd_ms = [e[2].elapsed_time(e[3]) for e in step_events]
+    total_ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    ms_per_step = total_ms / args.steps
+    rays = step.rays * world
+    value = rays / (ms_per_step * 1e-3) / 1e6
+
+    # roofline of the dominant kernel (algorithmic bytes of the reference's per-record layout)
+    R, R_prime = step.record_counts()
+    nd = step.state.geom_fields()[0]
+    V_vis = int((nd.view(N_VIEWS, -1) > 0).any(0).sum().item())
+    P = step.P
+    fwd_avg, bwd_avg = float(np.mean(fwd_ms)), float(np.mean(bwd_ms))
+    fwd_bytes = R * 72 + P * 52
+    bwd_bytes = R_prime * 72 + P * 68 + V_vis * 48
+    if bwd_avg >= fwd_avg:
+        kname, kbytes, kms = "render_bwd_kernel", bwd_bytes, bwd_avg
+    else:
+        kname, kbytes, kms = "render_fwd_kernel", fwd_bytes, fwd_avg
+    peak, peak_src = measured_peaks()
+    achieved = kbytes / (kms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak,
+                "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": load_traffic(kname, WORKLOAD), "algorithmic_bytes": int(kbytes),
+                "launch_ms": round(kms, 4)}
+
+    result = {"metric": "fwd+bwd Mrays/s", "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
+              "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
+              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+              "data": "synthetic (seeded procedural scene, N(0,1) upstream gradients)",
+              "config": {"workload": WORKLOAD, "n_voxels": scene.n_vox, "n_grid_pts": int(step.grid.numel()),
+                         "views_per_gpu": N_VIEWS, "image": f"{W}x{H}", "rays_per_step": rays,
+                         "records_R": R, "records_R_prime": R_prime, "visible_voxels": V_vis,
+                         "l2": "inputs larger than L2 (records + SH state > 126 MB)",
+                         "parallelism": f"dp{world} over views" if world > 1 else "single GPU"},
+              "stages_ms": {"render_fwd": round(fwd_avg, 3), "render_bwd": round(bwd_avg, 3)},
+              "roofline": roofline, "gpu_launches": int(launches), "clocks": clk.summary()}
+    return result, step, scene, cams
+
+
+def run_e2e(args, scene, cams, dev):
+    """The same metric through the drop-in per-view API with host-resident upstream gradients."""
+    import torch
+    from svraster_b200 import renderer, grid_loss_bw
+    from svraster_b200.sparse_adam import SparseAdam
+
+    t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
+    octpath = t(scene.octpath, torch.int64)
+    centers = t(scene.vox_center)
+    lengths = t(scene.vox_size)
+    is_leaf = t(scene.is_leaf, torch.uint8)
+    vox_key = t(scene.vox_key, torch.int64)
+    grid = t(scene.geo_grid_pts).requires_grad_(True)
+    sh0 = t(scene.sh0).requires_grad_(True)
+    shs = t(scene.shs).requires_grad_(True)
+    log_s = torch.tensor([scene.log_s], dtype=torch.float32, device=dev).requires_grad_(True)
+    vox_size_inv = 1.0 / lengths
+    opt = SparseAdam([{"params": [grid], "lr": 1e-3}, {"params": [sh0], "lr": 1e-3}, {"params": [shs], "lr": 1e-4}],
+                     betas=(0.1, 0.99), eps=1e-15)
+
+    def vox_fn(idx, cam_pos, color_mode):
+        geos = renderer.GatherGeoParams.apply("triinterp3", vox_key, vox_size_inv, idx, grid)
+        rgbs = renderer.SH_eval.apply(3, idx, centers, cam_pos, None, sh0, shs)
+        return {"geos": geos, "rgbs": rgbs, "subdiv_p": torch.zeros(scene.n_vox, 1, device=dev), "log_s": log_s}
+
+    rng = np.random.default_rng(0)
+    host = []
+    for c in cams:
+        P = c.width * c.height
+        planes = [torch.from_numpy(rng.normal(size=n * P).astype(np.float32)).pin_memory() for n in (3, 4, 3)]
+        gt = torch.from_numpy(rng.uniform(size=3 * P).astype(np.float32)).pin_memory()
+        host.append((planes, gt))
+    mats = [(t(c.w2c), t(c.c2w)) for c in cams]
+    bg = torch.zeros(3, device=dev)
+    # dense-grid table (static between prune / subdivide)
+    from svraster_b200 import utils
+    res_pow2 = min(int(scene.octlevel.max()), 9)
+    res = 1 << res_pow2
+    mask, keys, g2v = utils.valid_gradient_table(centers, lengths, torch.zeros(3, device=dev), scene.scene_extent,
+                                                 res_pow2, is_leaf)
+    ext = np.float32(scene.scene_extent)
+    coord = t(np.round(((scene.vox_center - scene.vox_size * np.float32(0.5)) + ext * np.float32(0.5)) / ext
+                       * np.float32(res)))
+    vsize = t(np.round(scene.vox_size / ext * np.float32(res))).reshape(-1)
+    active = torch.arange(keys.numel(), dtype=torch.int32, device=dev)
+    h2d = sum(sum(p.numel() for p in planes) * 4 + gt.numel() * 4 for planes, gt in host) + 2 * 64 * len(cams)
+
+    def one_step(it):
+        opt.zero_grad(set_to_none=False) if grid.grad is not None else None
+        tot = torch.zeros((), device=dev)
+        for (planes, gt_h), (w2c, c2w), c in zip(host, mats, cams):
+            dc, dd, dn = [p.to(dev, non_blocking=True) for p in planes]
+            gt = gt_h.to(dev, non_blocking=True).view(3, c.height, c.width)
+            rs = renderer.RasterSettings(color_mode="sh", vox_geo_mode="triinterp3", density_mode="sdf",
+                                         image_width=c.width, image_height=c.height, tanfovx=c.tanfovx,
+                                         tanfovy=c.tanfovy, cx=c.cx, cy=c.cy, w2c_matrix=w2c, c2w_matrix=c2w,
+                                         background=bg, near=c.near, need_depth=True, need_normal=True,
+                                         lambda_R_concen=0.1, gt_color=gt)
+            color, depth, normal, T, _, _ = renderer.rasterize_voxels(rs, octpath, centers, lengths, vox_fn, is_leaf)
+            torch.autograd.backward([color, depth, normal],
+                                    [dc.view(3, c.height, c.width), dd.view(4, c.height, c.width),
+                                     dn.view(3, c.height, c.width)])
+            tot = tot + T.detach().mean()
+        for fn in (grid_loss_bw.laplacian_smoothness, grid_loss_bw.grid_eikonal):
+            fn(grid, vox_key, coord, vsize, res, mask, keys, g2v, active, 1e-3, float(res) / scene.scene_extent,
+               True, False, grid.grad, seed=it)
+        opt.step()
+        return float(tot.item())   # device -> host read of the step's result
+
+    for i in range(args.warmup):
+        one_step(i)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for i in range(args.steps):
+        one_step(1000 + i)
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    rays = sum(c.width * c.height for c in cams)
+    return {"value": round(rays / (ms * 1e-3) / 1e6, 3), "unit": "Mrays/s", "ms_per_step": round(ms, 3),
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4,
+            "path": "svraster_b200.renderer.rasterize_voxels per view + autograd + grid_loss_bw + SparseAdam"}
+
+
+def oracle_view_step(scene, cam, threads):
+    """preprocess + binning + forward + backward of one view on the CPU oracle."""
+    from oracle import oracle as O
+    O.set_threads(threads)
+    nd, bb, bits = O.preprocess(cam, scene.vox_center, scene.vox_size, scene.is_leaf)
+    keys, vals, ranges = O.binning(cam, scene.octpath, nd, bb, bits)
+    vis = np.where(nd > 0)[0]
+    geos = O.gather_geo(vis, scene.vox_key, scene.geo_grid_pts, scene.n_vox)
+    rgbs = O.sh_eval(3, vis, scene.vox_center, cam.position, scene.sh0, scene.shs)
+    f = O.render_fwd(cam, np.zeros(3, np.float32), 3, True, True, ranges, vals, bb, scene.vox_center, scene.vox_size,
+                     geos, rgbs, scene.s_val)
+    rng = np.random.default_rng(0)
+    Hc, Wc = cam.height, cam.width
+    g = [rng.normal(size=s).astype(np.float32) for s in ((3, Hc, Wc), (4, Hc, Wc), (3, Hc, Wc))]
+    O.render_bwd(cam, np.zeros(3, np.float32), True, True, ranges, f["tile_last"], vals, bb, scene.vox_center,
+                 scene.vox_size, geos, rgbs, scene.s_val, f["T"], f["n_contrib"], g[0], g[1], g[2],
+                 np.zeros((1, Hc, Wc), np.float32))
+    return Hc * Wc
+
+
+def cpu_baseline(scene, cams):
+    t0 = time.perf_counter()
+    rays = oracle_view_step(scene, cams[0], threads=1)
+    dt = time.perf_counter() - t0
+    return {"value": round(rays / dt / 1e6, 5), "unit": "Mrays/s", "cores": 1, "kind": "port",
+            "sample": f"1 of {N_VIEWS} views ({cams[0].width}x{cams[0].height}) preprocess+binning+fwd+bwd, "
+                      f"single thread, {dt:.1f} s"}
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args):
+    scene, cams = make_workload(0)
+    threads = os.cpu_count() or 1
+    oracle_view_step(scene, cams[0], threads)  # warm caches / page in
+    for i in range(max(0, args.warmup - 1)):
+        oracle_view_step(scene, cams[(i + 1) % len(cams)], threads)
+    times, rays = [], 0
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        rays_i = oracle_view_step(scene, cams[i % len(cams)], threads)
+        times.append(time.perf_counter() - t0)
+        rays += rays_i
+    total = sum(times)
+    value = rays / total / 1e6
+    return {"metric": "fwd+bwd Mrays/s", "value": round(value, 5), "unit": "Mrays/s", "impl": "reference",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_voxels": scene.n_vox,
+                       "sample": "one view per step (rotating), preprocess+binning+fwd+bwd"},
+            "cpu_baseline": {"value": round(value, 5), "unit": "Mrays/s", "cores": threads, "kind": "port",
+                             "sample": "one 800x800 view per step of the 8-view workload"},
+            "e2e": {"value": round(value, 5), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    result, step, scene, cams = run_ours(args, rank, world)
+    if rank == 0:
+        import torch
+        if not args.no_e2e:
+            del step
+            torch.cuda.empty_cache()
+            result["e2e"] = run_e2e(args, scene, cams, torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
+        if not args.no_cpu:
+            result["cpu_baseline"] = cpu_baseline(scene, cams)
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

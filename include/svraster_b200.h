@@ -60,6 +60,9 @@ typedef struct {
 
 SVR_API const char* svr_last_error(void);
 SVR_API int svr_version(void);
+/* Number of this library's own kernels launched by this process so far (no counterpart in
+ * the reference; used to report launches inside a timed region). */
+SVR_API long long svr_kernel_launches(void);
 
 /* ---------------------------------------------------------------- preprocess
  * Replaces _C.rasterize_preprocess (cuda/src/preprocess.cu:158-228).
@@ -138,6 +141,12 @@ SVR_API int svr_gather_geo(int64_t n_care, const int64_t* care_idx, const int64_
 SVR_API int svr_gather_geo_bw(int64_t n_care, const int64_t* care_idx, const int64_t* vox_key,
                       const float* dL_dgeos, float* dL_dgrid, void* stream);
 
+/* Scatter per-voxel corner gradients with row stride ld (8 for dL_dgeos, 12 for the render
+ * adjoint's dL_dvox) into dL_dgrid f32[M] for all N voxels: the gather adjoint of
+ * geo_params_gather.cu:48-72 applied directly to the render output (batched training step). */
+SVR_API int svr_scatter_vox_grads(int64_t N, int ld, const int64_t* vox_key, const float* dvox,
+                                  float* dL_dgrid, void* stream);
+
 /* Replace _C.sh_compute / _C.sh_compute_bw (cuda/src/sh_compute.cu:243-299).  n_idx == 0
  * means all N voxels.  sh0 f32[N,3], shs f32[N,M-1,3]. */
 SVR_API int svr_sh_eval(int N, int64_t n_idx, const int64_t* idx, int degree, int M,
@@ -146,6 +155,16 @@ SVR_API int svr_sh_eval(int N, int64_t n_idx, const int64_t* idx, int degree, in
 SVR_API int svr_sh_eval_bw(int N, int64_t n_idx, const int64_t* idx, int degree, int M,
                    const float* centers, const float* cam_pos, const float* dL_drgbs,
                    float* dL_dsh0, float* dL_dshs, void* stream);
+
+/* Multi-view SH for a batch of views (sh_compute.cu:55-176 per view): rgbs f32[V,N,3] for
+ * camera positions cam_pos f32[V,3]; the adjoint sums every view's colour gradient
+ * drgbs f32[V,N,3] into dL_dsh0 f32[N,3] / dL_dshs f32[N,M-1,3] (written, not accumulated). */
+SVR_API int svr_sh_eval_views(int N, int n_views, int degree, int M, const float* centers,
+                              const float* cam_pos, const float* sh0, const float* shs, float* rgbs,
+                              void* stream);
+SVR_API int svr_sh_eval_views_bw(int N, int n_views, int degree, int M, const float* centers,
+                                 const float* cam_pos, const float* drgbs, float* dL_dsh0,
+                                 float* dL_dshs, void* stream);
 
 /* ---------------------------------------------------------------- grid regularisers
  * Replace _C.valid_gradient_table (cuda/src/utils.cu:362-408) + the key sort of

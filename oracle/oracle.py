@@ -33,6 +33,12 @@ def lib(bits=32):
     return _libs[bits]
 
 
+def set_threads(n: int):
+    """Host threads for the render loops of both builds (1 = deterministic)."""
+    for b in (32, 64):
+        lib(b).svo_set_threads(C.c_int(int(n)))
+
+
 def _r(x, bits):
     return C.c_double(float(x)) if bits == 64 else C.c_float(float(x))
 

@@ -11,6 +11,7 @@
  * extension (tests/golden/).
  */
 #include <math.h>
+#include <omp.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -36,6 +37,12 @@ typedef float real;
 #define MAX_LEVELS 16
 #define MIN_ALPHA 0.00001f
 #define EARLY_STOP_T 0.0001f
+
+/* Host threads used by the render loops (tiles are independent; the adjoint scatters with
+ * atomics).  Default 1 so results are deterministic; the CPU baseline raises it. */
+static int g_threads = 1;
+void svo_set_threads(int n) { g_threads = n > 0 ? n : 1; }
+int svo_get_threads(void) { return g_threads; }
 
 typedef struct { float x, y, z; } f3;
 
@@ -269,8 +276,11 @@ void svo_render_fwd(int W, int H, float tanfovx, float tanfovy, float cx, float 
 {
     const int gx = (W + TILE - 1) / TILE, gy = (H + TILE - 1) / TILE;
     const int HW = H * W;
-    for (int ty = 0; ty < gy; ++ty) for (int tx = 0; tx < gx; ++tx) {
-        const int tile = ty * gx + tx;
+    /* max_w is a shared running maximum: keep that variant single-threaded */
+    const int nth = max_w ? 1 : g_threads;
+    #pragma omp parallel for schedule(dynamic, 4) num_threads(nth)
+    for (int tile = 0; tile < gx * gy; ++tile) {
+        const int ty = tile / gx, tx = tile % gx;
         const uint32_t r0 = ranges[2 * tile], r1 = ranges[2 * tile + 1];
         uint32_t tl = r0;
         for (int py = ty * TILE; py < ty * TILE + TILE && py < H; ++py)
@@ -407,8 +417,10 @@ void svo_render_bwd(int W, int H, float tanfovx, float tanfovy, float cx, float 
     const real WH_inv = (real)1 / ((real)(W * H));
     const real wR = lambda_R_concen * WH_inv;
     double ds_acc = 0.0;
-    for (int ty = 0; ty < gy; ++ty) for (int tx = 0; tx < gx; ++tx) {
-        const int tile = ty * gx + tx;
+    const int nth = g_threads;
+    #pragma omp parallel for schedule(dynamic, 4) num_threads(nth) reduction(+ : ds_acc)
+    for (int tile = 0; tile < gx * gy; ++tile) {
+        const int ty = tile / gx, tx = tile % gx;
         const uint32_t r0 = ranges[2 * tile], r1 = tile_last[tile];
         for (int py = ty * TILE; py < ty * TILE + TILE && py < H; ++py)
         for (int px = tx * TILE; px < tx * TILE + TILE && px < W; ++px) {
@@ -533,9 +545,18 @@ void svo_render_bwd(int W, int H, float tanfovx, float tanfovy, float cx, float 
                     drgb[2] += wR * pw * 2.0f * (c.z - gt.z);
                 }
                 real* o = dL_dvox + 12 * (size_t)vid;
-                for (int i = 0; i < 8; ++i) o[i] += dg[i];
-                o[8] += drgb[0]; o[9] += drgb[1]; o[10] += drgb[2];
-                o[11] += FABSR(dalpha * alpha);
+                real pack[12];
+                for (int i = 0; i < 8; ++i) pack[i] = dg[i];
+                pack[8] = drgb[0]; pack[9] = drgb[1]; pack[10] = drgb[2];
+                pack[11] = FABSR(dalpha * alpha);
+                if (nth == 1) {
+                    for (int i = 0; i < 12; ++i) o[i] += pack[i];
+                } else {
+                    for (int i = 0; i < 12; ++i) {
+                        #pragma omp atomic update
+                        o[i] += pack[i];
+                    }
+                }
             }
         }
     }

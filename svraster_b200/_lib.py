@@ -36,6 +36,10 @@ _P, _I, _I64, _U64, _F, _D, _SZ = C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.
 _SIGS = {
     "svr_last_error": (C.c_char_p, []),
     "svr_version": (_I, []),
+    "svr_kernel_launches": (C.c_longlong, []),
+    "svr_scatter_vox_grads": (_I, [_I64, _I, _P, _P, _P, _P]),
+    "svr_sh_eval_views": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P]),
+    "svr_sh_eval_views_bw": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P]),
     "svr_geom_buffer_bytes": (_SZ, [_I64]),
     "svr_preprocess": (_I, [_P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
     "svr_unpack_geom": (_I, [_P, _I64, _P, _P, _P, _P]),

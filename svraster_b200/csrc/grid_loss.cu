@@ -16,6 +16,7 @@
 using namespace svr;
 
 int svr_fail(int code, const char* what);
+void svr_note_launch(int n);
 #define CUDA_TRY(x)                                                                      \
     do {                                                                                 \
         cudaError_t e_ = (x);                                                            \
@@ -119,6 +120,7 @@ extern "C" int svr_valid_table_count(int N, const float* centers, const float* s
     const int res = 1 << res_pow2;
     cell_count_kernel<<<(N + 255) / 256, 256, 0, st>>>(N, centers, sizes, scene_center, inside_extent, res, is_leaf,
                                                       (uint32_t*)(w + L.counts));
+    svr_note_launch(1);
     CUDA_TRY(cudaGetLastError());
     size_t tb = L.scan_tmp_bytes;
     CUDA_TRY(cub::DeviceScan::InclusiveSum(w + L.scan_tmp, tb, (const uint32_t*)(w + L.counts),
@@ -145,6 +147,7 @@ extern "C" int svr_valid_table_fill(int N, const float* centers, const float* si
     cell_fill_kernel<<<(N + 255) / 256, 256, 0, st>>>(N, centers, sizes, scene_center, inside_extent, res, is_leaf,
                                                      (const uint32_t*)(w + L.counts), (const uint32_t*)(w + L.scan),
                                                      grid_mask, (int32_t*)(w + L.keys_in), (int32_t*)(w + L.vox_in));
+    svr_note_launch(1);
     CUDA_TRY(cudaGetLastError());
     int bits = 1;
     while ((1ll << bits) < (long long)res * res * res) ++bits;
@@ -305,6 +308,7 @@ static int grid_loss(bool lap, int G, int A, const int32_t* active, const int32_
     cudaStream_t st = (cudaStream_t)stream;
     if (lap) laplacian_kernel<<<(A + 255) / 256, 256, 0, st>>>(c, A, active, mask, weight, vox_size_inv, seed, grad, status);
     else eikonal_kernel<<<(A + 255) / 256, 256, 0, st>>>(c, A, active, mask, weight, vox_size_inv, seed, grad, status);
+    svr_note_launch(1);
     CUDA_TRY(cudaGetLastError());
     return SVR_OK;
 }

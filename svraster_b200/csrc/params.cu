@@ -10,11 +10,13 @@
 using namespace svr;
 
 int svr_fail(int code, const char* what);
+void svr_note_launch(int n);
 #define CUDA_TRY(x)                                                                      \
     do {                                                                                 \
         cudaError_t e_ = (x);                                                            \
         if (e_ != cudaSuccess) return svr_fail(SVR_ERR_CUDA, cudaGetErrorString(e_));    \
     } while (0)
+#define LAUNCHED() do { svr_note_launch(1); CUDA_TRY(cudaGetLastError()); } while (0)
 
 static inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
@@ -51,7 +53,7 @@ extern "C" int svr_gather_geo(int64_t n_care, const int64_t* care_idx, const int
     if (n_care <= 0) return SVR_OK;
     if (!care_idx || !vox_key || !grid_pts || !geos) return svr_fail(SVR_ERR_ARG, "gather: null argument");
     gather_geo_kernel<<<nblk(n_care * 8, 256), 256, 0, (cudaStream_t)stream>>>(n_care, care_idx, vox_key, grid_pts, geos);
-    CUDA_TRY(cudaGetLastError());
+    LAUNCHED();
     return SVR_OK;
 }
 
@@ -61,7 +63,30 @@ extern "C" int svr_gather_geo_bw(int64_t n_care, const int64_t* care_idx, const 
     if (n_care <= 0) return SVR_OK;
     if (!care_idx || !vox_key || !dgeos || !dgrid) return svr_fail(SVR_ERR_ARG, "gather_bw: null argument");
     gather_geo_bw_kernel<<<nblk(n_care * 8, 256), 256, 0, (cudaStream_t)stream>>>(n_care, care_idx, vox_key, dgeos, dgrid);
-    CUDA_TRY(cudaGetLastError());
+    LAUNCHED();
+    return SVR_OK;
+}
+
+// Scatter per-voxel corner gradients (row stride `ld`, e.g. the 12-wide render adjoint
+// output) into the grid-point gradient for all N voxels; rows of zeros cost no atomics.
+__global__ void scatter_vox_grads_kernel(int64_t N, int ld, const int64_t* __restrict__ vox_key,
+                                         const float* __restrict__ dvox, float* __restrict__ dgrid)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N * 8) return;
+    const int64_t i = t >> 3;
+    const int k = (int)(t & 7);
+    const float d = dvox[i * ld + k];
+    if (d != 0.f) atomicAdd(dgrid + vox_key[8 * i + k], d);
+}
+
+extern "C" int svr_scatter_vox_grads(int64_t N, int ld, const int64_t* vox_key, const float* dvox, float* dgrid,
+                                     void* stream)
+{
+    if (N <= 0) return SVR_OK;
+    if (ld < 8 || !vox_key || !dvox || !dgrid) return svr_fail(SVR_ERR_ARG, "scatter_vox_grads: bad argument");
+    scatter_vox_grads_kernel<<<nblk(N * 8, 256), 256, 0, (cudaStream_t)stream>>>(N, ld, vox_key, dvox, dgrid);
+    LAUNCHED();
     return SVR_OK;
 }
 
@@ -163,7 +188,7 @@ extern "C" int svr_sh_eval(int N, int64_t n_idx, const int64_t* idx, int degree,
         case 2: sh_eval_kernel<2><<<g, 256, 0, st>>>(N, n_idx, idx, M, c, cp, s0, ss, o); break;
         default: sh_eval_kernel<3><<<g, 256, 0, st>>>(N, n_idx, idx, M, c, cp, s0, ss, o); break;
     }
-    CUDA_TRY(cudaGetLastError());
+    LAUNCHED();
     return SVR_OK;
 }
 
@@ -183,7 +208,106 @@ extern "C" int svr_sh_eval_bw(int N, int64_t n_idx, const int64_t* idx, int degr
         case 2: sh_eval_bw_kernel<2><<<g, 256, 0, st>>>(N, n_idx, idx, M, c, cp, d, o0, o1); break;
         default: sh_eval_bw_kernel<3><<<g, 256, 0, st>>>(N, n_idx, idx, M, c, cp, d, o0, o1); break;
     }
-    CUDA_TRY(cudaGetLastError());
+    LAUNCHED();
+    return SVR_OK;
+}
+
+// Multi-view SH: one thread per voxel reads its coefficients once and serves every view
+// (forward writes rgbs[v, i]; the adjoint sums the views' colour gradients into one
+// coefficient gradient).  Same per-view arithmetic as sh_compute.cu:55-176.
+template <int DEG>
+__global__ void sh_views_kernel(int N, int V, int M, const float3* __restrict__ centers,
+                                const float3* __restrict__ cam_pos, const float3* __restrict__ sh0,
+                                const float3* __restrict__ shs, float3* __restrict__ rgbs)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    constexpr int NB = (DEG + 1) * (DEG + 1);
+    float3 c[NB];
+    c[0] = sh0[i];
+#pragma unroll
+    for (int k = 1; k < NB; ++k) c[k] = shs[i * (M - 1) + k - 1];
+    const float3 ctr = centers[i];
+    for (int v = 0; v < V; ++v) {
+        float3 dir = ctr - cam_pos[v];
+        dir = dir * rnorm3df(dir.x, dir.y, dir.z);
+        float B[16];
+        sh_basis<DEG>(dir, B);
+        float3 res = B[0] * c[0];
+#pragma unroll
+        for (int k = 1; k < NB; ++k) res = res + B[k] * c[k];
+        res = res + 0.5f;
+        res.x *= (res.x > 0.0f);
+        res.y *= (res.y > 0.0f);
+        res.z *= (res.z > 0.0f);
+        rgbs[(int64_t)v * N + i] = res;
+    }
+}
+
+template <int DEG>
+__global__ void sh_views_bw_kernel(int N, int V, int M, const float3* __restrict__ centers,
+                                   const float3* __restrict__ cam_pos, const float3* __restrict__ drgbs,
+                                   float3* __restrict__ dsh0, float3* __restrict__ dshs)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    constexpr int NB = (DEG + 1) * (DEG + 1);
+    float3 acc[NB];
+#pragma unroll
+    for (int k = 0; k < NB; ++k) acc[k] = f3(0.f, 0.f, 0.f);
+    const float3 ctr = centers[i];
+    for (int v = 0; v < V; ++v) {
+        const float3 d = drgbs[(int64_t)v * N + i];
+        if (d.x == 0.f && d.y == 0.f && d.z == 0.f) continue;
+        float3 dir = ctr - cam_pos[v];
+        dir = dir * rnorm3df(dir.x, dir.y, dir.z);
+        float B[16];
+        sh_basis<DEG>(dir, B);
+#pragma unroll
+        for (int k = 0; k < NB; ++k) acc[k] = acc[k] + B[k] * d;
+    }
+    dsh0[i] = acc[0];
+#pragma unroll
+    for (int k = 1; k < NB; ++k) dshs[i * (M - 1) + k - 1] = acc[k];
+}
+
+extern "C" int svr_sh_eval_views(int N, int n_views, int degree, int M, const float* centers, const float* cam_pos,
+                                 const float* sh0, const float* shs, float* rgbs, void* stream)
+{
+    if (degree < 0 || degree > 3 || M < (degree + 1) * (degree + 1) || n_views <= 0)
+        return svr_fail(SVR_ERR_ARG, "sh views: bad degree / view count");
+    if (N <= 0) return SVR_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned g = nblk(N, 128);
+    auto c = (const float3*)centers; auto cp = (const float3*)cam_pos; auto s0 = (const float3*)sh0;
+    auto ss = (const float3*)shs; auto o = (float3*)rgbs;
+    switch (degree) {
+        case 0: sh_views_kernel<0><<<g, 128, 0, st>>>(N, n_views, M, c, cp, s0, ss, o); break;
+        case 1: sh_views_kernel<1><<<g, 128, 0, st>>>(N, n_views, M, c, cp, s0, ss, o); break;
+        case 2: sh_views_kernel<2><<<g, 128, 0, st>>>(N, n_views, M, c, cp, s0, ss, o); break;
+        default: sh_views_kernel<3><<<g, 128, 0, st>>>(N, n_views, M, c, cp, s0, ss, o); break;
+    }
+    LAUNCHED();
+    return SVR_OK;
+}
+
+extern "C" int svr_sh_eval_views_bw(int N, int n_views, int degree, int M, const float* centers,
+                                    const float* cam_pos, const float* drgbs, float* dsh0, float* dshs, void* stream)
+{
+    if (degree < 0 || degree > 3 || M < (degree + 1) * (degree + 1) || n_views <= 0)
+        return svr_fail(SVR_ERR_ARG, "sh views bw: bad degree / view count");
+    if (N <= 0) return SVR_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned g = nblk(N, 128);
+    auto c = (const float3*)centers; auto cp = (const float3*)cam_pos; auto d = (const float3*)drgbs;
+    auto o0 = (float3*)dsh0; auto o1 = (float3*)dshs;
+    switch (degree) {
+        case 0: sh_views_bw_kernel<0><<<g, 128, 0, st>>>(N, n_views, M, c, cp, d, o0, o1); break;
+        case 1: sh_views_bw_kernel<1><<<g, 128, 0, st>>>(N, n_views, M, c, cp, d, o0, o1); break;
+        case 2: sh_views_bw_kernel<2><<<g, 128, 0, st>>>(N, n_views, M, c, cp, d, o0, o1); break;
+        default: sh_views_bw_kernel<3><<<g, 128, 0, st>>>(N, n_views, M, c, cp, d, o0, o1); break;
+    }
+    LAUNCHED();
     return SVR_OK;
 }
 
@@ -199,6 +323,18 @@ __device__ __forceinline__ void adam_one(float& p, float g, float& m, float& v, 
     v = lerp_fma(g * g, v, b2);
     const float denom = BIASED ? sqrtf(v) + eps : fmaf(sqrtf(v), rbc2, eps);
     p -= step_size * (m / denom);
+}
+
+template <bool SPARSE, bool BIASED>
+__global__ void adam_scalar_kernel(int64_t n, float* __restrict__ p, const float* __restrict__ g,
+                                   float* __restrict__ m, float* __restrict__ v, float step_size, float b1, float b2,
+                                   float rbc2, float eps)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float P = p[i], Mv = m[i], Vv = v[i];
+    adam_one<SPARSE, BIASED>(P, g[i], Mv, Vv, step_size, b1, b2, rbc2, eps);
+    p[i] = P; m[i] = Mv; v[i] = Vv;
 }
 
 template <bool SPARSE, bool BIASED>
@@ -235,7 +371,6 @@ extern "C" int svr_adam_step(int64_t numel, int biased, int sparse, float* param
     if (numel <= 0) return SVR_OK;
     if (!param || !grad || !exp_avg || !exp_avg_sq) return svr_fail(SVR_ERR_ARG, "adam: null argument");
     const bool aligned = (((uintptr_t)param | (uintptr_t)grad | (uintptr_t)exp_avg | (uintptr_t)exp_avg_sq) & 15) == 0;
-    if (!aligned) return svr_fail(SVR_ERR_ARG, "adam: buffers must be 16-byte aligned");
     float step_size, rbc2;
     if (biased) { step_size = (float)lr; rbc2 = 1.f; }
     else {
@@ -247,6 +382,15 @@ extern "C" int svr_adam_step(int64_t numel, int biased, int sparse, float* param
     cudaStream_t st = (cudaStream_t)stream;
     const unsigned g = nblk((numel + 3) / 4, 256);
     const float b1 = (float)beta1, b2 = (float)beta2;
+    if (!aligned) {
+        const unsigned gs = nblk(numel, 256);
+        if (biased && sparse) adam_scalar_kernel<true, true><<<gs, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
+        else if (biased) adam_scalar_kernel<false, true><<<gs, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
+        else if (sparse) adam_scalar_kernel<true, false><<<gs, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
+        else adam_scalar_kernel<false, false><<<gs, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
+        LAUNCHED();
+        return SVR_OK;
+    }
     if (biased) {
         if (sparse) adam_kernel<true, true><<<g, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
         else adam_kernel<false, true><<<g, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
@@ -254,6 +398,6 @@ extern "C" int svr_adam_step(int64_t numel, int biased, int sparse, float* param
         if (sparse) adam_kernel<true, false><<<g, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
         else adam_kernel<false, false><<<g, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
     }
-    CUDA_TRY(cudaGetLastError());
+    LAUNCHED();
     return SVR_OK;
 }

@@ -10,6 +10,7 @@
 //    warp (8x4 pixel footprint + octant set) once per record instead of once per pixel,
 //    and the adjoint accumulates per-record gradients in shared memory so each record
 //    reaches global memory with one vector atomic per CTA instead of one per pixel.
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -23,8 +24,11 @@ using namespace svr;
 
 // ------------------------------------------------------------------ error plumbing
 static thread_local std::string g_last_error;
+static std::atomic<long long> g_launches{0};
 extern "C" const char* svr_last_error(void) { return g_last_error.c_str(); }
 extern "C" int svr_version(void) { return 1; }
+extern "C" long long svr_kernel_launches(void) { return g_launches.load(); }
+void svr_note_launch(int n) { g_launches += n; }
 
 int svr_fail(int code, const char* what) {
     g_last_error = what;
@@ -37,7 +41,7 @@ int svr_fail(int code, const char* what) {
             return svr_fail(SVR_ERR_CUDA, (std::string(#x) + ": " + cudaGetErrorString(e_)).c_str()); \
         }                                                                                \
     } while (0)
-#define LAUNCH_CHECK() CUDA_TRY(cudaGetLastError())
+#define LAUNCH_CHECK() do { svr_note_launch(1); CUDA_TRY(cudaGetLastError()); } while (0)
 
 static inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 

@@ -1,0 +1,152 @@
+"""Batched multi-view training step on the sm_100a library.
+
+One step renders every view of a batch forward and backward and applies the shipped SDF
+regularisers and Adam (train.py:324-709 for one view at a time): corner-SDF gather, SH
+colour for all views, preprocess, binning, render forward, render adjoint, gradient scatter
+to grid points, SH adjoint, Laplacian + grid-Eikonal smoothness adjoints, Adam on the grid
+SDF and the SH coefficients.  Each stage is one launch for the whole batch.
+
+The upstream gradients dL/d(color, depth, normal, T) stand in for the photometric and
+normal-consistency losses, which run upstream of the rasterizer and are out of scope.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, ptr, stream_ptr
+from .raster import RasterState
+from . import utils
+
+
+class BatchedTrainStep:
+
+    def __init__(self, scene, cams, device="cuda", lr=(1e-3, 1e-3, 1e-4), betas=(0.1, 0.99), eps=1e-15,
+                 lambda_ls=1e-3, lambda_ge=1e-3, lambda_R_concen=0.0, sh_degree=3, seed=0):
+        dev = torch.device(device)
+        self.dev = dev
+        t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
+        self.N = scene.n_vox
+        self.octpath = t(scene.octpath, torch.int64)
+        self.centers = t(scene.vox_center)
+        self.lengths = t(scene.vox_size).reshape(-1).contiguous()
+        self.is_leaf = t(scene.is_leaf, torch.uint8)
+        self.vox_key = t(scene.vox_key, torch.int64)
+        self.grid = t(scene.geo_grid_pts)
+        self.sh0 = t(scene.sh0)
+        self.shs = t(scene.shs)
+        self.M_sh = 1 + scene.shs.shape[1]
+        self.sh_degree = sh_degree
+        self.s_val = torch.tensor([scene.s_val], dtype=torch.float32, device=dev)
+        self.views = [dict(width=c.width, height=c.height, tanfovx=c.tanfovx, tanfovy=c.tanfovy, cx=c.cx, cy=c.cy,
+                           near=c.near, w2c=t(c.w2c), c2w=t(c.c2w), bg=torch.zeros(3, device=dev))
+                      for c in cams]
+        self.V = len(cams)
+        self.cam_pos = torch.stack([v["c2w"][:3, 3] for v in self.views]).contiguous()
+        self.P = sum(c.width * c.height for c in cams)
+        self.rays = self.P
+        self.lr, self.betas, self.eps = lr, betas, eps
+        self.lambda_R = float(lambda_R_concen)
+        self.params = [self.grid, self.sh0, self.shs]
+        self.adam_m = [torch.zeros_like(p) for p in self.params]
+        self.adam_v = [torch.zeros_like(p) for p in self.params]
+        self.adam_step = 0
+        # dense-grid table for the smoothness losses (rebuilt only on prune / subdivide)
+        lv_max = int(scene.octlevel.max())
+        self.res_pow2 = min(lv_max, 9)
+        res = 1 << self.res_pow2
+        self.grid_mask, self.grid_keys, self.grid2voxel = utils.valid_gradient_table(
+            self.centers, self.lengths, torch.zeros(3, device=dev), scene.scene_extent, self.res_pow2, self.is_leaf)
+        ext = np.float32(scene.scene_extent)
+        coord = ((scene.vox_center - scene.vox_size * np.float32(0.5)) + ext * np.float32(0.5)) / ext * np.float32(res)
+        self.grid_voxel_coord = t(np.round(coord))
+        self.grid_voxel_size = t(np.round(scene.vox_size / ext * np.float32(res))).reshape(-1)
+        self.vox_size_min_inv = float(res) / float(scene.scene_extent)
+        self.active = torch.arange(self.grid_keys.numel(), dtype=torch.int32, device=dev)
+        self.lambda_ls, self.lambda_ge = lambda_ls, lambda_ge
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.seed = seed
+        # upstream gradients (seeded synthetic)
+        g = torch.Generator(device=dev).manual_seed(seed)
+        P = self.P
+        self.dcolor = torch.randn(3 * P, device=dev, generator=g)
+        self.ddepth = torch.randn(4 * P, device=dev, generator=g)
+        self.dnormal = torch.randn(3 * P, device=dev, generator=g)
+        self.dT = torch.zeros(P, device=dev)
+        self.gt = torch.rand(3 * P, device=dev, generator=g) if self.lambda_R > 0 else None
+        # per-step buffers
+        self.geos = torch.empty(self.N, 8, device=dev)
+        self.rgbs = torch.empty(self.V * self.N, 3, device=dev)
+        self.dvox = torch.zeros(self.N, 12, device=dev)
+        self.drgbs = torch.zeros(self.V * self.N, 3, device=dev)
+        self.ds = torch.zeros(1, device=dev)
+        self.grads = [torch.zeros_like(p) for p in self.params]
+        self.all_idx = torch.arange(self.N, dtype=torch.int64, device=dev)
+        self.state = None
+        self.ev = None
+
+    # ------------------------------------------------------------------ one step
+    def step(self, time_render=False, grad_hook=None):
+        """One training step.  ``grad_hook(grads)`` runs between the adjoints and Adam (the
+        data-parallel all-reduce of the gradients goes there)."""
+        L = _lib.load()
+        st = stream_ptr(self.dev)
+        N = self.N
+        check(L.svr_gather_geo(N, ptr(self.all_idx), ptr(self.vox_key), ptr(self.grid), ptr(self.geos), st),
+              "gather")
+        check(L.svr_sh_eval_views(N, self.V, self.sh_degree, self.M_sh, ptr(self.centers), ptr(self.cam_pos),
+                                  ptr(self.sh0), ptr(self.shs), ptr(self.rgbs), st), "sh views")
+        state = RasterState(self.views, N, self.dev)
+        state.preprocess(self.octpath, self.centers, self.lengths, self.is_leaf)
+        state.bin(self.octpath)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)] if time_render else None
+        if ev:
+            ev[0].record()
+        color, depth, normal, T, _ = state.render(3, True, True, self.centers, self.lengths, self.geos, self.rgbs,
+                                                  self.s_val, rgb_per_view=True)
+        if ev:
+            ev[1].record()
+        self.dvox.zero_()
+        self.drgbs.zero_()
+        self.ds.zero_()
+        if ev:
+            ev[2].record()
+        state.render_backward(True, True, self.s_val, T, self.dcolor, self.ddepth, self.dnormal, self.dT,
+                              lambda_R_concen=self.lambda_R, gt_color=self.gt, drgbs=self.drgbs, dvox=self.dvox,
+                              ds=self.ds)
+        if ev:
+            ev[3].record()
+        for gr in self.grads:
+            gr.zero_()
+        check(L.svr_scatter_vox_grads(N, 12, ptr(self.vox_key), ptr(self.dvox), ptr(self.grads[0]), st), "scatter")
+        check(L.svr_sh_eval_views_bw(N, self.V, self.sh_degree, self.M_sh, ptr(self.centers), ptr(self.cam_pos),
+                                     ptr(self.drgbs), ptr(self.grads[1]), ptr(self.grads[2]), st), "sh views bw")
+        G, A = self.grid_keys.numel(), self.active.numel()
+        for fn, lam in ((L.svr_laplacian_bw, self.lambda_ls), (L.svr_eikonal_bw, self.lambda_ge)):
+            check(fn(G, A, ptr(self.active), ptr(self.grid_keys), ptr(self.grid2voxel), 1 << self.res_pow2,
+                     ptr(self.grid_mask), ptr(self.grid_voxel_coord), ptr(self.grid_voxel_size), N,
+                     ptr(self.vox_key), ptr(self.grid), self.grid.numel(), float(lam), self.vox_size_min_inv,
+                     self.seed + self.adam_step, ptr(self.grads[0]), ptr(self.status), st), "grid loss")
+        if grad_hook is not None:
+            grad_hook(self.grads)
+        self.adam_step += 1
+        for p, g, m, v, lr in zip(self.params, self.grads, self.adam_m, self.adam_v, self.lr):
+            check(L.svr_adam_step(p.numel(), 0, 0, ptr(p), ptr(g), ptr(m), ptr(v), float(self.adam_step), float(lr),
+                                  self.betas[0], self.betas[1], self.eps, st), "adam")
+        self.state = state
+        self.ev = ev
+        return color, T
+
+    def render_times_ms(self):
+        """(forward, adjoint) kernel-call times of the last timed step, from CUDA events."""
+        if not self.ev:
+            return None
+        return self.ev[0].elapsed_time(self.ev[1]), self.ev[2].elapsed_time(self.ev[3])
+
+    def record_counts(self):
+        """R (records) and R' (records up to tile_last) of the last step."""
+        st = self.state
+        _, ranges, tl, _ = st.binning_fields()
+        r_prime = int((tl.to(torch.int64) - ranges[:, 0].to(torch.int64)).clamp_min(0).sum().item())
+        return st.num_rendered, r_prime
