@@ -182,19 +182,26 @@ SVR_API int svr_valid_table_fill(int N, const float* centers, const float* sizes
                          uint8_t* grid_mask, int32_t* grid_keys, int32_t* grid2voxel,
                          void* stream);
 
+/* Direct-mapped index of the sorted grid keys: dense_index i32[grid_res^3] gets the table row
+ * of every registered cell and -1 elsewhere.  Optional input of the smoothness adjoints (no
+ * counterpart in the reference, which binary-searches the keys, auxiliary.h:418-427). */
+SVR_API int svr_grid_index_build(int G, const int32_t* grid_keys, int grid_res,
+                                 int32_t* dense_index, uint32_t* status, void* stream);
+
 /* Replace _C.laplacian_smoothness_bw (cuda/src/ls_compute.cu:111-153) and
  * _C.grid_eikonal_bw (cuda/src/ge_compute.cu:119-160); accumulate into grid_grad f32[M].
  * `seed` replaces the reference's clock64() seed so runs are reproducible; `status` is a
- * device u32 that collects index errors (0 when clean). */
+ * device u32 that collects index errors (0 when clean).  dense_index (from
+ * svr_grid_index_build) may be NULL, in which case keys are binary-searched. */
 SVR_API int svr_laplacian_bw(int G, int A, const int32_t* active, const int32_t* grid_keys,
                      const int32_t* grid2voxel, int grid_res, const uint8_t* grid_mask,
-                     const float* voxel_coords, const float* voxel_sizes, int N,
+                     const int32_t* dense_index, const float* voxel_coords, const float* voxel_sizes, int N,
                      const int64_t* vox_key, const float* grid_pts, int M, float weight,
                      float vox_size_inv, int seed, float* grid_grad, uint32_t* status,
                      void* stream);
 SVR_API int svr_eikonal_bw(int G, int A, const int32_t* active, const int32_t* grid_keys,
                    const int32_t* grid2voxel, int grid_res, const uint8_t* grid_mask,
-                   const float* voxel_coords, const float* voxel_sizes, int N,
+                   const int32_t* dense_index, const float* voxel_coords, const float* voxel_sizes, int N,
                    const int64_t* vox_key, const float* grid_pts, int M, float weight,
                    float vox_size_inv, int seed, float* grid_grad, uint32_t* status,
                    void* stream);

@@ -60,8 +60,9 @@ _SIGS = {
     "svr_valid_table_workspace_bytes": (_SZ, [_I, _I64]),
     "svr_valid_table_count": (_I, [_I, _P, _P, _P, _F, _I, _P, _P, C.POINTER(C.c_int64), _P]),
     "svr_valid_table_fill": (_I, [_I, _P, _P, _P, _F, _I, _P, _I64, _P, _P, _P, _P, _P]),
-    "svr_laplacian_bw": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P]),
-    "svr_eikonal_bw": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P]),
+    "svr_grid_index_build": (_I, [_I, _P, _I, _P, _P, _P]),
+    "svr_laplacian_bw": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P]),
+    "svr_eikonal_bw": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P]),
     "svr_adam_step": (_I, [_I64, _I, _I, _P, _P, _P, _P, _D, _D, _D, _D, _F, _P]),
 }
 

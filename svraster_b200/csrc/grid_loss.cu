@@ -157,6 +157,34 @@ extern "C" int svr_valid_table_fill(int N, const float* centers, const float* si
     return SVR_OK;
 }
 
+// ------------------------------------------------------------------ direct-mapped key index
+// dense[key] = row of `key` in the sorted table, -1 elsewhere (first row when a key repeats).
+// One 4-byte read replaces each 20+-step binary search of the smoothness adjoints; the
+// table costs 4 * res^3 bytes (512 MB at res 512) and is rebuilt with the grid table.
+__global__ void grid_index_kernel(int G, const int32_t* __restrict__ keys, int cells, int32_t* __restrict__ dense,
+                                  unsigned* status)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= G) return;
+    const int k = keys[i];
+    if (k < 0 || k >= cells) { atomicOr(status, ERR_BAD_INDEX); return; }
+    if (i == 0 || keys[i - 1] != k) dense[k] = i;
+}
+
+extern "C" int svr_grid_index_build(int G, const int32_t* grid_keys, int grid_res, int32_t* dense_index,
+                                    uint32_t* status, void* stream)
+{
+    if (grid_res <= 0 || grid_res > 1024) return svr_fail(SVR_ERR_ARG, "grid index: resolution");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int cells = grid_res * grid_res * grid_res;
+    CUDA_TRY(cudaMemsetAsync(dense_index, 0xFF, 4 * (size_t)cells, st));
+    if (G <= 0) return SVR_OK;
+    grid_index_kernel<<<(G + 255) / 256, 256, 0, st>>>(G, grid_keys, cells, dense_index, status);
+    svr_note_launch(1);
+    CUDA_TRY(cudaGetLastError());
+    return SVR_OK;
+}
+
 // ------------------------------------------------------------------ smoothness adjoints
 __device__ __forceinline__ float hash_to_float(uint32_t x) {
     x ^= x >> 17; x *= 0xed5ad4bbu; x ^= x >> 11; x *= 0xac4c1b51u; x ^= x >> 15; x *= 0x31848babu; x ^= x >> 14;
@@ -186,6 +214,7 @@ __device__ __forceinline__ bool neighbours_ok(int x, int y, int z, int res, cons
 
 struct SampleCtx {
     int G, N, M, res;
+    const int32_t* dense;   // optional direct-mapped key -> table row (-1 when absent)
     const int32_t* keys;
     const int32_t* g2v;
     const float* coords;
@@ -199,7 +228,8 @@ struct SampleCtx {
 __device__ __forceinline__ int sample_cell(const SampleCtx& c, int x, int y, int z, float3 rv, float w[8], float& sdf,
                                            unsigned* status) {
     sdf = 0.f;
-    const int id = find_key(c.keys, c.G, x + y * c.res + z * c.res * c.res);
+    const int key = x + y * c.res + z * c.res * c.res;
+    const int id = c.dense ? c.dense[key] : find_key(c.keys, c.G, key);
     if (id < 0) return -1;
     const int v = c.g2v[id];
     if (v < 0 || v >= c.N) { atomicOr(status, ERR_BAD_INDEX); return -1; }
@@ -225,42 +255,96 @@ __device__ __forceinline__ void scatter8(const SampleCtx& c, int v, const float*
     for (int i = 0; i < 8; ++i) atomicAdd(grad + c.vox_key[8 * (int64_t)v + i], d * w[i]);
 }
 
+// Gradient scatter of one key's samples with two levels of aggregation before the atomics:
+// samples whose owner voxel equals the primary sample's are merged in registers, then lanes
+// of a warp holding the same primary voxel in a contiguous run (consecutive keys inside one
+// coarse voxel) are summed by a segmented shuffle reduction, and only the run head issues
+// the 8 atomics.  Inside a level-6 voxel this turns 56 atomics per key into 8 per warp.
+template <int S>
+__device__ __forceinline__ void scatter_samples(const SampleCtx& c, bool valid, const int* vid, float (*w)[8],
+                                                const float* d, float* grad) {
+    const int primary = valid ? vid[0] : -1;
+    float acc[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) acc[i] = 0.f;
+    if (valid) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            if (vid[s] == primary) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) acc[i] += d[s] * w[s][i];
+            } else {
+                scatter8(c, vid[s], w[s], d[s], grad);
+            }
+        }
+    }
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int prev = __shfl_up_sync(FULL, primary, 1);
+    const bool head = lane == 0 || prev != primary;
+    const unsigned heads = __ballot_sync(FULL, head);
+    // segment of each lane = [its head, next head)
+    const int my_head = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int other_head = __shfl_down_sync(FULL, my_head, off);
+        const bool same = (lane + off < 32) && other_head == my_head;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float v = __shfl_down_sync(FULL, acc[i], off);
+            if (same) acc[i] += v;
+        }
+    }
+    if (head && primary >= 0) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) atomicAdd(grad + c.vox_key[8 * (int64_t)primary + i], acc[i]);
+    }
+}
+
 __global__ void __launch_bounds__(256) laplacian_kernel(SampleCtx c, int A, const int32_t* __restrict__ active,
                                                         const uint8_t* __restrict__ mask, float weight,
                                                         float vox_size_inv, int seed, float* __restrict__ grad,
                                                         unsigned* status)
 {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= A) return;
-    const int a = active[tid];
-    if (a < 0 || a >= c.G) { atomicOr(status, ERR_BAD_INDEX); return; }
-    const int gk = c.keys[a];
+    bool valid = tid < A;
+    int x = 0, y = 0, z = 0, gk = 0;
     const int res = c.res;
-    if (gk < 0 || gk >= res * res * res) { atomicOr(status, ERR_BAD_INDEX); return; }
-    const int x = gk % res, y = (gk / res) % res, z = gk / (res * res);
-    if (!mask[gk] || !neighbours_ok(x, y, z, res, mask)) return;
-    const float3 rv = rand_vec(tid, seed);
-    const int dx[6] = {+1, -1, 0, 0, 0, 0}, dy[6] = {0, 0, +1, -1, 0, 0}, dz[6] = {0, 0, 0, 0, +1, -1};
+    if (valid) {
+        const int a = active[tid];
+        if (a < 0 || a >= c.G) { atomicOr(status, ERR_BAD_INDEX); valid = false; }
+        else {
+            gk = c.keys[a];
+            if (gk < 0 || gk >= res * res * res) { atomicOr(status, ERR_BAD_INDEX); valid = false; }
+            else {
+                x = gk % res; y = (gk / res) % res; z = gk / (res * res);
+                valid = mask[gk] && neighbours_ok(x, y, z, res, mask);
+            }
+        }
+    }
     float w[7][8];
     int vid[7];
-    float nb[6], center;
-    vid[0] = sample_cell(c, x, y, z, rv, w[0], center, status);
+    float dd[7];
+    if (valid) {
+        const float3 rv = rand_vec(tid, seed);
+        const int dx[6] = {+1, -1, 0, 0, 0, 0}, dy[6] = {0, 0, +1, -1, 0, 0}, dz[6] = {0, 0, 0, 0, +1, -1};
+        float nb[6], center;
+        vid[0] = sample_cell(c, x, y, z, rv, w[0], center, status);
 #pragma unroll
-    for (int i = 0; i < 6; ++i) vid[i + 1] = sample_cell(c, x + dx[i], y + dy[i], z + dz[i], rv, w[i + 1], nb[i], status);
-    const float lx = nb[0] + nb[1] - 2.0f * center;
-    const float ly = nb[2] + nb[3] - 2.0f * center;
-    const float lz = nb[4] + nb[5] - 2.0f * center;
-    const float lr = sqrtf(lx * lx + ly * ly + lz * lz + 1e-10f);
-    // ls_compute.cu:79-83 evaluates these in double (0.5 is a double literal there)
-    const float size = weight * 0.5 * vox_size_inv * vox_size_inv;
-    const float gx = 0.5 / lr * 2 * lx * size;
-    const float gy = 0.5 / lr * 2 * ly * size;
-    const float gz = 0.5 / lr * 2 * lz * size;
-    const float gc = -2.0f * (gx + gy + gz);
-    scatter8(c, vid[0], w[0], gc, grad);
-    scatter8(c, vid[1], w[1], gx, grad); scatter8(c, vid[2], w[2], gx, grad);
-    scatter8(c, vid[3], w[3], gy, grad); scatter8(c, vid[4], w[4], gy, grad);
-    scatter8(c, vid[5], w[5], gz, grad); scatter8(c, vid[6], w[6], gz, grad);
+        for (int i = 0; i < 6; ++i) vid[i + 1] = sample_cell(c, x + dx[i], y + dy[i], z + dz[i], rv, w[i + 1], nb[i], status);
+        const float lx = nb[0] + nb[1] - 2.0f * center;
+        const float ly = nb[2] + nb[3] - 2.0f * center;
+        const float lz = nb[4] + nb[5] - 2.0f * center;
+        const float lr = sqrtf(lx * lx + ly * ly + lz * lz + 1e-10f);
+        // ls_compute.cu:79-83 evaluates these in double (0.5 is a double literal there)
+        const float size = weight * 0.5 * vox_size_inv * vox_size_inv;
+        const float gx = 0.5 / lr * 2 * lx * size;
+        const float gy = 0.5 / lr * 2 * ly * size;
+        const float gz = 0.5 / lr * 2 * lz * size;
+        dd[0] = -2.0f * (gx + gy + gz);
+        dd[1] = gx; dd[2] = gx; dd[3] = gy; dd[4] = gy; dd[5] = gz; dd[6] = gz;
+    }
+    scatter_samples<7>(c, valid, vid, w, dd, grad);
 }
 
 __global__ void __launch_bounds__(256) eikonal_kernel(SampleCtx c, int A, const int32_t* __restrict__ active,
@@ -269,42 +353,51 @@ __global__ void __launch_bounds__(256) eikonal_kernel(SampleCtx c, int A, const 
                                                       unsigned* status)
 {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= A) return;
-    const int a = active[tid];
-    if (a < 0 || a >= c.G) { atomicOr(status, ERR_BAD_INDEX); return; }
-    const int gk = c.keys[a];
+    bool valid = tid < A;
+    int x = 0, y = 0, z = 0, gk = 0;
     const int res = c.res;
-    if (gk < 0 || gk >= res * res * res) { atomicOr(status, ERR_BAD_INDEX); return; }
-    const int x = gk % res, y = (gk / res) % res, z = gk / (res * res);
-    if (!mask[gk] || !neighbours_ok(x, y, z, res, mask)) return;
-    const float3 rv = rand_vec(tid, seed);
-    const int dx[6] = {+1, -1, 0, 0, 0, 0}, dy[6] = {0, 0, +1, -1, 0, 0}, dz[6] = {0, 0, 0, 0, +1, -1};
+    if (valid) {
+        const int a = active[tid];
+        if (a < 0 || a >= c.G) { atomicOr(status, ERR_BAD_INDEX); valid = false; }
+        else {
+            gk = c.keys[a];
+            if (gk < 0 || gk >= res * res * res) { atomicOr(status, ERR_BAD_INDEX); valid = false; }
+            else {
+                x = gk % res; y = (gk / res) % res; z = gk / (res * res);
+                valid = mask[gk] && neighbours_ok(x, y, z, res, mask);
+            }
+        }
+    }
     float w[6][8];
     int vid[6];
-    float s[6];
+    float dd[6];
+    if (valid) {
+        const float3 rv = rand_vec(tid, seed);
+        const int dx[6] = {+1, -1, 0, 0, 0, 0}, dy[6] = {0, 0, +1, -1, 0, 0}, dz[6] = {0, 0, 0, 0, +1, -1};
+        float s[6];
 #pragma unroll
-    for (int i = 0; i < 6; ++i) vid[i] = sample_cell(c, x + dx[i], y + dy[i], z + dz[i], rv, w[i], s[i], status);
-    const float dxv = (s[0] - s[1]) * 0.5f, dyv = (s[2] - s[3]) * 0.5f, dzv = (s[4] - s[5]) * 0.5f;
-    const float gn = sqrtf(dxv * dxv + dyv * dyv + dzv * dzv + 1e-6f);
-    const float gw = gn * 0.5 * vox_size_inv;   // ge_compute.cu:93, double literal
-    const float dg = 2.0f * (gw - 1.0f) * weight;
-    const float ddx = dg * dxv / gn * 0.5f * vox_size_inv;
-    const float ddy = dg * dyv / gn * 0.5f * vox_size_inv;
-    const float ddz = dg * dzv / gn * 0.5f * vox_size_inv;
-    scatter8(c, vid[0], w[0], ddx, grad); scatter8(c, vid[1], w[1], -ddx, grad);
-    scatter8(c, vid[2], w[2], ddy, grad); scatter8(c, vid[3], w[3], -ddy, grad);
-    scatter8(c, vid[4], w[4], ddz, grad); scatter8(c, vid[5], w[5], -ddz, grad);
+        for (int i = 0; i < 6; ++i) vid[i] = sample_cell(c, x + dx[i], y + dy[i], z + dz[i], rv, w[i], s[i], status);
+        const float dxv = (s[0] - s[1]) * 0.5f, dyv = (s[2] - s[3]) * 0.5f, dzv = (s[4] - s[5]) * 0.5f;
+        const float gn = sqrtf(dxv * dxv + dyv * dyv + dzv * dzv + 1e-6f);
+        const float gw = gn * 0.5 * vox_size_inv;   // ge_compute.cu:93, double literal
+        const float dg = 2.0f * (gw - 1.0f) * weight;
+        const float ddx = dg * dxv / gn * 0.5f * vox_size_inv;
+        const float ddy = dg * dyv / gn * 0.5f * vox_size_inv;
+        const float ddz = dg * dzv / gn * 0.5f * vox_size_inv;
+        dd[0] = ddx; dd[1] = -ddx; dd[2] = ddy; dd[3] = -ddy; dd[4] = ddz; dd[5] = -ddz;
+    }
+    scatter_samples<6>(c, valid, vid, w, dd, grad);
 }
 
 static int grid_loss(bool lap, int G, int A, const int32_t* active, const int32_t* keys, const int32_t* g2v, int res,
-                     const uint8_t* mask, const float* coords, const float* vsizes, int N, const int64_t* vox_key,
+                     const uint8_t* mask, const int32_t* dense, const float* coords, const float* vsizes, int N, const int64_t* vox_key,
                      const float* grid, int M, float weight, float vox_size_inv, int seed, float* grad,
                      unsigned* status, void* stream)
 {
     if (A <= 0) return SVR_OK;
     if (!active || !keys || !g2v || !mask || !coords || !vsizes || !vox_key || !grid || !grad || !status)
         return svr_fail(SVR_ERR_ARG, "grid loss: null argument");
-    SampleCtx c{G, N, M, res, keys, g2v, coords, vsizes, vox_key, grid};
+    SampleCtx c{G, N, M, res, dense, keys, g2v, coords, vsizes, vox_key, grid};
     cudaStream_t st = (cudaStream_t)stream;
     if (lap) laplacian_kernel<<<(A + 255) / 256, 256, 0, st>>>(c, A, active, mask, weight, vox_size_inv, seed, grad, status);
     else eikonal_kernel<<<(A + 255) / 256, 256, 0, st>>>(c, A, active, mask, weight, vox_size_inv, seed, grad, status);
@@ -314,21 +407,21 @@ static int grid_loss(bool lap, int G, int A, const int32_t* active, const int32_
 }
 
 extern "C" int svr_laplacian_bw(int G, int A, const int32_t* active, const int32_t* grid_keys, const int32_t* grid2voxel,
-                                int grid_res, const uint8_t* grid_mask, const float* voxel_coords,
+                                int grid_res, const uint8_t* grid_mask, const int32_t* dense_index, const float* voxel_coords,
                                 const float* voxel_sizes, int N, const int64_t* vox_key, const float* grid_pts, int M,
                                 float weight, float vox_size_inv, int seed, float* grid_grad, uint32_t* status,
                                 void* stream)
 {
-    return grid_loss(true, G, A, active, grid_keys, grid2voxel, grid_res, grid_mask, voxel_coords, voxel_sizes, N,
+    return grid_loss(true, G, A, active, grid_keys, grid2voxel, grid_res, grid_mask, dense_index, voxel_coords, voxel_sizes, N,
                      vox_key, grid_pts, M, weight, vox_size_inv, seed, grid_grad, status, stream);
 }
 
 extern "C" int svr_eikonal_bw(int G, int A, const int32_t* active, const int32_t* grid_keys, const int32_t* grid2voxel,
-                              int grid_res, const uint8_t* grid_mask, const float* voxel_coords,
+                                int grid_res, const uint8_t* grid_mask, const int32_t* dense_index, const float* voxel_coords,
                               const float* voxel_sizes, int N, const int64_t* vox_key, const float* grid_pts, int M,
                               float weight, float vox_size_inv, int seed, float* grid_grad, uint32_t* status,
                               void* stream)
 {
-    return grid_loss(false, G, A, active, grid_keys, grid2voxel, grid_res, grid_mask, voxel_coords, voxel_sizes, N,
+    return grid_loss(false, G, A, active, grid_keys, grid2voxel, grid_res, grid_mask, dense_index, voxel_coords, voxel_sizes, N,
                      vox_key, grid_pts, M, weight, vox_size_inv, seed, grid_grad, status, stream);
 }

@@ -483,259 +483,8 @@ __global__ void __launch_bounds__(256) pack_records_kernel(
     for (int q = 0; q < 5; ++q) dst[q] = src[q];
 }
 
-// ------------------------------------------------------------------ forward render
-struct alignas(16) FwdSmem {
-    Rec buf[2][BLOCK];
-    uint8_t wmask[BLOCK];
-    uint64_t bar[2];
-    uint32_t warp_quads[8];
-    uint32_t red[8];
-};
-
-template <int NS, bool DEPTH, bool NORMAL, bool MAXW>
-__global__ void __launch_bounds__(BLOCK) render_fwd_kernel(
-    const __grid_constant__ Views V, const uint2* __restrict__ ranges, const Rec* __restrict__ recs,
-    const float* __restrict__ s_ptr, uint32_t* __restrict__ tile_last, uint32_t* __restrict__ n_contrib,
-    float* __restrict__ out_color, float* __restrict__ out_depth, float* __restrict__ out_normal,
-    float* __restrict__ out_T, float* __restrict__ max_w, unsigned* __restrict__ status)
-{
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    FwdSmem& S = *reinterpret_cast<FwdSmem*>(smem_raw);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int tile = blockIdx.x;
-    const int vi = view_of_tile(V, tile);
-    const svr_view_t& view = V.v[vi];
-    const int W = view.width, H = view.height;
-    const int lt = tile - view.tile_offset;
-    const int tx = lt % view.tiles_x, ty = lt / view.tiles_x;
-    int dx, dy;
-    tile_pixel(tid, dx, dy);
-    const uint32_t px = tx * TILE + dx, py = ty * TILE + dy;
-    const bool inside = (px < (uint32_t)W) && (py < (uint32_t)H);
-    const Ray ray = pixel_ray(view, px, py);
-    const uint32_t pq = ray_octant(ray.rd);
-    const float s_val = *s_ptr;
-
-    // octants present in each warp (only inside pixels can match a record)
-    const uint32_t wq = __reduce_or_sync(0xffffffffu, inside ? (1u << pq) : 0u);
-    if (lane == 0) S.warp_quads[warp] = wq;
-    if (tid == 0) {
-        mbar_init(&S.bar[0], 1);
-        mbar_init(&S.bar[1], 1);
-        fence_mbar_init();
-    }
-    const uint2 range = ranges[tile];
-    const int n = (int)(range.y - range.x);
-    const int nbatch = (n + BLOCK - 1) / BLOCK;
-    __syncthreads();
-    if (tid == 0 && nbatch > 0) {
-        const uint32_t bytes = (uint32_t)min(BLOCK, n) * sizeof(Rec);
-        mbar_arrive_tx(&S.bar[0], bytes);
-        bulk_g2s(S.buf[0], recs + range.x, bytes, &S.bar[0]);
-    }
-
-    float T = 1.f, D = 0.f;
-    float3 C = f3(0.f, 0.f, 0.f), Nn = f3(0.f, 0.f, 0.f);
-    int64_t med_rec = -1;
-    float med_T = 0.f;
-    uint32_t last = 0;
-    bool done = !inside;
-    uint32_t parity = 0;   // bit b: parity of the next wait on bar[b]
-    int b = 0;
-    bool failed = false;
-    for (; b < nbatch; ++b) {
-        const int ndone = __syncthreads_count(done);
-        if (ndone == BLOCK) break;
-        if (tid == 0 && b + 1 < nbatch) {
-            const int nb1 = min(BLOCK, n - (b + 1) * BLOCK);
-            const uint32_t bytes = (uint32_t)nb1 * sizeof(Rec);
-            mbar_arrive_tx(&S.bar[(b + 1) & 1], bytes);
-            bulk_g2s(S.buf[(b + 1) & 1], recs + range.x + (size_t)(b + 1) * BLOCK, bytes, &S.bar[(b + 1) & 1]);
-        }
-        const int sb = b & 1;
-        if (!mbar_wait(&S.bar[sb], (parity >> sb) & 1)) { failed = true; break; }
-        parity ^= (1u << sb);
-        const int cnt = min(BLOCK, n - b * BLOCK);
-        const Rec* buf = S.buf[sb];
-        // per-record warp footprint mask: bbox overlap with each warp's 8x4 block and the
-        // record's octant present in that warp
-        if (tid < cnt) {
-            const Rec& r = buf[tid];
-            const uint32_t x0 = r.bbox0 >> 16, y0 = r.bbox0 & 0xFFFF, x1 = r.bbox1 >> 16, y1 = r.bbox1 & 0xFFFF;
-            const uint32_t q = r.val >> 29;
-            uint32_t m = 0;
-#pragma unroll
-            for (int w = 0; w < 8; ++w) {
-                const uint32_t wx0 = tx * TILE + (w & 1) * 8, wy0 = ty * TILE + (w >> 1) * 4;
-                const bool hit = x0 <= wx0 + 7 && x1 >= wx0 && y0 <= wy0 + 3 && y1 >= wy0 &&
-                                 ((S.warp_quads[w] >> q) & 1);
-                m |= (uint32_t)hit << w;
-            }
-            S.wmask[tid] = (uint8_t)m;
-        }
-        __syncthreads();
-        const int nchunk = (cnt + 31) >> 5;
-        for (int c = 0; c < nchunk; ++c) {
-            const int j = c * 32 + lane;
-            const uint32_t rel = __ballot_sync(0xffffffffu, j < cnt && ((S.wmask[j] >> warp) & 1));
-            if (rel == 0) continue;
-            uint32_t cand = 0;
-            if (!done) {
-                uint32_t rr = rel;
-                while (rr) {
-                    const int k = __ffs(rr) - 1;
-                    rr &= rr - 1;
-                    const Rec& r = buf[c * 32 + k];
-                    if (!pix_in_bbox(px, py, r.bbox0, r.bbox1) || pq != (r.val >> 29)) continue;
-                    const float2 ab = ray_box(f3(r.cx, r.cy, r.cz), r.len, ray.ro, ray.rd_inv);
-                    if (ab.x > ab.y) continue;
-                    cand |= 1u << k;
-                }
-            }
-            while (cand && !done) {
-                const int k = __ffs(cand) - 1;
-                cand &= cand - 1;
-                const int j2 = c * 32 + k;
-                const Rec& r = buf[j2];
-                const float3 vox_c = f3(r.cx, r.cy, r.cz);
-                const float vox_l = r.len;
-                const float2 ab = ray_box(vox_c, vox_l, ray.ro, ray.rd_inv);
-                const float a = ab.x, bb = ab.y;
-                float g[8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) g[q] = r.g[q];
-                // forward.cu:255-306: NeuS alpha from the logistic CDF at entry and exit
-                float w8[8];
-                float local_a[NS > 1 ? NS : 1];
-                const float vox_l_inv = 1.f / vox_l;
-                const float3 p_entry = ray.ro + a * ray.rd;
-                const float3 P_step = (bb - a) * ray.rd / (float)NS;
-                const float3 qt_entry = (p_entry - (vox_c - 0.5f * vox_l)) * vox_l_inv;
-                const float3 qt_step = P_step * vox_l_inv;
-                tri_weights(qt_entry, w8);
-                float sdf_former = interp8(g, w8);
-                float phi_former = 1.f / (1.f + expf(-s_val * sdf_former));
-                const float phi_entry = phi_former;
-#pragma unroll
-                for (int s = 0; s < NS; ++s) {
-                    const float3 qt_curr = qt_entry + qt_step * (float)(s + 1);
-                    tri_weights(qt_curr, w8);
-                    const float sdf_curr = interp8(g, w8);
-                    const float phi_curr = 1.f / (1.f + expf(-s_val * sdf_curr));
-                    if (DEPTH && NS > 1) local_a[s] = fmaxf((phi_former - phi_curr) / (phi_former + 1e-6f), 0.f);
-                    phi_former = phi_curr;
-                    sdf_former = sdf_curr;
-                }
-                const float alpha = fmaxf((phi_entry - phi_former) / (phi_entry + 1e-6f), 0.f);
-                if (alpha < MIN_ALPHA) continue;
-                const float pt_w = T * alpha;
-                C = C + pt_w * f3(r.r, r.gr, r.b);
-                if (DEPTH) {
-                    float dval;
-                    if (NS == 3) {
-                        const float step_sz = 0.3333333f * (bb - a);
-                        const float a0 = local_a[0], a1 = local_a[NS > 1 ? 1 : 0], a2 = local_a[NS > 2 ? 2 : 0];
-                        const float t0 = a + 0.5f * step_sz, t1 = a + 1.5f * step_sz, t2 = a + 2.5f * step_sz;
-                        dval = a0 * t0 + (1.f - a0) * a1 * t1 + (1.f - a0) * (1.f - a1) * a2 * t2;
-                    } else if (NS == 2) {
-                        const float step_sz = 0.5f * (bb - a);
-                        const float a0 = local_a[0], a1 = local_a[NS > 1 ? 1 : 0];
-                        const float t0 = a + 0.5f * step_sz, t1 = a + 1.5f * step_sz;
-                        dval = a0 * t0 + (1.f - a0) * a1 * t1;
-                    } else {
-                        dval = alpha * 0.5f * (a + bb);
-                    }
-                    D = D + T * dval;
-                    if (T > 0.5f) { med_rec = (int64_t)range.x + b * BLOCK + j2; med_T = T; }
-                }
-                if (NORMAL) {
-                    const float lin_nx = (g[4] + g[5] + g[6] + g[7]) - (g[0] + g[1] + g[2] + g[3]);
-                    const float lin_ny = (g[2] + g[3] + g[6] + g[7]) - (g[0] + g[1] + g[4] + g[5]);
-                    const float lin_nz = (g[1] + g[3] + g[5] + g[7]) - (g[0] + g[2] + g[4] + g[6]);
-                    const float r_lin = safe_rnorm(lin_nx, lin_ny, lin_nz);
-                    Nn = Nn + pt_w * r_lin * f3(lin_nx, lin_ny, lin_nz);
-                }
-                T *= (1.f - alpha);
-                done |= (T < EARLY_STOP_T);
-                last = (uint32_t)(b * BLOCK + j2 + 1);
-                if (MAXW) atomicMax(((int*)max_w) + (r.val & 0x1FFFFFFFu), __float_as_int(pt_w));
-            }
-        }
-    }
-    // drain a copy still in flight when the loop left early
-    if (!failed && b < nbatch) {
-        const int sb = b & 1;
-        if (!mbar_wait(&S.bar[sb], (parity >> sb) & 1)) failed = true;
-    }
-    if (failed && tid == 0) atomicOr(status, ERR_WAIT_TIMEOUT);
-
-    float D_med = 0.f;
-    if (DEPTH && inside && med_rec >= 0) {
-        // forward.cu:450-521: 16-step refinement of the median-depth crossing
-        const Rec& r = recs[med_rec];
-        const float3 vox_c = f3(r.cx, r.cy, r.cz);
-        const float vox_l = r.len;
-        float g[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) g[q] = r.g[q];
-        const float2 ab = ray_box(vox_c, vox_l, ray.ro, ray.rd_inv);
-        const float a = ab.x, bb = ab.y;
-        const float vox_l_inv = 1.f / vox_l;
-        const float step_sz = (bb - a) * (1.f / 16);
-        const float3 step = step_sz * ray.rd;
-        D_med = a - 0.5f * step_sz;
-        float3 q_edge = ((ray.ro + a * ray.rd) - (vox_c - 0.5f * vox_l)) * vox_l_inv;
-        const float3 q_edge_step = step * vox_l_inv;
-        float w8[8];
-        tri_weights(q_edge, w8);
-        float phi_prev = 1.f / (1.f + expf(-s_val * interp8(g, w8)));
-        for (int k = 0; k < 16 && med_T > 0.5f; ++k) {
-            D_med += step_sz;
-            q_edge = q_edge + q_edge_step;
-            tri_weights(q_edge, w8);
-            const float phi_curr = 1.f / (1.f + expf(-s_val * interp8(g, w8)));
-            const float alpha_k = (phi_prev - phi_curr) / (phi_prev + 1e-6f);
-            med_T *= (1.f - alpha_k);
-            phi_prev = phi_curr;
-        }
-    }
-
-    uint32_t my_last = 0;
-    if (inside) {
-        const int64_t HW = (int64_t)W * H;
-        const int64_t pix = (int64_t)py * W + px;
-        const float* bg = view.bg;
-        n_contrib[view.pix_offset + pix] = last;
-        float* oc = out_color + 3 * view.pix_offset;
-        oc[pix] = C.x + T * bg[0];
-        oc[HW + pix] = C.y + T * bg[1];
-        oc[2 * HW + pix] = C.z + T * bg[2];
-        out_T[view.pix_offset + pix] = T;
-        if (DEPTH) {
-            float* od = out_depth + 4 * view.pix_offset;
-            od[pix] = D * ray.rd_norm_inv;
-            od[HW + pix] = 0.f;
-            od[2 * HW + pix] = D_med * ray.rd_norm_inv;
-            od[3 * HW + pix] = 0.f;
-        }
-        if (NORMAL) {
-            float* on = out_normal + 3 * view.pix_offset;
-            on[pix] = Nn.x; on[HW + pix] = Nn.y; on[2 * HW + pix] = Nn.z;
-        }
-        my_last = last;
-    }
-    const uint32_t wl = __reduce_max_sync(0xffffffffu, my_last);
-    if (lane == 0) S.red[warp] = wl;
-    __syncthreads();
-    if (tid == 0) {
-        uint32_t m = 0;
-#pragma unroll
-        for (int w = 0; w < 8; ++w) m = max(m, S.red[w]);
-        tile_last[tile] = range.x + m;
-        mbar_inval(&S.bar[0]);
-        mbar_inval(&S.bar[1]);
-    }
-}
+// ------------------------------------------------------------------ render kernels
+#include "render_kernels.cuh"
 
 template <int NS, bool DEPTH, bool NORMAL, bool MAXW>
 static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint2* ranges, const Rec* recs,
@@ -800,319 +549,6 @@ extern "C" int svr_render_fwd(const svr_view_t* views_host, int n_views, int N, 
     FWD_CASE(3)
 #undef FWD_CASE
     return svr_fail(SVR_ERR_UNSUPPORTED, "n_samp");
-}
-
-// ------------------------------------------------------------------ adjoint render
-struct alignas(16) BwdSmem {
-    Rec buf[2][BLOCK];
-    float acc[BLOCK][12];
-    uint8_t wmask[BLOCK];
-    uint8_t touched[BLOCK];
-    uint64_t bar[2];
-    uint32_t warp_quads[8];
-    float red[8];
-};
-
-template <bool DEPTH, bool NORMAL, bool RCONC>
-__global__ void __launch_bounds__(BLOCK) render_bwd_kernel(
-    const __grid_constant__ Views V, int N, const uint2* __restrict__ ranges, const uint32_t* __restrict__ tile_last,
-    const uint32_t* __restrict__ n_contrib, const Rec* __restrict__ recs, const float* __restrict__ s_ptr,
-    const float* __restrict__ out_T, const float* __restrict__ dL_dcolor, const float* __restrict__ dL_ddepth,
-    const float* __restrict__ dL_dnormal, const float* __restrict__ dL_dT, float lambda_R, const float* __restrict__ gt_color,
-    float* __restrict__ dL_dvox, float* __restrict__ drgbs, float* __restrict__ dL_ds, unsigned* __restrict__ status)
-{
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    BwdSmem& S = *reinterpret_cast<BwdSmem*>(smem_raw);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int tile = blockIdx.x;
-    const int vi = view_of_tile(V, tile);
-    const svr_view_t& view = V.v[vi];
-    const int W = view.width, H = view.height;
-    const int lt = tile - view.tile_offset;
-    const int tx = lt % view.tiles_x, ty = lt / view.tiles_x;
-    int dx, dy;
-    tile_pixel(tid, dx, dy);
-    const uint32_t px = tx * TILE + dx, py = ty * TILE + dy;
-    const bool inside = (px < (uint32_t)W) && (py < (uint32_t)H);
-    const Ray ray = pixel_ray(view, px, py);
-    const uint32_t pq = ray_octant(ray.rd);
-    const float s_val = *s_ptr;
-
-    const uint32_t wq = __reduce_or_sync(0xffffffffu, inside ? (1u << pq) : 0u);
-    if (lane == 0) S.warp_quads[warp] = wq;
-    if (tid == 0) {
-        mbar_init(&S.bar[0], 1);
-        mbar_init(&S.bar[1], 1);
-        fence_mbar_init();
-    }
-#pragma unroll
-    for (int k = 0; k < 12; ++k) S.acc[tid][k] = 0.f;
-    S.touched[tid] = 0;
-
-    const uint32_t r0 = ranges[tile].x;
-    const uint32_t r1 = tile_last[tile];
-    const int n = r1 > r0 ? (int)(r1 - r0) : 0;
-    const int nbatch = (n + BLOCK - 1) / BLOCK;
-
-    // per-pixel adjoint state (backward.cu:156-216)
-    const int64_t HW = (int64_t)W * H;
-    const int64_t pix = (int64_t)py * W + px;
-    float T = 0.f;
-    uint32_t last_c = 0;
-    float3 dpix = f3(0.f, 0.f, 0.f), dN = f3(0.f, 0.f, 0.f), gt = f3(0.f, 0.f, 0.f);
-    float last_dT = 0.f, dD = 0.f;
-    if (inside) {
-        T = out_T[view.pix_offset + pix];
-        last_c = n_contrib[view.pix_offset + pix];
-        const float* dc = dL_dcolor + 3 * view.pix_offset;
-        dpix = f3(dc[pix], dc[HW + pix], dc[2 * HW + pix]);
-        const float* bg = view.bg;
-        last_dT = dL_dT[view.pix_offset + pix] + dot3(f3(bg[0], bg[1], bg[2]), dpix);
-        if (DEPTH) dD = dL_ddepth[4 * view.pix_offset + pix] * ray.rd_norm_inv;
-        if (NORMAL) {
-            const float* dn = dL_dnormal + 3 * view.pix_offset;
-            dN = f3(dn[pix], dn[HW + pix], dn[2 * HW + pix]);
-        }
-        if (RCONC) {
-            const float* gc = gt_color + 3 * view.pix_offset;
-            gt = f3(gc[pix], gc[HW + pix], gc[2 * HW + pix]);
-        }
-    }
-    const float WH_inv = 1.f / ((float)(W * H));
-    const float weight_R = lambda_R * WH_inv;
-    float ds_acc = 0.f;
-    const bool active = inside && last_c > 0;
-
-    __syncthreads();
-    if (tid == 0 && nbatch > 0) {
-        const int c0 = min(BLOCK, n);
-        const uint32_t bytes = (uint32_t)c0 * sizeof(Rec);
-        mbar_arrive_tx(&S.bar[0], bytes);
-        bulk_g2s(S.buf[0], recs + (r1 - c0), bytes, &S.bar[0]);
-    }
-    uint32_t parity = 0;
-    bool failed = false;
-    int b = 0;
-    for (; b < nbatch; ++b) {
-        __syncthreads();   // batch b-1 processed and flushed: its buffer may be refilled
-        if (tid == 0 && b + 1 < nbatch) {
-            const int hi1 = n - (b + 1) * BLOCK;           // exclusive end (relative)
-            const int c1 = min(BLOCK, hi1);
-            const uint32_t bytes = (uint32_t)c1 * sizeof(Rec);
-            mbar_arrive_tx(&S.bar[(b + 1) & 1], bytes);
-            bulk_g2s(S.buf[(b + 1) & 1], recs + r0 + (hi1 - c1), bytes, &S.bar[(b + 1) & 1]);
-        }
-        const int sb = b & 1;
-        if (!mbar_wait(&S.bar[sb], (parity >> sb) & 1)) { failed = true; break; }
-        parity ^= (1u << sb);
-        const int hi = n - b * BLOCK;
-        const int cnt = min(BLOCK, hi);
-        const int lo = hi - cnt;                    // relative index of slot 0
-        const Rec* buf = S.buf[sb];
-        if (tid < cnt) {
-            const Rec& r = buf[tid];
-            const uint32_t x0 = r.bbox0 >> 16, y0 = r.bbox0 & 0xFFFF, x1 = r.bbox1 >> 16, y1 = r.bbox1 & 0xFFFF;
-            const uint32_t q = r.val >> 29;
-            uint32_t m = 0;
-#pragma unroll
-            for (int w = 0; w < 8; ++w) {
-                const uint32_t wx0 = tx * TILE + (w & 1) * 8, wy0 = ty * TILE + (w >> 1) * 4;
-                const bool hit = x0 <= wx0 + 7 && x1 >= wx0 && y0 <= wy0 + 3 && y1 >= wy0 &&
-                                 ((S.warp_quads[w] >> q) & 1);
-                m |= (uint32_t)hit << w;
-            }
-            S.wmask[tid] = (uint8_t)m;
-        }
-        __syncthreads();
-        const int nchunk = (cnt + 31) >> 5;
-        for (int c = nchunk - 1; c >= 0; --c) {
-            const int j = c * 32 + lane;
-            const uint32_t rel = __ballot_sync(0xffffffffu, j < cnt && ((S.wmask[j] >> warp) & 1));
-            if (rel == 0) continue;
-            uint32_t cand = 0;
-            if (active) {
-                uint32_t rr = rel;
-                while (rr) {
-                    const int k = __ffs(rr) - 1;
-                    rr &= rr - 1;
-                    const int jj = c * 32 + k;
-                    if ((uint32_t)(lo + jj) >= last_c) continue;
-                    const Rec& r = buf[jj];
-                    if (!pix_in_bbox(px, py, r.bbox0, r.bbox1) || pq != (r.val >> 29)) continue;
-                    const float2 ab = ray_box(f3(r.cx, r.cy, r.cz), r.len, ray.ro, ray.rd_inv);
-                    if (ab.x > ab.y) continue;
-                    cand |= 1u << k;
-                }
-            }
-            while (cand) {
-                const int k = 31 - __clz(cand);           // back to front
-                cand &= ~(1u << k);
-                const int jj = c * 32 + k;
-                const Rec& r = buf[jj];
-                const float3 vox_c = f3(r.cx, r.cy, r.cz);
-                const float vox_l = r.len;
-                const float2 ab = ray_box(vox_c, vox_l, ray.ro, ray.rd_inv);
-                const float a = ab.x, bb = ab.y;
-                float g[8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) g[q] = r.g[q];
-                const float vox_l_inv = 1.f / vox_l;
-                // backward.cu:313-388: entry / exit from ro + t rd, three sub-segment alphas
-                const float3 p_entry = ray.ro + a * ray.rd;
-                const float3 p_exit = ray.ro + bb * ray.rd;
-                const float3 qt_entry = (p_entry - (vox_c - 0.5f * vox_l)) * vox_l_inv;
-                const float3 qt_exit = (p_exit - (vox_c - 0.5f * vox_l)) * vox_l_inv;
-                float we[8], wx[8];
-                tri_weights(qt_entry, we);
-                tri_weights(qt_exit, wx);
-                float sdf_entry = 0.f, sdf_exit = 0.f;
-#pragma unroll
-                for (int i = 0; i < 8; ++i) { sdf_entry += g[i] * we[i]; sdf_exit += g[i] * wx[i]; }
-                const float phi_entry = 1.f / (1.f + expf(-s_val * sdf_entry));
-                const float phi_exit = 1.f / (1.f + expf(-s_val * sdf_exit));
-                const float denom = phi_entry + 1e-6f;
-                const float alpha = fmaxf((phi_entry - phi_exit) / denom, 0.f);
-                if (alpha < MIN_ALPHA) continue;   // lambda_ascending == 0
-                float dg[8];
-#pragma unroll
-                for (int i = 0; i < 8; ++i) dg[i] = 0.f;
-                float la[3] = {0.f, 0.f, 0.f};
-                float eg[3][8];
-                if (DEPTH) {
-                    const float3 qt0 = ((ray.ro + a * ray.rd) - (vox_c - 0.5f * vox_l)) * vox_l_inv;
-                    const float3 qt_step = ((bb - a) * ray.rd / 3.0f) * vox_l_inv;
-#pragma unroll
-                    for (int kk = 0; kk < 3; ++kk) {
-                        const float3 qk = qt0 + qt_step * (float)kk;
-                        const float3 qk1 = qt0 + qt_step * (float)(kk + 1);
-                        float wk[8], wk1[8];
-                        tri_weights(qk, wk);
-                        tri_weights(qk1, wk1);
-                        float sdf_k = 0.f, sdf_k1 = 0.f;
-#pragma unroll
-                        for (int i = 0; i < 8; ++i) { sdf_k += g[i] * wk[i]; sdf_k1 += g[i] * wk1[i]; }
-                        const float phi_k = 1.f / (1.f + expf(-s_val * sdf_k));
-                        const float phi_k1 = 1.f / (1.f + expf(-s_val * sdf_k1));
-                        const float denom_k = phi_k + 1e-6f;
-                        const float raw_k = (phi_k - phi_k1) / denom_k;
-                        const float allow = raw_k > 0.f ? 1.f : 0.f;
-                        la[kk] = fmaxf(raw_k, 0.f);
-                        const float d_ad_phi_k = allow * ((phi_k1) / (denom_k * denom_k));
-                        const float d_ad_phi_k1 = allow * (-1.f / denom_k);
-                        const float dphi_k = s_val * phi_k * (1.f - phi_k);
-                        const float dphi_k1 = s_val * phi_k1 * (1.f - phi_k1);
-#pragma unroll
-                        for (int i = 0; i < 8; ++i) eg[kk][i] = d_ad_phi_k * dphi_k * wk[i] + d_ad_phi_k1 * dphi_k1 * wk1[i];
-                    }
-                }
-                T = T / (1.f - alpha);
-                const float pt_w = alpha * T;
-                const float3 c3 = f3(r.r, r.gr, r.b);
-                float dL_dpt_w = dot3(dpix, c3);
-                if (NORMAL) {
-                    // backward.cu:604-639
-                    const float lin_nx = (g[4] + g[5] + g[6] + g[7]) - (g[0] + g[1] + g[2] + g[3]);
-                    const float lin_ny = (g[2] + g[3] + g[6] + g[7]) - (g[0] + g[1] + g[4] + g[5]);
-                    const float lin_nz = (g[1] + g[3] + g[5] + g[7]) - (g[0] + g[2] + g[4] + g[6]);
-                    const float3 lin_n = f3(lin_nx, lin_ny, lin_nz);
-                    const float r_lin = safe_rnorm(lin_nx, lin_ny, lin_nz);
-                    const float3 surf_n = r_lin * lin_n;
-                    dL_dpt_w += dot3(dN, surf_n);
-                    const float3 dL_dsurf_n = pt_w * dN;
-                    const float3 d = r_lin * (dL_dsurf_n - dot3(dL_dsurf_n, lin_n) * r_lin * surf_n);
-                    dg[0] += -d.x - d.y - d.z; dg[1] += -d.x - d.y + d.z;
-                    dg[2] += -d.x + d.y - d.z; dg[3] += -d.x + d.y + d.z;
-                    dg[4] += +d.x - d.y - d.z; dg[5] += +d.x - d.y + d.z;
-                    dg[6] += +d.x + d.y - d.z; dg[7] += +d.x + d.y + d.z;
-                }
-                const float dL_dalpha = T * (dL_dpt_w - last_dT);
-                last_dT += alpha * (dL_dpt_w - last_dT);
-                {
-                    // backward.cu:650-671
-                    const float pe = s_val * phi_entry * (1.f - phi_entry);
-                    const float px_ = s_val * phi_exit * (1.f - phi_exit);
-                    const float d_alpha_d_entry = (pe * (1.f - alpha)) / denom;
-                    const float d_alpha_d_exit = -px_ / denom;
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        dg[i] += d_alpha_d_entry * we[i] * dL_dalpha;
-                        dg[i] += d_alpha_d_exit * wx[i] * dL_dalpha;
-                    }
-                    const float d_phi_entry_ds = phi_entry * (1.f - phi_entry) * sdf_entry;
-                    const float d_phi_exit_ds = phi_exit * (1.f - phi_exit) * sdf_exit;
-                    const float d_alpha_ds = ((d_phi_entry_ds * (1.f - alpha)) + (-d_phi_exit_ds)) / denom;
-                    ds_acc += dL_dalpha * d_alpha_ds;
-                }
-                if (DEPTH) {
-                    // backward.cu:682-768 (n_samp 3, SDF)
-                    const float step_sz = 0.3333333f * (bb - a);
-                    const float a0 = la[0], a1 = la[1], a2 = la[2];
-                    const float t0 = a + 0.5f * step_sz, t1 = a + 1.5f * step_sz, t2 = a + 2.5f * step_sz;
-                    const float dval = a0 * t0 + (1.f - a0) * a1 * t1 + (1.f - a0) * (1.f - a1) * a2 * t2;
-                    const float d0 = dD * T * (t0 + a1 * a2 * t2 - a1 * t1 - a2 * t2);
-                    const float d1 = dD * T * (t1 + a0 * a2 * t2 - a0 * t1 - a2 * t2);
-                    const float d2 = dD * T * (t2 + a0 * a1 * t2 - a0 * t2 - a1 * t2);
-                    last_dT += dD * dval;
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) dg[i] += d0 * eg[0][i] + d1 * eg[1][i] + d2 * eg[2][i];
-                }
-                float drgb0 = pt_w * dpix.x, drgb1 = pt_w * dpix.y, drgb2 = pt_w * dpix.z;
-                if (RCONC) {
-                    const float3 gr = weight_R * pt_w * 2.0f * (c3 - gt);
-                    drgb0 += gr.x; drgb1 += gr.y; drgb2 += gr.z;
-                }
-                float* acc = S.acc[jj];
-#pragma unroll
-                for (int i = 0; i < 8; ++i) atomicAdd(acc + i, dg[i]);
-                atomicAdd(acc + 8, drgb0);
-                atomicAdd(acc + 9, drgb1);
-                atomicAdd(acc + 10, drgb2);
-                atomicAdd(acc + 11, fabsf(dL_dalpha * alpha));
-                S.touched[jj] = 1;
-            }
-        }
-        __syncthreads();
-        // one vector atomic per touched record per CTA
-        if (tid < cnt && S.touched[tid]) {
-            const uint32_t vid = buf[tid].val & 0x1FFFFFFFu;
-            float* a = S.acc[tid];
-            if (vid < (uint32_t)N) {
-                float4* dst = reinterpret_cast<float4*>(dL_dvox + 12 * (size_t)vid);
-                atomicAdd(dst, make_float4(a[0], a[1], a[2], a[3]));
-                atomicAdd(dst + 1, make_float4(a[4], a[5], a[6], a[7]));
-                if (drgbs) {
-                    float* cr = drgbs + 3 * ((size_t)vi * N + vid);
-                    atomicAdd(cr, a[8]); atomicAdd(cr + 1, a[9]); atomicAdd(cr + 2, a[10]);
-                    atomicAdd(dL_dvox + 12 * (size_t)vid + 11, a[11]);
-                } else {
-                    atomicAdd(dst + 2, make_float4(a[8], a[9], a[10], a[11]));
-                }
-            } else {
-                atomicOr(status, ERR_BAD_INDEX);
-            }
-#pragma unroll
-            for (int k = 0; k < 12; ++k) a[k] = 0.f;
-            S.touched[tid] = 0;
-        }
-    }
-    if (!failed && b < nbatch) {
-        const int sb = b & 1;
-        if (!mbar_wait(&S.bar[sb], (parity >> sb) & 1)) failed = true;
-    }
-    if (failed && tid == 0) atomicOr(status, ERR_WAIT_TIMEOUT);
-    // one dL/ds atomic per CTA
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) ds_acc += __shfl_xor_sync(0xffffffffu, ds_acc, o);
-    if (lane == 0) S.red[warp] = ds_acc;
-    __syncthreads();
-    if (tid == 0) {
-        float s = 0.f;
-#pragma unroll
-        for (int w = 0; w < 8; ++w) s += S.red[w];
-        if (s != 0.f) atomicAdd(dL_ds, s);
-        mbar_inval(&S.bar[0]);
-        mbar_inval(&S.bar[1]);
-    }
 }
 
 template <bool DEPTH, bool NORMAL, bool RCONC>

@@ -64,6 +64,8 @@ class BatchedTrainStep:
         self.grid_voxel_size = t(np.round(scene.vox_size / ext * np.float32(res))).reshape(-1)
         self.vox_size_min_inv = float(res) / float(scene.scene_extent)
         self.active = torch.arange(self.grid_keys.numel(), dtype=torch.int32, device=dev)
+        from .grid_loss_bw import dense_index
+        self.grid_index = dense_index(self.grid_keys, res)
         self.lambda_ls, self.lambda_ge = lambda_ls, lambda_ge
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.seed = seed
@@ -89,60 +91,74 @@ class BatchedTrainStep:
     # ------------------------------------------------------------------ one step
     def step(self, time_render=False, grad_hook=None):
         """One training step.  ``grad_hook(grads)`` runs between the adjoints and Adam (the
-        data-parallel all-reduce of the gradients goes there)."""
+        data-parallel all-reduce of the gradients goes there).  With ``time_render`` every
+        stage is bracketed by CUDA events on the launching stream (see ``stage_ms``)."""
         L = _lib.load()
         st = stream_ptr(self.dev)
         N = self.N
+        marks = []
+
+        def mark(name):
+            if time_render:
+                e = torch.cuda.Event(enable_timing=True)
+                e.record()
+                marks.append((name, e))
+
+        mark("start")
         check(L.svr_gather_geo(N, ptr(self.all_idx), ptr(self.vox_key), ptr(self.grid), ptr(self.geos), st),
               "gather")
         check(L.svr_sh_eval_views(N, self.V, self.sh_degree, self.M_sh, ptr(self.centers), ptr(self.cam_pos),
                                   ptr(self.sh0), ptr(self.shs), ptr(self.rgbs), st), "sh views")
+        mark("gather+sh")
         state = RasterState(self.views, N, self.dev)
         state.preprocess(self.octpath, self.centers, self.lengths, self.is_leaf)
+        mark("preprocess")
         state.bin(self.octpath)
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)] if time_render else None
-        if ev:
-            ev[0].record()
+        mark("count+sort")
         color, depth, normal, T, _ = state.render(3, True, True, self.centers, self.lengths, self.geos, self.rgbs,
                                                   self.s_val, rgb_per_view=True)
-        if ev:
-            ev[1].record()
+        mark("render_fwd")   # includes the record packing launch
         self.dvox.zero_()
         self.drgbs.zero_()
         self.ds.zero_()
-        if ev:
-            ev[2].record()
+        mark("zero")
         state.render_backward(True, True, self.s_val, T, self.dcolor, self.ddepth, self.dnormal, self.dT,
                               lambda_R_concen=self.lambda_R, gt_color=self.gt, drgbs=self.drgbs, dvox=self.dvox,
                               ds=self.ds)
-        if ev:
-            ev[3].record()
+        mark("render_bwd")
         for gr in self.grads:
             gr.zero_()
         check(L.svr_scatter_vox_grads(N, 12, ptr(self.vox_key), ptr(self.dvox), ptr(self.grads[0]), st), "scatter")
         check(L.svr_sh_eval_views_bw(N, self.V, self.sh_degree, self.M_sh, ptr(self.centers), ptr(self.cam_pos),
                                      ptr(self.drgbs), ptr(self.grads[1]), ptr(self.grads[2]), st), "sh views bw")
+        mark("scatter+sh_bw")
         G, A = self.grid_keys.numel(), self.active.numel()
         for fn, lam in ((L.svr_laplacian_bw, self.lambda_ls), (L.svr_eikonal_bw, self.lambda_ge)):
             check(fn(G, A, ptr(self.active), ptr(self.grid_keys), ptr(self.grid2voxel), 1 << self.res_pow2,
-                     ptr(self.grid_mask), ptr(self.grid_voxel_coord), ptr(self.grid_voxel_size), N,
+                     ptr(self.grid_mask), ptr(self.grid_index), ptr(self.grid_voxel_coord),
+                     ptr(self.grid_voxel_size), N,
                      ptr(self.vox_key), ptr(self.grid), self.grid.numel(), float(lam), self.vox_size_min_inv,
                      self.seed + self.adam_step, ptr(self.grads[0]), ptr(self.status), st), "grid loss")
+        mark("smoothness")
         if grad_hook is not None:
             grad_hook(self.grads)
+            mark("allreduce")
         self.adam_step += 1
         for p, g, m, v, lr in zip(self.params, self.grads, self.adam_m, self.adam_v, self.lr):
             check(L.svr_adam_step(p.numel(), 0, 0, ptr(p), ptr(g), ptr(m), ptr(v), float(self.adam_step), float(lr),
                                   self.betas[0], self.betas[1], self.eps, st), "adam")
+        mark("adam")
         self.state = state
-        self.ev = ev
+        self.ev = marks if time_render else None
         return color, T
 
-    def render_times_ms(self):
-        """(forward, adjoint) kernel-call times of the last timed step, from CUDA events."""
-        if not self.ev:
-            return None
-        return self.ev[0].elapsed_time(self.ev[1]), self.ev[2].elapsed_time(self.ev[3])
+    @staticmethod
+    def stage_ms(marks):
+        """{stage: ms} from the event marks of one timed step (call after synchronising)."""
+        out = {}
+        for (_, a), (name, b) in zip(marks[:-1], marks[1:]):
+            out[name] = a.elapsed_time(b)
+        return out
 
     def record_counts(self):
         """R (records) and R' (records up to tile_last) of the last step."""

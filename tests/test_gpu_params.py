@@ -91,8 +91,9 @@ def test_valid_table_bitexact(kind, res_pow2):
     assert np.array_equal(g2v.cpu().numpy(), rv)
 
 
+@pytest.mark.parametrize("use_index", [True, False])
 @pytest.mark.parametrize("which", ["lap", "eik"])
-def test_smoothness_adjoints_match_oracle(which):
+def test_smoothness_adjoints_match_oracle(which, use_index):
     sc = S.scene_small(seed=3)
     res_pow2 = 7
     mask, keys, g2v = _table(sc, res_pow2)
@@ -103,7 +104,8 @@ def test_smoothness_adjoints_match_oracle(which):
     grad = torch.zeros(len(sc.geo_grid_pts), 1, device=dev)
     fn = grid_loss_bw.laplacian_smoothness if which == "lap" else grid_loss_bw.grid_eikonal
     fn(T(sc.geo_grid_pts), T(sc.vox_key, torch.int64), T(coord), T(vsize), 1 << res_pow2, mask, keys, g2v,
-       T(active, torch.int32), 0.01, float(1 << res_pow2) / sc.scene_extent, True, False, grad, seed=777)
+       T(active, torch.int32), 0.01, float(1 << res_pow2) / sc.scene_extent, True, False, grad, seed=777,
+       use_index=use_index)
     ofn = O.laplacian_bw if which == "lap" else O.eikonal_bw
     ref = ofn(sc.geo_grid_pts, sc.vox_key, coord, vsize, 1 << res_pow2, mask.cpu().numpy(), keys.cpu().numpy(),
               g2v.cpu().numpy(), active, 0.01, float(1 << res_pow2) / sc.scene_extent, 777,
