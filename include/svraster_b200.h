@@ -206,6 +206,22 @@ SVR_API int svr_eikonal_bw(int G, int A, const int32_t* active, const int32_t* g
                    float vox_size_inv, int seed, float* grid_grad, uint32_t* status,
                    void* stream);
 
+/* Allocation-free variant of svr_laplacian_bw, for callers that cannot allocate device
+ * memory (a host that reserves all device memory in a fixed arena at start-up and forbids
+ * later cudaMalloc calls).  It has no counterpart in the reference.  The direct-mapped key
+ * index lives in a static 8 MiB device array inside the library instead of caller memory,
+ * so grid_res must be at most 128 (larger grids return SVR_ERR_CAPACITY).  Inputs, outputs
+ * and the status word are the caller's, as for svr_laplacian_bw, and no device memory is
+ * allocated.  The first call on each device resolves the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share
+ * the one array and rebuild it each time, so calls that overlap on the GPU race. */
+SVR_API int svr_laplacian_bw_noalloc(int G, int A, const int32_t* active, const int32_t* grid_keys,
+                                     const int32_t* grid2voxel, int grid_res, const uint8_t* grid_mask,
+                                     const float* voxel_coords, const float* voxel_sizes, int N,
+                                     const int64_t* vox_key, const float* grid_pts, int M, float weight,
+                                     float vox_size_inv, int seed, float* grid_grad, uint32_t* status,
+                                     void* stream);
+
 /* ---------------------------------------------------------------- optimiser
  * Replace _C.unbiased_adam_step / _C.biased_adam_step (cuda/src/adam_step.cu:106-159). */
 SVR_API int svr_adam_step(int64_t numel, int biased, int sparse, float* param, const float* grad,

@@ -6,6 +6,7 @@
 // no N*64 over-allocation) and a stable radix sort orders the (key, voxel) pairs.
 // Laplacian / grid-Eikonal adjoints: cuda/src/ls_compute.cu:14-109, ge_compute.cu:14-117
 // with the sample helpers of auxiliary.h:392-471.  The jitter seed is an argument.
+#include <mutex>
 #include <string>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -424,4 +425,54 @@ extern "C" int svr_eikonal_bw(int G, int A, const int32_t* active, const int32_t
 {
     return grid_loss(false, G, A, active, grid_keys, grid2voxel, grid_res, grid_mask, dense_index, voxel_coords, voxel_sizes, N,
                      vox_key, grid_pts, M, weight, vox_size_inv, seed, grid_grad, status, stream);
+}
+
+// ------------------------------------------------------------------ allocation-free variant
+// For callers that cannot allocate device memory themselves (for example a host framework
+// that hands out all device memory from a fixed arena reserved at start-up and forbids any
+// later cudaMalloc): the direct-mapped key index of the Laplacian adjoint lives in this
+// file-scope device array instead of caller memory.  Every GPU that loads the library holds
+// it (8 MiB) until the process exits.
+#define SVR_NOALLOC_MAX_RES 128
+static __device__ __align__(256) int32_t g_noalloc_grid_index[SVR_NOALLOC_MAX_RES * SVR_NOALLOC_MAX_RES *
+                                                                SVR_NOALLOC_MAX_RES];
+
+// Device address of g_noalloc_grid_index per device.  The host-side name of the array is a
+// stand-in, not a device address, so the address comes from cudaGetSymbolAddress, resolved
+// once per device with that device current.
+static int32_t* g_noalloc_index_ptr[64];
+static std::mutex g_noalloc_mutex;
+
+static int noalloc_index_ptr(int32_t** out) {
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return svr_fail(SVR_ERR_UNSUPPORTED, "noalloc: device ordinal above 63");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_index_ptr[dev]) {
+        void* p = nullptr;
+        CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_grid_index));
+        g_noalloc_index_ptr[dev] = (int32_t*)p;
+    }
+    *out = g_noalloc_index_ptr[dev];
+    return SVR_OK;
+}
+
+extern "C" int svr_laplacian_bw_noalloc(int G, int A, const int32_t* active, const int32_t* grid_keys,
+                                        const int32_t* grid2voxel, int grid_res, const uint8_t* grid_mask,
+                                        const float* voxel_coords, const float* voxel_sizes, int N,
+                                        const int64_t* vox_key, const float* grid_pts, int M, float weight,
+                                        float vox_size_inv, int seed, float* grid_grad, uint32_t* status,
+                                        void* stream)
+{
+    if (grid_res <= 0 || grid_res > SVR_NOALLOC_MAX_RES)
+        return svr_fail(SVR_ERR_CAPACITY, "svr_laplacian_bw_noalloc: grid_res exceeds the static index capacity "
+                                          "(maximum 128)");
+    int32_t* index = nullptr;
+    int rc = noalloc_index_ptr(&index);
+    if (rc) return rc;
+    // the array keeps the previous call's index: rebuild it (the build clears it to -1 first)
+    rc = svr_grid_index_build(G, grid_keys, grid_res, index, status, stream);
+    if (rc) return rc;
+    return grid_loss(true, G, A, active, grid_keys, grid2voxel, grid_res, grid_mask, index, voxel_coords,
+                     voxel_sizes, N, vox_key, grid_pts, M, weight, vox_size_inv, seed, grid_grad, status, stream);
 }
