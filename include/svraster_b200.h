@@ -222,6 +222,38 @@ SVR_API int svr_laplacian_bw_noalloc(int G, int A, const int32_t* active, const 
                                      float vox_size_inv, int seed, float* grid_grad, uint32_t* status,
                                      void* stream);
 
+/* ---------------------------------------------------------------- surface extraction
+ * TSDF fusion, replacing src/utils/fuser_utils.py:54-156 (Fuser.integrate / tsdf): fold a batch
+ * of views into the running weight / weighted-SDF sums of M grid points xyz f32[M,3].
+ * Depth (and optional alpha) maps are packed per view like the render outputs: view v's
+ * plane `sel` of a `ch`-channel image starts at ch * pix_offset_v + sel * H_v * W_v
+ * (pix_offset is recomputed from the view sizes).  alpha_is_T reads alpha as 1 - T.
+ * proj_host (may be NULL) holds per view the double tanfovx, tanfovy, cx/W, cy/H of the
+ * camera (src/cameras.py:89-103).  Per-point 1/trunc (inv_trunc_pts) overrides `trunc`.
+ * fp64 != 0: accumulators are f64, else f32 (the reference's order of rounding). */
+SVR_API int svr_tsdf_integrate(const svr_view_t* views_host, const double* proj_host, int n_views,
+                               int64_t M, const float* xyz, const float* depth, int depth_ch,
+                               int depth_sel, const float* alpha, int alpha_ch, int alpha_sel,
+                               int alpha_is_T, const float* inv_trunc_pts, double trunc,
+                               double crop_border, float alpha_thres, int use_trunc,
+                               int depth_weight, int border_weight, float max_norm_dist, int fp64,
+                               void* weight_acc, void* sdf_acc, void* stream);
+
+/* Sparse marching cubes, replacing cuda/svraster_cuda/marching_cubes.py:278-380
+ * (torch_marching_cubes_grid): voxels vox_key i64[n_vox,8] over grid values f32[M] and
+ * positions f32[M,3].  svr_mc_count classifies the voxels and returns the triangle count
+ * (synchronises); svr_mc_emit writes the unique vertices (lexicographically sorted, as
+ * unique(dim=0) returns them) into verts f32[>=3*n_tri,3] and faces i64[n_tri,3], and returns
+ * the vertex count.  Both use one workspace: >= svr_mc_workspace_bytes(n_vox, 0) for the
+ * count and >= svr_mc_workspace_bytes(n_vox, n_tri) for the emit, whose prefix must hold the
+ * count's results.  fp64 interpolates the vertices in double (precision mode). */
+SVR_API size_t svr_mc_workspace_bytes(int64_t n_vox, int64_t n_tri);
+SVR_API int svr_mc_count(int64_t n_vox, const int64_t* vox_key, int64_t M, const float* grid_val,
+                         float iso, void* workspace, int64_t* n_tri_host, void* stream);
+SVR_API int svr_mc_emit(int64_t n_vox, const int64_t* vox_key, const float* grid_val,
+                        const float* grid_xyz, float iso, int64_t n_tri, int fp64, void* workspace,
+                        float* verts, int64_t* faces, int64_t* n_verts_host, void* stream);
+
 /* ---------------------------------------------------------------- optimiser
  * Replace _C.unbiased_adam_step / _C.biased_adam_step (cuda/src/adam_step.cu:106-159). */
 SVR_API int svr_adam_step(int64_t numel, int biased, int sparse, float* param, const float* grad,

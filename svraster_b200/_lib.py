@@ -64,6 +64,11 @@ _SIGS = {
     "svr_laplacian_bw": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P]),
     "svr_eikonal_bw": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P]),
     "svr_laplacian_bw_noalloc": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P]),
+    "svr_tsdf_integrate": (_I, [_P, _P, _I, _I64, _P, _P, _I, _I, _P, _I, _I, _I, _P, _D, _D, _F, _I, _I, _I, _F,
+                                _I, _P, _P, _P]),
+    "svr_mc_workspace_bytes": (_SZ, [_I64, _I64]),
+    "svr_mc_count": (_I, [_I64, _P, _I64, _P, _F, _P, C.POINTER(C.c_int64), _P]),
+    "svr_mc_emit": (_I, [_I64, _P, _P, _P, _F, _I64, _I, _P, _P, _P, C.POINTER(C.c_int64), _P]),
     "svr_adam_step": (_I, [_I64, _I, _I, _P, _P, _P, _P, _D, _D, _D, _D, _F, _P]),
 }
 
