@@ -53,7 +53,7 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms during the timed region."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -67,7 +67,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (FileNotFoundError, OSError):
             self.proc = None
@@ -283,6 +283,67 @@ def run_e2e(args, scene, cams, dev):
             "path": "svraster_b200.renderer.rasterize_voxels per view + autograd + grid_loss_bw + SparseAdam"}
 
 
+def run_extraction(step, scene, cams, dev):
+    """TSDF fusion of the 8 rendered median-depth maps into every grid point (one launch) and
+    marching cubes over every voxel of the trained SDF (extract_mesh_sdf.py:337-381 path),
+    timed with CUDA events; CPU baseline: the NumPy restatement on a sample."""
+    import torch
+    from svraster_b200 import _lib
+    from svraster_b200._lib import check, ptr, stream_ptr
+    from svraster_b200.marching_cubes import torch_marching_cubes_grid
+    from svraster_b200.raster import RasterState
+    st_ = RasterState(step.views, step.N, dev)
+    st_.preprocess(step.octpath, step.centers, step.lengths, step.is_leaf)
+    st_.bin(step.octpath)
+    color, depth, normal, T, _ = st_.render(3, True, False, step.centers, step.lengths, step.geos, step.rgbs,
+                                            step.s_val, rgb_per_view=True)
+    xyz = torch.as_tensor(scene.grid_pts_xyz).to(dev).contiguous()
+    M = xyz.shape[0]
+    finest = scene.scene_extent * 2.0 ** -int(scene.octlevel.max())
+    trunc = 3.0 * finest
+    wacc = torch.zeros(M, device=dev)
+    sacc = torch.zeros(M, device=dev)
+    proj = []
+    for c in cams:
+        proj += [c.tanfovx, c.tanfovy, 0.5, 0.5]
+    proj_h = (len(proj) * _lib.C.c_double)(*proj)
+    L = _lib.load()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    for rep in range(2):   # first pass warms up
+        wacc.zero_(); sacc.zero_()
+        torch.cuda.synchronize()
+        e[0].record()
+        check(L.svr_tsdf_integrate(st_.views, proj_h, len(cams), M, ptr(xyz), ptr(depth), 4, 2, ptr(T), 1, 0, 1, None,
+                                   trunc, 0.01, 0.5, 1, 0, 0, 10.0, 0, ptr(wacc), ptr(sacc), stream_ptr(dev)), "tsdf")
+        e[1].record()
+        grid_val = step.grid.reshape(-1)
+        v, f = torch_marching_cubes_grid(grid_val, xyz, step.vox_key, 0.0)
+        e[2].record()
+        torch.cuda.synchronize()
+    tsdf_ms, mc_ms = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+    fused = int((wacc > 0).sum().item())
+    # CPU baseline: NumPy restatements on a sample (one view of TSDF, 1/16 of the voxels for MC)
+    from oracle import extract_oracle as X
+    d0 = depth[: 4 * cams[0].width * cams[0].height].view(4, cams[0].height, cams[0].width)[2].cpu().numpy()
+    a0 = (1 - T[: cams[0].width * cams[0].height]).view(cams[0].height, cams[0].width).cpu().numpy()
+    wc = np.zeros((M, 1), np.float32); sc_ = np.zeros((M, 1), np.float32)
+    t0 = time.perf_counter()
+    X.tsdf_integrate(wc, sc_, scene.grid_pts_xyz, cams[0].w2c, cams[0].c2w, cams[0].tanfovx, cams[0].tanfovy, 0.5,
+                     0.5, d0, a0, trunc, crop_border=0.01)
+    cpu_tsdf = time.perf_counter() - t0
+    sub = scene.vox_key[::16]
+    t0 = time.perf_counter()
+    X.marching_cubes(step.grid.reshape(-1).cpu().numpy(), scene.grid_pts_xyz, sub, 0.0)
+    cpu_mc = time.perf_counter() - t0
+    return {"tsdf_ms": round(tsdf_ms, 3), "tsdf_views": len(cams), "grid_points": M, "fused_points": fused,
+            "tsdf_Mpoint_views_per_s": round(M * len(cams) / tsdf_ms / 1e3, 1),
+            "mc_ms": round(mc_ms, 3), "mc_voxels": scene.n_vox, "mc_faces": int(f.shape[0]),
+            "mc_Mvoxels_per_s": round(scene.n_vox / mc_ms / 1e3, 1),
+            "cpu_numpy_restatement": {"tsdf_Mpoint_views_per_s": round(M / cpu_tsdf / 1e6, 3),
+                                      "mc_Mvoxels_per_s": round(len(sub) / cpu_mc / 1e6, 3), "cores": 1,
+                                      "sample": "TSDF: 1 of 8 views; MC: every 16th voxel"}}
+
+
 def oracle_view_step(scene, cam, threads):
     """preprocess + binning + forward + backward of one view on the CPU oracle."""
     from oracle import oracle as O
@@ -341,12 +402,13 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--views", type=int, default=N_VIEWS, help="views per GPU (8 = the benchmark workload)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extract", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))
@@ -366,6 +428,9 @@ def main():
     result, step, scene, cams = run_ours(args, rank, world)
     if rank == 0:
         import torch
+        if not args.no_extract:
+            result["extraction"] = run_extraction(step, scene, cams,
+                                                  torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
         if not args.no_e2e:
             del step
             torch.cuda.empty_cache()
