@@ -133,28 +133,51 @@ def run_ours(args, rank, world):
         for g in grads:
             dist.all_reduce(g)
     hook = allreduce_grads if world > 1 else None
+    # one GPU: the timed steps replay one CUDA graph holding the whole step (the record count
+    # stays on the device); several GPUs: eager steps with the all-reduce between them
+    use_graph = world == 1 and not args.no_graph
     for _ in range(args.warmup):
         step.step(grad_hook=hook)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    launches0 = L.svr_kernel_launches()
+
+    def timed(fn):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n0 = L.svr_kernel_launches()
+        with ClockSampler(dev.index) as clk:
+            torch.cuda.synchronize()
+            ev0.record()
+            for _ in range(args.steps):
+                fn()
+            ev1.record()
+            torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1), L.svr_kernel_launches() - n0, clk.summary()
+
+    # eager steps, every stage bracketed by events (the per-stage breakdown)
     step_events = []
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(dev.index) as clk:
-        torch.cuda.synchronize()
-        ev0.record()
-        for _ in range(args.steps):
-            step.step(time_render=True, grad_hook=hook)
-            step_events.append(step.ev)
-        ev1.record()
-        torch.cuda.synchronize()
-    launches = L.svr_kernel_launches() - launches0
+
+    def eager():
+        step.step(time_render=True, grad_hook=hook)
+        step_events.append(step.ev)
+    eager_ms, launches, clocks = timed(eager)
     stages = [BatchedTrainStep.stage_ms(m) for m in step_events]
     stage_avg = {k: float(np.mean([s_[k] for s_ in stages])) for k in stages[0]}
     fwd_ms = [s_["render_fwd"] for s_ in stages]
     bwd_ms = [s_["render_bwd"] for s_ in stages]
-    total_ms = ev0.elapsed_time(ev1)
+    total_ms = eager_ms
+    graph_info = None
+    if use_graph:
+        per_step = step.capture()
+        for _ in range(args.warmup):
+            step.replay()
+        total_ms, _, clocks = timed(step.replay)
+        launches = per_step * args.steps
+        st_raster, st_misc = step.graph_status()
+        if st_raster or st_misc:
+            raise RuntimeError(f"graph replay status raster={st_raster} misc={st_misc}")
+        graph_info = {"captured": True, "kernels_per_step": per_step, "record_capacity": step.capacity,
+                      "eager_ms_per_step": round(eager_ms / args.steps, 3)}
     if world > 1:
         t = torch.tensor([total_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -193,7 +216,8 @@ def run_ours(args, rank, world):
                          "l2": "inputs larger than L2 (records + SH state > 126 MB)",
                          "parallelism": f"dp{world} over views" if world > 1 else "single GPU"},
               "stages_ms": {k: round(v, 3) for k, v in stage_avg.items()},
-              "roofline": roofline, "gpu_launches": int(launches), "clocks": clk.summary()}
+              "roofline": roofline, "gpu_launches": int(launches), "clocks": clocks,
+              "cuda_graph": graph_info or {"captured": False}}
     return result, step, scene, cams
 
 
@@ -409,6 +433,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extract", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="time eager steps instead of graph replays")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))

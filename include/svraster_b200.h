@@ -85,6 +85,11 @@ SVR_API int svr_unpack_geom(const void* geom_buffer, int64_t n_items, uint32_t* 
 SVR_API int svr_count_rendered(int64_t n_items, void* geom_buffer, int64_t* num_rendered_host,
                        uint64_t* path_or_host, void* stream);
 
+/* The prefix sum of svr_count_rendered without the read-back or the synchronisation (no
+ * counterpart in the reference): for a step captured into a CUDA graph, which bins into a
+ * buffer of fixed capacity and never learns the record total on the host. */
+SVR_API int svr_scan_rendered(int64_t n_items, void* geom_buffer, void* stream);
+
 /* ---------------------------------------------------------------- binning
  * Replaces the duplicate/sort/range part of rasterize_voxels_procedure
  * (cuda/src/forward.cu:749-829, 882-939): emits (tile | order-rank, octant | voxel) pairs,
@@ -95,6 +100,15 @@ SVR_API size_t svr_image_buffer_bytes(int64_t total_pixels, int total_tiles);
 SVR_API int svr_bin_and_sort(const svr_view_t* views_host, int n_views, int N, int64_t num_rendered,
                      uint64_t path_or, const int64_t* octpaths, void* geom_buffer,
                      void* binning_buffer, size_t binning_bytes, void* image_buffer, void* stream);
+/* num_rendered above (and in the render calls) is the capacity of the binning buffer: the
+ * record total from svr_count_rendered, or any bound on it.  The device bins
+ * min(total, capacity) records (read back by svr_binning_count) and sets status bit 8 when
+ * records were dropped; path_or may be the OR over all voxel paths (a superset; status bit
+ * 16 flags a path with bits the trimmed key would drop).  svr_workspace_query returns the
+ * geom, binning and image buffer sizes {sizes[0], sizes[1], sizes[2]} for a capacity. */
+SVR_API int svr_binning_count(const void* binning_buffer, int64_t* count_host, void* stream);
+SVR_API int svr_workspace_query(int n_views, int N, int64_t capacity, int64_t total_pixels,
+                                int total_tiles, size_t* sizes_host);
 
 /* Sorted per-tile values (octant << 29 | voxel id) and tile ranges, for tests. */
 SVR_API int svr_unpack_binning(const void* binning_buffer, int64_t num_rendered, int total_tiles,
@@ -128,7 +142,8 @@ SVR_API int svr_render_bwd(const svr_view_t* views_host, int n_views, int N, int
                    float* dL_dvox, float* drgbs, float* dL_ds, void* stream);
 
 /* Device status word of the raster launches that used this image buffer (0 = clean;
- * bit 1 wait timeout, bit 2 index out of range, bit 4 duplicate count mismatch).
+ * bit 1 wait timeout, bit 2 index out of range, bit 4 duplicate count mismatch, bit 8
+ * records beyond the binning capacity, bit 16 sort-key format).
  * Synchronises `stream`.  Replaces the reference's __trap() sanity checks
  * (preprocess.cu:141-146, forward.cu:796-801, backward.cu:126-137). */
 SVR_API int svr_read_status(const void* image_buffer, int64_t total_pixels, int total_tiles,
@@ -206,6 +221,23 @@ SVR_API int svr_eikonal_bw(int G, int A, const int32_t* active, const int32_t* g
                    float vox_size_inv, int seed, float* grid_grad, uint32_t* status,
                    void* stream);
 
+/* Graph-replayable forms (no counterpart in the reference): the jitter seed is
+ * seed_base + *step, read from a device counter (svr_counter_add) when the kernel runs. */
+SVR_API int svr_laplacian_bw_at_step(int G, int A, const int32_t* active, const int32_t* grid_keys,
+                                     const int32_t* grid2voxel, int grid_res, const uint8_t* grid_mask,
+                                     const int32_t* dense_index, const float* voxel_coords,
+                                     const float* voxel_sizes, int N, const int64_t* vox_key,
+                                     const float* grid_pts, int M, float weight, float vox_size_inv,
+                                     int seed_base, const int64_t* step, float* grid_grad,
+                                     uint32_t* status, void* stream);
+SVR_API int svr_eikonal_bw_at_step(int G, int A, const int32_t* active, const int32_t* grid_keys,
+                                   const int32_t* grid2voxel, int grid_res, const uint8_t* grid_mask,
+                                   const int32_t* dense_index, const float* voxel_coords,
+                                   const float* voxel_sizes, int N, const int64_t* vox_key,
+                                   const float* grid_pts, int M, float weight, float vox_size_inv,
+                                   int seed_base, const int64_t* step, float* grid_grad,
+                                   uint32_t* status, void* stream);
+
 /* Allocation-free variant of svr_laplacian_bw, for callers that cannot allocate device
  * memory (a host that reserves all device memory in a fixed arena at start-up and forbids
  * later cudaMalloc calls).  It has no counterpart in the reference.  The direct-mapped key
@@ -259,6 +291,20 @@ SVR_API int svr_mc_emit(int64_t n_vox, const int64_t* vox_key, const float* grid
 SVR_API int svr_adam_step(int64_t numel, int biased, int sparse, float* param, const float* grad,
                   float* exp_avg, float* exp_avg_sq, double step, double lr, double beta1,
                   double beta2, float eps, void* stream);
+
+/* Graph-replayable Adam (no counterpart in the reference): the step number is read from a
+ * device counter when the kernel runs and indexes a table of per-step coefficients
+ * {lr / (1 - beta1^t), 1 / sqrt(1 - beta2^t)} that svr_adam_coef_table fills on the host
+ * in double, exactly as svr_adam_step computes them.  A step outside [1, rows) sets bit 2
+ * of `status` and leaves the parameters unchanged.  svr_counter_add adds `delta` to a
+ * device int64 counter in stream order. */
+SVR_API int svr_adam_coef_table(int biased, double lr, double beta1, double beta2, int64_t rows,
+                                float* table_host);
+SVR_API int svr_adam_step_at(int64_t numel, int biased, int sparse, float* param, const float* grad,
+                             float* exp_avg, float* exp_avg_sq, const float* coef_table, int64_t rows,
+                             const int64_t* step, double beta1, double beta2, float eps,
+                             uint32_t* status, void* stream);
+SVR_API int svr_counter_add(int64_t* counter, int64_t delta, void* stream);
 
 #ifdef __cplusplus
 }

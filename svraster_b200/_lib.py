@@ -44,6 +44,9 @@ _SIGS = {
     "svr_preprocess": (_I, [_P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
     "svr_unpack_geom": (_I, [_P, _I64, _P, _P, _P, _P]),
     "svr_count_rendered": (_I, [_I64, _P, C.POINTER(C.c_int64), C.POINTER(C.c_uint64), _P]),
+    "svr_scan_rendered": (_I, [_I64, _P, _P]),
+    "svr_binning_count": (_I, [_P, C.POINTER(C.c_int64), _P]),
+    "svr_workspace_query": (_I, [_I, _I, _I64, _I64, _I, C.POINTER(C.c_size_t)]),
     "svr_binning_buffer_bytes": (_SZ, [_I64, _I]),
     "svr_image_buffer_bytes": (_SZ, [_I64, _I]),
     "svr_bin_and_sort": (_I, [_P, _I, _I, _I64, _U64, _P, _P, _P, _SZ, _P, _P]),
@@ -62,6 +65,10 @@ _SIGS = {
     "svr_valid_table_fill": (_I, [_I, _P, _P, _P, _F, _I, _P, _I64, _P, _P, _P, _P, _P]),
     "svr_grid_index_build": (_I, [_I, _P, _I, _P, _P, _P]),
     "svr_laplacian_bw": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P]),
+    "svr_laplacian_bw_at_step": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P,
+                                      _P]),
+    "svr_eikonal_bw_at_step": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P,
+                                    _P]),
     "svr_eikonal_bw": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P]),
     "svr_laplacian_bw_noalloc": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P]),
     "svr_tsdf_integrate": (_I, [_P, _P, _I, _I64, _P, _P, _I, _I, _P, _I, _I, _I, _P, _D, _D, _F, _I, _I, _I, _F,
@@ -70,6 +77,9 @@ _SIGS = {
     "svr_mc_count": (_I, [_I64, _P, _I64, _P, _F, _P, C.POINTER(C.c_int64), _P]),
     "svr_mc_emit": (_I, [_I64, _P, _P, _P, _F, _I64, _I, _P, _P, _P, C.POINTER(C.c_int64), _P]),
     "svr_adam_step": (_I, [_I64, _I, _I, _P, _P, _P, _P, _D, _D, _D, _D, _F, _P]),
+    "svr_adam_coef_table": (_I, [_I, _D, _D, _D, _I64, _P]),
+    "svr_adam_step_at": (_I, [_I64, _I, _I, _P, _P, _P, _P, _P, _I64, _P, _D, _D, _F, _P, _P]),
+    "svr_counter_add": (_I, [_P, _I64, _P]),
 }
 
 _lib = None

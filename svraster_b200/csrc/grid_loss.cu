@@ -304,8 +304,9 @@ __device__ __forceinline__ void scatter_samples(const SampleCtx& c, bool valid, 
 
 __global__ void __launch_bounds__(256) laplacian_kernel(SampleCtx c, int A, const int32_t* __restrict__ active,
                                                         const uint8_t* __restrict__ mask, float weight,
-                                                        float vox_size_inv, int seed, float* __restrict__ grad,
-                                                        unsigned* status)
+                                                        float vox_size_inv, int seed,
+                                                        const int64_t* __restrict__ seed_step,
+                                                        float* __restrict__ grad, unsigned* status)
 {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = tid < A;
@@ -327,7 +328,7 @@ __global__ void __launch_bounds__(256) laplacian_kernel(SampleCtx c, int A, cons
     int vid[7];
     float dd[7];
     if (valid) {
-        const float3 rv = rand_vec(tid, seed);
+        const float3 rv = rand_vec(tid, seed_step ? seed + (int)*seed_step : seed);
         const int dx[6] = {+1, -1, 0, 0, 0, 0}, dy[6] = {0, 0, +1, -1, 0, 0}, dz[6] = {0, 0, 0, 0, +1, -1};
         float nb[6], center;
         vid[0] = sample_cell(c, x, y, z, rv, w[0], center, status);
@@ -350,8 +351,9 @@ __global__ void __launch_bounds__(256) laplacian_kernel(SampleCtx c, int A, cons
 
 __global__ void __launch_bounds__(256) eikonal_kernel(SampleCtx c, int A, const int32_t* __restrict__ active,
                                                       const uint8_t* __restrict__ mask, float weight,
-                                                      float vox_size_inv, int seed, float* __restrict__ grad,
-                                                      unsigned* status)
+                                                      float vox_size_inv, int seed,
+                                                      const int64_t* __restrict__ seed_step,
+                                                      float* __restrict__ grad, unsigned* status)
 {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = tid < A;
@@ -373,7 +375,7 @@ __global__ void __launch_bounds__(256) eikonal_kernel(SampleCtx c, int A, const 
     int vid[6];
     float dd[6];
     if (valid) {
-        const float3 rv = rand_vec(tid, seed);
+        const float3 rv = rand_vec(tid, seed_step ? seed + (int)*seed_step : seed);
         const int dx[6] = {+1, -1, 0, 0, 0, 0}, dy[6] = {0, 0, +1, -1, 0, 0}, dz[6] = {0, 0, 0, 0, +1, -1};
         float s[6];
 #pragma unroll
@@ -393,15 +395,17 @@ __global__ void __launch_bounds__(256) eikonal_kernel(SampleCtx c, int A, const 
 static int grid_loss(bool lap, int G, int A, const int32_t* active, const int32_t* keys, const int32_t* g2v, int res,
                      const uint8_t* mask, const int32_t* dense, const float* coords, const float* vsizes, int N, const int64_t* vox_key,
                      const float* grid, int M, float weight, float vox_size_inv, int seed, float* grad,
-                     unsigned* status, void* stream)
+                     unsigned* status, void* stream, const int64_t* seed_step = nullptr)
 {
     if (A <= 0) return SVR_OK;
     if (!active || !keys || !g2v || !mask || !coords || !vsizes || !vox_key || !grid || !grad || !status)
         return svr_fail(SVR_ERR_ARG, "grid loss: null argument");
     SampleCtx c{G, N, M, res, dense, keys, g2v, coords, vsizes, vox_key, grid};
     cudaStream_t st = (cudaStream_t)stream;
-    if (lap) laplacian_kernel<<<(A + 255) / 256, 256, 0, st>>>(c, A, active, mask, weight, vox_size_inv, seed, grad, status);
-    else eikonal_kernel<<<(A + 255) / 256, 256, 0, st>>>(c, A, active, mask, weight, vox_size_inv, seed, grad, status);
+    if (lap) laplacian_kernel<<<(A + 255) / 256, 256, 0, st>>>(c, A, active, mask, weight, vox_size_inv, seed, seed_step,
+                                                                 grad, status);
+    else eikonal_kernel<<<(A + 255) / 256, 256, 0, st>>>(c, A, active, mask, weight, vox_size_inv, seed, seed_step, grad,
+                                                         status);
     svr_note_launch(1);
     CUDA_TRY(cudaGetLastError());
     return SVR_OK;
@@ -425,6 +429,36 @@ extern "C" int svr_eikonal_bw(int G, int A, const int32_t* active, const int32_t
 {
     return grid_loss(false, G, A, active, grid_keys, grid2voxel, grid_res, grid_mask, dense_index, voxel_coords, voxel_sizes, N,
                      vox_key, grid_pts, M, weight, vox_size_inv, seed, grid_grad, status, stream);
+}
+
+// Graph-replayable variants: the jitter seed is seed_base + *step (a device counter), so a
+// captured step draws fresh jitter on every replay like the per-call seed does.
+extern "C" int svr_laplacian_bw_at_step(int G, int A, const int32_t* active, const int32_t* grid_keys,
+                                        const int32_t* grid2voxel, int grid_res, const uint8_t* grid_mask,
+                                        const int32_t* dense_index, const float* voxel_coords,
+                                        const float* voxel_sizes, int N, const int64_t* vox_key,
+                                        const float* grid_pts, int M, float weight, float vox_size_inv,
+                                        int seed_base, const int64_t* step, float* grid_grad, uint32_t* status,
+                                        void* stream)
+{
+    if (!step) return svr_fail(SVR_ERR_ARG, "grid loss: null step counter");
+    return grid_loss(true, G, A, active, grid_keys, grid2voxel, grid_res, grid_mask, dense_index, voxel_coords,
+                     voxel_sizes, N, vox_key, grid_pts, M, weight, vox_size_inv, seed_base, grid_grad, status, stream,
+                     step);
+}
+
+extern "C" int svr_eikonal_bw_at_step(int G, int A, const int32_t* active, const int32_t* grid_keys,
+                                      const int32_t* grid2voxel, int grid_res, const uint8_t* grid_mask,
+                                      const int32_t* dense_index, const float* voxel_coords,
+                                      const float* voxel_sizes, int N, const int64_t* vox_key,
+                                      const float* grid_pts, int M, float weight, float vox_size_inv,
+                                      int seed_base, const int64_t* step, float* grid_grad, uint32_t* status,
+                                      void* stream)
+{
+    if (!step) return svr_fail(SVR_ERR_ARG, "grid loss: null step counter");
+    return grid_loss(false, G, A, active, grid_keys, grid2voxel, grid_res, grid_mask, dense_index, voxel_coords,
+                     voxel_sizes, N, vox_key, grid_pts, M, weight, vox_size_inv, seed_base, grid_grad, status, stream,
+                     step);
 }
 
 // ------------------------------------------------------------------ allocation-free variant

@@ -325,13 +325,38 @@ __device__ __forceinline__ void adam_one(float& p, float g, float& m, float& v, 
     p -= step_size * (m / denom);
 }
 
+// Coefficients of one update: from the launch arguments, or (graph replay) from row *step
+// of a host-computed table [rows][2] = {lr / bc1, 1 / sqrt(bc2)}.
+struct AdamCoef {
+    float step_size, rbc2;
+    const float* table;
+    const int64_t* step;
+    int64_t rows;
+    unsigned* status;
+};
+
+__device__ __forceinline__ bool adam_coef(const AdamCoef& c, float& step_size, float& rbc2) {
+    step_size = c.step_size; rbc2 = c.rbc2;
+    if (!c.table) return true;
+    const int64_t t = *c.step;
+    if (t < 0 || t >= c.rows) {
+        if (threadIdx.x == 0 && blockIdx.x == 0 && c.status) atomicOr(c.status, ERR_BAD_INDEX);
+        return false;
+    }
+    step_size = c.table[2 * t];
+    rbc2 = c.table[2 * t + 1];
+    return true;
+}
+
 template <bool SPARSE, bool BIASED>
 __global__ void adam_scalar_kernel(int64_t n, float* __restrict__ p, const float* __restrict__ g,
-                                   float* __restrict__ m, float* __restrict__ v, float step_size, float b1, float b2,
-                                   float rbc2, float eps)
+                                   float* __restrict__ m, float* __restrict__ v, AdamCoef co, float b1, float b2,
+                                   float eps)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    float step_size, rbc2;
+    if (!adam_coef(co, step_size, rbc2)) return;
     float P = p[i], Mv = m[i], Vv = v[i];
     adam_one<SPARSE, BIASED>(P, g[i], Mv, Vv, step_size, b1, b2, rbc2, eps);
     p[i] = P; m[i] = Mv; v[i] = Vv;
@@ -339,10 +364,13 @@ __global__ void adam_scalar_kernel(int64_t n, float* __restrict__ p, const float
 
 template <bool SPARSE, bool BIASED>
 __global__ void adam_kernel(int64_t n, float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
-                            float* __restrict__ v, float step_size, float b1, float b2, float rbc2, float eps)
+                            float* __restrict__ v, AdamCoef co, float b1, float b2, float eps)
 {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t i4 = t * 4;
+    if (i4 >= n) return;
+    float step_size, rbc2;
+    if (!adam_coef(co, step_size, rbc2)) return;
     if (i4 + 3 < n) {
         float4 P = reinterpret_cast<float4*>(p)[t];
         const float4 G = reinterpret_cast<const float4*>(g)[t];
@@ -364,40 +392,80 @@ __global__ void adam_kernel(int64_t n, float* __restrict__ p, const float* __res
     }
 }
 
-extern "C" int svr_adam_step(int64_t numel, int biased, int sparse, float* param, const float* grad, float* exp_avg,
-                             float* exp_avg_sq, double step, double lr, double beta1, double beta2, float eps,
-                             void* stream)
+static void adam_host_coefs(int biased, double step, double lr, double beta1, double beta2, float& step_size,
+                            float& rbc2)
+{
+    if (biased) { step_size = (float)lr; rbc2 = 1.f; return; }
+    const double bc1 = 1.0 - std::pow(beta1, step);
+    const double bc2 = 1.0 - std::pow(beta2, step);
+    step_size = (float)(lr / bc1);
+    rbc2 = (float)(1.0 / std::sqrt(bc2));
+}
+
+static int adam_launch(int64_t numel, int biased, int sparse, float* param, const float* grad, float* exp_avg,
+                       float* exp_avg_sq, const AdamCoef& co, double beta1, double beta2, float eps, void* stream)
 {
     if (numel <= 0) return SVR_OK;
     if (!param || !grad || !exp_avg || !exp_avg_sq) return svr_fail(SVR_ERR_ARG, "adam: null argument");
     const bool aligned = (((uintptr_t)param | (uintptr_t)grad | (uintptr_t)exp_avg | (uintptr_t)exp_avg_sq) & 15) == 0;
-    float step_size, rbc2;
-    if (biased) { step_size = (float)lr; rbc2 = 1.f; }
-    else {
-        const double bc1 = 1.0 - std::pow(beta1, step);
-        const double bc2 = 1.0 - std::pow(beta2, step);
-        step_size = (float)(lr / bc1);
-        rbc2 = (float)(1.0 / std::sqrt(bc2));
-    }
     cudaStream_t st = (cudaStream_t)stream;
     const unsigned g = nblk((numel + 3) / 4, 256);
     const float b1 = (float)beta1, b2 = (float)beta2;
     if (!aligned) {
         const unsigned gs = nblk(numel, 256);
-        if (biased && sparse) adam_scalar_kernel<true, true><<<gs, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
-        else if (biased) adam_scalar_kernel<false, true><<<gs, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
-        else if (sparse) adam_scalar_kernel<true, false><<<gs, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
-        else adam_scalar_kernel<false, false><<<gs, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
+        if (biased && sparse) adam_scalar_kernel<true, true><<<gs, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, co, b1, b2, eps);
+        else if (biased) adam_scalar_kernel<false, true><<<gs, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, co, b1, b2, eps);
+        else if (sparse) adam_scalar_kernel<true, false><<<gs, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, co, b1, b2, eps);
+        else adam_scalar_kernel<false, false><<<gs, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, co, b1, b2, eps);
         LAUNCHED();
         return SVR_OK;
     }
     if (biased) {
-        if (sparse) adam_kernel<true, true><<<g, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
-        else adam_kernel<false, true><<<g, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
+        if (sparse) adam_kernel<true, true><<<g, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, co, b1, b2, eps);
+        else adam_kernel<false, true><<<g, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, co, b1, b2, eps);
     } else {
-        if (sparse) adam_kernel<true, false><<<g, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
-        else adam_kernel<false, false><<<g, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, step_size, b1, b2, rbc2, eps);
+        if (sparse) adam_kernel<true, false><<<g, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, co, b1, b2, eps);
+        else adam_kernel<false, false><<<g, 256, 0, st>>>(numel, param, grad, exp_avg, exp_avg_sq, co, b1, b2, eps);
     }
+    LAUNCHED();
+    return SVR_OK;
+}
+
+extern "C" int svr_adam_step(int64_t numel, int biased, int sparse, float* param, const float* grad, float* exp_avg,
+                             float* exp_avg_sq, double step, double lr, double beta1, double beta2, float eps,
+                             void* stream)
+{
+    AdamCoef co{};
+    adam_host_coefs(biased, step, lr, beta1, beta2, co.step_size, co.rbc2);
+    return adam_launch(numel, biased, sparse, param, grad, exp_avg, exp_avg_sq, co, beta1, beta2, eps, stream);
+}
+
+extern "C" int svr_adam_coef_table(int biased, double lr, double beta1, double beta2, int64_t rows, float* table_host)
+{
+    if (rows <= 0 || !table_host) return svr_fail(SVR_ERR_ARG, "adam coefficient table");
+    table_host[0] = 0.f;   // row 0: no step has that number
+    table_host[1] = 1.f;
+    for (int64_t t = 1; t < rows; ++t)
+        adam_host_coefs(biased, (double)t, lr, beta1, beta2, table_host[2 * t], table_host[2 * t + 1]);
+    return SVR_OK;
+}
+
+extern "C" int svr_adam_step_at(int64_t numel, int biased, int sparse, float* param, const float* grad,
+                                float* exp_avg, float* exp_avg_sq, const float* coef_table, int64_t rows,
+                                const int64_t* step, double beta1, double beta2, float eps, uint32_t* status,
+                                void* stream)
+{
+    if (!coef_table || !step || rows <= 0) return svr_fail(SVR_ERR_ARG, "adam: null coefficient table or step");
+    AdamCoef co{0.f, 1.f, coef_table, step, rows, status};
+    return adam_launch(numel, biased, sparse, param, grad, exp_avg, exp_avg_sq, co, beta1, beta2, eps, stream);
+}
+
+__global__ void counter_add_kernel(int64_t* c, int64_t d) { *c += d; }
+
+extern "C" int svr_counter_add(int64_t* counter, int64_t delta, void* stream)
+{
+    if (!counter) return svr_fail(SVR_ERR_ARG, "counter: null");
+    counter_add_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(counter, delta);
     LAUNCHED();
     return SVR_OK;
 }

@@ -11,6 +11,7 @@
 //    and the adjoint accumulates per-record gradients in shared memory so each record
 //    reaches global memory with one vector atomic per CTA instead of one per pixel.
 #include <atomic>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -74,9 +75,10 @@ static GeomLayout geom_layout(int64_t M) {
 
 // binning buffer: meta | keys_in | keys_out | vals_in | vals_out | sort tmp | records
 struct BinMeta {
-    int rank_bits;   // rank bits kept in the sort key (tile id sits above them)
-    int key64;       // 1 when keys are 64-bit
-    int pad[62];
+    int rank_bits;     // rank bits kept in the sort key (tile id sits above them)
+    int key64;         // 1 when keys are 64-bit
+    long long count;   // records binned: min(total from preprocess, capacity)
+    int pad[60];
 };
 static_assert(sizeof(BinMeta) == 256, "bin meta block");
 struct BinLayout {
@@ -269,8 +271,7 @@ extern "C" int svr_unpack_geom(const void* geom_buffer, int64_t M, uint32_t* ndu
     return SVR_OK;
 }
 
-extern "C" int svr_count_rendered(int64_t M, void* geom_buffer, int64_t* num_rendered_host,
-                                  uint64_t* path_or_host, void* stream)
+extern "C" int svr_scan_rendered(int64_t M, void* geom_buffer, void* stream)
 {
     cudaStream_t st = (cudaStream_t)stream;
     char* g = (char*)geom_buffer;
@@ -280,6 +281,16 @@ extern "C" int svr_count_rendered(int64_t M, void* geom_buffer, int64_t* num_ren
         CUDA_TRY(cub::DeviceScan::InclusiveSum(g + L.tmp, tb, (const uint32_t*)(g + L.ndup),
                                                (uint32_t*)(g + L.scan), (int)M, st));
     }
+    return SVR_OK;
+}
+
+extern "C" int svr_count_rendered(int64_t M, void* geom_buffer, int64_t* num_rendered_host,
+                                  uint64_t* path_or_host, void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    char* g = (char*)geom_buffer;
+    int rc = svr_scan_rendered(M, geom_buffer, stream);
+    if (rc) return rc;
     GeomMeta meta;
     CUDA_TRY(cudaMemcpyAsync(&meta, g, 16, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
@@ -320,15 +331,25 @@ __device__ __forceinline__ uint64_t rep3(uint32_t q) {
 
 // forward.cu:749-802: emit one (key, value) per (octant, tile) of every rendered voxel,
 // in voxel-major, octant, row, column order (the order the stable sort preserves on ties).
+// Records past the capacity `cap` of the binning buffer are dropped and flagged
+// (ERR_CAPACITY); the record count read by the later stages is min(total, cap), taken
+// from the device, so the host need not know the total (graph capture).
 template <typename KeyT>
 __global__ void __launch_bounds__(256) duplicate_kernel(
     const __grid_constant__ Views V, int N, const int64_t* __restrict__ octpaths,
     const uint32_t* __restrict__ ndup, const uint32_t* __restrict__ scan, const uint2* __restrict__ bboxes,
     const uint32_t* __restrict__ bitsets, KeyT* __restrict__ keys, uint32_t* __restrict__ vals,
-    int rank_shift, int rank_bits, BinMeta* __restrict__ meta, unsigned* status)
+    int rank_shift, int rank_bits, const GeomMeta* __restrict__ gmeta, int64_t cap, BinMeta* __restrict__ meta,
+    unsigned* status)
 {
     const int64_t item = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (item == 0) { meta->rank_bits = rank_bits; meta->key64 = sizeof(KeyT) == 8; }
+    if (item == 0) {
+        const unsigned long long total = gmeta->total;
+        meta->rank_bits = rank_bits;
+        meta->key64 = sizeof(KeyT) == 8;
+        meta->count = total < (unsigned long long)cap ? (long long)total : (long long)cap;
+        if (total > (unsigned long long)cap) atomicOr(status, ERR_CAPACITY);
+    }
     const int64_t M = (int64_t)N * V.n;
     if (item >= M) return;
     const uint32_t cnt = ndup[item];
@@ -345,6 +366,7 @@ __global__ void __launch_bounds__(256) duplicate_kernel(
     const int tx1 = max(0, min(gx - 1, (int)((bb.y >> 16) / TILE)));
     const int ty1 = max(0, min(gy - 1, (int)((bb.y << 16 >> 16) / TILE)));
     const uint64_t path = (uint64_t)octpaths[i];
+    if (rank_shift > 0 && (path & ((1ull << rank_shift) - 1ull))) atomicOr(status, ERR_KEY_FORMAT);
     const uint32_t qb = bitsets[item];
     for (uint32_t q = 0; q < 8; ++q) {
         if (!(qb & (1u << q))) continue;
@@ -352,6 +374,7 @@ __global__ void __launch_bounds__(256) duplicate_kernel(
         for (int y = ty0; y <= ty1; ++y)
             for (int x = tx0; x <= tx1; ++x) {
                 if (off >= end) { atomicOr(status, ERR_COUNT_MISMATCH); return; }
+                if ((int64_t)off >= cap) return;   // flagged above
                 const uint64_t tile = (uint64_t)(view.tile_offset + y * gx + x);
                 keys[off] = (KeyT)((tile << rank_bits) | rank);
                 vals[off] = (q << 29) | (uint32_t)i;
@@ -361,12 +384,27 @@ __global__ void __launch_bounds__(256) duplicate_kernel(
     if (off != end) atomicOr(status, ERR_COUNT_MISMATCH);
 }
 
+// Slots [count, cap) of the key array get the largest key of the format, so the stable
+// sort leaves them after every real record.
+template <typename KeyT>
+__global__ void pad_keys_kernel(const BinMeta* __restrict__ meta, int64_t cap, KeyT sentinel,
+                                KeyT* __restrict__ keys, uint32_t* __restrict__ vals)
+{
+    const int64_t count = meta->count;
+    for (int64_t k = count + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < cap;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        keys[k] = sentinel;
+        vals[k] = 0u;
+    }
+}
+
 // forward.cu:807-829
 template <typename KeyT>
-__global__ void tile_ranges_kernel(int64_t R, const KeyT* __restrict__ keys, int rank_bits, int T,
-                                   uint2* __restrict__ ranges, unsigned* status)
+__global__ void tile_ranges_kernel(const BinMeta* __restrict__ meta, const KeyT* __restrict__ keys, int rank_bits,
+                                   int T, uint2* __restrict__ ranges, unsigned* status)
 {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t R = meta->count;
     if (k >= R) return;
     const uint32_t t = (uint32_t)((uint64_t)keys[k] >> rank_bits);
     if (t >= (uint32_t)T) { atomicOr(status, ERR_BAD_INDEX); return; }
@@ -376,6 +414,56 @@ __global__ void tile_ranges_kernel(int64_t R, const KeyT* __restrict__ keys, int
         if (p != t) { ranges[p].y = (uint32_t)k; ranges[t].x = (uint32_t)k; }
     }
     if (k == R - 1) ranges[t].y = (uint32_t)R;
+}
+
+template <typename KeyT>
+static int bin_sort_typed(const Views& V, int N, int64_t R, const KeyFmt& kf, int T, const int64_t* octpaths,
+                          char* g, const GeomLayout& GL, char* b, const BinLayout& BL, char* im, const ImgLayout& IL,
+                          unsigned* status, cudaStream_t st)
+{
+    const int64_t M = (int64_t)N * V.n;
+    const int nb = (int)((M + 255) / 256);
+    const int rb = (int)((R + 255) / 256);
+    BinMeta* meta = (BinMeta*)b;
+    KeyT* keys_in = (KeyT*)(b + BL.keys_in);
+    uint32_t* vals_in = (uint32_t*)(b + BL.vals_in);
+    duplicate_kernel<KeyT><<<nb, 256, 0, st>>>(V, N, octpaths, (const uint32_t*)(g + GL.ndup),
+        (const uint32_t*)(g + GL.scan), (const uint2*)(g + GL.bbox), (const uint32_t*)(g + GL.bits),
+        keys_in, vals_in, kf.rank_shift, kf.rank_bits, (const GeomMeta*)g, R, meta, status);
+    LAUNCH_CHECK();
+    const KeyT sentinel = kf.key_bits >= (int)(8 * sizeof(KeyT)) ? (KeyT)~(KeyT)0
+                                                                    : (KeyT)((((KeyT)1) << kf.key_bits) - 1);
+    pad_keys_kernel<KeyT><<<2 * 148, 256, 0, st>>>(meta, R, sentinel, keys_in, vals_in);
+    LAUNCH_CHECK();
+    size_t tb = BL.tmp_bytes;
+    CUDA_TRY(cub::DeviceRadixSort::SortPairs(b + BL.tmp, tb, (const KeyT*)keys_in, (KeyT*)(b + BL.keys_out),
+                                             (const uint32_t*)vals_in, (uint32_t*)(b + BL.vals_out), (int)R, 0,
+                                             kf.key_bits, st));
+    tile_ranges_kernel<KeyT><<<rb, 256, 0, st>>>(meta, (const KeyT*)(b + BL.keys_out), kf.rank_bits, T,
+                                                 (uint2*)(im + IL.ranges), status);
+    LAUNCH_CHECK();
+    return SVR_OK;
+}
+
+extern "C" int svr_binning_count(const void* binning_buffer, int64_t* count_host, void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    long long c = 0;
+    CUDA_TRY(cudaMemcpyAsync(&c, (const char*)binning_buffer + offsetof(BinMeta, count), 8, cudaMemcpyDeviceToHost,
+                             st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    *count_host = c;
+    return SVR_OK;
+}
+
+extern "C" int svr_workspace_query(int n_views, int N, int64_t capacity, int64_t total_pixels, int total_tiles,
+                                   size_t* sizes_host)
+{
+    if (!sizes_host || n_views <= 0 || N < 0 || capacity < 0) return svr_fail(SVR_ERR_ARG, "workspace query");
+    sizes_host[0] = geom_layout((int64_t)N * n_views).total;
+    sizes_host[1] = bin_layout(capacity).total;
+    sizes_host[2] = img_layout(total_pixels, total_tiles).total;
+    return SVR_OK;
 }
 
 extern "C" int svr_bin_and_sort(const svr_view_t* views_host, int n_views, int N, int64_t R, uint64_t path_or,
@@ -400,35 +488,10 @@ extern "C" int svr_bin_and_sort(const svr_view_t* views_host, int n_views, int N
     CUDA_TRY(cudaMemsetAsync(status, 0, 4, st));
     if (R == 0) return SVR_OK;
     const KeyFmt kf = key_format(path_or, T);
-    const int nb = (int)((M + 255) / 256);
-    const int rb = (int)((R + 255) / 256);
-    if (kf.key_bits <= 32) {
-        duplicate_kernel<uint32_t><<<nb, 256, 0, st>>>(V, N, octpaths, (const uint32_t*)(g + GL.ndup),
-            (const uint32_t*)(g + GL.scan), (const uint2*)(g + GL.bbox), (const uint32_t*)(g + GL.bits),
-            (uint32_t*)(b + BL.keys_in), (uint32_t*)(b + BL.vals_in), kf.rank_shift, kf.rank_bits, (BinMeta*)b, status);
-        LAUNCH_CHECK();
-        size_t tb = BL.tmp_bytes;
-        CUDA_TRY(cub::DeviceRadixSort::SortPairs(b + BL.tmp, tb, (const uint32_t*)(b + BL.keys_in),
-                                                 (uint32_t*)(b + BL.keys_out), (const uint32_t*)(b + BL.vals_in),
-                                                 (uint32_t*)(b + BL.vals_out), (int)R, 0, kf.key_bits, st));
-        tile_ranges_kernel<uint32_t><<<rb, 256, 0, st>>>(R, (const uint32_t*)(b + BL.keys_out), kf.rank_bits, T,
-                                                          (uint2*)(im + IL.ranges), status);
-        LAUNCH_CHECK();
-    } else {
-        if (kf.key_bits > 64) return svr_fail(SVR_ERR_UNSUPPORTED, "sort key wider than 64 bits");
-        duplicate_kernel<uint64_t><<<nb, 256, 0, st>>>(V, N, octpaths, (const uint32_t*)(g + GL.ndup),
-            (const uint32_t*)(g + GL.scan), (const uint2*)(g + GL.bbox), (const uint32_t*)(g + GL.bits),
-            (uint64_t*)(b + BL.keys_in), (uint32_t*)(b + BL.vals_in), kf.rank_shift, kf.rank_bits, (BinMeta*)b, status);
-        LAUNCH_CHECK();
-        size_t tb = BL.tmp_bytes;
-        CUDA_TRY(cub::DeviceRadixSort::SortPairs(b + BL.tmp, tb, (const uint64_t*)(b + BL.keys_in),
-                                                 (uint64_t*)(b + BL.keys_out), (const uint32_t*)(b + BL.vals_in),
-                                                 (uint32_t*)(b + BL.vals_out), (int)R, 0, kf.key_bits, st));
-        tile_ranges_kernel<uint64_t><<<rb, 256, 0, st>>>(R, (const uint64_t*)(b + BL.keys_out), kf.rank_bits, T,
-                                                          (uint2*)(im + IL.ranges), status);
-        LAUNCH_CHECK();
-    }
-    return SVR_OK;
+    if (kf.key_bits > 64) return svr_fail(SVR_ERR_UNSUPPORTED, "sort key wider than 64 bits");
+    if (kf.key_bits <= 32)
+        return bin_sort_typed<uint32_t>(V, N, R, kf, T, octpaths, g, GL, b, BL, im, IL, status, st);
+    return bin_sort_typed<uint64_t>(V, N, R, kf, T, octpaths, g, GL, b, BL, im, IL, status, st);
 }
 
 extern "C" int svr_unpack_binning(const void* binning_buffer, int64_t R, int T, const void* image_buffer,
@@ -457,7 +520,7 @@ __global__ void __launch_bounds__(256) pack_records_kernel(
     const float* __restrict__ rgbs, int rgb_per_view, Rec* __restrict__ recs, unsigned* status)
 {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= R) return;
+    if (k >= R || k >= meta->count) return;
     const int rank_bits = meta->rank_bits;
     const uint64_t key = meta->key64 ? ((const uint64_t*)keys)[k] : (uint64_t)((const uint32_t*)keys)[k];
     const int vi = V.n == 1 ? 0 : view_of_tile(V, (int)(key >> rank_bits));
@@ -486,6 +549,20 @@ __global__ void __launch_bounds__(256) pack_records_kernel(
 // ------------------------------------------------------------------ render kernels
 #include "render_kernels.cuh"
 
+// Raise a kernel's dynamic shared-memory limit once per device (kept out of the launch
+// path so that launches can be captured into a graph without extra API calls).
+template <typename K>
+static int ensure_smem(K k, int smem, std::atomic<unsigned long long>& done)
+{
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return SVR_OK;
+    CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    done.fetch_or(bit, std::memory_order_acq_rel);
+    return SVR_OK;
+}
+
 template <int NS, bool DEPTH, bool NORMAL, bool MAXW>
 static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint2* ranges, const Rec* recs,
                       const float* s_val, uint32_t* tile_last, uint32_t* n_contrib, float* color, float* depth,
@@ -493,7 +570,9 @@ static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint2* range
 {
     auto k = render_fwd_kernel<NS, DEPTH, NORMAL, MAXW>;
     const int smem = (int)sizeof(FwdSmem);
-    CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    static std::atomic<unsigned long long> done{0};
+    int rc = ensure_smem(k, smem, done);
+    if (rc) return rc;
     k<<<T, BLOCK, smem, st>>>(V, ranges, recs, s_val, tile_last, n_contrib, color, depth, normal, outT, max_w, status);
     LAUNCH_CHECK();
     return SVR_OK;
@@ -559,7 +638,9 @@ static int launch_bwd(int T, int N, cudaStream_t st, const Views& V, const uint2
 {
     auto k = render_bwd_kernel<DEPTH, NORMAL, RCONC>;
     const int smem = (int)sizeof(BwdSmem);
-    CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    static std::atomic<unsigned long long> done{0};
+    int rc = ensure_smem(k, smem, done);
+    if (rc) return rc;
     k<<<T, BLOCK, smem, st>>>(V, N, ranges, tl, nc, recs, s_val, out_T, dc, dd, dn, dT, lam, gt, dvox, drgbs, ds,
                                status);
     LAUNCH_CHECK();

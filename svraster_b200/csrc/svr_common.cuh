@@ -23,6 +23,8 @@ constexpr float EARLY_STOP_T = 0.0001f;    // config.h:20
 constexpr unsigned ERR_WAIT_TIMEOUT = 1u;
 constexpr unsigned ERR_BAD_INDEX = 2u;
 constexpr unsigned ERR_COUNT_MISMATCH = 4u;
+constexpr unsigned ERR_CAPACITY = 8u;      // more records than the binning buffer holds
+constexpr unsigned ERR_KEY_FORMAT = 16u;   // a rendered path has bits the trimmed key drops
 
 struct Views {
     int n;

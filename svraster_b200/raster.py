@@ -50,13 +50,24 @@ class RasterState:
         return n_dup
 
     # -------------------------------------------------------------- binning
-    def bin(self, octpaths):
+    def bin(self, octpaths, capacity=None, path_or=None):
+        """Duplicate, sort and range the records.  By default the record total is read back
+        (one host synchronisation, as the reference does).  With ``capacity`` (and ``path_or``,
+        the OR of every voxel's octree path) nothing is read back: the buffers hold
+        ``capacity`` records and the device bins min(total, capacity) of them (status bit 8
+        if any were dropped), which lets the call be captured into a CUDA graph."""
         L = _lib.load()
         M = self.N * self.n_views
-        R, por = C.c_int64(0), C.c_uint64(0)
-        check(L.svr_count_rendered(M, ptr(self.geom), C.byref(R), C.byref(por), stream_ptr(self.device)),
-              "svr_count_rendered")
-        self.num_rendered, self.path_or = int(R.value), int(por.value)
+        if capacity is None:
+            R, por = C.c_int64(0), C.c_uint64(0)
+            check(L.svr_count_rendered(M, ptr(self.geom), C.byref(R), C.byref(por), stream_ptr(self.device)),
+                  "svr_count_rendered")
+            self.num_rendered, self.path_or = int(R.value), int(por.value)
+        else:
+            if path_or is None:
+                raise ValueError("bin(capacity=...) needs path_or")
+            check(L.svr_scan_rendered(M, ptr(self.geom), stream_ptr(self.device)), "svr_scan_rendered")
+            self.num_rendered, self.path_or = int(capacity), int(path_or)
         nb = L.svr_binning_buffer_bytes(self.num_rendered, self.total_tiles)
         self.binning = _empty_bytes(nb, self.device)
         self.image = _empty_bytes(L.svr_image_buffer_bytes(self.total_pix, self.total_tiles), self.device)
@@ -96,6 +107,13 @@ class RasterState:
                                ptr(dnormal), ptr(dT), ptr(dvox), ptr(drgbs), ptr(ds), stream_ptr(dev)),
               "svr_render_bwd")
         return dvox, ds
+
+    def binned_count(self):
+        """Records actually binned (min(total, capacity)); synchronises."""
+        n = C.c_int64(0)
+        check(_lib.load().svr_binning_count(ptr(self.binning), C.byref(n), stream_ptr(self.device)),
+              "svr_binning_count")
+        return int(n.value)
 
     # -------------------------------------------------------------- introspection (tests)
     def status(self):

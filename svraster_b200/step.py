@@ -11,6 +11,8 @@ normal-consistency losses, which run upstream of the rasterizer and are out of s
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 import torch
 
@@ -87,12 +89,30 @@ class BatchedTrainStep:
         self.all_idx = torch.arange(self.N, dtype=torch.int64, device=dev)
         self.state = None
         self.ev = None
+        # graph replay state: OR of every leaf's octree path (a superset of the rendered
+        # paths, so the trimmed sort key stays exact for any camera), device step counter,
+        # per-group Adam coefficient tables
+        leaf_paths = np.asarray(scene.octpath, dtype=np.int64)[np.asarray(scene.is_leaf).astype(bool).reshape(-1)]
+        self.path_or_all = int(np.bitwise_or.reduce(leaf_paths.view(np.uint64))) if leaf_paths.size else 0
+        self.graph = None
+        self.graph_out = None
+        self.capacity = None
+        self.step_dev = None
+        self.coef_tables = None
+        self.coef_rows = 0
+        self._dev_step_synced = False
 
     # ------------------------------------------------------------------ one step
     def step(self, time_render=False, grad_hook=None):
         """One training step.  ``grad_hook(grads)`` runs between the adjoints and Adam (the
         data-parallel all-reduce of the gradients goes there).  With ``time_render`` every
         stage is bracketed by CUDA events on the launching stream (see ``stage_ms``)."""
+        out = self._body(False, time_render, grad_hook)
+        self.adam_step += 1
+        self._dev_step_synced = False
+        return out
+
+    def _body(self, graph, time_render=False, grad_hook=None):
         L = _lib.load()
         st = stream_ptr(self.dev)
         N = self.N
@@ -113,7 +133,10 @@ class BatchedTrainStep:
         state = RasterState(self.views, N, self.dev)
         state.preprocess(self.octpath, self.centers, self.lengths, self.is_leaf)
         mark("preprocess")
-        state.bin(self.octpath)
+        if graph:
+            state.bin(self.octpath, capacity=self.capacity, path_or=self.path_or_all)
+        else:
+            state.bin(self.octpath)
         mark("count+sort")
         color, depth, normal, T, _ = state.render(3, True, True, self.centers, self.lengths, self.geos, self.rgbs,
                                                   self.s_val, rgb_per_view=True)
@@ -133,24 +156,90 @@ class BatchedTrainStep:
                                      ptr(self.drgbs), ptr(self.grads[1]), ptr(self.grads[2]), st), "sh views bw")
         mark("scatter+sh_bw")
         G, A = self.grid_keys.numel(), self.active.numel()
-        for fn, lam in ((L.svr_laplacian_bw, self.lambda_ls), (L.svr_eikonal_bw, self.lambda_ge)):
-            check(fn(G, A, ptr(self.active), ptr(self.grid_keys), ptr(self.grid2voxel), 1 << self.res_pow2,
-                     ptr(self.grid_mask), ptr(self.grid_index), ptr(self.grid_voxel_coord),
-                     ptr(self.grid_voxel_size), N,
-                     ptr(self.vox_key), ptr(self.grid), self.grid.numel(), float(lam), self.vox_size_min_inv,
-                     self.seed + self.adam_step, ptr(self.grads[0]), ptr(self.status), st), "grid loss")
+        common = lambda: (G, A, ptr(self.active), ptr(self.grid_keys), ptr(self.grid2voxel), 1 << self.res_pow2,
+                          ptr(self.grid_mask), ptr(self.grid_index), ptr(self.grid_voxel_coord),
+                          ptr(self.grid_voxel_size), N, ptr(self.vox_key), ptr(self.grid), self.grid.numel())
+        if graph:
+            for fn, lam in ((L.svr_laplacian_bw_at_step, self.lambda_ls), (L.svr_eikonal_bw_at_step, self.lambda_ge)):
+                check(fn(*common(), float(lam), self.vox_size_min_inv, self.seed, ptr(self.step_dev),
+                         ptr(self.grads[0]), ptr(self.status), st), "grid loss")
+        else:
+            for fn, lam in ((L.svr_laplacian_bw, self.lambda_ls), (L.svr_eikonal_bw, self.lambda_ge)):
+                check(fn(*common(), float(lam), self.vox_size_min_inv, self.seed + self.adam_step,
+                         ptr(self.grads[0]), ptr(self.status), st), "grid loss")
         mark("smoothness")
         if grad_hook is not None:
             grad_hook(self.grads)
             mark("allreduce")
-        self.adam_step += 1
-        for p, g, m, v, lr in zip(self.params, self.grads, self.adam_m, self.adam_v, self.lr):
-            check(L.svr_adam_step(p.numel(), 0, 0, ptr(p), ptr(g), ptr(m), ptr(v), float(self.adam_step), float(lr),
-                                  self.betas[0], self.betas[1], self.eps, st), "adam")
+        if graph:
+            check(L.svr_counter_add(ptr(self.step_dev), 1, st), "counter")
+            for p, g, m, v, tab in zip(self.params, self.grads, self.adam_m, self.adam_v, self.coef_tables):
+                check(L.svr_adam_step_at(p.numel(), 0, 0, ptr(p), ptr(g), ptr(m), ptr(v), ptr(tab), self.coef_rows,
+                                         ptr(self.step_dev), self.betas[0], self.betas[1], self.eps,
+                                         ptr(self.status), st), "adam")
+        else:
+            for p, g, m, v, lr in zip(self.params, self.grads, self.adam_m, self.adam_v, self.lr):
+                check(L.svr_adam_step(p.numel(), 0, 0, ptr(p), ptr(g), ptr(m), ptr(v), float(self.adam_step + 1),
+                                      float(lr), self.betas[0], self.betas[1], self.eps, st), "adam")
         mark("adam")
         self.state = state
         self.ev = marks if time_render else None
         return color, T
+
+    # ------------------------------------------------------------------ CUDA graph
+    def capture(self, capacity=None, rows=1 << 20):
+        """Capture one whole step (gather, SH, preprocess, scan, duplicate, sort, pack, render
+        forward and adjoint, scatter, SH adjoint, smoothness adjoints, Adam) into a CUDA graph.
+        ``capacity`` bounds the records per step (default: this batch's record total, found by
+        one counting pass); a replay that needs more sets status bit 8 (``graph_status``).
+        Returns the number of this library's kernels in the graph."""
+        L = _lib.load()
+        if capacity is None:
+            probe = RasterState(self.views, self.N, self.dev)
+            probe.preprocess(self.octpath, self.centers, self.lengths, self.is_leaf)
+            R, por = C.c_int64(0), C.c_uint64(0)
+            check(L.svr_count_rendered(self.N * self.V, ptr(probe.geom), C.byref(R), C.byref(por),
+                                       stream_ptr(self.dev)), "count")
+            capacity = int(R.value)
+            del probe
+        self.capacity = max(int(capacity), 1)
+        self.coef_rows = int(rows)
+        self.coef_tables = []
+        for lr in self.lr:
+            tab = np.empty((self.coef_rows, 2), np.float32)
+            check(L.svr_adam_coef_table(0, float(lr), self.betas[0], self.betas[1], self.coef_rows,
+                                        tab.ctypes.data_as(C.c_void_p)), "adam table")
+            self.coef_tables.append(torch.from_numpy(tab).to(self.dev))
+        self.step_dev = torch.full((1,), self.adam_step, dtype=torch.int64, device=self.dev)
+        torch.cuda.synchronize(self.dev)
+        self.graph = torch.cuda.CUDAGraph()
+        n0 = L.svr_kernel_launches()
+        # the step counter and parameters must not move during capture: capture runs no work
+        with torch.cuda.graph(self.graph):
+            self.graph_out = self._body(True)
+        self.graph_launches = int(L.svr_kernel_launches() - n0)
+        torch.cuda.synchronize(self.dev)
+        self._dev_step_synced = True
+        return self.graph_launches
+
+    def replay(self):
+        """One step by graph replay (capture first).  Returns (color, T) of the replayed step;
+        their storage is reused by the next replay."""
+        if self.graph is None:
+            raise RuntimeError("capture() first")
+        if self.adam_step + 1 >= self.coef_rows:
+            raise RuntimeError("Adam coefficient table exhausted; capture again with more rows")
+        if not self._dev_step_synced:
+            self.step_dev.fill_(self.adam_step)
+            self._dev_step_synced = True
+        self.graph.replay()
+        self.adam_step += 1
+        return self.graph_out
+
+    def graph_status(self):
+        """Status words after replays: (raster status, smoothness / Adam status)."""
+        torch.cuda.synchronize(self.dev)
+        return self.state.status(), int(self.status.item())
 
     @staticmethod
     def stage_ms(marks):
