@@ -238,6 +238,22 @@ SVR_API int svr_eikonal_bw_at_step(int G, int A, const int32_t* active, const in
                                    int seed_base, const int64_t* step, float* grid_grad,
                                    uint32_t* status, void* stream);
 
+/* Fused Laplacian + grid-Eikonal adjoint accumulated per voxel corner (no counterpart in
+ * the reference; equal, up to the order of floating-point additions, to svr_laplacian_bw
+ * with weight w_ls plus svr_eikonal_bw with weight w_ge, both with `seed`, followed by the
+ * grid scatter of dvox): adds each sample's corner gradients to dvox[v*ld + 0..7] of its
+ * owner voxel v, for svr_scatter_vox_grads to move to the grid points.  geos f32[N,8]
+ * (16-byte aligned) must hold grid[vox_key] of the current grid (svr_gather_geo);
+ * dense_index is required; active may be NULL for all G table rows in order (A <= G);
+ * seed_step may be NULL, else the seed is seed + *seed_step read on the device.  A zero
+ * weight skips that loss. */
+SVR_API int svr_smoothness_bw_vox(int G, int A, const int32_t* active, const int32_t* grid_keys,
+                                  const int32_t* grid2voxel, int grid_res, const uint8_t* grid_mask,
+                                  const int32_t* dense_index, const float* voxel_coords,
+                                  const float* voxel_sizes, int N, const float* geos, float w_ls,
+                                  float w_ge, float vox_size_inv, int seed, const int64_t* seed_step,
+                                  float* dvox, int ld, uint32_t* status, void* stream);
+
 /* Allocation-free variant of svr_laplacian_bw, for callers that cannot allocate device
  * memory (a host that reserves all device memory in a fixed arena at start-up and forbids
  * later cudaMalloc calls).  It has no counterpart in the reference.  The direct-mapped key

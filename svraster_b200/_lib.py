@@ -67,6 +67,8 @@ _SIGS = {
     "svr_laplacian_bw": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P]),
     "svr_laplacian_bw_at_step": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P,
                                       _P]),
+    "svr_smoothness_bw_vox": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P, _I, _P, _F, _F, _F, _I, _P, _P, _I, _P,
+                                   _P]),
     "svr_eikonal_bw_at_step": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P,
                                     _P]),
     "svr_eikonal_bw": (_I, [_I, _I, _P, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _I, _F, _F, _I, _P, _P, _P]),

@@ -461,6 +461,220 @@ extern "C" int svr_eikonal_bw_at_step(int G, int A, const int32_t* active, const
                      step);
 }
 
+// ------------------------------------------------------------------ fused per-voxel form
+// Laplacian and grid-Eikonal adjoints in one pass, accumulated per voxel corner.  With one
+// seed both losses sample the same six neighbour cells at the same jittered offset, so each
+// neighbour is sampled once and its two gradient terms are added before the scatter.  The
+// corner SDF values come from geos[v] (= grid[vox_key[v]], the gather at the start of the
+// step) and the corner gradients accumulate into dvox[v, 0:8] with vector atomics; the
+// per-voxel gradient scatter (svr_scatter_vox_grads) then moves them to the grid points with
+// the render adjoint's.  Sample values and per-sample gradient terms are computed exactly
+// as in laplacian_kernel / eikonal_kernel; only the summation order of the atomics differs.
+struct VoxCtx {
+    int G, N, res;
+    const int32_t* dense;
+    const int32_t* keys;
+    const int32_t* g2v;
+    const float* coords;
+    const float* vsizes;
+    const float4* geos;   // [N][2] float4 = 8 corner values
+};
+
+// Owner voxel of table row `id` and the sample at cell (x,y,z) + rv: returns the SDF value,
+// writes the owner (-1 if absent) and the local coordinate q used for the weights.
+__device__ __forceinline__ float sample_vox(const VoxCtx& c, int id, int x, int y, int z, float3 rv, int& v,
+                                            float3& q, unsigned* status) {
+    v = -1;
+    q = f3(0.f, 0.f, 0.f);
+    if (id < 0) return 0.f;
+    const int vv = c.g2v[id];
+    if (vv < 0 || vv >= c.N) { atomicOr(status, ERR_BAD_INDEX); return 0.f; }
+    const float3 pt = f3(x + rv.x, y + rv.y, z + rv.z);
+    const float3 base = f3(c.coords[3 * vv], c.coords[3 * vv + 1], c.coords[3 * vv + 2]);
+    const float size = c.vsizes[vv];
+    q = (pt - base) / size;
+    const float4 g0 = c.geos[2 * (size_t)vv], g1 = c.geos[2 * (size_t)vv + 1];
+    const float g[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
+    float w[8];
+    tri_weights(q, w);
+    float s = 0.f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        if (w[i] < 0) w[i] = 0;
+        if (w[i] > 1) w[i] = 1;
+        s += g[i] * w[i];
+    }
+    v = vv;
+    return s;
+}
+
+__device__ __forceinline__ void clamped_weights(float3 q, float w[8]) {
+    tri_weights(q, w);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        if (w[i] < 0) w[i] = 0;
+        if (w[i] > 1) w[i] = 1;
+    }
+}
+
+__device__ __forceinline__ void add8(float* dvox, int ld, bool vec4, int v, const float* a) {
+    float* row = dvox + (size_t)v * ld;
+    if (vec4) {
+        atomicAdd(reinterpret_cast<float4*>(row), make_float4(a[0], a[1], a[2], a[3]));
+        atomicAdd(reinterpret_cast<float4*>(row + 4), make_float4(a[4], a[5], a[6], a[7]));
+    } else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) atomicAdd(row + i, a[i]);
+    }
+}
+
+template <bool LS, bool GE>
+__global__ void __launch_bounds__(256) smooth_vox_kernel(VoxCtx c, int A, const int32_t* __restrict__ active,
+                                                         const uint8_t* __restrict__ mask, float w_ls, float w_ge,
+                                                         float vox_size_inv, int seed,
+                                                         const int64_t* __restrict__ seed_step,
+                                                         float* __restrict__ dvox, int ld, bool vec4,
+                                                         unsigned* status)
+{
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = tid < A;
+    int a = 0, x = 0, y = 0, z = 0;
+    const int res = c.res;
+    if (valid) {
+        a = active ? active[tid] : tid;
+        if (a < 0 || a >= c.G) { atomicOr(status, ERR_BAD_INDEX); valid = false; }
+        else {
+            const int gk = c.keys[a];
+            if (gk < 0 || gk >= res * res * res) { atomicOr(status, ERR_BAD_INDEX); valid = false; }
+            else {
+                x = gk % res; y = (gk / res) % res; z = gk / (res * res);
+                valid = mask[gk] && neighbours_ok(x, y, z, res, mask);
+            }
+        }
+    }
+    constexpr int S = 7;
+    int vid[S];
+    float3 q[S];
+    float d[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) { vid[s] = -1; d[s] = 0.f; q[s] = f3(0.f, 0.f, 0.f); }
+    if (valid) {
+        const float3 rv = rand_vec(tid, seed_step ? seed + (int)*seed_step : seed);
+        const int rr = res * res;
+        const int cell = x + y * res + z * rr;
+        const int dx[6] = {+1, -1, 0, 0, 0, 0}, dy[6] = {0, 0, +1, -1, 0, 0}, dz[6] = {0, 0, 0, 0, +1, -1};
+        const int step[6] = {1, -1, res, -res, rr, -rr};
+        int id[S];
+        id[0] = LS ? c.dense[cell] : -1;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) id[i + 1] = c.dense[cell + step[i]];
+        float f[S];
+        f[0] = LS ? sample_vox(c, id[0], x, y, z, rv, vid[0], q[0], status) : 0.f;
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+            f[i + 1] = sample_vox(c, id[i + 1], x + dx[i], y + dy[i], z + dz[i], rv, vid[i + 1], q[i + 1], status);
+        if (LS) {
+            const float center = f[0];
+            const float lx = f[1] + f[2] - 2.0f * center;
+            const float ly = f[3] + f[4] - 2.0f * center;
+            const float lz = f[5] + f[6] - 2.0f * center;
+            const float lr = sqrtf(lx * lx + ly * ly + lz * lz + 1e-10f);
+            const float size = w_ls * 0.5 * vox_size_inv * vox_size_inv;
+            const float gx = 0.5 / lr * 2 * lx * size;
+            const float gy = 0.5 / lr * 2 * ly * size;
+            const float gz = 0.5 / lr * 2 * lz * size;
+            d[0] = -2.0f * (gx + gy + gz);
+            d[1] = gx; d[2] = gx; d[3] = gy; d[4] = gy; d[5] = gz; d[6] = gz;
+        }
+        if (GE) {
+            const float dxv = (f[1] - f[2]) * 0.5f, dyv = (f[3] - f[4]) * 0.5f, dzv = (f[5] - f[6]) * 0.5f;
+            const float gn = sqrtf(dxv * dxv + dyv * dyv + dzv * dzv + 1e-6f);
+            const float gw = gn * 0.5 * vox_size_inv;
+            const float dg = 2.0f * (gw - 1.0f) * w_ge;
+            const float ddx = dg * dxv / gn * 0.5f * vox_size_inv;
+            const float ddy = dg * dyv / gn * 0.5f * vox_size_inv;
+            const float ddz = dg * dzv / gn * 0.5f * vox_size_inv;
+            d[1] += ddx; d[2] += -ddx; d[3] += ddy; d[4] += -ddy; d[5] += ddz; d[6] += -ddz;
+        }
+    }
+    // merge samples owned by the primary voxel in registers, atomics for the others
+    int primary = -1;
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+        if (primary < 0 && vid[s] >= 0) primary = vid[s];
+    float acc[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) acc[i] = 0.f;
+    if (valid) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            if (vid[s] < 0) continue;
+            float w[8];
+            clamped_weights(q[s], w);
+            if (vid[s] == primary) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) acc[i] += d[s] * w[i];
+            } else {
+                float t[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) t[i] = d[s] * w[i];
+                add8(dvox, ld, vec4, vid[s], t);
+            }
+        }
+    }
+    // lanes holding the same primary voxel in a contiguous run are summed by a segmented
+    // shuffle reduction; the run head issues the atomics
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    if (!valid) primary = -1;
+    const int prev = __shfl_up_sync(FULL, primary, 1);
+    const bool head = lane == 0 || prev != primary;
+    const unsigned heads = __ballot_sync(FULL, head);
+    const int my_head = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int other_head = __shfl_down_sync(FULL, my_head, off);
+        const bool same = (lane + off < 32) && other_head == my_head;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float v = __shfl_down_sync(FULL, acc[i], off);
+            if (same) acc[i] += v;
+        }
+    }
+    if (head && primary >= 0) add8(dvox, ld, vec4, primary, acc);
+}
+
+extern "C" int svr_smoothness_bw_vox(int G, int A, const int32_t* active, const int32_t* grid_keys,
+                                     const int32_t* grid2voxel, int grid_res, const uint8_t* grid_mask,
+                                     const int32_t* dense_index, const float* voxel_coords,
+                                     const float* voxel_sizes, int N, const float* geos, float w_ls,
+                                     float w_ge, float vox_size_inv, int seed, const int64_t* seed_step,
+                                     float* dvox, int ld, uint32_t* status, void* stream)
+{
+    if (A <= 0 || (w_ls == 0.f && w_ge == 0.f)) return SVR_OK;
+    if (!grid_keys || !grid2voxel || !grid_mask || !dense_index || !voxel_coords || !voxel_sizes || !geos || !dvox ||
+        !status || ld < 8)
+        return svr_fail(SVR_ERR_ARG, "smoothness: null argument or ld < 8");
+    if (!active && A > G) return svr_fail(SVR_ERR_ARG, "smoothness: A > G without an active list");
+    if (((uintptr_t)geos & 15) != 0) return svr_fail(SVR_ERR_ARG, "smoothness: geos must be 16-byte aligned");
+    const bool vec4 = (ld % 4 == 0) && (((uintptr_t)dvox & 15) == 0);
+    VoxCtx c{G, N, grid_res, dense_index, grid_keys, grid2voxel, voxel_coords, voxel_sizes, (const float4*)geos};
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned nb = (unsigned)((A + 255) / 256);
+    if (w_ls != 0.f && w_ge != 0.f)
+        smooth_vox_kernel<true, true><<<nb, 256, 0, st>>>(c, A, active, grid_mask, w_ls, w_ge, vox_size_inv, seed,
+                                                          seed_step, dvox, ld, vec4, status);
+    else if (w_ls != 0.f)
+        smooth_vox_kernel<true, false><<<nb, 256, 0, st>>>(c, A, active, grid_mask, w_ls, w_ge, vox_size_inv, seed,
+                                                           seed_step, dvox, ld, vec4, status);
+    else
+        smooth_vox_kernel<false, true><<<nb, 256, 0, st>>>(c, A, active, grid_mask, w_ls, w_ge, vox_size_inv, seed,
+                                                           seed_step, dvox, ld, vec4, status);
+    svr_note_launch(1);
+    CUDA_TRY(cudaGetLastError());
+    return SVR_OK;
+}
+
 // ------------------------------------------------------------------ allocation-free variant
 // For callers that cannot allocate device memory themselves (for example a host framework
 // that hands out all device memory from a fixed arena reserved at start-up and forbids any

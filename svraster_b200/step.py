@@ -25,7 +25,7 @@ from . import utils
 class BatchedTrainStep:
 
     def __init__(self, scene, cams, device="cuda", lr=(1e-3, 1e-3, 1e-4), betas=(0.1, 0.99), eps=1e-15,
-                 lambda_ls=1e-3, lambda_ge=1e-3, lambda_R_concen=0.0, sh_degree=3, seed=0):
+                 lambda_ls=1e-3, lambda_ge=1e-3, lambda_R_concen=0.0, sh_degree=3, seed=0, fused_smoothness=True):
         dev = torch.device(device)
         self.dev = dev
         t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
@@ -69,6 +69,7 @@ class BatchedTrainStep:
         from .grid_loss_bw import dense_index
         self.grid_index = dense_index(self.grid_keys, res)
         self.lambda_ls, self.lambda_ge = lambda_ls, lambda_ge
+        self.fused_smoothness = fused_smoothness
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.seed = seed
         # upstream gradients (seeded synthetic)
@@ -149,25 +150,38 @@ class BatchedTrainStep:
                               lambda_R_concen=self.lambda_R, gt_color=self.gt, drgbs=self.drgbs, dvox=self.dvox,
                               ds=self.ds)
         mark("render_bwd")
+        G, A = self.grid_keys.numel(), self.active.numel()
+        seed = self.seed if graph else self.seed + self.adam_step
+        step_ptr = ptr(self.step_dev) if graph else None
+        if self.fused_smoothness:
+            # both adjoints in one pass, accumulated per voxel corner into dvox, then moved to
+            # the grid points with the render adjoint's corner gradients
+            check(L.svr_smoothness_bw_vox(G, G, None, ptr(self.grid_keys), ptr(self.grid2voxel), 1 << self.res_pow2,
+                                          ptr(self.grid_mask), ptr(self.grid_index), ptr(self.grid_voxel_coord),
+                                          ptr(self.grid_voxel_size), N, ptr(self.geos), float(self.lambda_ls),
+                                          float(self.lambda_ge), self.vox_size_min_inv, seed, step_ptr,
+                                          ptr(self.dvox), 12, ptr(self.status), st), "smoothness")
+            mark("smoothness")
         for gr in self.grads:
             gr.zero_()
         check(L.svr_scatter_vox_grads(N, 12, ptr(self.vox_key), ptr(self.dvox), ptr(self.grads[0]), st), "scatter")
         check(L.svr_sh_eval_views_bw(N, self.V, self.sh_degree, self.M_sh, ptr(self.centers), ptr(self.cam_pos),
                                      ptr(self.drgbs), ptr(self.grads[1]), ptr(self.grads[2]), st), "sh views bw")
         mark("scatter+sh_bw")
-        G, A = self.grid_keys.numel(), self.active.numel()
-        common = lambda: (G, A, ptr(self.active), ptr(self.grid_keys), ptr(self.grid2voxel), 1 << self.res_pow2,
-                          ptr(self.grid_mask), ptr(self.grid_index), ptr(self.grid_voxel_coord),
-                          ptr(self.grid_voxel_size), N, ptr(self.vox_key), ptr(self.grid), self.grid.numel())
-        if graph:
-            for fn, lam in ((L.svr_laplacian_bw_at_step, self.lambda_ls), (L.svr_eikonal_bw_at_step, self.lambda_ge)):
-                check(fn(*common(), float(lam), self.vox_size_min_inv, self.seed, ptr(self.step_dev),
-                         ptr(self.grads[0]), ptr(self.status), st), "grid loss")
-        else:
-            for fn, lam in ((L.svr_laplacian_bw, self.lambda_ls), (L.svr_eikonal_bw, self.lambda_ge)):
-                check(fn(*common(), float(lam), self.vox_size_min_inv, self.seed + self.adam_step,
-                         ptr(self.grads[0]), ptr(self.status), st), "grid loss")
-        mark("smoothness")
+        if not self.fused_smoothness:
+            common = (G, A, ptr(self.active), ptr(self.grid_keys), ptr(self.grid2voxel), 1 << self.res_pow2,
+                      ptr(self.grid_mask), ptr(self.grid_index), ptr(self.grid_voxel_coord),
+                      ptr(self.grid_voxel_size), N, ptr(self.vox_key), ptr(self.grid), self.grid.numel())
+            if graph:
+                for fn, lam in ((L.svr_laplacian_bw_at_step, self.lambda_ls),
+                                (L.svr_eikonal_bw_at_step, self.lambda_ge)):
+                    check(fn(*common, float(lam), self.vox_size_min_inv, seed, step_ptr, ptr(self.grads[0]),
+                             ptr(self.status), st), "grid loss")
+            else:
+                for fn, lam in ((L.svr_laplacian_bw, self.lambda_ls), (L.svr_eikonal_bw, self.lambda_ge)):
+                    check(fn(*common, float(lam), self.vox_size_min_inv, seed, ptr(self.grads[0]),
+                             ptr(self.status), st), "grid loss")
+            mark("smoothness")
         if grad_hook is not None:
             grad_hook(self.grads)
             mark("allreduce")
