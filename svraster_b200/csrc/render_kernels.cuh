@@ -26,10 +26,20 @@ namespace svr {
 #ifndef SVR_NSLOT
 #define SVR_NSLOT 4
 #endif
+// Minimum resident CTAs per SM requested from the register allocator.  Left to itself the
+// allocator gives the adjoint 127-133 registers: 2 CTAs per SM at best, 1 when it crosses 128.
+// Measured on the mid-size workload (8 views 800x800): forward 4 CTAs (64 registers)
+// 3.57 ms vs 3 CTAs 3.69 ms; adjoint 3 CTAs (80 registers, 160 B spilled to L1) 5.96 ms vs
+// 2 CTAs 6.8-7.0 ms vs 1 CTA 11.7 ms.
+#ifndef SVR_FWD_MINB
+#define SVR_FWD_MINB 4
+#endif
+#ifndef SVR_BWD_MINB
+#define SVR_BWD_MINB 3
+#endif
 constexpr int BATCH = SVR_BATCH;   // records per slot (80 B each)
 constexpr int NSLOT = SVR_NSLOT;   // ring depth
 constexpr int NWARP = BLOCK / 32;
-constexpr int NCHUNK = BATCH / 32;
 static_assert(BATCH % 32 == 0 && BATCH <= 128, "slot holds at most 128 records (two 64-bit masks)");
 
 // Candidate set of one lane over a slot: bit j = record j of the slot (j < 128).
@@ -61,7 +71,7 @@ struct alignas(128) FwdSmem {
     Rec buf[NSLOT][BATCH];
     uint64_t full[NSLOT];
     uint32_t arrived[NSLOT];
-    uint32_t warp_quads[NWARP];
+    uint32_t octl[NWARP][8];
     uint32_t warps_done;
     int32_t stop;              // first batch not issued once every warp is done (INT_MAX before)
     uint32_t red[NWARP];
@@ -73,28 +83,55 @@ struct alignas(128) BwdSmem {
     uint32_t touched[NSLOT][BATCH / 32];
     uint64_t full[NSLOT];
     uint32_t arrived[NSLOT];
-    uint32_t warp_quads[NWARP];
+    uint32_t octl[NWARP][8];
     float red[NWARP];
 };
 
-// Per-warp relevance of the 32 records of chunk c: bbox overlaps the warp's 8x4 block and
-// the record's octant occurs among the warp's rays.  Exact pre-filter of pix_in_bbox /
-// octant test below (a lane can only pass them when its warp's block overlaps).
-__device__ __forceinline__ uint32_t warp_relevance(const Rec* buf, int c, int cnt, int lane, uint32_t wx0,
-                                                   uint32_t wy0, uint32_t wq) {
+// Candidates of chunk c (records 32c .. 32c+31 of the slot) for every lane of the warp.
+// Lane j takes record 32c+j and forms the set of the warp's pixels (lane = row * 8 + col of
+// its 8x4 block) inside the record's pixel bbox (pix_in_bbox, inclusive) whose ray octant
+// equals the record's (octl[q] = lanes with octant q) and that are still live; a 32x32 bit
+// transpose then hands each lane the records of the chunk that pass for its own pixel
+// (bit j = record 32c+j).  Same predicate as testing every record in every lane, at one
+// record per lane.
+__device__ __forceinline__ uint32_t chunk_candidates(const Rec* buf, int c, int cnt, int lane, int wx0, int wy0,
+                                                     const uint32_t* octl, uint32_t live) {
     const int j = c * 32 + lane;
-    bool hit = false;
+    uint32_t m = 0u;
     if (j < cnt) {
         const Rec& r = buf[j];
-        const uint32_t x0 = r.bbox0 >> 16, y0 = r.bbox0 & 0xFFFF, x1 = r.bbox1 >> 16, y1 = r.bbox1 & 0xFFFF;
-        hit = x0 <= wx0 + 7 && x1 >= wx0 && y0 <= wy0 + 3 && y1 >= wy0 && ((wq >> (r.val >> 29)) & 1);
+        const int c0 = max((int)(r.bbox0 >> 16) - wx0, 0), c1 = min((int)(r.bbox1 >> 16) - wx0, 7);
+        const int r0 = max((int)(r.bbox0 & 0xFFFFu) - wy0, 0), r1 = min((int)(r.bbox1 & 0xFFFFu) - wy0, 3);
+        if (c0 <= c1 && r0 <= r1) {
+            const uint32_t cm = (0xFFu >> (7 - c1)) & (0xFFu << c0);
+            const uint32_t rm = (0xFFFFFFFFu >> (8 * (3 - r1))) & (0xFFFFFFFFu << (8 * r0));
+            m = (cm * 0x01010101u) & rm & octl[r.val >> 29] & live;
+        }
     }
-    return __ballot_sync(0xffffffffu, hit);
+    // bit transpose: afterwards lane i holds bit j = (row j had bit i)
+#pragma unroll
+    for (int k = 16; k >= 1; k >>= 1) {
+        const uint32_t M = k == 16 ? 0x0000FFFFu : k == 8 ? 0x00FF00FFu : k == 4 ? 0x0F0F0F0Fu
+                         : k == 2 ? 0x33333333u : 0x55555555u;
+        const uint32_t y = __shfl_xor_sync(0xffffffffu, m, k);
+        m = (lane & k) ? ((m & ~M) | ((y >> k) & M)) : ((m & M) | ((y & M) << k));
+    }
+    return m;
+}
+
+// octl[q] = lanes of this warp whose pixel is in the image and whose ray octant is q
+__device__ __forceinline__ void warp_octant_lanes(uint32_t* octl, bool inside, uint32_t pq, int lane) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const uint32_t b = __ballot_sync(0xffffffffu, inside && pq == (uint32_t)q);
+        if (lane == q) octl[q] = b;
+    }
+    __syncwarp();
 }
 
 // ============================================================================ forward
 template <int NS, bool DEPTH, bool NORMAL, bool MAXW>
-__global__ void __launch_bounds__(BLOCK) render_fwd_kernel(
+__global__ void __launch_bounds__(BLOCK, SVR_FWD_MINB) render_fwd_kernel(
     const __grid_constant__ Views V, const uint2* __restrict__ ranges, const Rec* __restrict__ recs,
     const float* __restrict__ s_ptr, uint32_t* __restrict__ tile_last, uint32_t* __restrict__ n_contrib,
     float* __restrict__ out_color, float* __restrict__ out_depth, float* __restrict__ out_normal,
@@ -112,12 +149,12 @@ __global__ void __launch_bounds__(BLOCK) render_fwd_kernel(
     int dx, dy;
     tile_pixel(tid, dx, dy);
     const uint32_t px = tx * TILE + dx, py = ty * TILE + dy;
-    const uint32_t wx0 = tx * TILE + (warp & 1) * 8, wy0 = ty * TILE + (warp >> 1) * 4;
+    const int wx0 = tx * TILE + (warp & 1) * 8, wy0 = ty * TILE + (warp >> 1) * 4;
     const bool inside = (px < (uint32_t)W) && (py < (uint32_t)H);
     const Ray ray = pixel_ray(view, px, py);
     const uint32_t pq = ray_octant(ray.rd);
     const float s_val = *s_ptr;
-    const uint32_t wq = __reduce_or_sync(0xffffffffu, inside ? (1u << pq) : 0u);
+    warp_octant_lanes(S.octl[warp], inside, pq, lane);
 
     const uint2 range = ranges[tile];
     const int n = (int)(range.y - range.x);
@@ -159,14 +196,13 @@ __global__ void __launch_bounds__(BLOCK) render_fwd_kernel(
         if (!__all_sync(0xffffffffu, done)) {
             // candidate pairs of this lane over the whole slot, in record order
             CandMask cand{0ull, 0ull};
-            for (int c = 0; c < NCHUNK; ++c) {
-                uint32_t rel = warp_relevance(buf, c, cnt, lane, wx0, wy0, wq);
-                if (done) rel = 0;
-                while (rel) {
-                    const int k = __ffs(rel) - 1;
-                    rel &= rel - 1;
+            const uint32_t live = __ballot_sync(0xffffffffu, !done);
+            for (int c = 0; c * 32 < cnt; ++c) {
+                uint32_t bits = chunk_candidates(buf, c, cnt, lane, wx0, wy0, S.octl[warp], live);
+                while (bits) {
+                    const int k = __ffs(bits) - 1;
+                    bits &= bits - 1;
                     const Rec& r = buf[c * 32 + k];
-                    if (!pix_in_bbox(px, py, r.bbox0, r.bbox1) || pq != (r.val >> 29)) continue;
                     const float2 ab = ray_box(f3(r.cx, r.cy, r.cz), r.len, ray.ro, ray.rd_inv);
                     if (ab.x > ab.y) continue;
                     cand.set(c * 32 + k);
@@ -334,7 +370,7 @@ __global__ void __launch_bounds__(BLOCK) render_fwd_kernel(
 
 // ============================================================================ adjoint
 template <bool DEPTH, bool NORMAL, bool RCONC>
-__global__ void __launch_bounds__(BLOCK) render_bwd_kernel(
+__global__ void __launch_bounds__(BLOCK, SVR_BWD_MINB) render_bwd_kernel(
     const __grid_constant__ Views V, int N, const uint2* __restrict__ ranges, const uint32_t* __restrict__ tile_last,
     const uint32_t* __restrict__ n_contrib, const Rec* __restrict__ recs, const float* __restrict__ s_ptr,
     const float* __restrict__ out_T, const float* __restrict__ dL_dcolor, const float* __restrict__ dL_ddepth,
@@ -354,12 +390,12 @@ __global__ void __launch_bounds__(BLOCK) render_bwd_kernel(
     int dx, dy;
     tile_pixel(tid, dx, dy);
     const uint32_t px = tx * TILE + dx, py = ty * TILE + dy;
-    const uint32_t wx0 = tx * TILE + (warp & 1) * 8, wy0 = ty * TILE + (warp >> 1) * 4;
+    const int wx0 = tx * TILE + (warp & 1) * 8, wy0 = ty * TILE + (warp >> 1) * 4;
     const bool inside = (px < (uint32_t)W) && (py < (uint32_t)H);
     const Ray ray = pixel_ray(view, px, py);
     const uint32_t pq = ray_octant(ray.rd);
     const float s_val = *s_ptr;
-    const uint32_t wq = __reduce_or_sync(0xffffffffu, inside ? (1u << pq) : 0u);
+    warp_octant_lanes(S.octl[warp], inside, pq, lane);
 
     const uint32_t r0 = ranges[tile].x;
     const uint32_t r1 = tile_last[tile];
@@ -413,7 +449,8 @@ __global__ void __launch_bounds__(BLOCK) render_bwd_kernel(
     const float weight_R = lambda_R * WH_inv;
     float ds_acc = 0.f;
     const bool active = inside && last_c > 0;
-    const bool warp_active = __any_sync(0xffffffffu, active);
+    const uint32_t live = __ballot_sync(0xffffffffu, active);
+    const bool warp_active = live != 0u;
     uint32_t parity = 0;
     bool failed = false;
 
@@ -427,16 +464,16 @@ __global__ void __launch_bounds__(BLOCK) render_bwd_kernel(
         const Rec* buf = S.buf[slot];
         if (warp_active) {
             CandMask cand{0ull, 0ull};
-            for (int c = 0; c < NCHUNK; ++c) {
-                uint32_t rel = warp_relevance(buf, c, cnt, lane, wx0, wy0, wq);
-                if (!active) rel = 0;
-                while (rel) {
-                    const int k = __ffs(rel) - 1;
-                    rel &= rel - 1;
+            for (int c = 0; c * 32 < cnt; ++c) {
+                uint32_t bits = chunk_candidates(buf, c, cnt, lane, wx0, wy0, S.octl[warp], live);
+                // only records before this pixel's last contributor
+                const int lim = (int)last_c - lo - c * 32;
+                bits &= lim >= 32 ? 0xFFFFFFFFu : (lim <= 0 ? 0u : ((1u << lim) - 1u));
+                while (bits) {
+                    const int k = __ffs(bits) - 1;
+                    bits &= bits - 1;
                     const int jj = c * 32 + k;
-                    if ((uint32_t)(lo + jj) >= last_c) continue;
                     const Rec& r = buf[jj];
-                    if (!pix_in_bbox(px, py, r.bbox0, r.bbox1) || pq != (r.val >> 29)) continue;
                     const float2 ab = ray_box(f3(r.cx, r.cy, r.cz), r.len, ray.ro, ray.rd_inv);
                     if (ab.x > ab.y) continue;
                     cand.set(jj);
