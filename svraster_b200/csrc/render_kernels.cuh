@@ -10,8 +10,10 @@
 //  * each warp pre-filters a slot's records against its 8x4 footprint and octant set with
 //    one ballot per 32 records, then every lane collects its candidate pairs for the whole
 //    slot and processes them in record order;
-//  * the adjoint accumulates per-record gradients of the slot in shared memory and the
-//    last warp flushes them with one vector atomic set per record per CTA.
+//  * the adjoint sends each pair's 12 gradient terms to dL_dvox / drgbs with vector
+//    reductions (two or three float4 red per pair).  A shared-memory accumulator per slot,
+//    flushed by the slot's last warp, measured 5.40 ms against 3.58 ms for the direct
+//    reductions on 8 views 800x800: while one warp flushed, the others waited for the slot.
 #pragma once
 
 #include <climits>
@@ -79,8 +81,6 @@ struct alignas(128) FwdSmem {
 
 struct alignas(128) BwdSmem {
     Rec buf[NSLOT][BATCH];
-    float acc[NSLOT][BATCH][12];
-    uint32_t touched[NSLOT][BATCH / 32];
     uint64_t full[NSLOT];
     uint32_t arrived[NSLOT];
     uint32_t octl[NWARP][8];
@@ -406,8 +406,6 @@ __global__ void __launch_bounds__(BLOCK, SVR_BWD_MINB) render_bwd_kernel(
         for (int k = 0; k < NSLOT; ++k) { mbar_init(&S.full[k], 1); S.arrived[k] = 0; }
         fence_mbar_init();
     }
-    for (int i = tid; i < NSLOT * BATCH * 12; i += BLOCK) (&S.acc[0][0][0])[i] = 0.f;
-    for (int i = tid; i < NSLOT * (BATCH / 32); i += BLOCK) (&S.touched[0][0])[i] = 0u;
     __syncthreads();
     // batch b covers relative records [lo, hi) with hi = n - b*BATCH (back to front)
     auto issue = [&](int b) {
@@ -594,52 +592,31 @@ __global__ void __launch_bounds__(BLOCK, SVR_BWD_MINB) render_bwd_kernel(
                         const float3 gr = weight_R * pt_w * 2.0f * (c3 - gt);
                         drgb0 += gr.x; drgb1 += gr.y; drgb2 += gr.z;
                     }
-                    float* acc = S.acc[slot][jj];
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) atomicAdd(acc + i, dg[i]);
-                    atomicAdd(acc + 8, drgb0);
-                    atomicAdd(acc + 9, drgb1);
-                    atomicAdd(acc + 10, drgb2);
-                    atomicAdd(acc + 11, fabsf(dL_dalpha * alpha));
-                    atomicOr(&S.touched[slot][jj >> 5], 1u << (jj & 31));
+                    const uint32_t vid = r.val & 0x1FFFFFFFu;
+                    if (vid < (uint32_t)N) {
+                        float4* dst = reinterpret_cast<float4*>(dL_dvox + 12 * (size_t)vid);
+                        atomicAdd(dst, make_float4(dg[0], dg[1], dg[2], dg[3]));
+                        atomicAdd(dst + 1, make_float4(dg[4], dg[5], dg[6], dg[7]));
+                        if (drgbs) {
+                            float* cr = drgbs + 3 * ((size_t)vi * N + vid);
+                            atomicAdd(cr, drgb0); atomicAdd(cr + 1, drgb1); atomicAdd(cr + 2, drgb2);
+                            atomicAdd(dL_dvox + 12 * (size_t)vid + 11, fabsf(dL_dalpha * alpha));
+                        } else {
+                            atomicAdd(dst + 2, make_float4(drgb0, drgb1, drgb2, fabsf(dL_dalpha * alpha)));
+                        }
+                    } else {
+                        atomicOr(status, ERR_BAD_INDEX);
+                    }
                 }
             }
         }
-        // release the slot; the last warp flushes its gradients and refills it
+        // release the slot; the last warp to release it refills it
         __syncwarp();
-        uint32_t prev = 0;
         if (lane == 0) {
             __threadfence_block();
-            prev = atomicAdd(&S.arrived[slot], 1u);
-        }
-        prev = __shfl_sync(0xffffffffu, prev, 0);
-        if (prev == NWARP - 1) {
-            __threadfence_block();
-            for (int jj = lane; jj < cnt; jj += 32) {
-                if (!((S.touched[slot][jj >> 5] >> (jj & 31)) & 1u)) continue;
-                const uint32_t vid = buf[jj].val & 0x1FFFFFFFu;
-                float* a = S.acc[slot][jj];
-                if (vid < (uint32_t)N) {
-                    float4* dst = reinterpret_cast<float4*>(dL_dvox + 12 * (size_t)vid);
-                    atomicAdd(dst, make_float4(a[0], a[1], a[2], a[3]));
-                    atomicAdd(dst + 1, make_float4(a[4], a[5], a[6], a[7]));
-                    if (drgbs) {
-                        float* cr = drgbs + 3 * ((size_t)vi * N + vid);
-                        atomicAdd(cr, a[8]); atomicAdd(cr + 1, a[9]); atomicAdd(cr + 2, a[10]);
-                        atomicAdd(dL_dvox + 12 * (size_t)vid + 11, a[11]);
-                    } else {
-                        atomicAdd(dst + 2, make_float4(a[8], a[9], a[10], a[11]));
-                    }
-                } else {
-                    atomicOr(status, ERR_BAD_INDEX);
-                }
-#pragma unroll
-                for (int k = 0; k < 12; ++k) a[k] = 0.f;
-            }
-            __syncwarp();
-            if (lane < BATCH / 32) S.touched[slot][lane] = 0u;
-            __syncwarp();
-            if (lane == 0) {
+            const uint32_t prev = atomicAdd(&S.arrived[slot], 1u);
+            if (prev == NWARP - 1) {
+                __threadfence_block();
                 S.arrived[slot] = 0;
                 const int nb2 = b + NSLOT;
                 if (nb2 < nbatch) {
