@@ -103,17 +103,27 @@ static BinLayout bin_layout(int64_t R) {
     return L;
 }
 
-// image buffer: ranges uint2[T] | tile_last u32[T] | n_contrib u32[P] | status
+// image buffer: ranges uint2[T] | tile_last u32[T] | n_contrib u32[P] | status |
+//               launch order u32[T] | order sort keys / values / scratch
 struct ImgLayout {
-    size_t ranges, tile_last, n_contrib, status, total;
+    size_t ranges, tile_last, n_contrib, status, order, okeys_in, okeys_out, ovals_in, otmp, otmp_bytes, total;
 };
 static ImgLayout img_layout(int64_t P, int T) {
     ImgLayout L{};
     size_t off = 0;
+    const int nt = T > 0 ? T : 1;
     L.ranges = off; off = align_up(off + 8 * (size_t)T, 256);
     L.tile_last = off; off = align_up(off + 4 * (size_t)T, 256);
     L.n_contrib = off; off = align_up(off + 4 * (size_t)P, 256);
     L.status = off; off = align_up(off + 256, 256);
+    L.order = off; off = align_up(off + 4 * (size_t)nt, 256);
+    L.okeys_in = off; off = align_up(off + 4 * (size_t)nt, 256);
+    L.okeys_out = off; off = align_up(off + 4 * (size_t)nt, 256);
+    L.ovals_in = off; off = align_up(off + 4 * (size_t)nt, 256);
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                    (const uint32_t*)nullptr, (uint32_t*)nullptr, nt);
+    L.otmp = off; L.otmp_bytes = tb; off = align_up(off + tb, 256);
     L.total = off;
     return L;
 }
@@ -445,6 +455,33 @@ static int bin_sort_typed(const Views& V, int N, int64_t R, const KeyFmt& kf, in
     return SVR_OK;
 }
 
+// Launch order of the tiles: most records first (stable, so equal counts keep tile order).
+// CTAs start roughly in blockIdx order, so the long tiles no longer start in the last wave
+// and leave the GPU waiting on a few of them.
+__global__ void tile_order_keys_kernel(int T, const uint2* __restrict__ ranges, uint32_t* __restrict__ keys,
+                                       uint32_t* __restrict__ vals)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    const uint2 r = ranges[t];
+    keys[t] = 0xFFFFFFFFu - (r.y > r.x ? r.y - r.x : 0u);
+    vals[t] = (uint32_t)t;
+}
+
+static int tile_launch_order(int T, char* im, const ImgLayout& IL, cudaStream_t st)
+{
+    if (T <= 0) return SVR_OK;
+    tile_order_keys_kernel<<<(T + 255) / 256, 256, 0, st>>>(T, (const uint2*)(im + IL.ranges),
+                                                            (uint32_t*)(im + IL.okeys_in),
+                                                            (uint32_t*)(im + IL.ovals_in));
+    LAUNCH_CHECK();
+    size_t tb = IL.otmp_bytes;
+    CUDA_TRY(cub::DeviceRadixSort::SortPairs(im + IL.otmp, tb, (const uint32_t*)(im + IL.okeys_in),
+                                             (uint32_t*)(im + IL.okeys_out), (const uint32_t*)(im + IL.ovals_in),
+                                             (uint32_t*)(im + IL.order), T, 0, 32, st));
+    return SVR_OK;
+}
+
 extern "C" int svr_binning_count(const void* binning_buffer, int64_t* count_host, void* stream)
 {
     cudaStream_t st = (cudaStream_t)stream;
@@ -486,12 +523,13 @@ extern "C" int svr_bin_and_sort(const svr_view_t* views_host, int n_views, int N
     unsigned* status = (unsigned*)(im + IL.status);
     CUDA_TRY(cudaMemsetAsync(im + IL.ranges, 0, 8 * (size_t)T, st));
     CUDA_TRY(cudaMemsetAsync(status, 0, 4, st));
-    if (R == 0) return SVR_OK;
+    if (R == 0) return tile_launch_order(T, im, IL, st);
     const KeyFmt kf = key_format(path_or, T);
     if (kf.key_bits > 64) return svr_fail(SVR_ERR_UNSUPPORTED, "sort key wider than 64 bits");
-    if (kf.key_bits <= 32)
-        return bin_sort_typed<uint32_t>(V, N, R, kf, T, octpaths, g, GL, b, BL, im, IL, status, st);
-    return bin_sort_typed<uint64_t>(V, N, R, kf, T, octpaths, g, GL, b, BL, im, IL, status, st);
+    rc = kf.key_bits <= 32 ? bin_sort_typed<uint32_t>(V, N, R, kf, T, octpaths, g, GL, b, BL, im, IL, status, st)
+                           : bin_sort_typed<uint64_t>(V, N, R, kf, T, octpaths, g, GL, b, BL, im, IL, status, st);
+    if (rc) return rc;
+    return tile_launch_order(T, im, IL, st);
 }
 
 extern "C" int svr_unpack_binning(const void* binning_buffer, int64_t R, int T, const void* image_buffer,
@@ -564,7 +602,8 @@ static int ensure_smem(K k, int smem, std::atomic<unsigned long long>& done)
 }
 
 template <int NS, bool DEPTH, bool NORMAL, bool MAXW>
-static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint2* ranges, const Rec* recs,
+static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
+                      const Rec* recs,
                       const float* s_val, uint32_t* tile_last, uint32_t* n_contrib, float* color, float* depth,
                       float* normal, float* outT, float* max_w, unsigned* status)
 {
@@ -573,7 +612,8 @@ static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint2* range
     static std::atomic<unsigned long long> done{0};
     int rc = ensure_smem(k, smem, done);
     if (rc) return rc;
-    k<<<T, BLOCK, smem, st>>>(V, ranges, recs, s_val, tile_last, n_contrib, color, depth, normal, outT, max_w, status);
+    k<<<T, BLOCK, smem, st>>>(V, order, ranges, recs, s_val, tile_last, n_contrib, color,
+                              depth, normal, outT, max_w, status);
     LAUNCH_CHECK();
     return SVR_OK;
 }
@@ -602,6 +642,7 @@ extern "C" int svr_render_fwd(const svr_view_t* views_host, int n_views, int N, 
     char* im = (char*)image_buffer;
     unsigned* status = (unsigned*)(im + IL.status);
     const uint2* ranges = (const uint2*)(im + IL.ranges);
+    const uint32_t* order = (const uint32_t*)(im + IL.order);
     Rec* recs = (Rec*)(b + BL.recs);
     if (R > 0) {
         pack_records_kernel<<<(unsigned)((R + 255) / 256), 256, 0, st>>>(
@@ -614,14 +655,14 @@ extern "C" int svr_render_fwd(const svr_view_t* views_host, int n_views, int N, 
     const bool D = need_depth != 0, Nm = need_normal != 0, MW = max_w != nullptr;
 #define FWD_CASE(NS_)                                                                                   \
     if (n_samp == NS_) {                                                                                \
-        if (D && Nm && !MW) return launch_fwd<NS_, true, true, false>(T, st, V, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
-        if (D && Nm && MW) return launch_fwd<NS_, true, true, true>(T, st, V, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
-        if (D && !Nm && !MW) return launch_fwd<NS_, true, false, false>(T, st, V, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
-        if (D && !Nm && MW) return launch_fwd<NS_, true, false, true>(T, st, V, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
-        if (!D && Nm && !MW) return launch_fwd<NS_, false, true, false>(T, st, V, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
-        if (!D && Nm && MW) return launch_fwd<NS_, false, true, true>(T, st, V, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
-        if (!D && !Nm && !MW) return launch_fwd<NS_, false, false, false>(T, st, V, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
-        return launch_fwd<NS_, false, false, true>(T, st, V, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
+        if (D && Nm && !MW) return launch_fwd<NS_, true, true, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
+        if (D && Nm && MW) return launch_fwd<NS_, true, true, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
+        if (D && !Nm && !MW) return launch_fwd<NS_, true, false, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
+        if (D && !Nm && MW) return launch_fwd<NS_, true, false, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
+        if (!D && Nm && !MW) return launch_fwd<NS_, false, true, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
+        if (!D && Nm && MW) return launch_fwd<NS_, false, true, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
+        if (!D && !Nm && !MW) return launch_fwd<NS_, false, false, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
+        return launch_fwd<NS_, false, false, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
     }
     FWD_CASE(1)
     FWD_CASE(2)
@@ -631,7 +672,8 @@ extern "C" int svr_render_fwd(const svr_view_t* views_host, int n_views, int N, 
 }
 
 template <bool DEPTH, bool NORMAL, bool RCONC>
-static int launch_bwd(int T, int N, cudaStream_t st, const Views& V, const uint2* ranges, const uint32_t* tl,
+static int launch_bwd(int T, int N, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
+                      const uint32_t* tl,
                       const uint32_t* nc, const Rec* recs, const float* s_val, const float* out_T,
                       const float* dc, const float* dd, const float* dn, const float* dT, float lam,
                       const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status)
@@ -641,7 +683,7 @@ static int launch_bwd(int T, int N, cudaStream_t st, const Views& V, const uint2
     static std::atomic<unsigned long long> done{0};
     int rc = ensure_smem(k, smem, done);
     if (rc) return rc;
-    k<<<T, BLOCK, smem, st>>>(V, N, ranges, tl, nc, recs, s_val, out_T, dc, dd, dn, dT, lam, gt, dvox, drgbs, ds,
+    k<<<T, BLOCK, smem, st>>>(V, N, order, ranges, tl, nc, recs, s_val, out_T, dc, dd, dn, dT, lam, gt, dvox, drgbs, ds,
                                status);
     LAUNCH_CHECK();
     return SVR_OK;
@@ -671,7 +713,7 @@ extern "C" int svr_render_bwd(const svr_view_t* views_host, int n_views, int N, 
     const uint32_t* nc = (const uint32_t*)(im + IL.n_contrib);
     const Rec* recs = (const Rec*)(b + BL.recs);
     const bool D = need_depth != 0, Nm = need_normal != 0, RC = lambda_R_concen > 0;
-#define BWD_ARGS T, N, st, V, ranges, tl, nc, recs, s_val, out_T, dL_dcolor, dL_ddepth, dL_dnormal, dL_dT, lambda_R_concen, gt_color, dL_dvox, drgbs, dL_ds, status
+#define BWD_ARGS T, N, st, V, (const uint32_t*)(im + IL.order), ranges, tl, nc, recs, s_val, out_T, dL_dcolor, dL_ddepth, dL_dnormal, dL_dT, lambda_R_concen, gt_color, dL_dvox, drgbs, dL_ds, status
     if (D && Nm && RC) return launch_bwd<true, true, true>(BWD_ARGS);
     if (D && Nm && !RC) return launch_bwd<true, true, false>(BWD_ARGS);
     if (D && !Nm && RC) return launch_bwd<true, false, true>(BWD_ARGS);

@@ -132,15 +132,16 @@ __device__ __forceinline__ void warp_octant_lanes(uint32_t* octl, bool inside, u
 // ============================================================================ forward
 template <int NS, bool DEPTH, bool NORMAL, bool MAXW>
 __global__ void __launch_bounds__(BLOCK, SVR_FWD_MINB) render_fwd_kernel(
-    const __grid_constant__ Views V, const uint2* __restrict__ ranges, const Rec* __restrict__ recs,
-    const float* __restrict__ s_ptr, uint32_t* __restrict__ tile_last, uint32_t* __restrict__ n_contrib,
+    const __grid_constant__ Views V, const uint32_t* __restrict__ order, const uint2* __restrict__ ranges,
+    const Rec* __restrict__ recs, const float* __restrict__ s_ptr, uint32_t* __restrict__ tile_last,
+    uint32_t* __restrict__ n_contrib,
     float* __restrict__ out_color, float* __restrict__ out_depth, float* __restrict__ out_normal,
     float* __restrict__ out_T, float* __restrict__ max_w, unsigned* __restrict__ status)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     FwdSmem& S = *reinterpret_cast<FwdSmem*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int tile = blockIdx.x;
+    const int tile = order ? (int)order[blockIdx.x] : (int)blockIdx.x;   // heavy tiles first
     const int vi = view_of_tile(V, tile);
     const svr_view_t& view = V.v[vi];
     const int W = view.width, H = view.height;
@@ -371,7 +372,8 @@ __global__ void __launch_bounds__(BLOCK, SVR_FWD_MINB) render_fwd_kernel(
 // ============================================================================ adjoint
 template <bool DEPTH, bool NORMAL, bool RCONC>
 __global__ void __launch_bounds__(BLOCK, SVR_BWD_MINB) render_bwd_kernel(
-    const __grid_constant__ Views V, int N, const uint2* __restrict__ ranges, const uint32_t* __restrict__ tile_last,
+    const __grid_constant__ Views V, int N, const uint32_t* __restrict__ order, const uint2* __restrict__ ranges,
+    const uint32_t* __restrict__ tile_last,
     const uint32_t* __restrict__ n_contrib, const Rec* __restrict__ recs, const float* __restrict__ s_ptr,
     const float* __restrict__ out_T, const float* __restrict__ dL_dcolor, const float* __restrict__ dL_ddepth,
     const float* __restrict__ dL_dnormal, const float* __restrict__ dL_dT, float lambda_R,
@@ -381,7 +383,7 @@ __global__ void __launch_bounds__(BLOCK, SVR_BWD_MINB) render_bwd_kernel(
     extern __shared__ __align__(128) unsigned char smem_raw[];
     BwdSmem& S = *reinterpret_cast<BwdSmem*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int tile = blockIdx.x;
+    const int tile = order ? (int)order[blockIdx.x] : (int)blockIdx.x;   // heavy tiles first
     const int vi = view_of_tile(V, tile);
     const svr_view_t& view = V.v[vi];
     const int W = view.width, H = view.height;
