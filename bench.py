@@ -32,15 +32,28 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = "mid-size: 3 spheres + torus, levels 6-10, SH deg 3, 8 views 800x800"
+CONFIGS = {
+    # the headline: plain method, mid-size scene
+    "mid": dict(workload="mid-size: 3 spheres + torus, levels 6-10, SH deg 3, 8 views 800x800", views=8,
+                image="800x800"),
+    # batched: one step over 64 views of four resolutions
+    "batched": dict(workload="batched: sphere with 64 bumps, levels 7-11, SH deg 3, 64 views (16 each of "
+                             "480x360, 960x540, 1280x720, 1920x1080, shuffled)", views=64, image="mixed"),
+}
+WORKLOAD = CONFIGS["mid"]["workload"]
 N_VIEWS, W, H = 8, 800, 800
 
 
-def make_workload(rank=0, n_views=N_VIEWS):
+def make_workload(rank=0, n_views=None, config="mid"):
     from svraster_b200 import synthetic as S
-    scene = S.scene_mid(seed=0)
-    cams = S.fibonacci_cameras(N_VIEWS * (rank + 1), 3.0, W, H, fovx_deg=50.0)[N_VIEWS * rank:N_VIEWS * (rank + 1)]
-    return scene, cams[:n_views]
+    n = CONFIGS[config]["views"]
+    if config == "batched":
+        scene = S.scene_batched(seed=0)
+        cams = S.mixed_resolution_cameras(n * (rank + 1), 3.0, seed=0)[n * rank:n * (rank + 1)]
+    else:
+        scene = S.scene_mid(seed=0)
+        cams = S.fibonacci_cameras(n * (rank + 1), 3.0, W, H, fovx_deg=50.0)[n * rank:n * (rank + 1)]
+    return scene, cams[:n_views or n]
 
 
 def measured_peaks():
@@ -123,7 +136,8 @@ def run_ours(args, rank, world):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    scene, cams = make_workload(rank, args.views)
+    scene, cams = make_workload(rank, args.views, args.config)
+    workload = CONFIGS[args.config]["workload"]
     step = BatchedTrainStep(scene, cams, device=dev, lambda_R_concen=0.1)
     L = _lib.load()
 
@@ -203,15 +217,15 @@ def run_ours(args, rank, world):
     achieved = kbytes / (kms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak,
                 "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": load_traffic(kname, WORKLOAD), "algorithmic_bytes": int(kbytes),
+                "traffic": load_traffic(kname, workload), "algorithmic_bytes": int(kbytes),
                 "launch_ms": round(kms, 4)}
 
     result = {"metric": "fwd+bwd Mrays/s", "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
               "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
               "data": "synthetic (seeded procedural scene, N(0,1) upstream gradients)",
-              "config": {"workload": WORKLOAD, "n_voxels": scene.n_vox, "n_grid_pts": int(step.grid.numel()),
-                         "views_per_gpu": len(cams), "image": f"{W}x{H}", "rays_per_step": rays,
+              "config": {"workload": workload, "n_voxels": scene.n_vox, "n_grid_pts": int(step.grid.numel()),
+                         "views_per_gpu": len(cams), "image": CONFIGS[args.config]["image"], "rays_per_step": rays,
                          "records_R": R, "records_R_prime": R_prime, "visible_voxels": V_vis,
                          "l2": "inputs larger than L2 (records + SH state > 126 MB)",
                          "parallelism": f"dp{world} over views" if world > 1 else "single GPU"},
@@ -365,7 +379,7 @@ def run_extraction(step, scene, cams, dev):
             "mc_Mvoxels_per_s": round(scene.n_vox / mc_ms / 1e3, 1),
             "cpu_numpy_restatement": {"tsdf_Mpoint_views_per_s": round(M / cpu_tsdf / 1e6, 3),
                                       "mc_Mvoxels_per_s": round(len(sub) / cpu_mc / 1e6, 3), "cores": 1,
-                                      "sample": "TSDF: 1 of 8 views; MC: every 16th voxel"}}
+                                      "sample": f"TSDF: 1 of {len(cams)} views; MC: every 16th voxel"}}
 
 
 def oracle_view_step(scene, cam, threads):
@@ -393,7 +407,7 @@ def cpu_baseline(scene, cams):
     rays = oracle_view_step(scene, cams[0], threads=1)
     dt = time.perf_counter() - t0
     return {"value": round(rays / dt / 1e6, 5), "unit": "Mrays/s", "cores": 1, "kind": "port",
-            "sample": f"1 of {N_VIEWS} views ({cams[0].width}x{cams[0].height}) preprocess+binning+fwd+bwd, "
+            "sample": f"1 of {len(cams)} views ({cams[0].width}x{cams[0].height}) preprocess+binning+fwd+bwd, "
                       f"single thread, {dt:.1f} s"}
 
 
@@ -429,7 +443,8 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--views", type=int, default=N_VIEWS, help="views per GPU (8 = the benchmark workload)")
+    ap.add_argument("--config", default="mid", choices=sorted(CONFIGS), help="workload (mid = the headline)")
+    ap.add_argument("--views", type=int, default=None, help="views per GPU (default: the workload's)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extract", action="store_true")

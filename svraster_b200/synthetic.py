@@ -92,12 +92,17 @@ def make_bumpy_sphere(n_bumps=64, amp=0.05, r=0.5, width=0.25, seed=0):
     dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
 
     def f(p):
-        n = np.linalg.norm(p, axis=-1)
-        u = p / np.maximum(n, 1e-9)[..., None]
-        h = np.zeros(n.shape)
-        for d in dirs:
-            h += amp * np.exp(-np.sum((u - d) ** 2, axis=-1) / width ** 2)
-        return n - (r + h)
+        # |u - d|^2 = 2 - 2 u.d for unit u, d: one matrix product per chunk of points
+        shape = p.shape[:-1]
+        p = p.reshape(-1, 3)
+        out = np.empty(len(p))
+        for s in range(0, len(p), 1 << 20):
+            q = p[s:s + (1 << 20)]
+            n = np.linalg.norm(q, axis=-1)
+            u = q / np.maximum(n, 1e-9)[:, None]
+            h = amp * np.exp((2.0 * (u @ dirs.T) - 2.0) / width ** 2).sum(axis=1)
+            out[s:s + len(q)] = n - (r + h)
+        return out.reshape(shape)
     return f
 
 
@@ -262,15 +267,18 @@ def ring_cameras(n, radius, width, height, fovx_deg=50.0, elev_deg=20.0, phase=0
     return cams
 
 
-def fibonacci_cameras(n, radius, width, height, fovx_deg=50.0):
-    cams = []
+def fibonacci_points(n, radius):
     ga = math.pi * (3.0 - math.sqrt(5.0))
+    pts = []
     for i in range(n):
         z = 1 - 2 * (i + 0.5) / n
         r = math.sqrt(max(0.0, 1 - z * z))
-        p = radius * np.array([math.cos(ga * i) * r, math.sin(ga * i) * r, z])
-        cams.append(look_at_camera(p, width, height, fovx_deg))
-    return cams
+        pts.append(radius * np.array([math.cos(ga * i) * r, math.sin(ga * i) * r, z]))
+    return pts
+
+
+def fibonacci_cameras(n, radius, width, height, fovx_deg=50.0):
+    return [look_at_camera(p, width, height, fovx_deg) for p in fibonacci_points(n, radius)]
 
 
 # ----------------------------------------------------------------------------- workloads
@@ -287,7 +295,19 @@ def scene_mid(seed=0):
 
 
 def scene_batched(seed=0):
-    return build_scene(make_bumpy_sphere(seed=seed), 7, 11, seed=seed, band=0.5, keep=2.0)
+    """Sphere with 64 Gaussian bumps (amplitude 0.05) at levels 7-11, about 4M voxels."""
+    return build_scene(make_bumpy_sphere(seed=seed), 7, 11, seed=seed, band=0.42, keep=1.1, kept_parent_frac=0.02)
+
+
+MIXED_RESOLUTIONS = ((480, 360), (960, 540), (1280, 720), (1920, 1080))
+
+
+def mixed_resolution_cameras(n=64, radius=3.0, fovx_deg=50.0, seed=0):
+    """n views on a Fibonacci sphere, n/4 at each of MIXED_RESOLUTIONS, shuffled by `seed`."""
+    sizes = [MIXED_RESOLUTIONS[i % len(MIXED_RESOLUTIONS)] for i in range(n)]
+    order = np.random.default_rng(seed).permutation(n)
+    return [look_at_camera(p, sizes[order[i]][0], sizes[order[i]][1], fovx_deg=fovx_deg)
+            for i, p in enumerate(fibonacci_points(n, radius))]
 
 
 def scene_tiny(seed=0, lv_min=3, lv_max=5):
