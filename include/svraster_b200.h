@@ -308,6 +308,24 @@ SVR_API int svr_adam_step(int64_t numel, int biased, int sparse, float* param, c
                   float* exp_avg, float* exp_avg_sq, double step, double lr, double beta1,
                   double beta2, float eps, void* stream);
 
+/* BF16 storage of SH coefficients (no counterpart in the reference; the precision
+ * configuration): svr_sh_eval_views_bf16 reads sh0 / shs as bf16 triples (converted exactly to
+ * f32; all arithmetic f32) and writes f32 colours like svr_sh_eval_views.  The adjoint stays
+ * svr_sh_eval_views_bw with f32 gradients.  svr_adam_step_bf16[_at] update bf16 parameters
+ * with f32 moments: the step is computed in f32 from the stored value and rounded to nearest
+ * bf16. */
+SVR_API int svr_sh_eval_views_bf16(int N, int n_views, int degree, int M, const float* centers,
+                                   const float* cam_pos, const uint16_t* sh0, const uint16_t* shs,
+                                   float* rgbs, void* stream);
+SVR_API int svr_adam_step_bf16(int64_t numel, int biased, int sparse, uint16_t* param, const float* grad,
+                               float* exp_avg, float* exp_avg_sq, double step, double lr, double beta1,
+                               double beta2, float eps, void* stream);
+SVR_API int svr_adam_step_bf16_at(int64_t numel, int biased, int sparse, uint16_t* param,
+                                  const float* grad, float* exp_avg, float* exp_avg_sq,
+                                  const float* coef_table, int64_t rows, const int64_t* step,
+                                  double beta1, double beta2, float eps, uint32_t* status,
+                                  void* stream);
+
 /* Graph-replayable Adam (no counterpart in the reference): the step number is read from a
  * device counter when the kernel runs and indexes a table of per-step coefficients
  * {lr / (1 - beta1^t), 1 / sqrt(1 - beta2^t)} that svr_adam_coef_table fills on the host

@@ -79,6 +79,21 @@ def binning(cam, octpath, ndup, bboxes, bits):
     return keys[:R], vals[:R], ranges
 
 
+def set_pixel_mask(mask, bits=32):
+    """Render only the pixels where ``mask`` (uint8[H*W]) is nonzero in later render_fwd /
+    render_bwd calls of that build; None renders every pixel.  The array is kept alive here."""
+    global _mask_keep
+    if mask is None:
+        _mask_keep = None
+        lib(bits).svo_set_pixel_mask(None)
+        return
+    _mask_keep = np.ascontiguousarray(mask, dtype=np.uint8)
+    lib(bits).svo_set_pixel_mask(_p(_mask_keep))
+
+
+_mask_keep = None
+
+
 def render_fwd(cam, bg, n_samp, need_depth, need_normal, ranges, vals, bboxes, centers, lengths, geos, rgbs,
                s_val, track_max_w=False, bits=32):
     """forward.cu:41-564 (SDF) -> dict of outputs in the reference layouts.  ``bits=64``

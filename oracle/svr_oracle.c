@@ -42,6 +42,12 @@ typedef float real;
  * atomics).  Default 1 so results are deterministic; the CPU baseline raises it. */
 static int g_threads = 1;
 void svo_set_threads(int n) { g_threads = n > 0 ? n : 1; }
+
+/* Optional pixel mask (uint8[H*W], nonzero = render) for the per-ray checks: masked-out
+ * pixels are skipped by both render passes (their outputs stay as the caller initialised
+ * them; they contribute no gradient).  NULL renders every pixel. */
+static const uint8_t* g_pixel_mask = NULL;
+void svo_set_pixel_mask(const uint8_t* mask) { g_pixel_mask = mask; }
 int svo_get_threads(void) { return g_threads; }
 
 typedef struct { float x, y, z; } f3;
@@ -285,6 +291,7 @@ void svo_render_fwd(int W, int H, float tanfovx, float tanfovy, float cx, float 
         uint32_t tl = r0;
         for (int py = ty * TILE; py < ty * TILE + TILE && py < H; ++py)
         for (int px = tx * TILE; px < tx * TILE + TILE && px < W; ++px) {
+            if (g_pixel_mask && !g_pixel_mask[py * W + px]) continue;
             r3 ro, rd, rd_inv; real rni;
             ray_of_pixel(px, py, W, H, tanfovx, tanfovy, cx, cy, c2w, &ro, &rd, &rd_inv, &rni);
             const int pq = ray_quadrant(rd);
@@ -424,6 +431,7 @@ void svo_render_bwd(int W, int H, float tanfovx, float tanfovy, float cx, float 
         const uint32_t r0 = ranges[2 * tile], r1 = tile_last[tile];
         for (int py = ty * TILE; py < ty * TILE + TILE && py < H; ++py)
         for (int px = tx * TILE; px < tx * TILE + TILE && px < W; ++px) {
+            if (g_pixel_mask && !g_pixel_mask[py * W + px]) continue;
             r3 ro, rd, rd_inv; real rni;
             ray_of_pixel(px, py, W, H, tanfovx, tanfovy, cx, cy, c2w, &ro, &rd, &rd_inv, &rni);
             const int pq = ray_quadrant(rd);

@@ -80,6 +80,9 @@ _SIGS = {
     "svr_mc_emit": (_I, [_I64, _P, _P, _P, _F, _I64, _I, _P, _P, _P, C.POINTER(C.c_int64), _P]),
     "svr_adam_step": (_I, [_I64, _I, _I, _P, _P, _P, _P, _D, _D, _D, _D, _F, _P]),
     "svr_adam_coef_table": (_I, [_I, _D, _D, _D, _I64, _P]),
+    "svr_sh_eval_views_bf16": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P]),
+    "svr_adam_step_bf16": (_I, [_I64, _I, _I, _P, _P, _P, _P, _D, _D, _D, _D, _F, _P]),
+    "svr_adam_step_bf16_at": (_I, [_I64, _I, _I, _P, _P, _P, _P, _P, _I64, _P, _D, _D, _F, _P, _P]),
     "svr_adam_step_at": (_I, [_I64, _I, _I, _P, _P, _P, _P, _P, _I64, _P, _D, _D, _F, _P, _P]),
     "svr_counter_add": (_I, [_P, _I64, _P]),
 }

@@ -3,6 +3,7 @@
 // HBM-bound elementwise/gather work, mapped one thread per (voxel, corner) or per element
 // with 16-byte accesses where the layout allows.
 #include <cmath>
+#include <cuda_bf16.h>
 #include <string>
 
 #include "svr_common.cuh"
@@ -215,18 +216,35 @@ extern "C" int svr_sh_eval_bw(int N, int64_t n_idx, const int64_t* idx, int degr
 // Multi-view SH: one thread per voxel reads its coefficients once and serves every view
 // (forward writes rgbs[v, i]; the adjoint sums the views' colour gradients into one
 // coefficient gradient).  Same per-view arithmetic as sh_compute.cu:55-176.
-template <int DEG>
+// Coefficient storage: float3, or bf16 triples (converted exactly to f32 on load; all SH
+// arithmetic, compositing and gradient accumulation stay f32).
+struct ShF32 {
+    const float3* sh0;
+    const float3* shs;
+    __device__ __forceinline__ float3 dc(int64_t i) const { return sh0[i]; }
+    __device__ __forceinline__ float3 rest(int64_t j) const { return shs[j]; }
+};
+struct ShBF16 {
+    const __nv_bfloat16* sh0;
+    const __nv_bfloat16* shs;
+    __device__ __forceinline__ static float3 get(const __nv_bfloat16* p, int64_t j) {
+        return f3(__bfloat162float(p[3 * j]), __bfloat162float(p[3 * j + 1]), __bfloat162float(p[3 * j + 2]));
+    }
+    __device__ __forceinline__ float3 dc(int64_t i) const { return get(sh0, i); }
+    __device__ __forceinline__ float3 rest(int64_t j) const { return get(shs, j); }
+};
+
+template <int DEG, typename Coef>
 __global__ void sh_views_kernel(int N, int V, int M, const float3* __restrict__ centers,
-                                const float3* __restrict__ cam_pos, const float3* __restrict__ sh0,
-                                const float3* __restrict__ shs, float3* __restrict__ rgbs)
+                                const float3* __restrict__ cam_pos, Coef sh, float3* __restrict__ rgbs)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     constexpr int NB = (DEG + 1) * (DEG + 1);
     float3 c[NB];
-    c[0] = sh0[i];
+    c[0] = sh.dc(i);
 #pragma unroll
-    for (int k = 1; k < NB; ++k) c[k] = shs[i * (M - 1) + k - 1];
+    for (int k = 1; k < NB; ++k) c[k] = sh.rest(i * (M - 1) + k - 1);
     const float3 ctr = centers[i];
     for (int v = 0; v < V; ++v) {
         float3 dir = ctr - cam_pos[v];
@@ -271,24 +289,42 @@ __global__ void sh_views_bw_kernel(int N, int V, int M, const float3* __restrict
     for (int k = 1; k < NB; ++k) dshs[i * (M - 1) + k - 1] = acc[k];
 }
 
+template <typename Coef>
+static int sh_views_launch(int degree, int N, int V, int M, const float3* c, const float3* cp, Coef sh, float3* o,
+                           void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned g = nblk(N, 128);
+    switch (degree) {
+        case 0: sh_views_kernel<0, Coef><<<g, 128, 0, st>>>(N, V, M, c, cp, sh, o); break;
+        case 1: sh_views_kernel<1, Coef><<<g, 128, 0, st>>>(N, V, M, c, cp, sh, o); break;
+        case 2: sh_views_kernel<2, Coef><<<g, 128, 0, st>>>(N, V, M, c, cp, sh, o); break;
+        default: sh_views_kernel<3, Coef><<<g, 128, 0, st>>>(N, V, M, c, cp, sh, o); break;
+    }
+    LAUNCHED();
+    return SVR_OK;
+}
+
 extern "C" int svr_sh_eval_views(int N, int n_views, int degree, int M, const float* centers, const float* cam_pos,
                                  const float* sh0, const float* shs, float* rgbs, void* stream)
 {
     if (degree < 0 || degree > 3 || M < (degree + 1) * (degree + 1) || n_views <= 0)
         return svr_fail(SVR_ERR_ARG, "sh views: bad degree / view count");
     if (N <= 0) return SVR_OK;
-    cudaStream_t st = (cudaStream_t)stream;
-    const unsigned g = nblk(N, 128);
-    auto c = (const float3*)centers; auto cp = (const float3*)cam_pos; auto s0 = (const float3*)sh0;
-    auto ss = (const float3*)shs; auto o = (float3*)rgbs;
-    switch (degree) {
-        case 0: sh_views_kernel<0><<<g, 128, 0, st>>>(N, n_views, M, c, cp, s0, ss, o); break;
-        case 1: sh_views_kernel<1><<<g, 128, 0, st>>>(N, n_views, M, c, cp, s0, ss, o); break;
-        case 2: sh_views_kernel<2><<<g, 128, 0, st>>>(N, n_views, M, c, cp, s0, ss, o); break;
-        default: sh_views_kernel<3><<<g, 128, 0, st>>>(N, n_views, M, c, cp, s0, ss, o); break;
-    }
-    LAUNCHED();
-    return SVR_OK;
+    auto c = (const float3*)centers; auto cp = (const float3*)cam_pos; auto o = (float3*)rgbs;
+    return sh_views_launch(degree, N, n_views, M, c, cp, ShF32{(const float3*)sh0, (const float3*)shs}, o, stream);
+}
+
+extern "C" int svr_sh_eval_views_bf16(int N, int n_views, int degree, int M, const float* centers,
+                                      const float* cam_pos, const uint16_t* sh0, const uint16_t* shs, float* rgbs,
+                                      void* stream)
+{
+    if (degree < 0 || degree > 3 || M < (degree + 1) * (degree + 1) || n_views <= 0)
+        return svr_fail(SVR_ERR_ARG, "sh views: bad degree / view count");
+    if (N <= 0) return SVR_OK;
+    auto c = (const float3*)centers; auto cp = (const float3*)cam_pos; auto o = (float3*)rgbs;
+    return sh_views_launch(degree, N, n_views, M, c, cp,
+                           ShBF16{(const __nv_bfloat16*)sh0, (const __nv_bfloat16*)shs}, o, stream);
 }
 
 extern "C" int svr_sh_eval_views_bw(int N, int n_views, int degree, int M, const float* centers,
@@ -458,6 +494,61 @@ extern "C" int svr_adam_step_at(int64_t numel, int biased, int sparse, float* pa
     if (!coef_table || !step || rows <= 0) return svr_fail(SVR_ERR_ARG, "adam: null coefficient table or step");
     AdamCoef co{0.f, 1.f, coef_table, step, rows, status};
     return adam_launch(numel, biased, sparse, param, grad, exp_avg, exp_avg_sq, co, beta1, beta2, eps, stream);
+}
+
+// Parameters stored in bf16 (SH coefficients in the precision configuration): moments stay
+// f32, the update is computed in f32 from the stored value and rounded to nearest.
+template <bool SPARSE, bool BIASED>
+__global__ void adam_bf16_kernel(int64_t n, __nv_bfloat16* __restrict__ p, const float* __restrict__ g,
+                                 float* __restrict__ m, float* __restrict__ v, AdamCoef co, float b1, float b2,
+                                 float eps)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float step_size, rbc2;
+    if (!adam_coef(co, step_size, rbc2)) return;
+    float P = __bfloat162float(p[i]), Mv = m[i], Vv = v[i];
+    const float G = g[i];
+    if (SPARSE && G == 0.0f) return;
+    adam_one<SPARSE, BIASED>(P, G, Mv, Vv, step_size, b1, b2, rbc2, eps);
+    p[i] = __float2bfloat16_rn(P);
+    m[i] = Mv; v[i] = Vv;
+}
+
+static int adam_bf16_launch(int64_t numel, int biased, int sparse, uint16_t* param, const float* grad, float* m,
+                            float* v, const AdamCoef& co, double beta1, double beta2, float eps, void* stream)
+{
+    if (numel <= 0) return SVR_OK;
+    if (!param || !grad || !m || !v) return svr_fail(SVR_ERR_ARG, "adam bf16: null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned gs = nblk(numel, 256);
+    auto P = (__nv_bfloat16*)param;
+    const float b1 = (float)beta1, b2 = (float)beta2;
+    if (biased && sparse) adam_bf16_kernel<true, true><<<gs, 256, 0, st>>>(numel, P, grad, m, v, co, b1, b2, eps);
+    else if (biased) adam_bf16_kernel<false, true><<<gs, 256, 0, st>>>(numel, P, grad, m, v, co, b1, b2, eps);
+    else if (sparse) adam_bf16_kernel<true, false><<<gs, 256, 0, st>>>(numel, P, grad, m, v, co, b1, b2, eps);
+    else adam_bf16_kernel<false, false><<<gs, 256, 0, st>>>(numel, P, grad, m, v, co, b1, b2, eps);
+    LAUNCHED();
+    return SVR_OK;
+}
+
+extern "C" int svr_adam_step_bf16(int64_t numel, int biased, int sparse, uint16_t* param, const float* grad,
+                                  float* exp_avg, float* exp_avg_sq, double step, double lr, double beta1,
+                                  double beta2, float eps, void* stream)
+{
+    AdamCoef co{};
+    adam_host_coefs(biased, step, lr, beta1, beta2, co.step_size, co.rbc2);
+    return adam_bf16_launch(numel, biased, sparse, param, grad, exp_avg, exp_avg_sq, co, beta1, beta2, eps, stream);
+}
+
+extern "C" int svr_adam_step_bf16_at(int64_t numel, int biased, int sparse, uint16_t* param, const float* grad,
+                                     float* exp_avg, float* exp_avg_sq, const float* coef_table, int64_t rows,
+                                     const int64_t* step, double beta1, double beta2, float eps, uint32_t* status,
+                                     void* stream)
+{
+    if (!coef_table || !step || rows <= 0) return svr_fail(SVR_ERR_ARG, "adam: null coefficient table or step");
+    AdamCoef co{0.f, 1.f, coef_table, step, rows, status};
+    return adam_bf16_launch(numel, biased, sparse, param, grad, exp_avg, exp_avg_sq, co, beta1, beta2, eps, stream);
 }
 
 __global__ void counter_add_kernel(int64_t* c, int64_t d) { *c += d; }

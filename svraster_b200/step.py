@@ -25,7 +25,11 @@ from . import utils
 class BatchedTrainStep:
 
     def __init__(self, scene, cams, device="cuda", lr=(1e-3, 1e-3, 1e-4), betas=(0.1, 0.99), eps=1e-15,
-                 lambda_ls=1e-3, lambda_ge=1e-3, lambda_R_concen=0.0, sh_degree=3, seed=0, fused_smoothness=True):
+                 lambda_ls=1e-3, lambda_ge=1e-3, lambda_R_concen=0.0, sh_degree=3, seed=0, fused_smoothness=True,
+                 sh_dtype="f32"):
+        """``sh_dtype="bf16"`` stores the SH coefficients in bf16 (the precision configuration):
+        colours, compositing, transmittance and every gradient stay f32, Adam keeps f32 moments
+        and rounds the updated coefficients to nearest bf16."""
         dev = torch.device(device)
         self.dev = dev
         t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
@@ -36,8 +40,12 @@ class BatchedTrainStep:
         self.is_leaf = t(scene.is_leaf, torch.uint8)
         self.vox_key = t(scene.vox_key, torch.int64)
         self.grid = t(scene.geo_grid_pts)
-        self.sh0 = t(scene.sh0)
-        self.shs = t(scene.shs)
+        if sh_dtype not in ("f32", "bf16"):
+            raise ValueError("sh_dtype must be 'f32' or 'bf16'")
+        self.sh_bf16 = sh_dtype == "bf16"
+        sh_t = torch.bfloat16 if self.sh_bf16 else torch.float32
+        self.sh0 = t(scene.sh0).to(sh_t).contiguous()
+        self.shs = t(scene.shs).to(sh_t).contiguous()
         self.M_sh = 1 + scene.shs.shape[1]
         self.sh_degree = sh_degree
         self.s_val = torch.tensor([scene.s_val], dtype=torch.float32, device=dev)
@@ -51,8 +59,9 @@ class BatchedTrainStep:
         self.lr, self.betas, self.eps = lr, betas, eps
         self.lambda_R = float(lambda_R_concen)
         self.params = [self.grid, self.sh0, self.shs]
-        self.adam_m = [torch.zeros_like(p) for p in self.params]
-        self.adam_v = [torch.zeros_like(p) for p in self.params]
+        self.param_bf16 = [False, self.sh_bf16, self.sh_bf16]
+        self.adam_m = [torch.zeros(p.shape, dtype=torch.float32, device=dev) for p in self.params]
+        self.adam_v = [torch.zeros(p.shape, dtype=torch.float32, device=dev) for p in self.params]
         self.adam_step = 0
         # dense-grid table for the smoothness losses (rebuilt only on prune / subdivide)
         lv_max = int(scene.octlevel.max())
@@ -86,7 +95,7 @@ class BatchedTrainStep:
         self.dvox = torch.zeros(self.N, 12, device=dev)
         self.drgbs = torch.zeros(self.V * self.N, 3, device=dev)
         self.ds = torch.zeros(1, device=dev)
-        self.grads = [torch.zeros_like(p) for p in self.params]
+        self.grads = [torch.zeros(p.shape, dtype=torch.float32, device=dev) for p in self.params]
         self.all_idx = torch.arange(self.N, dtype=torch.int64, device=dev)
         self.state = None
         self.ev = None
@@ -128,8 +137,9 @@ class BatchedTrainStep:
         mark("start")
         check(L.svr_gather_geo(N, ptr(self.all_idx), ptr(self.vox_key), ptr(self.grid), ptr(self.geos), st),
               "gather")
-        check(L.svr_sh_eval_views(N, self.V, self.sh_degree, self.M_sh, ptr(self.centers), ptr(self.cam_pos),
-                                  ptr(self.sh0), ptr(self.shs), ptr(self.rgbs), st), "sh views")
+        sh_eval = L.svr_sh_eval_views_bf16 if self.sh_bf16 else L.svr_sh_eval_views
+        check(sh_eval(N, self.V, self.sh_degree, self.M_sh, ptr(self.centers), ptr(self.cam_pos),
+                      ptr(self.sh0), ptr(self.shs), ptr(self.rgbs), st), "sh views")
         mark("gather+sh")
         state = RasterState(self.views, N, self.dev)
         state.preprocess(self.octpath, self.centers, self.lengths, self.is_leaf)
@@ -187,14 +197,16 @@ class BatchedTrainStep:
             mark("allreduce")
         if graph:
             check(L.svr_counter_add(ptr(self.step_dev), 1, st), "counter")
-            for p, g, m, v, tab in zip(self.params, self.grads, self.adam_m, self.adam_v, self.coef_tables):
-                check(L.svr_adam_step_at(p.numel(), 0, 0, ptr(p), ptr(g), ptr(m), ptr(v), ptr(tab), self.coef_rows,
-                                         ptr(self.step_dev), self.betas[0], self.betas[1], self.eps,
-                                         ptr(self.status), st), "adam")
+            for p, g, m, v, tab, bf in zip(self.params, self.grads, self.adam_m, self.adam_v, self.coef_tables,
+                                           self.param_bf16):
+                fn = L.svr_adam_step_bf16_at if bf else L.svr_adam_step_at
+                check(fn(p.numel(), 0, 0, ptr(p), ptr(g), ptr(m), ptr(v), ptr(tab), self.coef_rows,
+                         ptr(self.step_dev), self.betas[0], self.betas[1], self.eps, ptr(self.status), st), "adam")
         else:
-            for p, g, m, v, lr in zip(self.params, self.grads, self.adam_m, self.adam_v, self.lr):
-                check(L.svr_adam_step(p.numel(), 0, 0, ptr(p), ptr(g), ptr(m), ptr(v), float(self.adam_step + 1),
-                                      float(lr), self.betas[0], self.betas[1], self.eps, st), "adam")
+            for p, g, m, v, lr, bf in zip(self.params, self.grads, self.adam_m, self.adam_v, self.lr, self.param_bf16):
+                fn = L.svr_adam_step_bf16 if bf else L.svr_adam_step
+                check(fn(p.numel(), 0, 0, ptr(p), ptr(g), ptr(m), ptr(v), float(self.adam_step + 1),
+                         float(lr), self.betas[0], self.betas[1], self.eps, st), "adam")
         mark("adam")
         self.state = state
         self.ev = marks if time_render else None

@@ -294,6 +294,11 @@ def scene_mid(seed=0):
     return build_scene(sdf_spheres_torus, 6, 10, seed=seed, band=0.35, keep=2.0, kept_parent_frac=0.02)
 
 
+def scene_precision(seed=0):
+    """The mid-size procedure (3 spheres + torus) carried to level 11: about 7.9M voxels."""
+    return build_scene(sdf_spheres_torus, 6, 11, seed=seed, band=0.42, keep=1.6, kept_parent_frac=0.02)
+
+
 def scene_batched(seed=0):
     """Sphere with 64 Gaussian bumps (amplitude 0.05) at levels 7-11, about 4M voxels."""
     return build_scene(make_bumpy_sphere(seed=seed), 7, 11, seed=seed, band=0.42, keep=1.1, kept_parent_frac=0.02)

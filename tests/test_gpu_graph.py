@@ -141,3 +141,29 @@ def test_eager_step_after_replays_resyncs_counter():
     assert int(b.step_dev.item()) == 3
     for pa, pb, lr in zip(a.params, b.params, a.lr):
         assert _param_close(pa, pb, lr)
+
+
+def test_bf16_sh_step_eager_and_replay():
+    """SH coefficients stored in bf16: the step keeps them bf16, replay equals eager, and the
+    first image stays within the bf16 storage step of the f32 step's image."""
+    sc = S.scene_small(seed=2)
+    cams = S.fibonacci_cameras(3, 3.0, 144, 112, fovx_deg=50.0)
+    a = BatchedTrainStep(sc, cams, device="cuda", lambda_R_concen=0.1, sh_dtype="bf16")
+    b = BatchedTrainStep(sc, cams, device="cuda", lambda_R_concen=0.1, sh_dtype="bf16")
+    f = BatchedTrainStep(sc, cams, device="cuda", lambda_R_concen=0.1)
+    b.capture()
+    ca, _ = a.step()
+    cb, _ = b.replay()
+    cf, _ = f.step()
+    torch.cuda.synchronize()
+    assert a.sh0.dtype == torch.bfloat16 and a.shs.dtype == torch.bfloat16
+    assert torch.equal(ca, cb)
+    assert (ca - cf).abs().max().item() < 2e-2
+    for _ in range(2):
+        a.step()
+        b.replay()
+    torch.cuda.synchronize()
+    assert b.graph_status() == (0, 0)
+    assert _param_close(a.grid, b.grid, a.lr[0])
+    d = (a.sh0.float() - b.sh0.float()).abs()
+    assert (d > 0).float().mean().item() < 2e-3
