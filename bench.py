@@ -116,15 +116,20 @@ class ClockSampler:
 
 
 def load_traffic(kernel, workload):
-    path = os.path.join(ROOT, "profiles", "traffic.json")
+    """DRAM bytes per launch of `kernel` on `workload` from the ncu summary table in
+    profiles/traffic.md (None when the workload was not captured)."""
+    path = os.path.join(ROOT, "profiles", "traffic.md")
     if not os.path.exists(path):
         return None
     with open(path) as f:
-        d = json.load(f)
-    e = d.get(kernel)
-    if not e or e.get("workload") != workload:
-        return None
-    return e.get("bytes_per_launch")
+        for line in f:
+            cells = [c.strip() for c in line.strip().strip("|").split("|")]
+            if len(cells) == 3 and cells[0] == kernel and cells[1] == workload:
+                try:
+                    return int(cells[2])
+                except ValueError:
+                    return None
+    return None
 
 
 # ----------------------------------------------------------------------------- our arm
