@@ -1,0 +1,235 @@
+"""GPU adjoint against FP64 central finite differences on the mid-size workload.
+
+The 8 views of 800x800 of the benchmark scene are rendered and differentiated on the GPU
+(f32) with seeded N(0,1) upstream gradients on colour, mean depth and normal, giving
+dL/dgrid (corner SDF values scattered to grid points) and dL/dsh0.  For a random subset of
+voxels with a nonzero gradient, one corner grid point (and, for a quarter of them, one sh0
+channel) is perturbed by +-h and L is re-evaluated in double precision by the C oracle
+(libsvr_oracle64).  Only pixels inside the pixel bboxes of the voxels touching the perturbed
+parameter can change, so each evaluation renders just those pixels.
+
+h = 1e-5: with s = ln(99) / (4 h_min) ~ 588 the central-difference truncation error grows as
+h^2 s^2 / 6 (about 6e-4 relative at h = 1e-4, 6e-6 at 1e-5).
+
+Default: 128 probed voxels.  SVR_FD_FULL=1 probes 1024.  SVR_FD_OUT=<path> writes the errors.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from svraster_b200 import _lib
+from svraster_b200 import synthetic as S
+from svraster_b200._lib import check, ptr, stream_ptr
+from svraster_b200.raster import RasterState
+
+pytestmark = pytest.mark.gpu
+
+N_VOX = 1024 if os.environ.get("SVR_FD_FULL") == "1" else 128
+H_STEP = 1e-5
+C0 = 0.28209479177387814
+
+
+def test_adjoint_matches_fp64_central_differences_mid():
+    from oracle import oracle as O
+    from tests.test_gpu_precision import sh_eval64
+    dev = torch.device("cuda")
+    sc = S.scene_mid(seed=0)
+    cams = S.fibonacci_cameras(8, 3.0, 800, 800, fovx_deg=50.0)
+    N, V = sc.n_vox, len(cams)
+    rng = np.random.default_rng(7)
+    grads = []
+    for cam in cams:
+        P = cam.width * cam.height
+        grads.append(dict(color=rng.normal(size=(3, P)).astype(np.float32),
+                          depth=np.concatenate([rng.normal(size=(1, P)), np.zeros((3, P))]).astype(np.float32),
+                          normal=rng.normal(size=(3, P)).astype(np.float32), T=np.zeros(P, np.float32)))
+
+    # ---- GPU forward + adjoint (f32)
+    L = _lib.load()
+    st = stream_ptr(dev)
+    f32 = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
+    octpath, centers = f32(sc.octpath, torch.int64), f32(sc.vox_center)
+    lengths, is_leaf = f32(sc.vox_size).reshape(-1).contiguous(), f32(sc.is_leaf, torch.uint8)
+    vox_key, grid = f32(sc.vox_key, torch.int64), f32(sc.geo_grid_pts)
+    sh0, shs = f32(sc.sh0), f32(sc.shs)
+    cam_pos = torch.stack([f32(c.c2w)[:3, 3] for c in cams]).contiguous()
+    s_val = torch.tensor([sc.s_val], dtype=torch.float32, device=dev)
+    views = [dict(width=c.width, height=c.height, tanfovx=c.tanfovx, tanfovy=c.tanfovy, cx=c.cx, cy=c.cy,
+                  near=c.near, w2c=f32(c.w2c), c2w=f32(c.c2w), bg=torch.zeros(3, device=dev)) for c in cams]
+    geos = torch.empty(N, 8, device=dev)
+    idx = torch.arange(N, dtype=torch.int64, device=dev)
+    check(L.svr_gather_geo(N, ptr(idx), ptr(vox_key), ptr(grid), ptr(geos), st), "gather")
+    rgbs = torch.empty(V * N, 3, device=dev)
+    check(L.svr_sh_eval_views(N, V, 3, 16, ptr(centers), ptr(cam_pos), ptr(sh0), ptr(shs), ptr(rgbs), st), "sh")
+    state = RasterState(views, N, dev)
+    state.preprocess(octpath, centers, lengths, is_leaf)
+    state.bin(octpath)
+    _, _, _, T, _ = state.render(3, True, True, centers, lengths, geos, rgbs, s_val, rgb_per_view=True)
+    pk = {k: torch.as_tensor(np.concatenate([g[k].reshape(-1) for g in grads])).to(dev)
+          for k in ("color", "depth", "normal", "T")}
+    dvox = torch.zeros(N, 12, device=dev)
+    drgbs = torch.zeros(V * N, 3, device=dev)
+    ds = torch.zeros(1, device=dev)
+    state.render_backward(True, True, s_val, T, pk["color"], pk["depth"], pk["normal"], pk["T"], drgbs=drgbs,
+                          dvox=dvox, ds=ds)
+    dgrid = torch.zeros_like(grid)
+    check(L.svr_scatter_vox_grads(N, 12, ptr(vox_key), ptr(dvox), ptr(dgrid), st), "scatter")
+    dsh0 = torch.zeros(N, 3, device=dev)
+    dshs = torch.zeros(N, 15, 3, device=dev)
+    check(L.svr_sh_eval_views_bw(N, V, 3, 16, ptr(centers), ptr(cam_pos), ptr(drgbs), ptr(dsh0), ptr(dshs), st),
+          "sh bw")
+    torch.cuda.synchronize()
+    assert state.status() == 0
+    dgrid = dgrid.cpu().numpy().reshape(-1).astype(np.float64)
+    dsh0 = dsh0.cpu().numpy().astype(np.float64)
+    rgbs_np = rgbs.cpu().numpy().reshape(V, N, 3).astype(np.float64)
+    dv = dvox.cpu().numpy()
+    del state, rgbs, drgbs, dvox
+    torch.cuda.empty_cache()
+
+    # ---- FP64 finite differences through the oracle on the affected pixels only
+    O.set_threads(os.cpu_count() or 1)
+    geos64 = sc.geo_grid_pts.reshape(-1).astype(np.float64)[sc.vox_key]
+    per_view = []
+    for v, cam in enumerate(cams):
+        nd, bb, bits = O.preprocess(cam, sc.vox_center, sc.vox_size, sc.is_leaf)
+        _, vals, ranges = O.binning(cam, sc.octpath, nd, bb, bits)
+        per_view.append((nd, bb, vals, ranges))
+    # voxels sharing each grid point
+    order = np.argsort(sc.vox_key.reshape(-1), kind="stable")
+    keys_sorted = sc.vox_key.reshape(-1)[order]
+
+    def voxels_of_point(k):
+        lo, hi = np.searchsorted(keys_sorted, k), np.searchsorted(keys_sorted, k, side="right")
+        return np.unique(order[lo:hi] // 8)
+
+    def loss(vox_set, geos_x, rgb_override=None):
+        """L over the pixels the voxels in vox_set can reach, FP64."""
+        total = 0.0
+        for v, cam in enumerate(cams):
+            nd, bb, vals, ranges = per_view[v]
+            vis = vox_set[nd[vox_set] > 0]
+            if len(vis) == 0:
+                continue
+            W, H = cam.width, cam.height
+            mask = np.zeros((H, W), np.uint8)
+            for i in vis:
+                x0, y0, x1, y1 = bb[i, 0] >> 16, bb[i, 0] & 0xFFFF, bb[i, 1] >> 16, bb[i, 1] & 0xFFFF
+                mask[y0:min(y1, H - 1) + 1, x0:min(x1, W - 1) + 1] = 1
+            rg = rgbs_np[v]
+            if rgb_override is not None:
+                rg = rg.copy()
+                rg[rgb_override[0]] = rgb_override[1][v]
+            O.set_pixel_mask(mask.reshape(-1), bits=64)
+            try:
+                f = O.render_fwd(cam, np.zeros(3, np.float32), 3, True, True, ranges, vals, bb, sc.vox_center,
+                                 sc.vox_size, geos_x, rg, sc.s_val, bits=64)
+            finally:
+                O.set_pixel_mask(None, bits=64)
+            g = grads[v]
+            P = W * H
+            total += (np.dot(g["color"].reshape(-1).astype(np.float64), f["color"].reshape(-1))
+                      + np.dot(g["depth"][0].astype(np.float64), f["depth"].reshape(4, P)[0])
+                      + np.dot(g["normal"].reshape(-1).astype(np.float64), f["normal"].reshape(-1)))
+        return total
+
+    # FP64 adjoint of the same model (oracle, full images): separates the finite-difference
+    # effects of discrete decisions (early stop, MIN_ALPHA) from the f32 rounding of the GPU
+    dvox64 = np.zeros((N, 12))
+    drgb64 = np.zeros((N, 3))
+    for v, cam in enumerate(cams):
+        nd, bb, vals, ranges = per_view[v]
+        bg = np.zeros(3, np.float32)
+        f = O.render_fwd(cam, bg, 3, True, True, ranges, vals, bb, sc.vox_center, sc.vox_size, geos64, rgbs_np[v],
+                         sc.s_val, bits=64)
+        g = grads[v]
+        d64, _ = O.render_bwd(cam, bg, True, True, ranges, f["tile_last"], vals, bb, sc.vox_center, sc.vox_size,
+                              geos64, rgbs_np[v], sc.s_val, f["T"], f["n_contrib"], g["color"], g["depth"],
+                              g["normal"], g["T"], bits=64)
+        dvox64 += d64
+        drgb64 += d64[:, 8:11]
+    dgrid64 = np.zeros(len(dgrid))
+    np.add.at(dgrid64, sc.vox_key.reshape(-1), dvox64[:, :8].reshape(-1))
+    dsh0_64 = C0 * drgb64
+    # the same adjoint in f32 with the reference's expression order (the float oracle build):
+    # the rounding any f32 implementation of the reference algorithm carries
+    dvox32 = np.zeros((N, 12), np.float32)
+    drgb32 = np.zeros((N, 3), np.float32)
+    geos32 = sc.geo_grid_pts.reshape(-1)[sc.vox_key]
+    for v, cam in enumerate(cams):
+        nd, bb, vals, ranges = per_view[v]
+        bg = np.zeros(3, np.float32)
+        rg32 = rgbs_np[v].astype(np.float32)
+        f = O.render_fwd(cam, bg, 3, True, True, ranges, vals, bb, sc.vox_center, sc.vox_size, geos32, rg32,
+                         sc.s_val)
+        g = grads[v]
+        d32, _ = O.render_bwd(cam, bg, True, True, ranges, f["tile_last"], vals, bb, sc.vox_center, sc.vox_size,
+                              geos32, rg32, sc.s_val, f["T"], f["n_contrib"], g["color"], g["depth"], g["normal"],
+                              g["T"])
+        dvox32 += d32
+        drgb32 += d32[:, 8:11]
+    dgrid32 = np.zeros(len(dgrid), np.float32)
+    np.add.at(dgrid32, sc.vox_key.reshape(-1), dvox32[:, :8].reshape(-1))
+    dsh0_32 = np.float32(C0) * drgb32
+
+    cand = np.nonzero(np.abs(dv[:, :8]).sum(1) > 0)[0]
+    pick = rng.choice(cand, min(N_VOX, len(cand)), replace=False)
+    rows = []
+    for n_i, vi in enumerate(pick):
+        corner = int(rng.integers(8))
+        k = int(sc.vox_key[vi, corner])
+        vs = voxels_of_point(k)
+        hit = sc.vox_key[vs] == k
+        gp, gm = geos64.copy(), geos64.copy()
+        gp[vs] += np.where(hit, H_STEP, 0.0)
+        gm[vs] -= np.where(hit, H_STEP, 0.0)
+        fd = (loss(vs, gp) - loss(vs, gm)) / (2 * H_STEP)
+        rows.append(("grid", fd, dgrid[k], dgrid64[k], float(dgrid32[k])))
+        if n_i % 4 == 0:
+            ch = int(rng.integers(3))
+            one = np.array([vi])
+            rgb_pm = []
+            for sgn in (1.0, -1.0):
+                s0 = sc.sh0[one].astype(np.float64)
+                s0[0, ch] += sgn * H_STEP
+                rgb_pm.append(np.stack([sh_eval64(sc.vox_center[one].astype(np.float64),
+                                                  c.position.astype(np.float64), s0,
+                                                  sc.shs[one].astype(np.float64))[0] for c in cams]))
+            fd_sh = (loss(one, geos64, (vi, rgb_pm[0])) - loss(one, geos64, (vi, rgb_pm[1]))) / (2 * H_STEP)
+            rows.append(("sh0", fd_sh, dsh0[vi, ch], dsh0_64[vi, ch], float(dsh0_32[vi, ch])))
+
+    fd = np.array([r[1] for r in rows])
+    gpu = np.array([r[2] for r in rows])
+    a64 = np.array([r[3] for r in rows])
+    a32 = np.array([r[4] for r in rows])
+    kinds = np.array([r[0] for r in rows])
+
+    def stats(x, ref):
+        scale = np.maximum(np.abs(ref), 1e-3 * np.abs(ref).max())
+        rel = np.abs(x - ref) / scale
+        return {"median": float(np.median(rel)), "p90": float(np.quantile(rel, 0.9)),
+                "p95": float(np.quantile(rel, 0.95)), "p99": float(np.quantile(rel, 0.99)),
+                "max": float(rel.max()), "frac_below_1e-4": float((rel < 1e-4).mean()),
+                "frac_below_1e-3": float((rel < 1e-3).mean())}
+    report = {"probes": int(len(rows)), "grid_probes": int((kinds == "grid").sum()),
+              "sh0_probes": int((kinds == "sh0").sum()), "h": H_STEP,
+              "gpu_f32_vs_fd": stats(gpu, fd), "fp64_adjoint_vs_fd": stats(a64, fd),
+              "gpu_f32_vs_fp64_adjoint": stats(gpu, a64), "reference_order_f32_vs_fp64_adjoint": stats(a32, a64)}
+    report["rel_err"] = report["gpu_f32_vs_fd"]
+    print("FD_MID", json.dumps(report))
+    if os.environ.get("SVR_FD_OUT"):
+        with open(os.environ["SVR_FD_OUT"], "w") as fh:
+            json.dump(report, fh, indent=1)
+    # the adjoint itself: the f32 GPU path against the FP64 adjoint of the same model, no
+    # worse than a small factor of the rounding of an f32 evaluation in the reference's order
+    g64, r64 = report["gpu_f32_vs_fp64_adjoint"], report["reference_order_f32_vs_fp64_adjoint"]
+    assert g64["median"] < 2e-4, report
+    assert g64["p95"] < max(2e-3, 2.0 * r64["p95"]), report
+    # against finite differences the median holds; the far tail is shared with the FP64
+    # adjoint (discrete decisions at the early-stop and MIN_ALPHA thresholds)
+    assert report["gpu_f32_vs_fd"]["median"] < 2e-4, report
