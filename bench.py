@@ -157,6 +157,11 @@ def run_ours(args, rank, world):
     use_graph = world == 1 and not args.no_graph
     for _ in range(args.warmup):
         step.step(grad_hook=hook)
+    # the render launch configuration is chosen on this batch before anything is timed
+    tuned = None
+    if not args.no_autotune:
+        tuned = step.autotune()
+        step.step(grad_hook=hook)   # the tuner reused the gradient buffers: one clean step
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -197,6 +202,7 @@ def run_ours(args, rank, world):
             raise RuntimeError(f"graph replay status raster={st_raster} misc={st_misc}")
         graph_info = {"captured": True, "kernels_per_step": per_step, "record_capacity": step.capacity,
                       "eager_ms_per_step": round(eager_ms / args.steps, 3)}
+
     if world > 1:
         t = torch.tensor([total_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -236,7 +242,9 @@ def run_ours(args, rank, world):
                          "parallelism": f"dp{world} over views" if world > 1 else "single GPU"},
               "stages_ms": {k: round(v, 3) for k, v in stage_avg.items()},
               "roofline": roofline, "gpu_launches": int(launches), "clocks": clocks,
-              "cuda_graph": graph_info or {"captured": False}}
+              "cuda_graph": graph_info or {"captured": False},
+              "autotuned_render": ({k: tuned[k] for k in ("fwd_config", "bwd_config", "ms")} if tuned
+                                   else "default configuration")}
     return result, step, scene, cams
 
 
@@ -454,6 +462,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extract", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="time eager steps instead of graph replays")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default render launch configuration")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))

@@ -141,6 +141,16 @@ SVR_API int svr_render_bwd(const svr_view_t* views_host, int n_views, int N, int
                    const float* dL_dnormal, const float* dL_dT,
                    float* dL_dvox, float* drgbs, float* dL_ds, void* stream);
 
+/* Launch configurations of the render kernels (no counterpart in the reference): ring slots
+ * and CTAs per SM, which change the schedule only (every configuration gives the same
+ * outputs).  pass 0 = forward, 1 = adjoint; configuration 0 is the default.  The choice is
+ * process-wide and read when a launch is issued; svraster_b200.autotune times them on the
+ * caller's workload. */
+SVR_API int svr_render_config_count(int* n_fwd, int* n_bwd);
+SVR_API int svr_render_config_describe(int pass, int index, int* ring, int* ctas_per_sm);
+SVR_API int svr_render_set_config(int fwd_index, int bwd_index);
+SVR_API int svr_render_get_config(int* fwd_index, int* bwd_index);
+
 /* Device status word of the raster launches that used this image buffer (0 = clean;
  * bit 1 wait timeout, bit 2 index out of range, bit 4 duplicate count mismatch, bit 8
  * records beyond the binning capacity, bit 16 sort-key format).

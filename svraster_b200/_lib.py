@@ -45,6 +45,10 @@ _SIGS = {
     "svr_unpack_geom": (_I, [_P, _I64, _P, _P, _P, _P]),
     "svr_count_rendered": (_I, [_I64, _P, C.POINTER(C.c_int64), C.POINTER(C.c_uint64), _P]),
     "svr_scan_rendered": (_I, [_I64, _P, _P]),
+    "svr_render_config_count": (_I, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "svr_render_config_describe": (_I, [_I, _I, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "svr_render_set_config": (_I, [_I, _I]),
+    "svr_render_get_config": (_I, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "svr_binning_count": (_I, [_P, C.POINTER(C.c_int64), _P]),
     "svr_workspace_query": (_I, [_I, _I, _I64, _I64, _I, C.POINTER(C.c_size_t)]),
     "svr_binning_buffer_bytes": (_SZ, [_I64, _I]),

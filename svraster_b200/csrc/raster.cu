@@ -601,14 +601,56 @@ static int ensure_smem(K k, int smem, std::atomic<unsigned long long>& done)
     return SVR_OK;
 }
 
-template <int NS, bool DEPTH, bool NORMAL, bool MAXW>
-static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
-                      const Rec* recs,
-                      const float* s_val, uint32_t* tile_last, uint32_t* n_contrib, float* color, float* depth,
-                      float* normal, float* outT, float* max_w, unsigned* status)
+// Launch configurations (ring slots, CTAs per SM) the tuner chooses between for the
+// common flag sets (three sub-samples, depth and normal on; with or without the
+// R-concentration term).  Index 0 is the default build configuration.  The choice is process-
+// wide and read when a launch is issued (so a captured graph keeps the one in force then).
+struct RenderCfg { int ring, minb; };
+static const RenderCfg kFwdCfgs[] = {{SVR_NSLOT, SVR_FWD_MINB}, {3, 4}, {4, 3}, {3, 3}};
+static const RenderCfg kBwdCfgs[] = {{SVR_NSLOT, SVR_BWD_MINB}, {3, 3}, {4, 2}, {3, 2}};
+constexpr int N_FWD_CFGS = 4, N_BWD_CFGS = 4;
+static std::atomic<int> g_fwd_cfg{0}, g_bwd_cfg{0};
+
+extern "C" int svr_render_config_count(int* n_fwd, int* n_bwd)
 {
-    auto k = render_fwd_kernel<NS, DEPTH, NORMAL, MAXW>;
-    const int smem = (int)sizeof(FwdSmem);
+    if (n_fwd) *n_fwd = N_FWD_CFGS;
+    if (n_bwd) *n_bwd = N_BWD_CFGS;
+    return SVR_OK;
+}
+
+extern "C" int svr_render_config_describe(int pass, int index, int* ring, int* ctas_per_sm)
+{
+    const int n = pass == 0 ? N_FWD_CFGS : N_BWD_CFGS;
+    if (index < 0 || index >= n) return svr_fail(SVR_ERR_ARG, "render config index");
+    const RenderCfg c = pass == 0 ? kFwdCfgs[index] : kBwdCfgs[index];
+    if (ring) *ring = c.ring;
+    if (ctas_per_sm) *ctas_per_sm = c.minb;
+    return SVR_OK;
+}
+
+extern "C" int svr_render_set_config(int fwd_index, int bwd_index)
+{
+    if (fwd_index < 0 || fwd_index >= N_FWD_CFGS || bwd_index < 0 || bwd_index >= N_BWD_CFGS)
+        return svr_fail(SVR_ERR_ARG, "render config index");
+    g_fwd_cfg.store(fwd_index);
+    g_bwd_cfg.store(bwd_index);
+    return SVR_OK;
+}
+
+extern "C" int svr_render_get_config(int* fwd_index, int* bwd_index)
+{
+    if (fwd_index) *fwd_index = g_fwd_cfg.load();
+    if (bwd_index) *bwd_index = g_bwd_cfg.load();
+    return SVR_OK;
+}
+
+template <int NS, bool DEPTH, bool NORMAL, bool MAXW, int RING, int MINB>
+static int launch_fwd_cfg(int T, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
+                          const Rec* recs, const float* s_val, uint32_t* tile_last, uint32_t* n_contrib,
+                          float* color, float* depth, float* normal, float* outT, float* max_w, unsigned* status)
+{
+    auto k = render_fwd_kernel<NS, DEPTH, NORMAL, MAXW, RING, MINB>;
+    const int smem = (int)sizeof(FwdSmem<RING>);
     static std::atomic<unsigned long long> done{0};
     int rc = ensure_smem(k, smem, done);
     if (rc) return rc;
@@ -616,6 +658,25 @@ static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint32_t* or
                               depth, normal, outT, max_w, status);
     LAUNCH_CHECK();
     return SVR_OK;
+}
+
+template <int NS, bool DEPTH, bool NORMAL, bool MAXW>
+static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
+                      const Rec* recs,
+                      const float* s_val, uint32_t* tile_last, uint32_t* n_contrib, float* color, float* depth,
+                      float* normal, float* outT, float* max_w, unsigned* status)
+{
+#define FWD_CFG_ARGS T, st, V, order, ranges, recs, s_val, tile_last, n_contrib, color, depth, normal, outT, max_w, status
+    if constexpr (NS == 3 && DEPTH && NORMAL && !MAXW) {
+        switch (g_fwd_cfg.load()) {
+            case 1: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 3, 4>(FWD_CFG_ARGS);
+            case 2: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 4, 3>(FWD_CFG_ARGS);
+            case 3: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 3, 3>(FWD_CFG_ARGS);
+            default: break;
+        }
+    }
+    return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, SVR_NSLOT, SVR_FWD_MINB>(FWD_CFG_ARGS);
+#undef FWD_CFG_ARGS
 }
 
 extern "C" int svr_render_fwd(const svr_view_t* views_host, int n_views, int N, int64_t R, int n_samp,
@@ -671,15 +732,14 @@ extern "C" int svr_render_fwd(const svr_view_t* views_host, int n_views, int N, 
     return svr_fail(SVR_ERR_UNSUPPORTED, "n_samp");
 }
 
-template <bool DEPTH, bool NORMAL, bool RCONC>
-static int launch_bwd(int T, int N, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
-                      const uint32_t* tl,
-                      const uint32_t* nc, const Rec* recs, const float* s_val, const float* out_T,
-                      const float* dc, const float* dd, const float* dn, const float* dT, float lam,
-                      const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status)
+template <bool DEPTH, bool NORMAL, bool RCONC, int RING, int MINB>
+static int launch_bwd_cfg(int T, int N, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
+                          const uint32_t* tl, const uint32_t* nc, const Rec* recs, const float* s_val,
+                          const float* out_T, const float* dc, const float* dd, const float* dn, const float* dT,
+                          float lam, const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status)
 {
-    auto k = render_bwd_kernel<DEPTH, NORMAL, RCONC>;
-    const int smem = (int)sizeof(BwdSmem);
+    auto k = render_bwd_kernel<DEPTH, NORMAL, RCONC, RING, MINB>;
+    const int smem = (int)sizeof(BwdSmem<RING>);
     static std::atomic<unsigned long long> done{0};
     int rc = ensure_smem(k, smem, done);
     if (rc) return rc;
@@ -687,6 +747,26 @@ static int launch_bwd(int T, int N, cudaStream_t st, const Views& V, const uint3
                                status);
     LAUNCH_CHECK();
     return SVR_OK;
+}
+
+template <bool DEPTH, bool NORMAL, bool RCONC>
+static int launch_bwd(int T, int N, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
+                      const uint32_t* tl,
+                      const uint32_t* nc, const Rec* recs, const float* s_val, const float* out_T,
+                      const float* dc, const float* dd, const float* dn, const float* dT, float lam,
+                      const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status)
+{
+#define BWD_CFG_ARGS T, N, st, V, order, ranges, tl, nc, recs, s_val, out_T, dc, dd, dn, dT, lam, gt, dvox, drgbs, ds, status
+    if constexpr (DEPTH && NORMAL) {
+        switch (g_bwd_cfg.load()) {
+            case 1: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 3, 3>(BWD_CFG_ARGS);
+            case 2: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 4, 2>(BWD_CFG_ARGS);
+            case 3: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 3, 2>(BWD_CFG_ARGS);
+            default: break;
+        }
+    }
+    return launch_bwd_cfg<DEPTH, NORMAL, RCONC, SVR_NSLOT, SVR_BWD_MINB>(BWD_CFG_ARGS);
+#undef BWD_CFG_ARGS
 }
 
 extern "C" int svr_render_bwd(const svr_view_t* views_host, int n_views, int N, int64_t R, int need_depth,

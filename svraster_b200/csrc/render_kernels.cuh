@@ -69,20 +69,22 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+template <int RING>
 struct alignas(128) FwdSmem {
-    Rec buf[NSLOT][BATCH];
-    uint64_t full[NSLOT];
-    uint32_t arrived[NSLOT];
+    Rec buf[RING][BATCH];
+    uint64_t full[RING];
+    uint32_t arrived[RING];
     uint32_t octl[NWARP][8];
     uint32_t warps_done;
     int32_t stop;              // first batch not issued once every warp is done (INT_MAX before)
     uint32_t red[NWARP];
 };
 
+template <int RING>
 struct alignas(128) BwdSmem {
-    Rec buf[NSLOT][BATCH];
-    uint64_t full[NSLOT];
-    uint32_t arrived[NSLOT];
+    Rec buf[RING][BATCH];
+    uint64_t full[RING];
+    uint32_t arrived[RING];
     uint32_t octl[NWARP][8];
     float red[NWARP];
 };
@@ -130,8 +132,10 @@ __device__ __forceinline__ void warp_octant_lanes(uint32_t* octl, bool inside, u
 }
 
 // ============================================================================ forward
-template <int NS, bool DEPTH, bool NORMAL, bool MAXW>
-__global__ void __launch_bounds__(BLOCK, SVR_FWD_MINB) render_fwd_kernel(
+// RING (ring slots) and MINB (CTAs per SM asked of the register allocator) change only the
+// schedule, never the arithmetic: every (RING, MINB) instance produces the same outputs.
+template <int NS, bool DEPTH, bool NORMAL, bool MAXW, int RING = NSLOT, int MINB = SVR_FWD_MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) render_fwd_kernel(
     const __grid_constant__ Views V, const uint32_t* __restrict__ order, const uint2* __restrict__ ranges,
     const Rec* __restrict__ recs, const float* __restrict__ s_ptr, uint32_t* __restrict__ tile_last,
     uint32_t* __restrict__ n_contrib,
@@ -139,7 +143,7 @@ __global__ void __launch_bounds__(BLOCK, SVR_FWD_MINB) render_fwd_kernel(
     float* __restrict__ out_T, float* __restrict__ max_w, unsigned* __restrict__ status)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    FwdSmem& S = *reinterpret_cast<FwdSmem*>(smem_raw);
+    FwdSmem<RING>& S = *reinterpret_cast<FwdSmem<RING>*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tile = order ? (int)order[blockIdx.x] : (int)blockIdx.x;   // heavy tiles first
     const int vi = view_of_tile(V, tile);
@@ -162,20 +166,20 @@ __global__ void __launch_bounds__(BLOCK, SVR_FWD_MINB) render_fwd_kernel(
     const int nbatch = (n + BATCH - 1) / BATCH;
     if (tid == 0) {
 #pragma unroll
-        for (int k = 0; k < NSLOT; ++k) { mbar_init(&S.full[k], 1); S.arrived[k] = 0; }
+        for (int k = 0; k < RING; ++k) { mbar_init(&S.full[k], 1); S.arrived[k] = 0; }
         S.warps_done = 0;
         S.stop = INT_MAX;
         fence_mbar_init();
     }
     __syncthreads();
     auto issue = [&](int b) {
-        const int slot = b % NSLOT;
+        const int slot = b % RING;
         const uint32_t bytes = (uint32_t)min(BATCH, n - b * BATCH) * (uint32_t)sizeof(Rec);
         mbar_arrive_tx(&S.full[slot], bytes);
         bulk_g2s(S.buf[slot], recs + range.x + (size_t)b * BATCH, bytes, &S.full[slot]);
     };
     if (tid == 0)
-        for (int b = 0; b < min(NSLOT, nbatch); ++b) issue(b);
+        for (int b = 0; b < min(RING, nbatch); ++b) issue(b);
 
     float T = 1.f, D = 0.f;
     float3 C = f3(0.f, 0.f, 0.f), Nn = f3(0.f, 0.f, 0.f);
@@ -188,7 +192,7 @@ __global__ void __launch_bounds__(BLOCK, SVR_FWD_MINB) render_fwd_kernel(
     bool failed = false;
 
     for (int b = 0; b < nbatch; ++b) {
-        const int slot = b % NSLOT;
+        const int slot = b % RING;
         if (!mbar_wait(&S.full[slot], (parity >> slot) & 1)) { failed = true; break; }
         parity ^= 1u << slot;
         if (b >= *(volatile int32_t*)&S.stop) break;
@@ -284,7 +288,7 @@ __global__ void __launch_bounds__(BLOCK, SVR_FWD_MINB) render_fwd_kernel(
             if (prev == NWARP - 1) {
                 __threadfence_block();
                 S.arrived[slot] = 0;
-                const int nb2 = b + NSLOT;
+                const int nb2 = b + RING;
                 if (nb2 < nbatch) {
                     if (*(volatile uint32_t*)&S.warps_done == NWARP) {
                         atomicMin(&S.stop, nb2);
@@ -365,13 +369,13 @@ __global__ void __launch_bounds__(BLOCK, SVR_FWD_MINB) render_fwd_kernel(
         for (int w = 0; w < NWARP; ++w) m = max(m, S.red[w]);
         tile_last[tile] = range.x + m;
 #pragma unroll
-        for (int k = 0; k < NSLOT; ++k) mbar_inval(&S.full[k]);
+        for (int k = 0; k < RING; ++k) mbar_inval(&S.full[k]);
     }
 }
 
 // ============================================================================ adjoint
-template <bool DEPTH, bool NORMAL, bool RCONC>
-__global__ void __launch_bounds__(BLOCK, SVR_BWD_MINB) render_bwd_kernel(
+template <bool DEPTH, bool NORMAL, bool RCONC, int RING = NSLOT, int MINB = SVR_BWD_MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) render_bwd_kernel(
     const __grid_constant__ Views V, int N, const uint32_t* __restrict__ order, const uint2* __restrict__ ranges,
     const uint32_t* __restrict__ tile_last,
     const uint32_t* __restrict__ n_contrib, const Rec* __restrict__ recs, const float* __restrict__ s_ptr,
@@ -381,7 +385,7 @@ __global__ void __launch_bounds__(BLOCK, SVR_BWD_MINB) render_bwd_kernel(
     float* __restrict__ dL_ds, unsigned* __restrict__ status)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    BwdSmem& S = *reinterpret_cast<BwdSmem*>(smem_raw);
+    BwdSmem<RING>& S = *reinterpret_cast<BwdSmem<RING>*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tile = order ? (int)order[blockIdx.x] : (int)blockIdx.x;   // heavy tiles first
     const int vi = view_of_tile(V, tile);
@@ -405,13 +409,13 @@ __global__ void __launch_bounds__(BLOCK, SVR_BWD_MINB) render_bwd_kernel(
     const int nbatch = (n + BATCH - 1) / BATCH;
     if (tid == 0) {
 #pragma unroll
-        for (int k = 0; k < NSLOT; ++k) { mbar_init(&S.full[k], 1); S.arrived[k] = 0; }
+        for (int k = 0; k < RING; ++k) { mbar_init(&S.full[k], 1); S.arrived[k] = 0; }
         fence_mbar_init();
     }
     __syncthreads();
     // batch b covers relative records [lo, hi) with hi = n - b*BATCH (back to front)
     auto issue = [&](int b) {
-        const int slot = b % NSLOT;
+        const int slot = b % RING;
         const int hi = n - b * BATCH;
         const int c = min(BATCH, hi);
         const uint32_t bytes = (uint32_t)c * (uint32_t)sizeof(Rec);
@@ -419,7 +423,7 @@ __global__ void __launch_bounds__(BLOCK, SVR_BWD_MINB) render_bwd_kernel(
         bulk_g2s(S.buf[slot], recs + r0 + (hi - c), bytes, &S.full[slot]);
     };
     if (tid == 0)
-        for (int b = 0; b < min(NSLOT, nbatch); ++b) issue(b);
+        for (int b = 0; b < min(RING, nbatch); ++b) issue(b);
 
     // per-pixel adjoint state (backward.cu:156-216)
     const int64_t HW = (int64_t)W * H;
@@ -455,7 +459,7 @@ __global__ void __launch_bounds__(BLOCK, SVR_BWD_MINB) render_bwd_kernel(
     bool failed = false;
 
     for (int b = 0; b < nbatch; ++b) {
-        const int slot = b % NSLOT;
+        const int slot = b % RING;
         if (!mbar_wait(&S.full[slot], (parity >> slot) & 1)) { failed = true; break; }
         parity ^= 1u << slot;
         const int hi = n - b * BATCH;
@@ -620,7 +624,7 @@ __global__ void __launch_bounds__(BLOCK, SVR_BWD_MINB) render_bwd_kernel(
             if (prev == NWARP - 1) {
                 __threadfence_block();
                 S.arrived[slot] = 0;
-                const int nb2 = b + NSLOT;
+                const int nb2 = b + RING;
                 if (nb2 < nbatch) {
                     fence_proxy_async_smem();
                     issue(nb2);
@@ -641,7 +645,7 @@ __global__ void __launch_bounds__(BLOCK, SVR_BWD_MINB) render_bwd_kernel(
         for (int w = 0; w < NWARP; ++w) s += S.red[w];
         if (s != 0.f) atomicAdd(dL_ds, s);
 #pragma unroll
-        for (int k = 0; k < NSLOT; ++k) mbar_inval(&S.full[k]);
+        for (int k = 0; k < RING; ++k) mbar_inval(&S.full[k]);
     }
 }
 

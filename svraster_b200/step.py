@@ -111,6 +111,7 @@ class BatchedTrainStep:
         self.coef_tables = None
         self.coef_rows = 0
         self._dev_step_synced = False
+        self.tuned = None
 
     # ------------------------------------------------------------------ one step
     def step(self, time_render=False, grad_hook=None):
@@ -213,6 +214,31 @@ class BatchedTrainStep:
         return color, T
 
     # ------------------------------------------------------------------ CUDA graph
+    def autotune(self, reps=3, cache=None):
+        """Choose the render kernels' launch configuration for this batch by timing each
+        configuration on the last step's binned records (svraster_b200.autotune).  Runs one
+        eager step first if none ran yet; the gradient buffers are left as a step leaves them."""
+        from . import autotune as AT
+        if self.state is None:
+            self.step()
+        st = self.state
+
+        def fwd():
+            st.render(3, True, True, self.centers, self.lengths, self.geos, self.rgbs, self.s_val,
+                      rgb_per_view=True)
+
+        color, depth, normal, T, _ = st.render(3, True, True, self.centers, self.lengths, self.geos, self.rgbs,
+                                                self.s_val, rgb_per_view=True)
+
+        def bwd():
+            st.render_backward(True, True, self.s_val, T, self.dcolor, self.ddepth, self.dnormal, self.dT,
+                               lambda_R_concen=self.lambda_R, gt_color=self.gt, drgbs=self.drgbs, dvox=self.dvox,
+                               ds=self.ds)
+        key = AT.workload_key(self.dev, self.V, self.P, self.N, st.num_rendered)
+        self.tuned = AT.tune_render(fwd, bwd, reps=reps, key=key, cache=cache)
+        torch.cuda.synchronize(self.dev)
+        return self.tuned
+
     def capture(self, capacity=None, rows=1 << 20):
         """Capture one whole step (gather, SH, preprocess, scan, duplicate, sort, pack, render
         forward and adjoint, scatter, SH adjoint, smoothness adjoints, Adam) into a CUDA graph.
