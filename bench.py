@@ -295,12 +295,30 @@ def run_e2e(args, scene, cams, dev):
     active = torch.arange(keys.numel(), dtype=torch.int32, device=dev)
     h2d = sum(sum(p.numel() for p in planes) * 4 + gt.numel() * 4 for planes, gt in host) + 2 * 64 * len(cams)
 
+    # every step copies all views' upstream planes from pinned host memory on a copy stream;
+    # view v's render waits only for its own planes, so the copies overlap earlier views
+    dev_bufs = [([torch.empty_like(p, device=dev) for p in planes], torch.empty_like(gt, device=dev))
+                for planes, gt in host]
+    copy_stream = torch.cuda.Stream(device=dev)
+
     def one_step(it):
         opt.zero_grad(set_to_none=False) if grid.grad is not None else None
         tot = torch.zeros((), device=dev)
-        for (planes, gt_h), (w2c, c2w), c in zip(host, mats, cams):
-            dc, dd, dn = [p.to(dev, non_blocking=True) for p in planes]
-            gt = gt_h.to(dev, non_blocking=True).view(3, c.height, c.width)
+        compute = torch.cuda.current_stream(dev)
+        copy_stream.wait_stream(compute)          # buffers are free once the last step used them
+        ready = []
+        with torch.cuda.stream(copy_stream):
+            for (planes, gt_h), (dplanes, dgt) in zip(host, dev_bufs):
+                for hp, dp in zip(planes, dplanes):
+                    dp.copy_(hp, non_blocking=True)
+                dgt.copy_(gt_h, non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(copy_stream)
+                ready.append(ev)
+        for (dplanes, dgt), ev, (w2c, c2w), c in zip(dev_bufs, ready, mats, cams):
+            compute.wait_event(ev)
+            dc, dd, dn = dplanes
+            gt = dgt.view(3, c.height, c.width)
             rs = renderer.RasterSettings(color_mode="sh", vox_geo_mode="triinterp3", density_mode="sdf",
                                          image_width=c.width, image_height=c.height, tanfovx=c.tanfovx,
                                          tanfovy=c.tanfovy, cx=c.cx, cy=c.cy, w2c_matrix=w2c, c2w_matrix=c2w,
