@@ -10,6 +10,7 @@
 //    warp (8x4 pixel footprint + octant set) once per record instead of once per pixel,
 //    and the adjoint accumulates per-record gradients in shared memory so each record
 //    reaches global memory with one vector atomic per CTA instead of one per pixel.
+#include <algorithm>
 #include <atomic>
 #include <cstddef>
 #include <cstdio>
@@ -156,6 +157,9 @@ static int build_views(const svr_view_t* vh, int n, Views& V, int& total_tiles, 
 // ------------------------------------------------------------------ preprocess
 // Per (view, voxel): cull, projected bbox, octant bitset, duplicate count
 // (preprocess.cu:36-154).  Also ORs the octree paths and sums the counts in 64 bits.
+// Grid-stride over the voxels of view blockIdx.y with a bounded grid: the running total and
+// path OR are reduced over the block and leave with one atomic each (one per warp put tens
+// of millions of same-address atomics on one L2 slice for a 64-view batch).
 __global__ void __launch_bounds__(256) preprocess_kernel(
     const __grid_constant__ Views V, int N, const float3* __restrict__ centers,
     const float* __restrict__ lengths, const uint8_t* __restrict__ is_leaf,
@@ -163,28 +167,30 @@ __global__ void __launch_bounds__(256) preprocess_kernel(
     uint32_t* __restrict__ ndup, uint2* __restrict__ bboxes, uint32_t* __restrict__ bitsets,
     GeomMeta* __restrict__ meta)
 {
+    __shared__ unsigned long long s_tot[8], s_path[8];
     const int vi = blockIdx.y;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const svr_view_t& view = V.v[vi];
-    uint32_t cnt = 0;
-    unsigned long long path = 0;
-    if (i < N) {
+    const float* c2w = view.c2w;
+    const float3 ro = f3(c2w[3], c2w[7], c2w[11]);
+    float w2c[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) w2c[k] = view.w2c[k];
+    const float near = view.near_plane;
+    const float focal_x = 0.5f * view.width / view.tanfovx;
+    const float focal_y = 0.5f * view.height / view.tanfovy;
+    const float cx_h = view.cx - 0.5f, cy_h = view.cy - 0.5f;
+    const int gx = view.tiles_x, gy = view.tiles_y;
+    unsigned long long tot = 0, path = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         const size_t item = (size_t)vi * N + i;
+        uint32_t cnt = 0;
         uint2 bbox = make_uint2(0, 0);
         uint32_t qbits = 0;
         if (is_leaf[i] != 0) {
             const float3 vox_c = centers[i];
             const float vox_r = 0.5f * lengths[i];
-            const float* c2w = view.c2w;
-            const float3 ro = f3(c2w[3], c2w[7], c2w[11]);
-            float w2c[12];
-#pragma unroll
-            for (int k = 0; k < 12; ++k) w2c[k] = view.w2c[k];
             const float3 rel = vox_c - ro;
-            const float near = view.near_plane;
             if (!(dot3(rel, rel) < near * near)) {
-                const float focal_x = 0.5f * view.width / view.tanfovx;
-                const float focal_y = 0.5f * view.height / view.tanfovy;
                 float2 cmin = make_float2(1e9f, 1e9f), cmax = make_float2(-1e9f, -1e9f);
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
@@ -200,7 +206,6 @@ __global__ void __launch_bounds__(256) preprocess_kernel(
                     cmax = make_float2(fmaxf(cmax.x, u), fmaxf(cmax.y, v));
                     qbits |= (1u << q);
                 }
-                const float cx_h = view.cx - 0.5f, cy_h = view.cy - 0.5f;
                 const float bminx = fmaxf(focal_x * cmin.x + cx_h, 0.0f);
                 const float bminy = fmaxf(focal_y * cmin.y + cy_h, 0.0f);
                 const float bmaxx = fminf(focal_x * cmax.x + cx_h, (float)view.width);
@@ -209,13 +214,12 @@ __global__ void __launch_bounds__(256) preprocess_kernel(
                     bbox = make_uint2((((uint32_t)lrintf(bminx)) << 16) | ((uint32_t)lrintf(bminy)),
                                       (((uint32_t)lrintf(bmaxx)) << 16) | ((uint32_t)lrintf(bmaxy)));
                     // auxiliary.h:138-152
-                    const int gx = view.tiles_x, gy = view.tiles_y;
                     const int tx0 = max(0, min(gx - 1, (int)((bbox.x >> 16) / TILE)));
                     const int ty0 = max(0, min(gy - 1, (int)((bbox.x << 16 >> 16) / TILE)));
                     const int tx1 = max(0, min(gx - 1, (int)((bbox.y >> 16) / TILE)));
                     const int ty1 = max(0, min(gy - 1, (int)((bbox.y << 16 >> 16) / TILE)));
                     cnt = (uint32_t)((1 + ty1 - ty0) * (1 + tx1 - tx0)) * __popc(qbits);
-                    path = (unsigned long long)octpaths[i];
+                    if (cnt) path |= (unsigned long long)octpaths[i];
                 } else {
                     qbits = 0;
                     bbox = make_uint2(0, 0);
@@ -229,17 +233,25 @@ __global__ void __launch_bounds__(256) preprocess_kernel(
         ndup[item] = cnt;
         bboxes[item] = bbox;
         bitsets[item] = qbits;
+        tot += cnt;
     }
-    // warp-aggregated 64-bit total and path OR: one atomic per warp
-    unsigned long long tot = cnt;
+    // block reduction, then one atomic per block for each of the total and the path OR
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         tot += __shfl_xor_sync(0xffffffffu, tot, o);
         path |= __shfl_xor_sync(0xffffffffu, path, o);
     }
-    if ((threadIdx.x & 31) == 0 && tot) {
-        atomicAdd(&meta->total, tot);
-        atomicOr(&meta->path_or, path);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { s_tot[warp] = tot; s_path[warp] = path; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0, pth = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) { t += s_tot[w]; pth |= s_path[w]; }
+        if (t) {
+            atomicAdd(&meta->total, t);
+            atomicOr(&meta->path_or, pth);
+        }
     }
 }
 
@@ -260,7 +272,9 @@ extern "C" int svr_preprocess(const svr_view_t* views_host, int n_views, int N, 
     char* g = (char*)geom_buffer;
     CUDA_TRY(cudaMemsetAsync(g, 0, sizeof(GeomMeta), st));
     if (N == 0) return SVR_OK;
-    dim3 grid((N + 255) / 256, n_views);
+    // about 8 blocks per SM in total, split over the views
+    const int per_view = std::max(1, std::min((N + 255) / 256, (8 * 148 + n_views - 1) / n_views));
+    dim3 grid(per_view, n_views);
     preprocess_kernel<<<grid, 256, 0, st>>>(V, N, (const float3*)centers, lengths, is_leaf, octpaths, out_n_dup,
                                             (uint32_t*)(g + L.ndup), (uint2*)(g + L.bbox), (uint32_t*)(g + L.bits),
                                             (GeomMeta*)g);
