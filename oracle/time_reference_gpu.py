@@ -35,11 +35,12 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=2)
+    ap.add_argument("--config", default="mid", help="bench.py workload (mid | batched)")
     args = ap.parse_args()
     import bench
     R_ = load_module(os.path.join(ROOT, "oracle", "_ref", "svraster_ref_C.so"), "svraster_ref_C")
     dev = torch.device("cuda:0")
-    scene, cams = bench.make_workload(0)
+    scene, cams = bench.make_workload(0, config=args.config)
     t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
     octpath, centers, lengths = t(scene.octpath, torch.int64), t(scene.vox_center), t(scene.vox_size)
     is_leaf = t(scene.is_leaf, torch.uint8)
@@ -127,7 +128,7 @@ def main():
         times.append(e0.elapsed_time(e1))
     ms = float(np.median(times))
     rays = sum(c.width * c.height for c in cams)
-    print(json.dumps({"impl": "reference CUDA extension (per view, default stream)", "workload": bench.WORKLOAD,
+    print(json.dumps({"impl": "reference CUDA extension (per view, default stream)", "workload": bench.CONFIGS[args.config]["workload"],
                       "ms_per_step": round(ms, 3), "Mrays_per_s": round(rays / ms / 1e3, 3),
                       "stage_ms_per_step": {k: round(v / args.steps, 3) for k, v in stage.items()},
                       "grid_keys": int(keys.numel())}), flush=True)
