@@ -289,6 +289,53 @@ __global__ void sh_views_bw_kernel(int N, int V, int M, const float3* __restrict
     for (int k = 1; k < NB; ++k) dshs[i * (M - 1) + k - 1] = acc[k];
 }
 
+// Same adjoint with coalesced stores when every coefficient row is full (NB == M): the block's
+// rows are staged in shared memory and written back as one contiguous range (one thread per
+// voxel writing its 180-byte row left 32 scattered sectors per warp store).
+template <int DEG>
+__global__ void __launch_bounds__(128) sh_views_bw_full_kernel(int N, int V, const float3* __restrict__ centers,
+                                                               const float3* __restrict__ cam_pos,
+                                                               const float3* __restrict__ drgbs,
+                                                               float* __restrict__ dsh0, float* __restrict__ dshs)
+{
+    constexpr int NB = (DEG + 1) * (DEG + 1);
+    constexpr int ROW = 3 * (NB - 1);
+    __shared__ float rows[128 * ROW + 1];
+    __shared__ float dc[128 * 3];
+    const int64_t base = (int64_t)blockIdx.x * 128;
+    const int t = threadIdx.x;
+    const int64_t i = base + t;
+    float3 acc[NB];
+#pragma unroll
+    for (int k = 0; k < NB; ++k) acc[k] = f3(0.f, 0.f, 0.f);
+    if (i < N) {
+        const float3 ctr = centers[i];
+        for (int v = 0; v < V; ++v) {
+            const float3 d = drgbs[(int64_t)v * N + i];
+            if (d.x == 0.f && d.y == 0.f && d.z == 0.f) continue;
+            float3 dir = ctr - cam_pos[v];
+            dir = dir * rnorm3df(dir.x, dir.y, dir.z);
+            float B[16];
+            sh_basis<DEG>(dir, B);
+#pragma unroll
+            for (int k = 0; k < NB; ++k) acc[k] = acc[k] + B[k] * d;
+        }
+    }
+    dc[3 * t] = acc[0].x; dc[3 * t + 1] = acc[0].y; dc[3 * t + 2] = acc[0].z;
+#pragma unroll
+    for (int k = 1; k < NB; ++k) {
+        rows[t * ROW + 3 * (k - 1)] = acc[k].x;
+        rows[t * ROW + 3 * (k - 1) + 1] = acc[k].y;
+        rows[t * ROW + 3 * (k - 1) + 2] = acc[k].z;
+    }
+    __syncthreads();
+    const int nv = (int)min((int64_t)128, (int64_t)N - base);
+    float* o0 = dsh0 + 3 * base;
+    for (int j = t; j < 3 * nv; j += 128) o0[j] = dc[j];
+    float* o1 = dshs + (int64_t)ROW * base;
+    for (int j = t; j < ROW * nv; j += 128) o1[j] = rows[j];
+}
+
 template <typename Coef>
 static int sh_views_launch(int degree, int N, int V, int M, const float3* c, const float3* cp, Coef sh, float3* o,
                            void* stream)
@@ -334,6 +381,13 @@ extern "C" int svr_sh_eval_views_bw(int N, int n_views, int degree, int M, const
         return svr_fail(SVR_ERR_ARG, "sh views bw: bad degree / view count");
     if (N <= 0) return SVR_OK;
     cudaStream_t st = (cudaStream_t)stream;
+    if (degree == 3 && M == 16) {
+        sh_views_bw_full_kernel<3><<<nblk(N, 128), 128, 0, st>>>(N, n_views, (const float3*)centers,
+                                                                 (const float3*)cam_pos, (const float3*)drgbs,
+                                                                 dsh0, dshs);
+        LAUNCHED();
+        return SVR_OK;
+    }
     const unsigned g = nblk(N, 128);
     auto c = (const float3*)centers; auto cp = (const float3*)cam_pos; auto d = (const float3*)drgbs;
     auto o0 = (float3*)dsh0; auto o1 = (float3*)dshs;
