@@ -413,6 +413,64 @@ def run_extraction(step, scene, cams, dev):
                                       "sample": f"TSDF: 1 of {len(cams)} views; MC: every 16th voxel"}}
 
 
+def run_adaptive(step, scene, cams, dev):
+    """Subdivision support and training statistics on the bench scene: the grid-point link over
+    all voxels, subdivision of 5% of the voxels (children, trilinear corner values, relink,
+    mean aggregation), and the training statistics over the batch's views, each timed with
+    CUDA events beside the PyTorch calls the reference makes for the same results
+    (unique(dim=0, return_inverse=True), index_reduce_ mean; src/utils/octree_utils.py:203-222,
+    src/sparse_voxel_gears/adaptive.py:349-411)."""
+    import torch
+    from svraster_b200 import adaptive as A
+    octpath = step.octpath.reshape(-1, 1)
+    octlevel = torch.as_tensor(scene.octlevel.reshape(-1, 1).astype(np.int8), device=dev)
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps=3):
+        fn()
+        ts = []
+        for _ in range(reps):
+            a, b = ev(), ev()
+            a.record(); fn(); b.record(); torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return float(np.median(ts))
+
+    shift = torch.tensor([[(k >> 2) & 1, (k >> 1) & 1, k & 1] for k in range(8)], dtype=torch.int64, device=dev)
+
+    def torch_link():
+        from svraster_b200 import utils
+        ijk = utils.octpath_2_ijk(octpath, octlevel)
+        lv2 = (16 - octlevel).long()
+        g = ((ijk << lv2).view(-1, 1, 3) + (shift << lv2.view(-1, 1, 1))).reshape(-1, 3)
+        return g.unique(dim=0, return_inverse=True)
+
+    link_ms = timed(lambda: A.build_grid_pts_link(octpath, octlevel))
+    link_torch_ms = timed(torch_link, reps=1)
+    key, vkey = A.build_grid_pts_link(octpath, octlevel)
+    vals = step.grid.reshape(-1)[vkey].unsqueeze(-1).contiguous()
+    M = len(key)
+
+    def torch_agg():
+        import warnings
+        out = torch.zeros(M, 1, device=dev)
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")   # index_reduce_ is marked beta
+            out.index_reduce_(0, vkey.reshape(-1), vals.reshape(-1, 1), "mean", include_self=False)
+        return out
+    agg_ms = timed(lambda: A.agg_voxel_into_grid_pts(M, vkey, vals))
+    agg_torch_ms = timed(torch_agg)
+    sel = torch.arange(0, scene.n_vox, 20, device=dev)
+    interp_ms = timed(lambda: A.subdivide_by_interp(vals[sel]))
+    geos = step.grid.reshape(-1)[step.vox_key]
+    stat_ms = timed(lambda: A.compute_training_stat(cams, octpath, step.centers, step.lengths, step.is_leaf, geos,
+                                                    step.s_val), reps=2)
+    return {"voxels": scene.n_vox, "grid_points": M,
+            "grid_link_ms": round(link_ms, 3), "grid_link_torch_unique_ms": round(link_torch_ms, 3),
+            "agg_mean_ms": round(agg_ms, 3), "agg_mean_torch_index_reduce_ms": round(agg_torch_ms, 3),
+            "subdivide_interp_ms_5pct": round(interp_ms, 3),
+            "training_stat_ms": round(stat_ms, 3), "training_stat_views": len(cams)}
+
+
 def oracle_view_step(scene, cam, threads):
     """preprocess + binning + forward + backward of one view on the CPU oracle."""
     from oracle import oracle as O
@@ -503,6 +561,8 @@ def main():
         if not args.no_extract:
             result["extraction"] = run_extraction(step, scene, cams,
                                                   torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
+            result["adaptive"] = run_adaptive(step, scene, cams,
+                                              torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
         if not args.no_e2e:
             del step
             torch.cuda.empty_cache()

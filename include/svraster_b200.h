@@ -151,6 +151,18 @@ SVR_API int svr_render_config_describe(int pass, int index, int* ring, int* ctas
 SVR_API int svr_render_set_config(int fwd_index, int bwd_index);
 SVR_API int svr_render_get_config(int* fwd_index, int* bwd_index);
 
+/* Forward with per-view max blending weights (compute_training_stat,
+ * src/sparse_voxel_gears/adaptive.py:80-113, renders every view with track_max_w): as
+ * svr_render_fwd, but max_w_views f32[n_views, N] (caller zeroes it) gets one row per view. */
+SVR_API int svr_render_fwd_max_w_views(const svr_view_t* views_host, int n_views, int N,
+                                       int64_t num_rendered, int n_samp, int need_depth,
+                                       int need_normal, const float* centers, const float* lengths,
+                                       const float* geos, const float* rgbs, int n_rgb_views,
+                                       const float* s_val, void* geom_buffer, void* binning_buffer,
+                                       void* image_buffer, float* out_color, float* out_depth,
+                                       float* out_normal, float* out_T, float* max_w_views,
+                                       void* stream);
+
 /* Device status word of the raster launches that used this image buffer (0 = clean;
  * bit 1 wait timeout, bit 2 index out of range, bit 4 duplicate count mismatch, bit 8
  * records beyond the binning capacity, bit 16 sort-key format).
@@ -311,6 +323,31 @@ SVR_API int svr_mc_count(int64_t n_vox, const int64_t* vox_key, int64_t M, const
 SVR_API int svr_mc_emit(int64_t n_vox, const int64_t* vox_key, const float* grid_val,
                         const float* grid_xyz, float iso, int64_t n_tri, int fp64, void* workspace,
                         float* verts, int64_t* faces, int64_t* n_verts_host, void* stream);
+
+/* ---------------------------------------------------------------- adaptive pruning / subdivision
+ * svr_grid_link replaces octree_utils.build_grid_pts_link (src/utils/octree_utils.py:203-222):
+ * for N voxels (octpath i64[N], octlevel i8[N]) writes the M unique corner grid points
+ * grid_pts_key i64[M,3] (finest-level integer coordinates, lexicographic order as
+ * unique(dim=0); capacity 8N rows) and vox_key i64[N,8] (their indices), returns M
+ * (synchronises).  svr_subdivide_interp replaces adaptive.subdivide_by_interp
+ * (adaptive.py:374-411): vox_val f32[n,8,C] -> out f32[8n,8,C].  svr_agg_voxel_into_grid_pts
+ * replaces adaptive.agg_voxel_into_grid_pts (adaptive.py:349-372, index_reduce_ mean with
+ * include_self=False): out f32[M,C], count_ws f32[M] scratch.  svr_training_stat_reduce
+ * finishes compute_training_stat (adaptive.py:80-113) from per-view max weights
+ * f32[n_views,N]: max_w, min_samp_interval and view_cnt f32[N] (initialised by the caller to
+ * 0, 1e30 and 0) are updated in place; per view cam_pos / cam_lookat f32[3] and pix_size. */
+SVR_API size_t svr_grid_link_workspace_bytes(int64_t N);
+SVR_API int svr_grid_link(int64_t N, const int64_t* octpath, const int8_t* octlevel, void* workspace,
+                          size_t workspace_bytes, int64_t* grid_pts_key, int64_t* vox_key,
+                          int64_t* M_host, uint32_t* status, void* stream);
+SVR_API int svr_subdivide_interp(int64_t n, int C, const float* vox_val, float* out, void* stream);
+SVR_API int svr_agg_voxel_into_grid_pts(int64_t N, int C, const int64_t* vox_key, const float* vox_val,
+                                        int64_t M, float* out, float* count_ws, uint32_t* status,
+                                        void* stream);
+SVR_API int svr_training_stat_reduce(int n_views, int64_t N, const float* max_w_views,
+                                     const float* centers, const float* cam_pos,
+                                     const float* cam_lookat, const float* pix_size, float* max_w,
+                                     float* min_samp_interval, float* view_cnt, void* stream);
 
 /* ---------------------------------------------------------------- optimiser
  * Replace _C.unbiased_adam_step / _C.biased_adam_step (cuda/src/adam_step.cu:106-159). */

@@ -45,6 +45,13 @@ _SIGS = {
     "svr_unpack_geom": (_I, [_P, _I64, _P, _P, _P, _P]),
     "svr_count_rendered": (_I, [_I64, _P, C.POINTER(C.c_int64), C.POINTER(C.c_uint64), _P]),
     "svr_scan_rendered": (_I, [_I64, _P, _P]),
+    "svr_render_fwd_max_w_views": (_I, [_P, _I, _I, _I64, _I, _I, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P, _P,
+                                        _P, _P, _P]),
+    "svr_grid_link_workspace_bytes": (C.c_size_t, [_I64]),
+    "svr_grid_link": (_I, [_I64, _P, _P, _P, C.c_size_t, _P, _P, C.POINTER(C.c_int64), _P, _P]),
+    "svr_subdivide_interp": (_I, [_I64, _I, _P, _P, _P]),
+    "svr_agg_voxel_into_grid_pts": (_I, [_I64, _I, _P, _P, _I64, _P, _P, _P, _P]),
+    "svr_training_stat_reduce": (_I, [_I, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "svr_render_config_count": (_I, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "svr_render_config_describe": (_I, [_I, _I, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "svr_render_set_config": (_I, [_I, _I]),

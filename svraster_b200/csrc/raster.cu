@@ -661,7 +661,8 @@ extern "C" int svr_render_get_config(int* fwd_index, int* bwd_index)
 template <int NS, bool DEPTH, bool NORMAL, bool MAXW, int RING, int MINB>
 static int launch_fwd_cfg(int T, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
                           const Rec* recs, const float* s_val, uint32_t* tile_last, uint32_t* n_contrib,
-                          float* color, float* depth, float* normal, float* outT, float* max_w, unsigned* status)
+                          float* color, float* depth, float* normal, float* outT, float* max_w, int64_t mw_stride,
+                          unsigned* status)
 {
     auto k = render_fwd_kernel<NS, DEPTH, NORMAL, MAXW, RING, MINB>;
     const int smem = (int)sizeof(FwdSmem<RING>);
@@ -669,7 +670,7 @@ static int launch_fwd_cfg(int T, cudaStream_t st, const Views& V, const uint32_t
     int rc = ensure_smem(k, smem, done);
     if (rc) return rc;
     k<<<T, BLOCK, smem, st>>>(V, order, ranges, recs, s_val, tile_last, n_contrib, color,
-                              depth, normal, outT, max_w, status);
+                              depth, normal, outT, max_w, mw_stride, status);
     LAUNCH_CHECK();
     return SVR_OK;
 }
@@ -678,9 +679,9 @@ template <int NS, bool DEPTH, bool NORMAL, bool MAXW>
 static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
                       const Rec* recs,
                       const float* s_val, uint32_t* tile_last, uint32_t* n_contrib, float* color, float* depth,
-                      float* normal, float* outT, float* max_w, unsigned* status)
+                      float* normal, float* outT, float* max_w, int64_t mw_stride, unsigned* status)
 {
-#define FWD_CFG_ARGS T, st, V, order, ranges, recs, s_val, tile_last, n_contrib, color, depth, normal, outT, max_w, status
+#define FWD_CFG_ARGS T, st, V, order, ranges, recs, s_val, tile_last, n_contrib, color, depth, normal, outT, max_w, mw_stride, status
     if constexpr (NS == 3 && DEPTH && NORMAL && !MAXW) {
         switch (g_fwd_cfg.load()) {
             case 1: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 3, 4>(FWD_CFG_ARGS);
@@ -693,11 +694,44 @@ static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint32_t* or
 #undef FWD_CFG_ARGS
 }
 
+static int render_fwd_impl(const svr_view_t* views_host, int n_views, int N, int64_t R, int n_samp,
+                           int need_depth, int need_normal, const float* centers, const float* lengths,
+                           const float* geos, const float* rgbs, int n_rgb_views, const float* s_val,
+                           void* geom_buffer, void* binning_buffer, void* image_buffer, float* out_color,
+                           float* out_depth, float* out_normal, float* out_T, float* max_w, int64_t mw_stride,
+                           void* stream);
+
 extern "C" int svr_render_fwd(const svr_view_t* views_host, int n_views, int N, int64_t R, int n_samp,
                               int need_depth, int need_normal, const float* centers, const float* lengths,
                               const float* geos, const float* rgbs, int n_rgb_views, const float* s_val,
                               void* geom_buffer, void* binning_buffer, void* image_buffer, float* out_color,
                               float* out_depth, float* out_normal, float* out_T, float* max_w, void* stream)
+{
+    return render_fwd_impl(views_host, n_views, N, R, n_samp, need_depth, need_normal, centers, lengths, geos, rgbs,
+                           n_rgb_views, s_val, geom_buffer, binning_buffer, image_buffer, out_color, out_depth,
+                           out_normal, out_T, max_w, 0, stream);
+}
+
+extern "C" int svr_render_fwd_max_w_views(const svr_view_t* views_host, int n_views, int N, int64_t R, int n_samp,
+                                          int need_depth, int need_normal, const float* centers,
+                                          const float* lengths, const float* geos, const float* rgbs,
+                                          int n_rgb_views, const float* s_val, void* geom_buffer,
+                                          void* binning_buffer, void* image_buffer, float* out_color,
+                                          float* out_depth, float* out_normal, float* out_T,
+                                          float* max_w_views, void* stream)
+{
+    if (!max_w_views) return svr_fail(SVR_ERR_ARG, "render_fwd_max_w_views: null max_w");
+    return render_fwd_impl(views_host, n_views, N, R, n_samp, need_depth, need_normal, centers, lengths, geos, rgbs,
+                           n_rgb_views, s_val, geom_buffer, binning_buffer, image_buffer, out_color, out_depth,
+                           out_normal, out_T, max_w_views, (int64_t)N, stream);
+}
+
+static int render_fwd_impl(const svr_view_t* views_host, int n_views, int N, int64_t R, int n_samp,
+                           int need_depth, int need_normal, const float* centers, const float* lengths,
+                           const float* geos, const float* rgbs, int n_rgb_views, const float* s_val,
+                           void* geom_buffer, void* binning_buffer, void* image_buffer, float* out_color,
+                           float* out_depth, float* out_normal, float* out_T, float* max_w, int64_t mw_stride,
+                           void* stream)
 {
     Views V;
     int T; int64_t P;
@@ -730,14 +764,14 @@ extern "C" int svr_render_fwd(const svr_view_t* views_host, int n_views, int N, 
     const bool D = need_depth != 0, Nm = need_normal != 0, MW = max_w != nullptr;
 #define FWD_CASE(NS_)                                                                                   \
     if (n_samp == NS_) {                                                                                \
-        if (D && Nm && !MW) return launch_fwd<NS_, true, true, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
-        if (D && Nm && MW) return launch_fwd<NS_, true, true, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
-        if (D && !Nm && !MW) return launch_fwd<NS_, true, false, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
-        if (D && !Nm && MW) return launch_fwd<NS_, true, false, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
-        if (!D && Nm && !MW) return launch_fwd<NS_, false, true, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
-        if (!D && Nm && MW) return launch_fwd<NS_, false, true, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
-        if (!D && !Nm && !MW) return launch_fwd<NS_, false, false, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
-        return launch_fwd<NS_, false, false, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, status); \
+        if (D && Nm && !MW) return launch_fwd<NS_, true, true, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status); \
+        if (D && Nm && MW) return launch_fwd<NS_, true, true, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status); \
+        if (D && !Nm && !MW) return launch_fwd<NS_, true, false, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status); \
+        if (D && !Nm && MW) return launch_fwd<NS_, true, false, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status); \
+        if (!D && Nm && !MW) return launch_fwd<NS_, false, true, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status); \
+        if (!D && Nm && MW) return launch_fwd<NS_, false, true, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status); \
+        if (!D && !Nm && !MW) return launch_fwd<NS_, false, false, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status); \
+        return launch_fwd<NS_, false, false, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status); \
     }
     FWD_CASE(1)
     FWD_CASE(2)

@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_kernel(
     const Rec* __restrict__ recs, const float* __restrict__ s_ptr, uint32_t* __restrict__ tile_last,
     uint32_t* __restrict__ n_contrib,
     float* __restrict__ out_color, float* __restrict__ out_depth, float* __restrict__ out_normal,
-    float* __restrict__ out_T, float* __restrict__ max_w, unsigned* __restrict__ status)
+    float* __restrict__ out_T, float* __restrict__ max_w, int64_t max_w_stride, unsigned* __restrict__ status)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     FwdSmem<RING>& S = *reinterpret_cast<FwdSmem<RING>*>(smem_raw);
@@ -275,7 +275,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_kernel(
                     T *= (1.f - alpha);
                     done |= (T < EARLY_STOP_T);
                     last = (uint32_t)(b * BATCH + j2 + 1);
-                    if (MAXW) atomicMax(((int*)max_w) + (r.val & 0x1FFFFFFFu), __float_as_int(pt_w));
+                    if (MAXW)   // max_w_stride 0: one row for all views; N: a row per view
+                        atomicMax(((int*)max_w) + (size_t)vi * max_w_stride + (r.val & 0x1FFFFFFFu),
+                                  __float_as_int(pt_w));
                 }
             }
         }
