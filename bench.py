@@ -471,6 +471,82 @@ def run_adaptive(step, scene, cams, dev):
             "training_stat_ms": round(stat_ms, 3), "training_stat_views": len(cams)}
 
 
+REG_POINTS = 1 << 21
+
+
+def regulariser_inputs(scene, grid_mask, res, dev):
+    """Seeded inputs of the regulariser timings: a random half of the voxels active for the
+    voxel Eikonal (randperm(N)[:N/2], the default drop ratio 0.5 of train.py:562-564), 1/size
+    per voxel, and 2M points (grid units) uniform inside the masked cells for the points loss."""
+    import torch
+    g = torch.Generator(device=dev).manual_seed(5)
+    cells = torch.nonzero(grid_mask.reshape(-1)).reshape(-1)
+    pick = cells[torch.randint(0, cells.numel(), (REG_POINTS,), device=dev, generator=g)]
+    ijk = torch.stack([pick % res, (pick // res) % res, pick // (res * res)], 1).float()
+    pts = (ijk + torch.rand(REG_POINTS, 3, device=dev, generator=g)).contiguous()
+    vsi = (1.0 / torch.as_tensor(scene.vox_size.reshape(-1), device=dev)).contiguous()
+    active = torch.randperm(scene.n_vox, device=dev, generator=g)[:scene.n_vox // 2].to(torch.int32).contiguous()
+    return active, vsi, pts
+
+
+def run_regularisers(step, scene, dev):
+    """Voxel Eikonal, sign total variation (dense and tv_sparse) and the points loss on the
+    bench scene through the drop-in grid_loss_bw calls: CUDA events around 10 back-to-back
+    calls (the per-call host work overlaps the GPU), median of 5.  The voxel Eikonal and total
+    variation run with the voxels visited in spatial order (the default; the one-off order
+    build per octree is timed apart) and in storage order as the reference visits them.  Compulsory HBM bytes: per
+    voxel (active voxel for the voxel Eikonal) its 8 corner keys (64 B), 1/size (4 B) and its
+    active index (4 B, voxel Eikonal); per grid point one SDF read (4 B) and one gradient
+    read-modify-write (8 B)."""
+    import torch
+    from svraster_b200 import grid_loss_bw as GL
+    peak, _ = measured_peaks()
+    res = 1 << step.res_pow2
+    active, vsi, pts = regulariser_inputs(scene, step.grid_mask, res, dev)
+    N, M = scene.n_vox, step.grid.shape[0]
+    grad = torch.zeros_like(step.grid)
+
+    def timed(fn, calls=10, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(calls):
+                fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b) / calls)
+        return float(np.median(ts))
+
+    def order_build():
+        GL._ORDER_CACHE.clear()
+        GL.voxel_order(step.vox_key, M)
+    order_ms = timed(order_build, calls=1)
+    out = {"voxels": N, "active_voxels": active.numel(), "grid_points": M, "points": REG_POINTS,
+           "voxel_order_build_ms": round(order_ms, 4)}
+    vg_bytes, tv_bytes = active.numel() * 72 + M * 12, N * 68 + M * 12
+    for form, ordered in (("", True), ("_storage_order", False)):
+        vg_ms = timed(lambda: GL.voxel_gradient(step.grid, step.vox_key, vsi, active, 1e-3, False, False, grad,
+                                                ordered=ordered))
+        tv_ms = timed(lambda: GL.total_variation(step.grid, step.vox_key, 1e-3, vsi, False, False, grad,
+                                                 ordered=ordered))
+        tvs_ms = timed(lambda: GL.total_variation(step.grid, step.vox_key, 1e-3, vsi, False, True, grad,
+                                                  ordered=ordered))
+        out.update({f"voxel_gradient{form}_ms": round(vg_ms, 4),
+                    f"voxel_gradient{form}_frac": round(vg_bytes / vg_ms / 1e6 / peak, 3),
+                    f"total_variation{form}_ms": round(tv_ms, 4),
+                    f"total_variation{form}_frac": round(tv_bytes / tv_ms / 1e6 / peak, 3),
+                    f"total_variation_sparse{form}_ms": round(tvs_ms, 4)})
+    pl_ms = timed(lambda: GL.points_loss(pts, step.grid, step.vox_key, step.grid_voxel_coord, step.grid_voxel_size,
+                                         res, step.grid_mask, step.grid_keys, step.grid2voxel, 1e-3, 1.0, True,
+                                         False, grad))
+    out.update({"points_loss_ms": round(pl_ms, 4), "points_loss_Mpoints_per_s": round(REG_POINTS / pl_ms / 1e3, 1),
+                "compulsory_bytes": {"voxel_gradient": vg_bytes, "total_variation": tv_bytes}})
+    return out
+
+
 def oracle_view_step(scene, cam, threads):
     """preprocess + binning + forward + backward of one view on the CPU oracle."""
     from oracle import oracle as O
@@ -563,6 +639,8 @@ def main():
                                                   torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
             result["adaptive"] = run_adaptive(step, scene, cams,
                                               torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
+            result["regularisers"] = run_regularisers(step, scene,
+                                                      torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
         if not args.no_e2e:
             del step
             torch.cuda.empty_cache()

@@ -243,6 +243,50 @@ SVR_API int svr_eikonal_bw(int G, int A, const int32_t* active, const int32_t* g
                    float vox_size_inv, int seed, float* grid_grad, uint32_t* status,
                    void* stream);
 
+/* The other grid regularisers.  svr_voxel_gradient_bw replaces _C.voxel_gradient_bw
+ * (cuda/src/vg_compute.cu:23-118) for the A voxels of active; svr_total_variation_bw replaces
+ * _C.total_variation_bw (cuda/src/tv_compute.cu:23-176) for grid values f32[M,C]: with
+ * tv_sparse the participating voxels are decided from grid_grad as it is on entry (the
+ * reference reads it while adding to it), valid_ws u8[N*C] is scratch; svr_points_loss_bw
+ * replaces _C.points_loss_bw (cuda/src/pl_compute.cu:14-108) for points f32[P,3] in grid
+ * units, dense_index optional (svr_grid_index_build).  All add into grid_grad. */
+SVR_API int svr_voxel_gradient_bw(int N, int A, const int32_t* active, const int64_t* vox_key,
+                                  const float* grid_pts, int64_t M, const float* vox_size_inv,
+                                  float weight, float* grid_grad, uint32_t* status, void* stream);
+SVR_API int svr_total_variation_bw(int64_t N, int C, const int64_t* vox_key, const float* grid_pts,
+                                   int64_t M, float weight, const float* vox_size_inv, int no_tv_s,
+                                   int tv_sparse, uint8_t* valid_ws, float* grid_grad,
+                                   uint32_t* status, void* stream);
+SVR_API int svr_points_loss_bw(int P, const float* points_in_grid, int G, const int32_t* grid_keys,
+                               const int32_t* grid2voxel, int grid_res, const uint8_t* grid_mask,
+                               const int32_t* dense_index, const float* voxel_coords,
+                               const float* voxel_sizes, int N, const int64_t* vox_key,
+                               const float* grid_pts, int M, float weight, float* grid_grad,
+                               uint32_t* status, void* stream);
+
+/* Spatially ordered forms of svr_voxel_gradient_bw and svr_total_variation_bw (no
+ * counterpart in the reference, whose kernels visit voxels in storage order,
+ * vg_compute.cu:23-77, tv_compute.cu:22-158).  svr_voxel_order sorts the voxels once per
+ * octree by the grid-point index of their first corner: order i32[N] (visit position ->
+ * voxel, ties by voxel id) and rank i32[N] (its inverse); workspace from
+ * svr_voxel_order_workspace_bytes.  The _ordered adjoints take that order and rank as
+ * produced there (they are not range-checked); count_ws i32[N], valid_ws u8[N*C] are
+ * scratch.  Same results as the storage-order forms up to the order of float additions.
+ * vox_key 16-byte aligned. */
+SVR_API int svr_voxel_order_workspace_bytes(int64_t N, size_t* bytes);
+SVR_API int svr_voxel_order(int64_t N, const int64_t* vox_key, int64_t M, int32_t* order, int32_t* rank,
+                            void* ws, size_t ws_bytes, uint32_t* status, void* stream);
+SVR_API int svr_voxel_gradient_bw_ordered(int N, int A, const int32_t* active, const int32_t* order,
+                                          const int32_t* rank, const int64_t* vox_key, const float* grid_pts,
+                                          int64_t M, const float* vox_size_inv, float weight,
+                                          int32_t* count_ws, float* grid_grad, uint32_t* status,
+                                          void* stream);
+SVR_API int svr_total_variation_bw_ordered(int64_t N, int C, const int32_t* order, const int64_t* vox_key,
+                                           const float* grid_pts, int64_t M, float weight,
+                                           const float* vox_size_inv, int no_tv_s, int tv_sparse,
+                                           uint8_t* valid_ws, float* grid_grad, uint32_t* status,
+                                           void* stream);
+
 /* Graph-replayable forms (no counterpart in the reference): the jitter seed is
  * seed_base + *step, read from a device counter (svr_counter_add) when the kernel runs. */
 SVR_API int svr_laplacian_bw_at_step(int G, int A, const int32_t* active, const int32_t* grid_keys,

@@ -208,6 +208,39 @@ def eikonal_bw(*a, **k):
     return _grid_loss(lib().svo_eikonal_bw, *a, **k)
 
 
+def voxel_gradient_bw(grid, vox_key, vox_size_inv, active, weight, grad):
+    """vg_compute.cu:23-77 (voxel Eikonal); grid holds one channel."""
+    grad = _c(grad, np.float32).copy()
+    active = _c(active, np.int32)
+    lib().svo_voxel_gradient_bw(C.c_int(len(active)), _p(active), _p(_c(vox_key, np.int64)),
+                                _p(_c(grid, np.float32)), _p(_c(vox_size_inv, np.float32)), _f(weight), _p(grad))
+    return grad
+
+
+def total_variation_bw(grid, vox_key, weight, vox_size_inv, no_tv_s, tv_sparse, grad):
+    """tv_compute.cu:22-158; the tv_sparse test reads the gradient as it was on entry."""
+    grid = _c(grid, np.float32)
+    M = grid.shape[0]
+    Cc = grid.shape[1] if grid.ndim > 1 else 1
+    grad = _c(grad, np.float32).copy()
+    vox_key = _c(vox_key, np.int64)
+    lib().svo_total_variation_bw(C.c_int64(vox_key.shape[0]), C.c_int(Cc), _p(vox_key), _p(grid), _f(weight),
+                                 _p(_c(vox_size_inv, np.float32)), C.c_int(int(no_tv_s)), C.c_int(int(tv_sparse)),
+                                 _p(grad), C.c_int64(M))
+    return grad
+
+
+def points_loss_bw(points, grid, vox_key, coords, vsizes, res, mask, keys, g2v, weight, grad):
+    """pl_compute.cu:14-63; points in grid units [P, 3]."""
+    grad = _c(grad, np.float32).copy()
+    points = _c(points, np.float32)
+    lib().svo_points_loss_bw(C.c_int(points.shape[0]), _p(points), C.c_int(len(keys)), _p(_c(keys, np.int32)),
+                             _p(_c(g2v, np.int32)), C.c_int(res), _p(_c(mask, np.uint8)), _p(_c(coords, np.float32)),
+                             _p(_c(vsizes, np.float32)), _p(_c(vox_key, np.int64)), _p(_c(grid, np.float32)),
+                             _f(weight), _p(grad))
+    return grad
+
+
 def adam(param, grad, m, v, step, lr, beta1, beta2, eps, biased=False, sparse=False):
     p = _c(param, np.float32).copy(); m = _c(m, np.float32).copy(); v = _c(v, np.float32).copy()
     lib().svo_adam(C.c_int(p.size), C.c_int(int(biased)), C.c_int(int(sparse)), _p(p), _p(_c(grad, np.float32)),

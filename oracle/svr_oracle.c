@@ -814,6 +814,90 @@ void svo_eikonal_bw(int G, int A, const int32_t* active, const int32_t* keys, co
     }
 }
 
+/* ------------------------------------------------------------------ other grid regularisers
+ * Voxel Eikonal, cuda/src/vg_compute.cu:23-77: per active voxel the centre gradient from its
+ * 8 corners (sign of bit 2 / 1 / 0 for x / y / z), loss gradient 4 (|g|^2 - 2) w g, chained
+ * to the corners with the factor 0.25. */
+void svo_voxel_gradient_bw(int A, const int32_t* active, const int64_t* vox_key, const float* grid,
+                           const float* vox_size_inv, float weight, float* grad) {
+    for (int t = 0; t < A; ++t) {
+        int v = active[t];
+        float inv4h = 0.25f * vox_size_inv[v];
+        float S[8], gx = 0.f, gy = 0.f, gz = 0.f;
+        for (int i = 0; i < 8; ++i) S[i] = grid[vox_key[8 * (int64_t)v + i]];
+        for (int i = 0; i < 8; ++i) {
+            float sx = (i & 4) ? 1.f : -1.f, sy = (i & 2) ? 1.f : -1.f, sz = (i & 1) ? 1.f : -1.f;
+            gx += sx * S[i]; gy += sy * S[i]; gz += sz * S[i];
+        }
+        gx *= inv4h; gy *= inv4h; gz *= inv4h;
+        float g2 = gx * gx + gy * gy + gz * gz;
+        float sc = 4.f * (g2 - 2.f) * weight;
+        float dx = sc * gx, dy = sc * gy, dz = sc * gz;
+        for (int i = 0; i < 8; ++i) {
+            float sx = (i & 4) ? 1.f : -1.f, sy = (i & 2) ? 1.f : -1.f, sz = (i & 1) ? 1.f : -1.f;
+            grad[vox_key[8 * (int64_t)v + i]] += (dx * sx + dy * sy + dz * sz) * 0.25f;
+        }
+    }
+}
+
+/* Sign total variation, cuda/src/tv_compute.cu:22-158: per (voxel, channel) each corner gets
+ * w * (sum over its 3 edge neighbours of +1 if it is larger, else -1), w = weight, times
+ * 0.01 * vox_size_inv[voxel] unless no_tv_s.  With tv_sparse a (voxel, channel) takes part only
+ * if one of its corners has a nonzero gradient; the reference tests that while other threads
+ * add to the same gradient, so its outcome depends on timing.  Here the test reads the gradient
+ * as it was on entry (a snapshot), the deterministic form of the same rule. */
+void svo_total_variation_bw(int64_t N, int C, const int64_t* vox_key, const float* grid, float weight,
+                            const float* vox_size_inv, int no_tv_s, int tv_sparse, float* grad, int64_t M) {
+    float* snap = NULL;
+    if (tv_sparse) {
+        snap = (float*)malloc(sizeof(float) * (size_t)(M * C > 0 ? M * C : 1));
+        memcpy(snap, grad, sizeof(float) * (size_t)(M * C));
+    }
+    for (int64_t n = 0; n < N; ++n) for (int c = 0; c < C; ++c) {
+        const int64_t* k = vox_key + 8 * n;
+        if (tv_sparse) {
+            int valid = 0;
+            for (int i = 0; i < 8; ++i) valid |= snap[k[i] * C + c] != 0.f;
+            if (!valid) continue;
+        }
+        float v[8];
+        for (int i = 0; i < 8; ++i) v[i] = grid[k[i] * C + c];
+        float w = weight;
+        if (!no_tv_s) w *= 0.01f * vox_size_inv[n];
+        for (int i = 0; i < 8; ++i) {
+            int s = ((v[i] > v[i ^ 1]) * 2 - 1) + ((v[i] > v[i ^ 2]) * 2 - 1) + ((v[i] > v[i ^ 4]) * 2 - 1);
+            grad[k[i] * C + c] += w * (float)s;
+        }
+    }
+    free(snap);
+}
+
+/* Points on the surface, cuda/src/pl_compute.cu:14-63: each point (grid units) is placed in
+ * its cell by truncating casts, the owner voxel's trilinear SDF (weights not clamped, as in
+ * auxiliary.h:319-333) is driven to zero, dL/dsdf = 2 sdf weight spread over the 8 corners.
+ * A masked cell missing from the key table is skipped (the reference would read
+ * grid2voxel[-1]). */
+void svo_points_loss_bw(int P, const float* pts, int G, const int32_t* keys, const int32_t* g2v, int res,
+                        const uint8_t* mask, const float* coords, const float* vsizes, const int64_t* vox_key,
+                        const float* grid, float weight, float* grad) {
+    for (int t = 0; t < P; ++t) {
+        float px = pts[3 * t], py = pts[3 * t + 1], pz = pts[3 * t + 2];
+        int ix = (int)px, iy = (int)py, iz = (int)pz;
+        if (ix < 0 || ix >= res || iy < 0 || iy >= res || iz < 0 || iz >= res) continue;
+        int key = ix + iy * res + iz * res * res;
+        if (!mask[key]) continue;
+        int id = bsearch_key(keys, G, key);
+        if (id < 0) continue;
+        int v = g2v[id];
+        float sz = vsizes[v], w[8];
+        tri_w(mk((px - coords[3 * v]) / sz, (py - coords[3 * v + 1]) / sz, (pz - coords[3 * v + 2]) / sz), w);
+        float sdf = 0.f;
+        for (int i = 0; i < 8; ++i) sdf += w[i] * grid[vox_key[8 * (int64_t)v + i]];
+        float dL = 2.0f * (sdf - 0.0f) * weight;
+        for (int i = 0; i < 8; ++i) grad[vox_key[8 * (int64_t)v + i]] += dL * w[i];
+    }
+}
+
 /* ------------------------------------------------------------------ Adam
  * cuda/src/adam_step.cu:21-159 (host bias corrections in double). */
 static inline float lerp_(float v0, float v1, float t) { return fmaf(t, v1, fmaf(-t, v0, v0)); }

@@ -7,7 +7,7 @@ grid-Eikonal adjoints over every dense-grid key and Adam on grid / sh0 / shs, i.
 work as one batched step of svraster_b200.step.BatchedTrainStep.  CUDA events, median of
 the timed steps.  Prints one JSON line.
 
-Usage (GPU machine):  python oracle/time_reference_gpu.py [--steps 5 --warmup 2]
+Usage (GPU machine):  python oracle/time_reference_gpu.py [--steps 5 --warmup 2] [--regularisers]
 """
 from __future__ import annotations
 
@@ -31,11 +31,46 @@ def load_module(path, name):
     return mod
 
 
+def time_regularisers(R_, bench, scene, grid, vox_key, mask, keys, g2v, coord, vsize, res, dev):
+    """The reference's voxel_gradient_bw, total_variation_bw (dense, tv_sparse) and
+    points_loss_bw on the inputs bench.run_regularisers times, timed the same way: CUDA events
+    around 10 back-to-back calls, median of 5."""
+    active, vsi, pts = bench.regulariser_inputs(scene, mask, res, dev)
+    grad = torch.zeros_like(grid)
+
+    def timed(fn, calls=10, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(calls):
+                fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b) / calls)
+        return round(float(np.median(ts)), 4)
+
+    out = {"impl": "reference CUDA extension", "workload": "regularisers", "voxels": scene.n_vox,
+           "grid_points": int(grid.shape[0]), "points": int(pts.shape[0]),
+           "voxel_gradient_ms": timed(lambda: R_.voxel_gradient_bw(grid, vox_key, vsi, active, 1e-3, False, False,
+                                                                   grad)),
+           "total_variation_ms": timed(lambda: R_.total_variation_bw(grid, vox_key, 1e-3, vsi, False, False, grad)),
+           "total_variation_sparse_ms": timed(lambda: R_.total_variation_bw(grid, vox_key, 1e-3, vsi, False, True,
+                                                                            grad)),
+           "points_loss_ms": timed(lambda: R_.points_loss_bw(pts, grid, vox_key, coord, vsize, res, mask, keys, g2v,
+                                                             1e-3, 1.0, True, False, grad))}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=2)
     ap.add_argument("--config", default="mid", help="bench.py workload (mid | batched)")
+    ap.add_argument("--regularisers", action="store_true",
+                    help="time voxel_gradient_bw / total_variation_bw / points_loss_bw instead of the step")
     args = ap.parse_args()
     import bench
     R_ = load_module(os.path.join(ROOT, "oracle", "_ref", "svraster_ref_C.so"), "svraster_ref_C")
@@ -67,6 +102,9 @@ def main():
                        * np.float32(res)))
     vsize = t(np.round(scene.vox_size / ext * np.float32(res))).reshape(-1)
     active = torch.arange(keys.numel(), dtype=torch.int32, device=dev)
+    if args.regularisers:
+        time_regularisers(R_, bench, scene, grid, vox_key, mask, keys, g2v, coord, vsize, res, dev)
+        return
     params = [grid, sh0, shs]
     ms_ = [torch.zeros_like(p) for p in params]
     vs_ = [torch.zeros_like(p) for p in params]

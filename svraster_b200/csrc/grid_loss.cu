@@ -675,6 +675,127 @@ extern "C" int svr_smoothness_bw_vox(int G, int A, const int32_t* active, const 
     return SVR_OK;
 }
 
+// ------------------------------------------------------------------ other grid regularisers
+// vg_compute.cu:23-77 (voxel Eikonal): per active voxel, the centre gradient from the 8 corner
+// SDFs by averaged central differences, loss gradient 4 (|g|^2 - 2) w g, chained back to the
+// corners with the factor 0.25 (the reference's constants, kept).
+__global__ void __launch_bounds__(256) voxel_gradient_kernel(int A, const int32_t* __restrict__ active, int N,
+                                                             const int64_t* __restrict__ vox_key,
+                                                             const float* __restrict__ grid, int64_t M,
+                                                             const float* __restrict__ vox_size_inv, float weight,
+                                                             float* __restrict__ grad, unsigned* status)
+{
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= A) return;
+    const int v = active[tid];
+    if (v < 0 || v >= N) { atomicOr(status, ERR_BAD_INDEX); return; }
+    const float inv4h = 0.25f * vox_size_inv[v];
+    // all keys, then one range test, then all corner loads: the loads issue together
+    const longlong2* kp = reinterpret_cast<const longlong2*>(vox_key + 8 * (int64_t)v);
+    const longlong2 k0 = kp[0], k1 = kp[1], k2 = kp[2], k3 = kp[3];
+    const int64_t key[8] = {k0.x, k0.y, k1.x, k1.y, k2.x, k2.y, k3.x, k3.y};
+    float S[8];
+    bool bad = false;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) bad |= key[i] < 0 || key[i] >= M;
+    if (bad) { atomicOr(status, ERR_BAD_INDEX); return; }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) S[i] = grid[key[i]];
+    float gx = 0.f, gy = 0.f, gz = 0.f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const float sx = (i & 4) ? 1.f : -1.f, sy = (i & 2) ? 1.f : -1.f, sz = (i & 1) ? 1.f : -1.f;
+        gx += sx * S[i];
+        gy += sy * S[i];
+        gz += sz * S[i];
+    }
+    gx *= inv4h; gy *= inv4h; gz *= inv4h;
+    const float g2 = gx * gx + gy * gy + gz * gz;
+    const float scale = 4.f * (g2 - 2.f) * weight;
+    const float dx = scale * gx, dy = scale * gy, dz = scale * gz;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const float sx = (i & 4) ? 1.f : -1.f, sy = (i & 2) ? 1.f : -1.f, sz = (i & 1) ? 1.f : -1.f;
+        atomicAdd(grad + key[i], (dx * sx + dy * sy + dz * sz) * 0.25f);
+    }
+}
+
+extern "C" int svr_voxel_gradient_bw(int N, int A, const int32_t* active, const int64_t* vox_key,
+                                     const float* grid_pts, int64_t M, const float* vox_size_inv, float weight,
+                                     float* grid_grad, uint32_t* status, void* stream)
+{
+    if (A <= 0) return SVR_OK;
+    if (!active || !vox_key || !grid_pts || !vox_size_inv || !grid_grad || !status)
+        return svr_fail(SVR_ERR_ARG, "voxel gradient: null argument");
+    if (((uintptr_t)vox_key & 15) != 0) return svr_fail(SVR_ERR_ARG, "voxel gradient: vox_key not 16-byte aligned");
+    voxel_gradient_kernel<<<(A + 255) / 256, 256, 0, (cudaStream_t)stream>>>(A, active, N, vox_key, grid_pts, M,
+                                                                             vox_size_inv, weight, grid_grad,
+                                                                             status);
+    svr_note_launch(1);
+    CUDA_TRY(cudaGetLastError());
+    return SVR_OK;
+}
+
+// svr_total_variation_bw lives in voxel_order.cu beside its spatially ordered form.
+
+// pl_compute.cu:14-63 (points on the surface): each point (grid units) is located in its
+// cell (truncating casts, as there), the owner voxel's trilinear SDF (weights not clamped) is
+// driven to 0 with loss sdf^2 * weight.  A masked cell missing from the table is skipped
+// (the reference would index grid2voxel[-1]).
+__global__ void __launch_bounds__(256) points_loss_kernel(int P, const float* __restrict__ pts, SampleCtx c,
+                                                          const uint8_t* __restrict__ mask, float weight,
+                                                          float* __restrict__ grad, unsigned* status)
+{
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= P) return;
+    const float px = pts[3 * (int64_t)tid], py = pts[3 * (int64_t)tid + 1], pz = pts[3 * (int64_t)tid + 2];
+    const int ix = (int)px, iy = (int)py, iz = (int)pz;
+    const int res = c.res;
+    if (ix < 0 || ix >= res || iy < 0 || iy >= res || iz < 0 || iz >= res) return;
+    const int key = ix + iy * res + iz * res * res;
+    if (!mask[key]) return;
+    const int id = c.dense ? c.dense[key] : find_key(c.keys, c.G, key);
+    if (id < 0) return;
+    const int v = c.g2v[id];
+    if (v < 0 || v >= c.N) { atomicOr(status, ERR_BAD_INDEX); return; }
+    const float size = c.vsizes[v];
+    const float3 q = f3((px - c.coords[3 * v]) / size, (py - c.coords[3 * v + 1]) / size,
+                        (pz - c.coords[3 * v + 2]) / size);
+    float w[8];
+    tri_weights(q, w);
+    int64_t k[8];
+    float sdf = 0.f;
+    bool bad = false;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) k[i] = c.vox_key[8 * (int64_t)v + i];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) bad |= k[i] < 0 || k[i] >= c.M;
+    if (bad) { atomicOr(status, ERR_BAD_INDEX); return; }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) sdf += w[i] * c.grid[k[i]];
+    const float dL = 2.0f * (sdf - 0.0f) * weight;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) atomicAdd(grad + k[i], dL * w[i]);
+}
+
+extern "C" int svr_points_loss_bw(int P, const float* points_in_grid, int G, const int32_t* grid_keys,
+                                  const int32_t* grid2voxel, int grid_res, const uint8_t* grid_mask,
+                                  const int32_t* dense_index, const float* voxel_coords, const float* voxel_sizes,
+                                  int N, const int64_t* vox_key, const float* grid_pts, int M, float weight,
+                                  float* grid_grad, uint32_t* status, void* stream)
+{
+    if (P <= 0) return SVR_OK;
+    if (!points_in_grid || !grid_keys || !grid2voxel || !grid_mask || !voxel_coords || !voxel_sizes || !vox_key ||
+        !grid_pts || !grid_grad || !status)
+        return svr_fail(SVR_ERR_ARG, "points loss: null argument");
+    SampleCtx c{G, N, M, grid_res, dense_index, grid_keys, grid2voxel, voxel_coords, voxel_sizes, vox_key, grid_pts};
+    points_loss_kernel<<<(P + 255) / 256, 256, 0, (cudaStream_t)stream>>>(P, points_in_grid, c, grid_mask, weight,
+                                                                          grid_grad, status);
+    svr_note_launch(1);
+    CUDA_TRY(cudaGetLastError());
+    return SVR_OK;
+}
+
 // ------------------------------------------------------------------ allocation-free variant
 // For callers that cannot allocate device memory themselves (for example a host framework
 // that hands out all device memory from a fixed arena reserved at start-up and forbids any

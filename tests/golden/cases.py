@@ -18,6 +18,8 @@ CASES = {
 }
 TABLE_CASE = dict(seed=0, res_pow2=5, weight=0.01, vox_size_inv=16.0, drop=0.0)
 ADAM_CASE = dict(seed=3, n=4099, step=7, lr=0.01, beta1=0.1, beta2=0.99, eps=1e-15)
+# voxel Eikonal, sign total variation and points loss (vg / tv / pl_compute.cu)
+REG_CASE = dict(seed=0, res_pow2=5, weight=0.01, n_points=6000)
 
 
 def digest(inp):
@@ -81,3 +83,31 @@ def build_adam_inputs(case):
     grad[rng.random(n) < 0.2] = 0.0
     return dict(param=rng.normal(size=n).astype(np.float32), grad=grad,
                 m=(0.1 * rng.normal(size=n)).astype(np.float32), v=np.abs(0.1 * rng.normal(size=n)).astype(np.float32))
+
+
+def build_reg_inputs(case):
+    """Inputs of the voxel-Eikonal / total-variation / points-loss case: the table case's scene,
+    a voxel list with repeats, a 3-channel grid quantised to 1/4 so that neighbours tie, a
+    sparse nonzero starting gradient, and points (grid units) both inside masked cells and
+    scattered over and beyond the grid."""
+    from oracle import oracle as O
+    sc = S.scene_tiny(seed=case["seed"])
+    rng = np.random.default_rng(case["seed"] + 11)
+    N, M = sc.n_vox, sc.geo_grid_pts.shape[0]
+    res = 1 << case["res_pow2"]
+    coord, size = grid_voxel_geometry(sc, case["res_pow2"])
+    mask, keys, g2v = O.valid_table(sc.vox_center, sc.vox_size, np.zeros(3, np.float32), sc.scene_extent,
+                                    case["res_pow2"], sc.is_leaf)
+    active = rng.integers(0, N, size=int(N * 0.8)).astype(np.int32)
+    grid3 = (np.round(rng.normal(size=(M, 3)) * 4.0) / 4.0).astype(np.float32)
+    grad1 = np.where(rng.random((M, 1)) < 0.1, rng.normal(size=(M, 1)), 0.0).astype(np.float32)
+    grad3 = np.where(rng.random((M, 3)) < 0.1, rng.normal(size=(M, 3)), 0.0).astype(np.float32)
+    P = case["n_points"]
+    cells = np.flatnonzero(mask)
+    pick = cells[rng.integers(0, len(cells), size=P // 2)]
+    inside = np.stack([pick % res, (pick // res) % res, pick // (res * res)], 1) + rng.random((P // 2, 3))
+    spread = rng.uniform(-2.0, res + 2.0, size=(P - P // 2, 3))
+    points = np.concatenate([inside, spread]).astype(np.float32)
+    return dict(scene=sc, vox_size_inv=(1.0 / sc.vox_size.reshape(-1)).astype(np.float32), active=active,
+                grid3=grid3, grad1=grad1, grad3=grad3, points=points, grid_voxel_coord=coord,
+                grid_voxel_size=size, table=dict(mask=mask, keys=keys, g2v=g2v))

@@ -9,7 +9,7 @@ by the tests from the same seeds and checked against the stored input digest.
 The reference backward reads the depth and normal gradient planes unconditionally
 (backward.cu:180-184), so every case renders with need_depth and need_normal on.
 
-Usage (GPU machine):  python tests/golden/make_golden.py --out gpurun_out/golden
+Usage (GPU machine):  python tests/golden/make_golden.py --out gpurun_out/golden [--only reg ...]
 """
 from __future__ import annotations
 
@@ -25,8 +25,8 @@ import torch
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
 
-from tests.golden.cases import CASES, TABLE_CASE, ADAM_CASE, build_case_inputs, build_table_inputs, \
-    build_adam_inputs, digest  # noqa: E402
+from tests.golden.cases import CASES, TABLE_CASE, ADAM_CASE, REG_CASE, build_case_inputs, build_table_inputs, \
+    build_adam_inputs, build_reg_inputs, digest  # noqa: E402
 
 
 def load_module(path, name):
@@ -170,24 +170,60 @@ def run_adam_case(R_, case, dev):
     return out
 
 
+def run_reg_case(R_, case, dev):
+    inp = build_reg_inputs(case)
+    sc = inp["scene"]
+    t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
+    w = case["weight"]
+    grid1, grid3, vox_key = t(sc.geo_grid_pts), t(inp["grid3"]), t(sc.vox_key, torch.int64)
+    vsi = t(inp["vox_size_inv"])
+    out = dict(digest=digest(inp))
+    g = t(inp["grad1"])
+    R_.voxel_gradient_bw(grid1, vox_key, vsi, t(inp["active"], torch.int32), w, False, False, g)
+    torch.cuda.synchronize()
+    out["vg"] = g.cpu().numpy()
+    for no_tv_s in (False, True):
+        for name, grid, g0 in (("1", grid1, inp["grad1"]), ("3", grid3, inp["grad3"])):
+            g = t(g0)
+            R_.total_variation_bw(grid, vox_key, w, vsi, no_tv_s, False, g)
+            torch.cuda.synchronize()
+            out[f"tv{name}_{int(no_tv_s)}"] = g.cpu().numpy()
+    tb = inp["table"]
+    g = t(inp["grad1"])
+    R_.points_loss_bw(t(inp["points"]), grid1, vox_key, t(inp["grid_voxel_coord"]), t(inp["grid_voxel_size"]),
+                      1 << case["res_pow2"], t(tb["mask"], torch.bool), t(tb["keys"], torch.int32),
+                      t(tb["g2v"], torch.int32), w, 1.0, True, False, g)
+    torch.cuda.synchronize()
+    out["pl"] = g.cpu().numpy()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--only", nargs="*", default=None,
+                    help="fixtures to (re)write, e.g. reg table; default all")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     dev = torch.device("cuda:0")
     ref_dir = os.path.join(ROOT, "oracle", "_ref")
     R_ = load_module(os.path.join(ref_dir, "svraster_ref_C.so"), "svraster_ref_C")
     S_ = load_module(os.path.join(ref_dir, "seeded", "svraster_ref_seeded_C.so"), "svraster_ref_seeded_C")
+    want = lambda n: args.only is None or n in args.only
+    save = lambda n, res: np.savez_compressed(os.path.join(args.out, f"{n}.npz"), **res)
     for name, case in CASES.items():
-        res = run_render_case(R_, case, dev)
-        np.savez_compressed(os.path.join(args.out, f"{name}.npz"), **res)
-        print(name, "R =", res["num_rendered"])
-    res = run_table_case(R_, S_, TABLE_CASE, dev)
-    np.savez_compressed(os.path.join(args.out, "table.npz"), **res)
-    print("table G =", len(res["keys"]))
-    res = run_adam_case(R_, ADAM_CASE, dev)
-    np.savez_compressed(os.path.join(args.out, "adam.npz"), **res)
+        if want(name):
+            res = run_render_case(R_, case, dev)
+            save(name, res)
+            print(name, "R =", res["num_rendered"])
+    if want("table"):
+        res = run_table_case(R_, S_, TABLE_CASE, dev)
+        save("table", res)
+        print("table G =", len(res["keys"]))
+    if want("adam"):
+        save("adam", run_adam_case(R_, ADAM_CASE, dev))
+    if want("reg"):
+        save("reg", run_reg_case(R_, REG_CASE, dev))
     print("done")
 
 

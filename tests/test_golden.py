@@ -10,8 +10,8 @@ import os
 import numpy as np
 import pytest
 
-from tests.golden.cases import (ADAM_CASE, CASES, TABLE_CASE, build_adam_inputs, build_case_inputs,
-                                build_table_inputs, digest)
+from tests.golden.cases import (ADAM_CASE, CASES, REG_CASE, TABLE_CASE, build_adam_inputs, build_case_inputs,
+                                build_reg_inputs, build_table_inputs, digest)
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -105,6 +105,61 @@ def test_oracle_table_and_smoothness_match_reference_goldens():
                  np.zeros((len(sc.geo_grid_pts), 1), np.float32)).reshape(-1)
         scale = np.abs(g[name]).max() + 1e-20
         assert np.abs(out - g[name]).max() <= 1e-4 * scale, name
+
+
+def reg_outputs(inp, vg, tv, pl):
+    """Run one implementation of the three regularisers on the regulariser case; ``vg``, ``tv``
+    and ``pl`` take the reference argument order and return the updated gradient."""
+    sc, tb, w = inp["scene"], inp["table"], REG_CASE["weight"]
+    out = {"vg": vg(sc.geo_grid_pts, sc.vox_key, inp["vox_size_inv"], inp["active"], w, inp["grad1"])}
+    for no_tv_s in (0, 1):
+        for name, grid, g0 in (("1", sc.geo_grid_pts, inp["grad1"]), ("3", inp["grid3"], inp["grad3"])):
+            out[f"tv{name}_{no_tv_s}"] = tv(grid, sc.vox_key, w, inp["vox_size_inv"], no_tv_s, False, g0)
+    out["pl"] = pl(inp["points"], sc.geo_grid_pts, sc.vox_key, inp["grid_voxel_coord"], inp["grid_voxel_size"],
+                   1 << REG_CASE["res_pow2"], tb["mask"], tb["keys"], tb["g2v"], w, inp["grad1"])
+    return out
+
+
+# The reference adds with float atomics in thread-schedule order; sums of the same terms in
+# another order differ by a few ulps of the largest partial sum.
+REG_RTOL, REG_ATOL = 1e-5, 1e-6
+
+
+def check_reg(out, g):
+    for k, v in out.items():
+        ref = g[k]
+        assert v.shape == ref.shape, k
+        np.testing.assert_allclose(v, ref, rtol=REG_RTOL, atol=REG_ATOL * (np.abs(ref).max() + 1e-20), err_msg=k)
+
+
+def test_oracle_regularisers_match_reference_goldens():
+    from oracle import oracle as O
+    g = load("reg")
+    inp = build_reg_inputs(REG_CASE)
+    _check_inputs(g, inp)
+    out = reg_outputs(inp, O.voxel_gradient_bw, O.total_variation_bw, O.points_loss_bw)
+    check_reg(out, g)
+    # every output moved away from its starting gradient (the case exercises each path)
+    assert (g["vg"] != inp["grad1"]).sum() > 1000 and (g["pl"] != inp["grad1"]).sum() > 1000
+    assert (g["tv3_0"] != inp["grad3"]).mean() > 0.5
+
+
+def test_oracle_sparse_total_variation_rule():
+    """tv_sparse: a (voxel, channel) takes part iff one of its corners has a nonzero gradient on
+    entry; planted on a two-voxel grid sharing a face."""
+    from oracle import oracle as O
+    # corners x<<2|y<<1|z of voxel 0 are grid points 0..7; voxel 1 is shifted by +x (points 4..11)
+    key = np.array([[0, 1, 2, 3, 4, 5, 6, 7], [4, 5, 6, 7, 8, 9, 10, 11]], np.int64)
+    grid = np.arange(12, dtype=np.float32).reshape(12, 1)
+    vsi = np.ones(2, np.float32)
+    zero = np.zeros((12, 1), np.float32)
+    assert np.array_equal(O.total_variation_bw(grid, key, 1.0, vsi, 1, 1, zero), zero)
+    g0 = zero.copy(); g0[9] = 0.5          # only voxel 1 has a nonzero corner
+    dense = O.total_variation_bw(grid, key[1:], 1.0, vsi[1:], 1, 0, g0)
+    assert np.array_equal(O.total_variation_bw(grid, key, 1.0, vsi, 1, 1, g0), dense)
+    g0[4] = -1.0                           # a shared corner: both voxels take part
+    assert np.array_equal(O.total_variation_bw(grid, key, 1.0, vsi, 1, 1, g0),
+                          O.total_variation_bw(grid, key, 1.0, vsi, 1, 0, g0))
 
 
 def test_oracle_adam_matches_reference_goldens():
