@@ -547,6 +547,49 @@ def run_regularisers(step, scene, dev):
     return out
 
 
+def checkpoint_tensors(scene, dev):
+    """The fields of the bench model that a quantized checkpoint codes (io.py:111-114): the SDF
+    grid [M,1], sh0 [N,3] and shs [N,15,3], on the device."""
+    import torch
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
+    return {"_geo_grid_pts": t(scene.geo_grid_pts.reshape(-1, 1)), "_sh0": t(scene.sh0), "_shs": t(scene.shs)}
+
+
+def run_checkpoint(scene, dev):
+    """8-bit checkpoint coding of the bench model through svraster_b200.io: quantize_state_dict
+    (19 codebooks: the grid, 3 sh0 columns, 15 shs columns; each syncs once per round) and
+    dequantize_state_dict, wall clock around a synchronised call, median of 3."""
+    import torch
+    from svraster_b200 import io
+    fields = checkpoint_tensors(scene, dev)
+
+    def timed(fn, reps=3):
+        fn()
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            ts.append((time.perf_counter() - t0) * 1e3)
+        return float(np.median(ts))
+
+    def quant():
+        sd = dict(fields)
+        io.quantize_state_dict(sd)
+        return sd
+    q_ms = timed(quant)
+    sd = quant()
+    d_ms = timed(lambda: io.dequantize_state_dict(dict(sd)))
+    n = sum(v.numel() for v in fields.values())
+    deq = dict(sd)
+    io.dequantize_state_dict(deq)
+    err = float(max((deq[k] - fields[k]).abs().mean().item() / fields[k].abs().mean().item() for k in fields))
+    return {"values": n, "codebooks": 1 + fields["_sh0"].shape[1] + fields["_shs"].shape[1],
+            "quantize_ms": round(q_ms, 2), "quantize_Mvalues_per_s": round(n / q_ms / 1e3, 1),
+            "dequantize_ms": round(d_ms, 3), "mean_rel_abs_error": round(err, 5)}
+
+
 def oracle_view_step(scene, cam, threads):
     """preprocess + binning + forward + backward of one view on the CPU oracle."""
     from oracle import oracle as O
@@ -641,6 +684,7 @@ def main():
                                               torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
             result["regularisers"] = run_regularisers(step, scene,
                                                       torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
+            result["checkpoint"] = run_checkpoint(scene, torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
         if not args.no_e2e:
             del step
             torch.cuda.empty_cache()

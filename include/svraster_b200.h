@@ -393,6 +393,21 @@ SVR_API int svr_training_stat_reduce(int n_views, int64_t N, const float* max_w_
                                      const float* cam_lookat, const float* pix_size, float* max_w,
                                      float* min_samp_interval, float* view_cnt, void* stream);
 
+/* ---------------------------------------------------------------- checkpoint codebook
+ * svr_quantize replaces io.quantization (src/sparse_voxel_gears/io.py:123-167, torch in the
+ * reference): the 8-bit codebook of a quantized checkpoint for n float32 values (1 <= n <
+ * 2^31): index_out u8[n], codebook_out f32[256]; workspace from svr_quantize_workspace_bytes.
+ * Synchronises `stream` once per round (the rounds stop when nothing moves); *rounds_host
+ * (may be NULL) gets the number of rounds that moved values; status bit 32 flags a
+ * non-finite value.  Means are summed in float64, the reference's in float32.
+ * svr_dequantize replaces io.dequantization (io.py:169-170): out f32[n] = codebook[index]. */
+SVR_API int svr_quantize_workspace_bytes(int64_t n, size_t* bytes);
+SVR_API int svr_quantize(int64_t n, const float* values, int max_iter, uint8_t* index_out,
+                         float* codebook_out, void* ws, size_t ws_bytes, int* rounds_host,
+                         uint32_t* status, void* stream);
+SVR_API int svr_dequantize(int64_t n, const uint8_t* index, const float* codebook, float* out,
+                           void* stream);
+
 /* ---------------------------------------------------------------- optimiser
  * Replace _C.unbiased_adam_step / _C.biased_adam_step (cuda/src/adam_step.cu:106-159). */
 SVR_API int svr_adam_step(int64_t numel, int biased, int sparse, float* param, const float* grad,

@@ -241,6 +241,15 @@ def points_loss_bw(points, grid, vox_key, coords, vsizes, res, mask, keys, g2v, 
     return grad
 
 
+def quantize(values, max_iter=10):
+    """io.py:123-167: (index u8 shaped like values, codebook f32[256], rounds that moved values)."""
+    v = _c(values, np.float32)
+    idx = np.empty(v.shape, np.uint8)
+    book = np.empty(256, np.float32)
+    rounds = lib().svo_quantize(C.c_int64(v.size), _p(v), C.c_int(max_iter), _p(idx), _p(book))
+    return idx, book, rounds
+
+
 def adam(param, grad, m, v, step, lr, beta1, beta2, eps, biased=False, sparse=False):
     p = _c(param, np.float32).copy(); m = _c(m, np.float32).copy(); v = _c(v, np.float32).copy()
     lib().svo_adam(C.c_int(p.size), C.c_int(int(biased)), C.c_int(int(sparse)), _p(p), _p(_c(grad, np.float32)),

@@ -898,6 +898,79 @@ void svo_points_loss_bw(int P, const float* pts, int G, const int32_t* keys, con
     }
 }
 
+/* ------------------------------------------------------------------ 8-bit checkpoint codebook
+ * src/sparse_voxel_gears/io.py:123-167 (quantization): codebook initialised at the 257
+ * quantiles (float32 positions j/256 * (n-1), truncated) with entry 0 set to -inf, a left
+ * searchsorted, the nearer of the two candidate entries, then up to max_iter rounds of
+ * (per-entry mean, move each value one entry towards a nearer neighbour), a final mean.
+ * Index -1 reads entry 255 (torch's negative index), means are float sums in value order
+ * divided by the count, entries with no values stay 0.  Returns the rounds that moved
+ * values. */
+static int cmp_f32(const void* a, const void* b) {
+    float x = *(const float*)a, y = *(const float*)b;
+    return (x > y) - (x < y);
+}
+static void quant_mean(int64_t n, const float* v, const int32_t* ind, float* cb) {
+    float sum[256], cnt[256];
+    for (int b = 0; b < 256; ++b) { sum[b] = 0.f; cnt[b] = 0.f; }
+    for (int64_t i = 0; i < n; ++i) { sum[ind[i]] += v[i]; cnt[ind[i]] += 1.f; }
+    for (int b = 0; b < 256; ++b) cb[b] = cnt[b] > 0.f ? sum[b] / cnt[b] : 0.f;
+}
+static inline int quant_moves(float x, const float* book, int k, int* dir) {
+    float dl = fabsf(x - book[k - 1 < 0 ? 255 : k - 1]);
+    float dr = fabsf(x - book[k + 1 > 255 ? 255 : k + 1]);
+    float dm = fabsf(x - book[k]);
+    *dir = (dr < dl) ? 1 : -1;
+    return fminf(dl, dr) < dm;
+}
+int svo_quantize(int64_t n, const float* v, int max_iter, uint8_t* index_out, float* codebook_out) {
+    if (n <= 0) return -1;
+    float* sorted = (float*)malloc(sizeof(float) * (size_t)n);
+    int32_t* ind = (int32_t*)calloc((size_t)n, sizeof(int32_t));
+    memcpy(sorted, v, sizeof(float) * (size_t)n);
+    qsort(sorted, (size_t)n, sizeof(float), cmp_f32);
+    float full[257];
+    for (int j = 0; j < 257; ++j) {
+        volatile float pos = ((float)j / 256.0f) * (float)(n - 1);
+        int64_t q = (int64_t)pos;
+        if (q < 0) q = 0;
+        if (q > n - 1) q = n - 1;
+        full[j] = sorted[q];
+    }
+    full[0] = -INFINITY;
+    const float* cb = full + 1;
+    for (int64_t i = 0; i < n; ++i) {
+        int lo = 0, hi = 257;                       /* first entry >= v (searchsorted, left) */
+        while (lo < hi) { int mid = (lo + hi) / 2; if (full[mid] < v[i]) lo = mid + 1; else hi = mid; }
+        int k = lo - 1;
+        if (k < 0) k = 0;
+        if (k > 255) k = 255;
+        float dl = fabsf(v[i] - cb[k - 1 < 0 ? 255 : k - 1]), dm = fabsf(v[i] - cb[k]);
+        k = k - 1 + (dm < dl);
+        if (k < 0) k = 0;
+        if (k > 255) k = 255;
+        ind[i] = k;
+    }
+    float book[256];
+    int rounds = 0, dir = 0;
+    for (int it = 0; it < max_iter; ++it) {
+        quant_mean(n, v, ind, book);
+        int64_t moved = 0;
+        for (int64_t i = 0; i < n; ++i) moved += quant_moves(v[i], book, ind[i], &dir);
+        if (moved == 0) break;
+        for (int64_t i = 0; i < n; ++i) {
+            if (!quant_moves(v[i], book, ind[i], &dir)) continue;
+            int k = ind[i] + dir;
+            ind[i] = k < 0 ? 0 : (k > 255 ? 255 : k);
+        }
+        rounds++;
+    }
+    quant_mean(n, v, ind, codebook_out);
+    for (int64_t i = 0; i < n; ++i) index_out[i] = (uint8_t)ind[i];
+    free(sorted); free(ind);
+    return rounds;
+}
+
 /* ------------------------------------------------------------------ Adam
  * cuda/src/adam_step.cu:21-159 (host bias corrections in double). */
 static inline float lerp_(float v0, float v1, float t) { return fmaf(t, v1, fmaf(-t, v0, v0)); }

@@ -31,6 +31,26 @@ def load_module(path, name):
     return mod
 
 
+def time_checkpoint_oracle(args):
+    """The reference builds the checkpoint codebook with torch ops (io.py:123-167), which do not
+    exist outside its Python tree; its CPU behaviour is restated bit for bit by the C oracle,
+    timed here single-threaded on the same 19 tensors bench.run_checkpoint codes."""
+    import time
+    import bench
+    # this script's own folder is first on sys.path, so load the oracle front-end by path
+    O = load_module(os.path.join(ROOT, "oracle", "oracle.py"), "svr_oracle_front")
+    scene, _ = bench.make_workload(0, config=args.config)
+    cols = [scene.geo_grid_pts.reshape(-1)] + [scene.sh0[:, j] for j in range(scene.sh0.shape[1])] + \
+        [scene.shs[:, j] for j in range(scene.shs.shape[1])]
+    t0 = time.perf_counter()
+    for c in cols:
+        O.quantize(np.ascontiguousarray(c, dtype=np.float32))
+    ms = (time.perf_counter() - t0) * 1e3
+    print(json.dumps({"impl": "C oracle (restates io.py:123-167), 1 thread", "workload": "checkpoint",
+                      "values": int(sum(c.size for c in cols)), "codebooks": len(cols),
+                      "quantize_ms": round(ms, 1), "cores": 1}), flush=True)
+
+
 def time_regularisers(R_, bench, scene, grid, vox_key, mask, keys, g2v, coord, vsize, res, dev):
     """The reference's voxel_gradient_bw, total_variation_bw (dense, tv_sparse) and
     points_loss_bw on the inputs bench.run_regularisers times, timed the same way: CUDA events
@@ -71,7 +91,12 @@ def main():
     ap.add_argument("--config", default="mid", help="bench.py workload (mid | batched)")
     ap.add_argument("--regularisers", action="store_true",
                     help="time voxel_gradient_bw / total_variation_bw / points_loss_bw instead of the step")
+    ap.add_argument("--checkpoint", action="store_true",
+                    help="time the C oracle's 8-bit checkpoint codebook on the bench model instead")
     args = ap.parse_args()
+    if args.checkpoint:
+        time_checkpoint_oracle(args)
+        return
     import bench
     R_ = load_module(os.path.join(ROOT, "oracle", "_ref", "svraster_ref_C.so"), "svraster_ref_C")
     dev = torch.device("cuda:0")
