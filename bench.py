@@ -547,6 +547,74 @@ def run_regularisers(step, scene, dev):
     return out
 
 
+def run_normal_losses(step, cams, dev):
+    """The two normal-from-depth consistency losses with their gradients on the bench batch's
+    rendered depth / normal / transmittance planes (one render forward of the step's state;
+    all 8 views per launch), CUDA events around 10 back-to-back calls, median of 5.
+    Compulsory HBM bytes per pixel: the depth plane (4 B), normal (12 B), T (4 B, mean-depth
+    loss only), the depth-gradient plane and the normal gradient read and written (8 + 24 B)."""
+    import torch
+    from svraster_b200 import loss_utils as LU
+    from svraster_b200.raster import RasterState
+    peak, _ = measured_peaks()
+    state = RasterState(step.views, step.N, dev)
+    state.preprocess(step.octpath, step.centers, step.lengths, step.is_leaf)
+    state.bin(step.octpath)
+    # step.geos / step.rgbs hold the last step's gathered corner values and colours
+    _, depth, normal, T, _ = state.render(3, True, True, step.centers, step.lengths, step.geos, step.rgbs,
+                                          step.s_val, rgb_per_view=True)
+    gd, gn = torch.zeros_like(depth), torch.zeros_like(normal)
+    loss = torch.zeros(len(cams), dtype=torch.float64, device=dev)
+    P = T.numel()
+    out = {"views": len(cams), "pixels": P}
+    for name, mode, ks, tol, nbytes in (("mean_depth_ks3_tol90", "dmean", 3, float(np.float32(np.cos(np.pi / 2))), 52),
+                                        ("median_depth_ks3", "dmed", 3, -1.0, 48)):
+        fn = lambda: LU.normal_depth_loss_views(step.views, depth, normal, T, mode, ks, tol, 1e-3, gd, gn, loss)
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(5):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(10):
+                fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b) / 10)
+        ms = float(np.median(ts))
+        out[f"{name}_ms"] = round(ms, 4)
+        out[f"{name}_frac"] = round(P * nbytes / ms / 1e6 / peak, 3)
+    return out
+
+
+def run_step_with_normal_losses(scene, cams, dev, steps=10):
+    """The bench step with both normal-from-depth consistency losses switched on
+    (lambda_normal_dmean = lambda_normal_dmed = 0.001, the values train.py:1360-1362 sets),
+    graph replays, CUDA events around ``steps`` replays."""
+    import torch
+    from svraster_b200.step import BatchedTrainStep
+    step = BatchedTrainStep(scene, cams, device=dev, lambda_R_concen=0.1,
+                            normal_losses=dict(lambda_dmean=1e-3, dmean_ks=3, dmean_tol_deg=90.0, lambda_dmed=1e-3))
+    for _ in range(3):
+        step.step()
+    step.capture()
+    for _ in range(3):
+        step.replay()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        step.replay()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    out = {"ms_per_step": round(ms, 3), "Mrays_per_s": round(step.P / ms / 1e3, 2),
+           "nd_loss_last_step": round(float(step.nd_loss.sum()), 6), "graph_status": list(step.graph_status())}
+    del step
+    torch.cuda.empty_cache()
+    return out
+
+
 def checkpoint_tensors(scene, dev):
     """The fields of the bench model that a quantized checkpoint codes (io.py:111-114): the SDF
     grid [M,1], sh0 [N,3] and shs [N,15,3], on the device."""
@@ -685,6 +753,10 @@ def main():
             result["regularisers"] = run_regularisers(step, scene,
                                                       torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
             result["checkpoint"] = run_checkpoint(scene, torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
+            result["normal_losses"] = run_normal_losses(step, cams,
+                                                        torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
+            result["normal_losses"]["step_with_losses"] = run_step_with_normal_losses(
+                scene, cams, torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
         if not args.no_e2e:
             del step
             torch.cuda.empty_cache()

@@ -393,6 +393,20 @@ SVR_API int svr_training_stat_reduce(int n_views, int64_t N, const float* max_w_
                                      const float* cam_lookat, const float* pix_size, float* max_w,
                                      float* min_samp_interval, float* view_cnt, void* stream);
 
+/* ---------------------------------------------------------------- normal-from-depth losses
+ * svr_normal_depth_loss replaces the torch losses NormalDepthConsistencyLoss (mode 0,
+ * src/utils/loss_utils.py:345-379: depth plane 0, alpha = 1 - T weighting, tolerance mask
+ * tol_cos > 0) and NormalMedianConsistencyLoss (mode 1, loss_utils.py:381-407: depth plane
+ * 2; tol_cos ignored) with cameras.py:104-127 (depth2pts / depth2normal, ks odd <= 9), for
+ * all views in one launch.  depth f32[4*P], normal f32[3*P], T f32[P] packed per view as the
+ * render outputs; loss_out f64[n_views] += weight * loss of each view; the gradient of that
+ * is ADDED into grad_depth (the used plane) and grad_normal, the upstream planes of
+ * svr_render_bwd. */
+SVR_API int svr_normal_depth_loss(const svr_view_t* views_host, int n_views, int mode, int ks,
+                                  float tol_cos, float weight, const float* depth, const float* normal,
+                                  const float* T, double* loss_out, float* grad_depth,
+                                  float* grad_normal, void* stream);
+
 /* ---------------------------------------------------------------- checkpoint codebook
  * svr_quantize replaces io.quantization (src/sparse_voxel_gears/io.py:123-167, torch in the
  * reference): the 8-bit codebook of a quantized checkpoint for n float32 values (1 <= n <

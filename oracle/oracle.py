@@ -250,6 +250,23 @@ def quantize(values, max_iter=10):
     return idx, book, rounds
 
 
+def normal_depth_loss(W, H, cx, cy, tanfovx, tanfovy, c2w, depth, normal, T, ks, tol_cos):
+    """cameras.py:104-127 + loss_utils.py:345-407 for one view: (loss, dL/ddepth f32[H,W],
+    dL/dnormal f32[3,H,W]).  T given: NormalDepthConsistencyLoss on ``depth``; T None:
+    NormalMedianConsistencyLoss.  tol_cos <= 0 turns the tolerance mask off."""
+    L = lib()
+    L.svo_normal_depth_loss.restype = C.c_double
+    d = _c(depth, np.float32).reshape(H, W)
+    n = _c(normal, np.float32).reshape(3, H, W)
+    t = None if T is None else _c(T, np.float32).reshape(H, W)
+    gd = np.zeros((H, W), np.float32)
+    gn = np.zeros((3, H, W), np.float32)
+    m = _c(np.asarray(c2w, np.float32)[:3, :4], np.float32)
+    loss = L.svo_normal_depth_loss(C.c_int(W), C.c_int(H), _f(cx), _f(cy), _f(tanfovx), _f(tanfovy), _p(m), _p(d),
+                                   _p(n), _p(t), C.c_int(ks), _f(tol_cos), _p(gd), _p(gn))
+    return loss, gd, gn
+
+
 def adam(param, grad, m, v, step, lr, beta1, beta2, eps, biased=False, sparse=False):
     p = _c(param, np.float32).copy(); m = _c(m, np.float32).copy(); v = _c(v, np.float32).copy()
     lib().svo_adam(C.c_int(p.size), C.c_int(int(biased)), C.c_int(int(sparse)), _p(p), _p(_c(grad, np.float32)),

@@ -971,6 +971,96 @@ int svo_quantize(int64_t n, const float* v, int max_iter, uint8_t* index_out, fl
     return rounds;
 }
 
+/* ------------------------------------------------------------------ normal-from-depth losses
+ * src/cameras.py:104-127 (depth2pts: position + rd * depth, rd of cuda/src/utils.cu:47-72;
+ * depth2normal: normalize(cross(dx, dy)) on the interior, dx / dy the differences of the points
+ * pad = ks/2 to either side, optionally zeroed where dot(normal, normalize(pts - position)) <=
+ * tol_cos) and src/utils/loss_utils.py:345-407: NormalDepthConsistencyLoss (alpha = 1 - T,
+ * N = -normal * alpha, loss = mean((alpha^2 - <n_r, N>) * mask)) and
+ * NormalMedianConsistencyLoss (N = -normal, loss = mean((1 - <n_r, N>) * mask)), mask = N != 0
+ * anywhere.  Returns the loss (weight 1) and ADDS its gradient with respect to the depth plane
+ * and the rendered normals (alpha, the tolerance mask and the loss mask held constant, as the
+ * reference's no_grad / detach make them). */
+double svo_normal_depth_loss(int W, int H, float cx, float cy, float tanfovx, float tanfovy, const float* c2w,
+                             const float* depth, const float* nr, const float* T, int ks, float tol_cos,
+                             float* grad_depth, float* grad_normal) {
+    const int pad = ks / 2;
+    const int64_t P = (int64_t)W * H;
+    float* rd = (float*)malloc(sizeof(float) * 3 * P);
+    float* pts = (float*)malloc(sizeof(float) * 3 * P);
+    float* gdx = (float*)calloc((size_t)(3 * P), sizeof(float));
+    float* gdy = (float*)calloc((size_t)(3 * P), sizeof(float));
+    for (int y = 0; y < H; ++y) for (int x = 0; x < W; ++x) {
+        int64_t q = (int64_t)y * W + x;
+        float u = ((float)x + 0.5f - cx) * 2.f * tanfovx / (float)W;
+        float v = ((float)y + 0.5f - cy) * 2.f * tanfovy / (float)H;
+        for (int k = 0; k < 3; ++k) {
+            rd[k * P + q] = c2w[4 * k] * u + c2w[4 * k + 1] * v + c2w[4 * k + 2];
+            pts[k * P + q] = c2w[4 * k + 3] + rd[k * P + q] * depth[q];
+        }
+    }
+    const float inv_hw = 1.f / (float)P;
+    double loss = 0.0;
+    for (int y = pad; y < H - pad; ++y) for (int x = pad; x < W - pad; ++x) {
+        int64_t q = (int64_t)y * W + x;
+        int64_t xp = q + pad, xm = q - pad, yp = q + (int64_t)pad * W, ym = q - (int64_t)pad * W;
+        float dx[3], dy[3], c[3], n[3];
+        for (int k = 0; k < 3; ++k) { dx[k] = pts[k * P + xp] - pts[k * P + xm]; dy[k] = pts[k * P + yp] - pts[k * P + ym]; }
+        c[0] = dx[1] * dy[2] - dx[2] * dy[1];
+        c[1] = dx[2] * dy[0] - dx[0] * dy[2];
+        c[2] = dx[0] * dy[1] - dx[1] * dy[0];
+        float cn = sqrtf(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+        float den = cn > 1e-12f ? cn : 1e-12f;
+        for (int k = 0; k < 3; ++k) n[k] = c[k] / den;
+        float s = 1.f;
+        if (tol_cos > 0.f) {
+            float pd[3];
+            for (int k = 0; k < 3; ++k) pd[k] = pts[k * P + q] - c2w[4 * k + 3];
+            float pn = sqrtf(pd[0] * pd[0] + pd[1] * pd[1] + pd[2] * pd[2]);
+            pn = pn > 1e-12f ? pn : 1e-12f;
+            float dot = n[0] * (pd[0] / pn) + n[1] * (pd[1] / pn) + n[2] * (pd[2] / pn);
+            if (!(dot > tol_cos)) s = 0.f;
+        }
+        float alpha = T ? 1.f - T[q] : 1.f;
+        if (T) s *= alpha;
+        float N[3] = {-n[0] * s, -n[1] * s, -n[2] * s};
+        if (!(N[0] != 0.f || N[1] != 0.f || N[2] != 0.f)) continue;
+        float target = T ? alpha * alpha : 1.f;
+        float dotn = nr[q] * N[0] + nr[P + q] * N[1] + nr[2 * P + q] * N[2];
+        loss += (double)(target - dotn);
+        for (int k = 0; k < 3; ++k) grad_normal[k * P + q] += -N[k] * inv_hw;
+        /* dL/dn = s * n_r / HW; through the clamped normalisation; then dc = dx x dy */
+        float g[3], gc[3];
+        for (int k = 0; k < 3; ++k) g[k] = s * nr[k * P + q] * inv_hw;
+        if (cn > 1e-12f) {
+            float ng = n[0] * g[0] + n[1] * g[1] + n[2] * g[2];
+            for (int k = 0; k < 3; ++k) gc[k] = (g[k] - n[k] * ng) / cn;
+        } else {
+            for (int k = 0; k < 3; ++k) gc[k] = g[k] / 1e-12f;
+        }
+        float* a = gdx + q; float* b = gdy + q;
+        a[0] += dy[1] * gc[2] - dy[2] * gc[1];          /* dL/ddx = dy x gc */
+        a[P] += dy[2] * gc[0] - dy[0] * gc[2];
+        a[2 * P] += dy[0] * gc[1] - dy[1] * gc[0];
+        b[0] += gc[1] * dx[2] - gc[2] * dx[1];          /* dL/ddy = gc x dx */
+        b[P] += gc[2] * dx[0] - gc[0] * dx[2];
+        b[2 * P] += gc[0] * dx[1] - gc[1] * dx[0];
+    }
+    for (int y = 0; y < H; ++y) for (int x = 0; x < W; ++x) {
+        int64_t q = (int64_t)y * W + x;
+        float gp[3] = {0.f, 0.f, 0.f};
+        for (int k = 0; k < 3; ++k) {
+            if (x - pad >= 0) gp[k] += gdx[k * P + q - pad];
+            if (x + pad < W) gp[k] -= gdx[k * P + q + pad];
+            if (y - pad >= 0) gp[k] += gdy[k * P + q - (int64_t)pad * W];
+            if (y + pad < H) gp[k] -= gdy[k * P + q + (int64_t)pad * W];
+        }
+        grad_depth[q] += rd[q] * gp[0] + rd[P + q] * gp[1] + rd[2 * P + q] * gp[2];
+    }
+    free(rd); free(pts); free(gdx); free(gdy);
+    return loss / (double)P;
+}
+
 /* ------------------------------------------------------------------ Adam
  * cuda/src/adam_step.cu:21-159 (host bias corrections in double). */
 static inline float lerp_(float v0, float v1, float t) { return fmaf(t, v1, fmaf(-t, v0, v0)); }

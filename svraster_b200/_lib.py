@@ -81,6 +81,7 @@ _SIGS = {
     "svr_voxel_gradient_bw": (_I, [_I, _I, _P, _P, _P, _I64, _P, _F, _P, _P, _P]),
     "svr_total_variation_bw": (_I, [_I64, _I, _P, _P, _I64, _F, _P, _I, _I, _P, _P, _P, _P]),
     "svr_points_loss_bw": (_I, [_I, _P, _I, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _I, _F, _P, _P, _P]),
+    "svr_normal_depth_loss": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P, _P]),
     "svr_quantize_workspace_bytes": (_I, [_I64, C.POINTER(C.c_size_t)]),
     "svr_quantize": (_I, [_I64, _P, _I, _P, _P, _P, _SZ, C.POINTER(C.c_int), _P, _P]),
     "svr_dequantize": (_I, [_I64, _P, _P, _P, _P]),

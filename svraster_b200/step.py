@@ -26,10 +26,14 @@ class BatchedTrainStep:
 
     def __init__(self, scene, cams, device="cuda", lr=(1e-3, 1e-3, 1e-4), betas=(0.1, 0.99), eps=1e-15,
                  lambda_ls=1e-3, lambda_ge=1e-3, lambda_R_concen=0.0, sh_degree=3, seed=0, fused_smoothness=True,
-                 sh_dtype="f32"):
+                 sh_dtype="f32", normal_losses=None):
         """``sh_dtype="bf16"`` stores the SH coefficients in bf16 (the precision configuration):
         colours, compositing, transmittance and every gradient stay f32, Adam keeps f32 moments
-        and rounds the updated coefficients to nearest bf16."""
+        and rounds the updated coefficients to nearest bf16.  ``normal_losses`` (a dict with
+        any of lambda_dmean, dmean_ks, dmean_tol_deg, lambda_dmed; train.py:159-166, 418-425)
+        adds the normal-from-depth consistency losses of the rendered batch: one launch each
+        between the render forward and the adjoint, their gradients added to the upstream
+        depth / normal planes the adjoint reads."""
         dev = torch.device(device)
         self.dev = dev
         t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
@@ -89,6 +93,14 @@ class BatchedTrainStep:
         self.dnormal = torch.randn(3 * P, device=dev, generator=g)
         self.dT = torch.zeros(P, device=dev)
         self.gt = torch.rand(3 * P, device=dev, generator=g) if self.lambda_R > 0 else None
+        nl = dict(lambda_dmean=0.0, dmean_ks=3, dmean_tol_deg=90.0, lambda_dmed=0.0)
+        nl.update(normal_losses or {})
+        self.normal_losses = nl
+        self.nd_on = nl["lambda_dmean"] > 0 or nl["lambda_dmed"] > 0
+        if self.nd_on:
+            self.ddepth_w = torch.empty_like(self.ddepth)
+            self.dnormal_w = torch.empty_like(self.dnormal)
+            self.nd_loss = torch.zeros(self.V, dtype=torch.float64, device=dev)
         # per-step buffers
         self.geos = torch.empty(self.N, 8, device=dev)
         self.rgbs = torch.empty(self.V * self.N, 3, device=dev)
@@ -153,11 +165,30 @@ class BatchedTrainStep:
         color, depth, normal, T, _ = state.render(3, True, True, self.centers, self.lengths, self.geos, self.rgbs,
                                                   self.s_val, rgb_per_view=True)
         mark("render_fwd")   # includes the record packing launch
+        ddepth, dnormal = self.ddepth, self.dnormal
+        if self.nd_on:
+            # loss_utils.py:345-407 on the rendered planes, added to the upstream gradients
+            nl = self.normal_losses
+            self.ddepth_w.copy_(self.ddepth)
+            self.dnormal_w.copy_(self.dnormal)
+            self.nd_loss.zero_()
+            if nl["lambda_dmean"] > 0:
+                tol = float(np.float32(np.cos(np.deg2rad(nl["dmean_tol_deg"]))))
+                check(L.svr_normal_depth_loss(state.views, self.V, 0, int(nl["dmean_ks"]), tol if tol > 0 else -1.0,
+                                              float(nl["lambda_dmean"]), ptr(depth), ptr(normal), ptr(T),
+                                              ptr(self.nd_loss), ptr(self.ddepth_w), ptr(self.dnormal_w), st),
+                      "normal-depth loss")
+            if nl["lambda_dmed"] > 0:
+                check(L.svr_normal_depth_loss(state.views, self.V, 1, 3, -1.0, float(nl["lambda_dmed"]), ptr(depth),
+                                              ptr(normal), ptr(T), ptr(self.nd_loss), ptr(self.ddepth_w),
+                                              ptr(self.dnormal_w), st), "normal-median loss")
+            ddepth, dnormal = self.ddepth_w, self.dnormal_w
+            mark("normal_losses")
         self.dvox.zero_()
         self.drgbs.zero_()
         self.ds.zero_()
         mark("zero")
-        state.render_backward(True, True, self.s_val, T, self.dcolor, self.ddepth, self.dnormal, self.dT,
+        state.render_backward(True, True, self.s_val, T, self.dcolor, ddepth, dnormal, self.dT,
                               lambda_R_concen=self.lambda_R, gt_color=self.gt, drgbs=self.drgbs, dvox=self.dvox,
                               ds=self.ds)
         mark("render_bwd")
