@@ -5,9 +5,11 @@ a torus, SH degree 3, 8 views of 800x800 on a Fibonacci sphere of radius 3.  One
 all 8 views forward and backward and runs the SDF regularisers and Adam (svraster_b200.step).
 
   value : forward+backward Mrays/s of the batched step, inputs resident in HBM
-  e2e   : the same metric through the drop-in per-view API (svraster_b200.renderer with
-          autograd), upstream gradient planes copied from pinned host memory every step
-          and a scalar read back
+  e2e   : the same metric through the batched C-ABI training step (BatchedTrainStep, two
+          CUDA graphs), that step's upstream gradient planes and target image copied from
+          pinned host memory every step (overlapping the forward graph) and the mean
+          transmittance read back; ``e2e_dropin_per_view`` is the same through the drop-in
+          per-view API (svraster_b200.renderer with autograd, grid_loss_bw, SparseAdam)
   roofline : the dominant kernel's algorithmic bytes / CUDA-event duration vs the measured
           HBM copy bandwidth (MEASURED_PEAKS.json)
   cpu_baseline : the CPU oracle (single thread) on one view of the same workload
@@ -246,6 +248,70 @@ def run_ours(args, rank, world):
               "autotuned_render": ({k: tuned[k] for k in ("fwd_config", "bwd_config", "ms")} if tuned
                                    else "default configuration")}
     return result, step, scene, cams
+
+
+def run_e2e_batched(args, scene, cams, dev):
+    """The same metric through the batched C-ABI path (svraster_b200.step.BatchedTrainStep,
+    the step as a forward graph and two backward graphs) with host-resident inputs: every step
+    copies a step's upstream gradient planes and target image (dL/dcolor, dL/ddepth,
+    dL/dnormal, gt; 13 floats per pixel) from pinned host memory on a copy stream, one step
+    ahead into the other of two plane sets, and reads the mean transmittance back."""
+    import torch
+    from svraster_b200.step import BatchedTrainStep
+    step = BatchedTrainStep(scene, cams, device=dev, lambda_R_concen=0.1)
+    rng = np.random.default_rng(1)
+    P = step.P
+    host = [torch.from_numpy(rng.normal(size=n * P).astype(np.float32)).pin_memory() for n in (3, 4, 3)]
+    host.append(torch.from_numpy(rng.uniform(size=3 * P).astype(np.float32)).pin_memory())
+    h2d = sum(h.numel() * 4 for h in host)
+    for _ in range(args.warmup):
+        step.step()
+    # two sets of upstream planes, one backward graph each: the copies of step k+1's planes
+    # into one set overlap the whole of step k, whose adjoint reads the other set
+    step.capture(split=True, upstream_sets=2)
+    copy_stream = torch.cuda.Stream(device=dev)
+    done = [torch.cuda.Event(), torch.cuda.Event()]     # set i free again (its adjoint ran)
+    filled = [torch.cuda.Event(), torch.cuda.Event()]   # set i holds its step's planes
+    k = [0]
+
+    def fill(i):
+        copy_stream.wait_event(done[i])
+        with torch.cuda.stream(copy_stream):
+            for hsrc, ddst in zip(host, step.upstream(i)):
+                ddst.copy_(hsrc, non_blocking=True)
+        filled[i].record(copy_stream)
+
+    def one_step():
+        i = k[0] % 2
+        compute = torch.cuda.current_stream(dev)
+        fill(1 - i)                               # the next step's planes, during this step
+        step.replay_forward()
+        compute.wait_event(filled[i])
+        _, T = step.replay_backward(i)
+        done[i].record(compute)
+        k[0] += 1
+        return float(T.mean().item())             # device -> host read of the step's result
+
+    for e in done:
+        e.record(torch.cuda.current_stream(dev))
+    fill(0)
+    for _ in range(3):
+        one_step()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        one_step()
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    status = step.graph_status()
+    del step
+    torch.cuda.empty_cache()
+    return {"value": round(P / (ms * 1e-3) / 1e6, 3), "unit": "Mrays/s", "ms_per_step": round(ms, 3),
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4, "graph_status": list(status),
+            "path": "svraster_b200.step.BatchedTrainStep (C ABI, forward / backward graphs), "
+                    "upstream planes from pinned host memory every step, mean T read back"}
 
 
 def run_e2e(args, scene, cams, dev):
@@ -760,7 +826,9 @@ def main():
         if not args.no_e2e:
             del step
             torch.cuda.empty_cache()
-            result["e2e"] = run_e2e(args, scene, cams, torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
+            dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+            result["e2e"] = run_e2e_batched(args, scene, cams, dev)
+            result["e2e_dropin_per_view"] = run_e2e(args, scene, cams, dev)
         if not args.no_cpu:
             result["cpu_baseline"] = cpu_baseline(scene, cams)
         print(json.dumps(result), flush=True)

@@ -117,6 +117,7 @@ class BatchedTrainStep:
         leaf_paths = np.asarray(scene.octpath, dtype=np.int64)[np.asarray(scene.is_leaf).astype(bool).reshape(-1)]
         self.path_or_all = int(np.bitwise_or.reduce(leaf_paths.view(np.uint64))) if leaf_paths.size else 0
         self.graph = None
+        self.graph_b = None
         self.graph_out = None
         self.capacity = None
         self.step_dev = None
@@ -136,9 +137,6 @@ class BatchedTrainStep:
         return out
 
     def _body(self, graph, time_render=False, grad_hook=None):
-        L = _lib.load()
-        st = stream_ptr(self.dev)
-        N = self.N
         marks = []
 
         def mark(name):
@@ -148,6 +146,14 @@ class BatchedTrainStep:
                 marks.append((name, e))
 
         mark("start")
+        fw = self._forward_part(graph, mark)
+        return self._backward_part(graph, mark, grad_hook, fw, marks, time_render)
+
+    def _forward_part(self, graph, mark):
+        """Gather, SH, preprocess, binning and the render forward of the batch."""
+        L = _lib.load()
+        st = stream_ptr(self.dev)
+        N = self.N
         check(L.svr_gather_geo(N, ptr(self.all_idx), ptr(self.vox_key), ptr(self.grid), ptr(self.geos), st),
               "gather")
         sh_eval = L.svr_sh_eval_views_bf16 if self.sh_bf16 else L.svr_sh_eval_views
@@ -165,6 +171,15 @@ class BatchedTrainStep:
         color, depth, normal, T, _ = state.render(3, True, True, self.centers, self.lengths, self.geos, self.rgbs,
                                                   self.s_val, rgb_per_view=True)
         mark("render_fwd")   # includes the record packing launch
+        return state, color, depth, normal, T
+
+    def _backward_part(self, graph, mark, grad_hook, fw, marks, time_render):
+        """Normal losses (when on), the render adjoint, smoothness, scatter, SH adjoint and
+        Adam; reads the upstream gradient planes (dcolor, ddepth, dnormal, gt)."""
+        L = _lib.load()
+        st = stream_ptr(self.dev)
+        N = self.N
+        state, color, depth, normal, T = fw
         ddepth, dnormal = self.ddepth, self.dnormal
         if self.nd_on:
             # loss_utils.py:345-407 on the rendered planes, added to the upstream gradients
@@ -270,12 +285,19 @@ class BatchedTrainStep:
         torch.cuda.synchronize(self.dev)
         return self.tuned
 
-    def capture(self, capacity=None, rows=1 << 20):
+    def capture(self, capacity=None, rows=1 << 20, split=False, upstream_sets=1):
         """Capture one whole step (gather, SH, preprocess, scan, duplicate, sort, pack, render
         forward and adjoint, scatter, SH adjoint, smoothness adjoints, Adam) into a CUDA graph.
         ``capacity`` bounds the records per step (default: this batch's record total, found by
         one counting pass); a replay that needs more sets status bit 8 (``graph_status``).
-        Returns the number of this library's kernels in the graph."""
+        ``split=True`` captures two graphs sharing one memory pool: the forward part (up to
+        the render forward) and the backward part (everything that reads the upstream
+        gradient planes), replayed by ``replay_forward`` / ``replay_backward`` (``replay`` runs
+        both), so that a caller can refill the upstream planes while the forward part runs.  With
+        ``upstream_sets=2`` (split only) one backward graph is captured per set of upstream
+        planes (``upstream(i)``); ``replay_backward(i)`` reads set i, so the next step's
+        planes can be copied into the other set during the whole current step.
+        Returns the number of this library's kernels in the graph(s)."""
         L = _lib.load()
         if capacity is None:
             probe = RasterState(self.views, self.N, self.dev)
@@ -295,11 +317,36 @@ class BatchedTrainStep:
             self.coef_tables.append(torch.from_numpy(tab).to(self.dev))
         self.step_dev = torch.full((1,), self.adam_step, dtype=torch.int64, device=self.dev)
         torch.cuda.synchronize(self.dev)
-        self.graph = torch.cuda.CUDAGraph()
         n0 = L.svr_kernel_launches()
         # the step counter and parameters must not move during capture: capture runs no work
-        with torch.cuda.graph(self.graph):
-            self.graph_out = self._body(True)
+        nomark = lambda name: None
+        if upstream_sets not in (1, 2) or (upstream_sets == 2 and not split):
+            raise ValueError("upstream_sets is 1, or 2 with split=True")
+        names = ("dcolor", "ddepth", "dnormal", "gt")
+        sets = [tuple(getattr(self, n) for n in names)]
+        if upstream_sets == 2:
+            sets.append(tuple(None if t is None else t.clone() for t in sets[0]))
+        self._up_sets = sets
+        if split:
+            self.graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.graph):
+                self._graph_fw = self._forward_part(True, nomark)
+            self.graph_bs = []
+            for up in sets:
+                for n, t in zip(names, up):
+                    setattr(self, n, t)
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g, pool=self.graph.pool()):
+                    self.graph_out = self._backward_part(True, nomark, None, self._graph_fw, [], False)
+                self.graph_bs.append(g)
+            for n, t in zip(names, sets[0]):
+                setattr(self, n, t)
+            self.graph_b = self.graph_bs[0]
+        else:
+            self.graph = torch.cuda.CUDAGraph()
+            self.graph_b = None
+            with torch.cuda.graph(self.graph):
+                self.graph_out = self._body(True)
         self.graph_launches = int(L.svr_kernel_launches() - n0)
         torch.cuda.synchronize(self.dev)
         self._dev_step_synced = True
@@ -312,12 +359,38 @@ class BatchedTrainStep:
             raise RuntimeError("capture() first")
         if self.adam_step + 1 >= self.coef_rows:
             raise RuntimeError("Adam coefficient table exhausted; capture again with more rows")
+        self.replay_forward()
+        return self.replay_backward()
+
+    def replay_forward(self):
+        """The forward part of a step captured with ``split=True`` (or the whole step of an
+        unsplit capture, whose ``replay_backward`` is then a no-op)."""
+        if self.graph is None:
+            raise RuntimeError("capture() first")
+        if self.adam_step + 1 >= self.coef_rows:
+            raise RuntimeError("Adam coefficient table exhausted; capture again with more rows")
         if not self._dev_step_synced:
             self.step_dev.fill_(self.adam_step)
             self._dev_step_synced = True
         self.graph.replay()
-        self.adam_step += 1
+        if self.graph_b is None:
+            self.adam_step += 1
         return self.graph_out
+
+    def replay_backward(self, upstream_set=0):
+        """The backward part of a split capture: reads the upstream gradient planes of set
+        ``upstream_set`` as they are when it runs.  Returns (color, T) of the step."""
+        if self.graph_b is not None:
+            self.graph_bs[upstream_set].replay()
+            self.adam_step += 1
+        return self.graph_out
+
+    def upstream(self, i=0):
+        """The upstream tensors (dcolor, ddepth, dnormal, gt) of set i of the last capture
+        (set 0 is the step's own)."""
+        if getattr(self, "_up_sets", None):
+            return self._up_sets[i]
+        return (self.dcolor, self.ddepth, self.dnormal, self.gt)
 
     def graph_status(self):
         """Status words after replays: (raster status, smoothness / Adam status)."""

@@ -167,3 +167,58 @@ def test_bf16_sh_step_eager_and_replay():
     assert _param_close(a.grid, b.grid, a.lr[0])
     d = (a.sh0.float() - b.sh0.float()).abs()
     assert (d > 0).float().mean().item() < 2e-3
+
+
+def test_split_capture_matches_whole_capture():
+    """capture(split=True): the forward and backward graphs replayed in turn give the same
+    images and (up to atomic order) the same parameters as the whole-step graph, and the
+    backward graph reads the upstream planes as they are when it runs."""
+    a, b = _step_pair()
+    a.capture()
+    b.capture(split=True)
+    for k in range(2):
+        ca, Ta = a.replay()
+        b.replay_forward()
+        cb, Tb = b.replay_backward()
+        torch.cuda.synchronize()
+        if k == 0:
+            assert torch.equal(ca, cb) and torch.equal(Ta, Tb)
+    assert a.adam_step == b.adam_step == 2
+    assert b.graph_status() == (0, 0)
+    for pa, pb, lr in zip(a.params, b.params, a.lr):
+        assert _param_close(pa, pb, lr)
+    # upstream planes rewritten between the two parts are what that step's adjoint reads:
+    # zeroing them there equals an eager step with zeroed planes
+    c, d = _step_pair()
+    c.capture(split=True)
+    c.replay_forward()
+    for x in (c.dcolor, c.ddepth, c.dnormal):
+        x.zero_()
+    c.replay_backward()
+    for x in (d.dcolor, d.ddepth, d.dnormal):
+        x.zero_()
+    d.step()
+    torch.cuda.synchronize()
+    for pc, pd, lr in zip(c.params, d.params, c.lr):
+        assert _param_close(pc, pd, lr)
+
+
+def test_split_capture_with_two_upstream_sets():
+    """upstream_sets=2: the second backward graph reads the second plane set; alternating sets
+    that hold the same planes gives the single-set result."""
+    a, b = _step_pair()
+    a.capture(split=True)
+    b.capture(split=True, upstream_sets=2)
+    for x, y in zip(b.upstream(0), b.upstream(1)):
+        assert x is not y and (x is None or torch.equal(x, y))
+    for k in range(3):
+        a.replay_forward()
+        ca, Ta = a.replay_backward()
+        b.replay_forward()
+        cb, Tb = b.replay_backward(k % 2)
+        torch.cuda.synchronize()
+        if k == 0:
+            assert torch.equal(ca, cb) and torch.equal(Ta, Tb)
+    assert b.graph_status() == (0, 0)
+    for pa, pb, lr in zip(a.params, b.params, a.lr):
+        assert _param_close(pa, pb, lr)
