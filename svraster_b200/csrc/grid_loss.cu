@@ -213,6 +213,17 @@ __device__ __forceinline__ bool neighbours_ok(int x, int y, int z, int res, cons
     return mask[c + 1] && mask[c - 1] && mask[c + res] && mask[c - res] && mask[c + rr] && mask[c - rr];
 }
 
+// Cell index -> (x, y, z).  The dense grid's side is a power of two in every caller of the
+// reference (2^level), which takes shifts; any other side takes the divisions.
+__device__ __forceinline__ void cell_xyz(int gk, int res, int& x, int& y, int& z) {
+    if ((res & (res - 1)) == 0) {
+        const int lg = __ffs(res) - 1;
+        x = gk & (res - 1); y = (gk >> lg) & (res - 1); z = gk >> (2 * lg);
+    } else {
+        x = gk % res; y = (gk / res) % res; z = gk / (res * res);
+    }
+}
+
 struct SampleCtx {
     int G, N, M, res;
     const int32_t* dense;   // optional direct-mapped key -> table row (-1 when absent)
@@ -319,7 +330,7 @@ __global__ void __launch_bounds__(256) laplacian_kernel(SampleCtx c, int A, cons
             gk = c.keys[a];
             if (gk < 0 || gk >= res * res * res) { atomicOr(status, ERR_BAD_INDEX); valid = false; }
             else {
-                x = gk % res; y = (gk / res) % res; z = gk / (res * res);
+                cell_xyz(gk, res, x, y, z);
                 valid = mask[gk] && neighbours_ok(x, y, z, res, mask);
             }
         }
@@ -366,7 +377,7 @@ __global__ void __launch_bounds__(256) eikonal_kernel(SampleCtx c, int A, const 
             gk = c.keys[a];
             if (gk < 0 || gk >= res * res * res) { atomicOr(status, ERR_BAD_INDEX); valid = false; }
             else {
-                x = gk % res; y = (gk / res) % res; z = gk / (res * res);
+                cell_xyz(gk, res, x, y, z);
                 valid = mask[gk] && neighbours_ok(x, y, z, res, mask);
             }
         }
@@ -547,7 +558,7 @@ __global__ void __launch_bounds__(256) smooth_vox_kernel(VoxCtx c, int A, const 
             const int gk = c.keys[a];
             if (gk < 0 || gk >= res * res * res) { atomicOr(status, ERR_BAD_INDEX); valid = false; }
             else {
-                x = gk % res; y = (gk / res) % res; z = gk / (res * res);
+                cell_xyz(gk, res, x, y, z);
                 valid = mask[gk] && neighbours_ok(x, y, z, res, mask);
             }
         }
