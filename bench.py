@@ -151,8 +151,7 @@ def run_ours(args, rank, world):
     # data parallel over views: the gradients are summed across ranks between the adjoints
     # and Adam (the one exchange step of the path)
     def allreduce_grads(grads):
-        for g in grads:
-            dist.all_reduce(g)
+        dist.all_reduce(step.grad_flat)           # grid, sh0 and shs gradients in one call
     hook = allreduce_grads if world > 1 else None
     # one GPU: the timed steps replay one CUDA graph holding the whole step (the record count
     # stays on the device); several GPUs: eager steps with the all-reduce between them

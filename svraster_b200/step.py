@@ -107,7 +107,15 @@ class BatchedTrainStep:
         self.dvox = torch.zeros(self.N, 12, device=dev)
         self.drgbs = torch.zeros(self.V * self.N, 3, device=dev)
         self.ds = torch.zeros(1, device=dev)
-        self.grads = [torch.zeros(p.shape, dtype=torch.float32, device=dev) for p in self.params]
+        # the gradients are views into one flat buffer (each view 256-byte aligned), so that a
+        # step zeroes them with one fill and a data-parallel step exchanges them with one
+        # all-reduce (``grad_flat``)
+        offs, total = [], 0
+        for p in self.params:
+            offs.append(total)
+            total += (p.numel() + 63) // 64 * 64
+        self.grad_flat = torch.zeros(total, dtype=torch.float32, device=dev)
+        self.grads = [self.grad_flat[o:o + p.numel()].view(p.shape) for o, p in zip(offs, self.params)]
         self.all_idx = torch.arange(self.N, dtype=torch.int64, device=dev)
         self.state = None
         self.ev = None
@@ -129,7 +137,8 @@ class BatchedTrainStep:
     # ------------------------------------------------------------------ one step
     def step(self, time_render=False, grad_hook=None):
         """One training step.  ``grad_hook(grads)`` runs between the adjoints and Adam (the
-        data-parallel all-reduce of the gradients goes there).  With ``time_render`` every
+        data-parallel all-reduce of the gradients goes there; ``grad_flat`` holds all of them
+        contiguously).  With ``time_render`` every
         stage is bracketed by CUDA events on the launching stream (see ``stage_ms``)."""
         out = self._body(False, time_render, grad_hook)
         self.adam_step += 1
@@ -219,8 +228,7 @@ class BatchedTrainStep:
                                           float(self.lambda_ge), self.vox_size_min_inv, seed, step_ptr,
                                           ptr(self.dvox), 12, ptr(self.status), st), "smoothness")
             mark("smoothness")
-        for gr in self.grads:
-            gr.zero_()
+        self.grad_flat.zero_()
         check(L.svr_scatter_vox_grads(N, 12, ptr(self.vox_key), ptr(self.dvox), ptr(self.grads[0]), st), "scatter")
         check(L.svr_sh_eval_views_bw(N, self.V, self.sh_degree, self.M_sh, ptr(self.centers), ptr(self.cam_pos),
                                      ptr(self.drgbs), ptr(self.grads[1]), ptr(self.grads[2]), st), "sh views bw")
