@@ -224,6 +224,19 @@ __device__ __forceinline__ void cell_xyz(int gk, int res, int& x, int& y, int& z
     }
 }
 
+// (p - base) / size as the reference divides, per component.  Grid-unit voxel sizes are
+// powers of two, for which multiplying by the reciprocal (itself exact) gives the same bits
+// as the division; any other size divides.
+__device__ __forceinline__ float3 local_coord(float3 p, float3 base, float size) {
+    const float3 d = p - base;
+    const uint32_t b = __float_as_uint(size);
+    if ((b & 0x007FFFFFu) == 0u && ((b >> 23) & 0xFFu) - 1u < 0xFDu) {   // normal power of two
+        const float r = __uint_as_float(((254u - ((b >> 23) & 0xFFu)) << 23) | (b & 0x80000000u));
+        return f3(d.x * r, d.y * r, d.z * r);
+    }
+    return d / size;
+}
+
 struct SampleCtx {
     int G, N, M, res;
     const int32_t* dense;   // optional direct-mapped key -> table row (-1 when absent)
@@ -248,7 +261,7 @@ __device__ __forceinline__ int sample_cell(const SampleCtx& c, int x, int y, int
     const float3 pt = f3(x + rv.x, y + rv.y, z + rv.z);
     const float3 base = f3(c.coords[3 * v], c.coords[3 * v + 1], c.coords[3 * v + 2]);
     const float size = c.vsizes[v];
-    tri_weights((pt - base) / size, w);
+    tri_weights(local_coord(pt, base, size), w);
     float s = 0.f;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
@@ -503,7 +516,7 @@ __device__ __forceinline__ float sample_vox(const VoxCtx& c, int id, int x, int 
     const float3 pt = f3(x + rv.x, y + rv.y, z + rv.z);
     const float3 base = f3(c.coords[3 * vv], c.coords[3 * vv + 1], c.coords[3 * vv + 2]);
     const float size = c.vsizes[vv];
-    q = (pt - base) / size;
+    q = local_coord(pt, base, size);
     const float4 g0 = c.geos[2 * (size_t)vv], g1 = c.geos[2 * (size_t)vv + 1];
     const float g[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
     float w[8];
@@ -770,8 +783,8 @@ __global__ void __launch_bounds__(256) points_loss_kernel(int P, const float* __
     const int v = c.g2v[id];
     if (v < 0 || v >= c.N) { atomicOr(status, ERR_BAD_INDEX); return; }
     const float size = c.vsizes[v];
-    const float3 q = f3((px - c.coords[3 * v]) / size, (py - c.coords[3 * v + 1]) / size,
-                        (pz - c.coords[3 * v + 2]) / size);
+    const float3 q = local_coord(f3(px, py, pz), f3(c.coords[3 * v], c.coords[3 * v + 1], c.coords[3 * v + 2]),
+                                 size);
     float w[8];
     tri_weights(q, w);
     int64_t k[8];
