@@ -150,6 +150,59 @@ __global__ void sh_eval_kernel(int N, int64_t n_idx, const int64_t* __restrict__
     rgbs[i] = res;
 }
 
+// Same evaluation with coalesced row loads when every coefficient row is full (NB == M): each
+// warp loads its 32 voxels' 180-byte rows one row at a time with consecutive lanes into
+// shared memory, then every thread evaluates its voxel from there (same arithmetic and order).
+template <int DEG>
+__global__ void __launch_bounds__(128) sh_eval_rows_kernel(int N, int64_t n_idx, const int64_t* __restrict__ idx,
+                                                           const float3* __restrict__ centers,
+                                                           const float3* __restrict__ cam_pos,
+                                                           const float3* __restrict__ sh0, const float* __restrict__ shs,
+                                                           float3* __restrict__ rgbs)
+{
+    constexpr int NB = (DEG + 1) * (DEG + 1);
+    constexpr int ROW = 3 * (NB - 1);
+    __shared__ float rows[128 * ROW + 1];
+    __shared__ int64_t vox[128];
+    const int64_t n = n_idx > 0 ? n_idx : N;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int64_t tt = (int64_t)blockIdx.x * 128 + t;
+    const int64_t i = tt < n ? (n_idx > 0 ? idx[tt] : tt) : -1;
+    vox[t] = i;
+    __syncwarp();
+    // all 32 rows' loads issue before any store (a row is at most 45 floats: two per lane)
+    static_assert(ROW <= 64, "row wider than two loads per lane");
+    float a[32], b[32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+        const int64_t v = vox[warp * 32 + r];
+        a[r] = (v >= 0 && lane < ROW) ? shs[ROW * v + lane] : 0.f;
+        b[r] = (v >= 0 && lane + 32 < ROW) ? shs[ROW * v + lane + 32] : 0.f;
+    }
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+        float* row = rows + (warp * 32 + r) * ROW;
+        if (lane < ROW) row[lane] = a[r];
+        if (lane + 32 < ROW) row[lane + 32] = b[r];
+    }
+    __syncwarp();
+    if (i < 0) return;
+    const float3 ro = *cam_pos;
+    float3 dir = centers[i] - ro;
+    dir = dir * rnorm3df(dir.x, dir.y, dir.z);
+    float B[16];
+    sh_basis<DEG>(dir, B);
+    const float* sh = rows + t * ROW;
+    float3 res = B[0] * sh0[i];
+#pragma unroll
+    for (int k = 1; k < NB; ++k) res = res + B[k] * f3(sh[3 * (k - 1)], sh[3 * (k - 1) + 1], sh[3 * (k - 1) + 2]);
+    res = res + 0.5f;
+    res.x *= (res.x > 0.0f);
+    res.y *= (res.y > 0.0f);
+    res.z *= (res.z > 0.0f);
+    rgbs[i] = res;
+}
+
 template <int DEG>
 __global__ void sh_eval_bw_kernel(int N, int64_t n_idx, const int64_t* __restrict__ idx, int M,
                                   const float3* __restrict__ centers, const float3* __restrict__ cam_pos,
@@ -183,6 +236,11 @@ extern "C" int svr_sh_eval(int N, int64_t n_idx, const int64_t* idx, int degree,
     const unsigned g = nblk(n, 256);
     const auto c = (const float3*)centers; const auto cp = (const float3*)cam_pos;
     const auto s0 = (const float3*)sh0; const auto ss = (const float3*)shs; auto o = (float3*)rgbs;
+    if (degree == 3 && M == 16) {
+        sh_eval_rows_kernel<3><<<nblk(n, 128), 128, 0, st>>>(N, n_idx, idx, c, cp, s0, shs, o);
+        LAUNCHED();
+        return SVR_OK;
+    }
     switch (degree) {
         case 0: sh_eval_kernel<0><<<g, 256, 0, st>>>(N, n_idx, idx, M, c, cp, s0, ss, o); break;
         case 1: sh_eval_kernel<1><<<g, 256, 0, st>>>(N, n_idx, idx, M, c, cp, s0, ss, o); break;
@@ -191,6 +249,52 @@ extern "C" int svr_sh_eval(int N, int64_t n_idx, const int64_t* idx, int degree,
     }
     LAUNCHED();
     return SVR_OK;
+}
+
+// Same adjoint with coalesced row stores when every coefficient row is full (NB == M): each
+// thread stages its voxel's 3 + 3(NB-1) gradient values in shared memory, then each warp
+// writes its 32 voxels' rows one row at a time with consecutive lanes (a 180-byte row is 6
+// sectors; one thread per row left 32 scattered sectors per warp store).
+template <int DEG>
+__global__ void __launch_bounds__(128) sh_eval_bw_rows_kernel(int N, int64_t n_idx, const int64_t* __restrict__ idx,
+                                                              const float3* __restrict__ centers,
+                                                              const float3* __restrict__ cam_pos,
+                                                              const float3* __restrict__ drgbs,
+                                                              float* __restrict__ dsh0, float* __restrict__ dshs)
+{
+    constexpr int NB = (DEG + 1) * (DEG + 1);
+    constexpr int ROW = 3 * (NB - 1);
+    __shared__ float rows[128 * ROW + 1];
+    __shared__ float dc[128 * 3];
+    __shared__ int64_t vox[128];
+    const int64_t n = n_idx > 0 ? n_idx : N;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int64_t tt = (int64_t)blockIdx.x * 128 + t;
+    int64_t i = -1;
+    if (tt < n) {
+        i = n_idx > 0 ? idx[tt] : tt;
+        const float3 ro = *cam_pos;
+        float3 dir = centers[i] - ro;
+        dir = dir * rnorm3df(dir.x, dir.y, dir.z);
+        float B[16];
+        sh_basis<DEG>(dir, B);
+        const float3 d = drgbs[i];
+        dc[3 * t] = B[0] * d.x; dc[3 * t + 1] = B[0] * d.y; dc[3 * t + 2] = B[0] * d.z;
+#pragma unroll
+        for (int k = 1; k < NB; ++k) {
+            rows[t * ROW + 3 * (k - 1)] = B[k] * d.x;
+            rows[t * ROW + 3 * (k - 1) + 1] = B[k] * d.y;
+            rows[t * ROW + 3 * (k - 1) + 2] = B[k] * d.z;
+        }
+    }
+    vox[t] = i;
+    __syncwarp();
+    for (int r = warp * 32; r < warp * 32 + 32; ++r) {
+        const int64_t v = vox[r];
+        if (v < 0) break;                                  // the warp's remaining slots are empty too
+        if (lane < 3) dsh0[3 * v + lane] = dc[3 * r + lane];
+        for (int j = lane; j < ROW; j += 32) dshs[ROW * v + j] = rows[r * ROW + j];
+    }
 }
 
 extern "C" int svr_sh_eval_bw(int N, int64_t n_idx, const int64_t* idx, int degree, int M, const float* centers,
@@ -203,6 +307,11 @@ extern "C" int svr_sh_eval_bw(int N, int64_t n_idx, const int64_t* idx, int degr
     const unsigned g = nblk(n, 256);
     const auto c = (const float3*)centers; const auto cp = (const float3*)cam_pos;
     const auto d = (const float3*)drgbs; auto o0 = (float3*)dsh0; auto o1 = (float3*)dshs;
+    if (degree == 3 && M == 16) {
+        sh_eval_bw_rows_kernel<3><<<nblk(n, 128), 128, 0, st>>>(N, n_idx, idx, c, cp, d, dsh0, dshs);
+        LAUNCHED();
+        return SVR_OK;
+    }
     switch (degree) {
         case 0: sh_eval_bw_kernel<0><<<g, 256, 0, st>>>(N, n_idx, idx, M, c, cp, d, o0, o1); break;
         case 1: sh_eval_bw_kernel<1><<<g, 256, 0, st>>>(N, n_idx, idx, M, c, cp, d, o0, o1); break;
