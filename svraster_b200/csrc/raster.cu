@@ -620,9 +620,9 @@ static int ensure_smem(K k, int smem, std::atomic<unsigned long long>& done)
 // R-concentration term).  Index 0 is the default build configuration.  The choice is process-
 // wide and read when a launch is issued (so a captured graph keeps the one in force then).
 struct RenderCfg { int ring, minb; };
-static const RenderCfg kFwdCfgs[] = {{SVR_NSLOT, SVR_FWD_MINB}, {3, 4}, {4, 3}, {3, 3}};
-static const RenderCfg kBwdCfgs[] = {{SVR_NSLOT, SVR_BWD_MINB}, {3, 3}, {4, 2}, {3, 2}};
-constexpr int N_FWD_CFGS = 4, N_BWD_CFGS = 4;
+static const RenderCfg kFwdCfgs[] = {{SVR_NSLOT, SVR_FWD_MINB}, {3, 4}, {4, 3}, {3, 3}, {3, 5}, {4, 5}};
+static const RenderCfg kBwdCfgs[] = {{SVR_NSLOT, SVR_BWD_MINB}, {3, 3}, {4, 2}, {3, 2}, {3, 4}, {4, 4}};
+constexpr int N_FWD_CFGS = 6, N_BWD_CFGS = 6;
 static std::atomic<int> g_fwd_cfg{0}, g_bwd_cfg{0};
 
 extern "C" int svr_render_config_count(int* n_fwd, int* n_bwd)
@@ -687,6 +687,8 @@ static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint32_t* or
             case 1: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 3, 4>(FWD_CFG_ARGS);
             case 2: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 4, 3>(FWD_CFG_ARGS);
             case 3: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 3, 3>(FWD_CFG_ARGS);
+            case 4: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 3, 5>(FWD_CFG_ARGS);
+            case 5: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 4, 5>(FWD_CFG_ARGS);
             default: break;
         }
     }
@@ -810,6 +812,8 @@ static int launch_bwd(int T, int N, cudaStream_t st, const Views& V, const uint3
             case 1: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 3, 3>(BWD_CFG_ARGS);
             case 2: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 4, 2>(BWD_CFG_ARGS);
             case 3: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 3, 2>(BWD_CFG_ARGS);
+            case 4: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 3, 4>(BWD_CFG_ARGS);
+            case 5: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 4, 4>(BWD_CFG_ARGS);
             default: break;
         }
     }
