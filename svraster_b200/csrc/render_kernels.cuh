@@ -30,14 +30,18 @@ namespace svr {
 #endif
 // Minimum resident CTAs per SM requested from the register allocator.  Left to itself the
 // allocator gives the adjoint 127-133 registers: 2 CTAs per SM at best, 1 when it crosses 128.
-// Measured on the mid-size workload (8 views 800x800): forward 4 CTAs (64 registers)
-// 3.57 ms vs 3 CTAs 3.69 ms; adjoint 3 CTAs (80 registers, 160 B spilled to L1) 5.96 ms vs
-// 2 CTAs 6.8-7.0 ms vs 1 CTA 11.7 ms.
+// Defaults are the autotuner's choices on both bench workloads (mid-size 8 x 800x800 and
+// 64 mixed-resolution views): forward 4 ring slots x 4 CTAs (64 registers); adjoint 3 ring
+// slots x 4 CTAs (64 registers, 248 B spilled to L1), 3.02 ms vs 3.12 ms for 4 x 3 (80
+// registers) and 3.68 ms for 4 x 2 on the mid-size batch.
 #ifndef SVR_FWD_MINB
 #define SVR_FWD_MINB 4
 #endif
 #ifndef SVR_BWD_MINB
-#define SVR_BWD_MINB 3
+#define SVR_BWD_MINB 4
+#endif
+#ifndef SVR_BWD_NSLOT
+#define SVR_BWD_NSLOT 3
 #endif
 constexpr int BATCH = SVR_BATCH;   // records per slot (80 B each)
 constexpr int NSLOT = SVR_NSLOT;   // ring depth
@@ -376,7 +380,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_kernel(
 }
 
 // ============================================================================ adjoint
-template <bool DEPTH, bool NORMAL, bool RCONC, int RING = NSLOT, int MINB = SVR_BWD_MINB>
+template <bool DEPTH, bool NORMAL, bool RCONC, int RING = SVR_BWD_NSLOT, int MINB = SVR_BWD_MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_kernel(
     const __grid_constant__ Views V, int N, const uint32_t* __restrict__ order, const uint2* __restrict__ ranges,
     const uint32_t* __restrict__ tile_last,
