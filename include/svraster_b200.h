@@ -143,8 +143,9 @@ SVR_API int svr_render_bwd(const svr_view_t* views_host, int n_views, int N, int
 
 /* Launch configurations of the render kernels (no counterpart in the reference): ring slots
  * and CTAs per SM, which change the schedule only (every configuration gives the same
- * outputs).  pass 0 = forward, 1 = adjoint; configuration 0 is the default (for the adjoint
- * it switches to configuration 4 in launches of fewer than 8192 tiles).  The choice is
+ * outputs).  pass 0 = forward, 1 = adjoint; configuration 0 is the default, which follows
+ * the launch size: under 8192 tiles the forward takes configuration 2 and the adjoint 2,
+ * under 16384 tiles the adjoint takes 4.  The choice is
  * process-wide and read when a launch is issued; svraster_b200.autotune times them on the
  * caller's workload. */
 SVR_API int svr_render_config_count(int* n_fwd, int* n_bwd);

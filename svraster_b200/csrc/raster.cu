@@ -624,7 +624,15 @@ static const RenderCfg kFwdCfgs[] = {{SVR_NSLOT, SVR_FWD_MINB}, {3, 4}, {4, 3}, 
 static const RenderCfg kBwdCfgs[] = {{SVR_BWD_NSLOT, SVR_BWD_MINB}, {3, 3}, {4, 2}, {3, 2}, {4, 3}, {4, 4}};
 constexpr int N_FWD_CFGS = 6, N_BWD_CFGS = 6;
 static std::atomic<int> g_fwd_cfg{0}, g_bwd_cfg{0};
-constexpr int BWD_SMALL_LAUNCH_TILES = 8192;   // below this the default adjoint config is 4 x 3
+// The default configuration follows the launch size.  Launches of a few thousand tiles are
+// bound by their heaviest tiles and run best with more registers per thread; measured with
+// the tuner on the mid-size scene (800x800 views, 2500 tiles each):
+//   1 view  : forward 4x3 0.954 ms (4x4 1.006); adjoint 4x2 1.085 ms (4x3 1.185, 3x4 1.30)
+//   2 views : forward 4x3 1.089 ms (4x4 1.163); adjoint 4x2 1.139 ms (4x3 1.287)
+//   4 views : forward 4x4 1.382 ms;             adjoint 4x3 1.466 ms (3x4 1.664)
+//   8 views : forward 4x4 2.47 ms;              adjoint 3x4 3.02 ms (4x3 3.12)
+constexpr int SMALL_LAUNCH_TILES = 8192;    // below: forward 4x3, adjoint 4x2
+constexpr int MEDIUM_LAUNCH_TILES = 16384;  // below: adjoint 4x3
 
 extern "C" int svr_render_config_count(int* n_fwd, int* n_bwd)
 {
@@ -684,7 +692,9 @@ static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint32_t* or
 {
 #define FWD_CFG_ARGS T, st, V, order, ranges, recs, s_val, tile_last, n_contrib, color, depth, normal, outT, max_w, mw_stride, status
     if constexpr (NS == 3 && DEPTH && NORMAL && !MAXW) {
-        switch (g_fwd_cfg.load()) {
+        int cfg = g_fwd_cfg.load();
+        if (cfg == 0 && T < SMALL_LAUNCH_TILES) cfg = 2;          // 4 x 3
+        switch (cfg) {
             case 1: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 3, 4>(FWD_CFG_ARGS);
             case 2: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 4, 3>(FWD_CFG_ARGS);
             case 3: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 3, 3>(FWD_CFG_ARGS);
@@ -809,11 +819,9 @@ static int launch_bwd(int T, int N, cudaStream_t st, const Views& V, const uint3
 {
 #define BWD_CFG_ARGS T, N, st, V, order, ranges, tl, nc, recs, s_val, out_T, dc, dd, dn, dT, lam, gt, dvox, drgbs, ds, status
     if constexpr (DEPTH && NORMAL) {
-        // the default takes 4 ring slots x 3 CTAs for small launches: one 800x800 view (2500
-        // tiles) is bound by its heaviest tiles and ran 1.14 ms there against 1.30 ms for
-        // 3 x 4, which wins on batches (3.02 vs 3.12 ms on 8 views, 20000 tiles)
         int cfg = g_bwd_cfg.load();
-        if (cfg == 0 && T < BWD_SMALL_LAUNCH_TILES) cfg = 4;
+        if (cfg == 0 && T < SMALL_LAUNCH_TILES) cfg = 2;          // 4 x 2
+        else if (cfg == 0 && T < MEDIUM_LAUNCH_TILES) cfg = 4;    // 4 x 3
         switch (cfg) {
             case 1: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 3, 3>(BWD_CFG_ARGS);
             case 2: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 4, 2>(BWD_CFG_ARGS);
