@@ -10,6 +10,7 @@ import pytest
 import torch
 
 from svraster_b200 import grid_loss_bw as GL
+from svraster_b200 import synthetic as S
 from tests.golden.cases import REG_CASE, build_reg_inputs
 from tests.test_golden import _check_inputs, check_reg, load, reg_outputs
 
@@ -99,3 +100,49 @@ def test_out_of_range_voxel_is_reported(case, ordered):
     bad = np.array([0, sc.n_vox + 5], np.int32)
     with pytest.raises(RuntimeError, match="status"):
         gpu_vg(sc.geo_grid_pts, sc.vox_key, case["vox_size_inv"], bad, 0.01, case["grad1"], ordered=ordered)
+
+
+@pytest.mark.parametrize("ordered", [True, False], ids=["spatial-order", "storage-order"])
+def test_larger_scene_matches_oracle(ordered):
+    """53k voxels / 75k grid points: voxel Eikonal on a random half of the voxels, total
+    variation on 1 and 4 channels (both no_tv_s), against the oracle."""
+    from oracle import oracle as O
+    sc = S.scene_small(seed=4)
+    rng = np.random.default_rng(12)
+    N, M = sc.n_vox, sc.geo_grid_pts.shape[0]
+    vsi = (1.0 / sc.vox_size.reshape(-1)).astype(np.float32)
+    active = rng.permutation(N)[:N // 2].astype(np.int32)
+    g0 = np.where(rng.random((M, 1)) < 0.05, rng.normal(size=(M, 1)), 0).astype(np.float32)
+    ref = O.voxel_gradient_bw(sc.geo_grid_pts, sc.vox_key, vsi, active, 1e-3, g0)
+    got = gpu_vg(sc.geo_grid_pts, sc.vox_key, vsi, active, 1e-3, g0, ordered=ordered)
+    np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-6 * np.abs(ref).max())
+    grid4 = rng.normal(size=(M, 4)).astype(np.float32)
+    g4 = np.zeros((M, 4), np.float32)
+    for grid, g in ((sc.geo_grid_pts, g0), (grid4, g4)):
+        for no_tv_s in (0, 1):
+            ref = O.total_variation_bw(grid, sc.vox_key, 1e-3, vsi, no_tv_s, 0, g)
+            got = gpu_tv(grid, sc.vox_key, 1e-3, vsi, no_tv_s, 0, g, ordered=ordered)
+            np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-6 * np.abs(ref).max())
+
+
+def test_points_loss_larger_scene_matches_oracle():
+    """200k points on the 53k-voxel scene's dense table, both key lookups, against the oracle."""
+    from oracle import oracle as O
+    from tests.golden.cases import grid_voxel_geometry
+    sc = S.scene_small(seed=4)
+    res_pow2 = int(sc.octlevel.max())
+    res = 1 << res_pow2
+    coord, size = grid_voxel_geometry(sc, res_pow2)
+    mask, keys, g2v = O.valid_table(sc.vox_center, sc.vox_size, np.zeros(3, np.float32), sc.scene_extent, res_pow2,
+                                    sc.is_leaf)
+    rng = np.random.default_rng(13)
+    cells = np.flatnonzero(mask)
+    pick = cells[rng.integers(0, len(cells), size=200000)]
+    pts = (np.stack([pick % res, (pick // res) % res, pick // (res * res)], 1) + rng.random((200000, 3)))
+    pts = pts.astype(np.float32)
+    g0 = np.zeros_like(sc.geo_grid_pts)
+    ref = O.points_loss_bw(pts, sc.geo_grid_pts, sc.vox_key, coord, size, res, mask, keys, g2v, 1e-3, g0)
+    for use_index in (True, False):
+        got = gpu_pl(pts, sc.geo_grid_pts, sc.vox_key, coord, size, res, mask, keys, g2v, 1e-3, g0,
+                     use_index=use_index)
+        np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-6 * np.abs(ref).max())
