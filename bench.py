@@ -253,7 +253,8 @@ def run_e2e_batched(args, scene, cams, dev):
     the step as a forward graph and two backward graphs) with host-resident inputs: every step
     copies a step's upstream gradient planes and target image (dL/dcolor, dL/ddepth,
     dL/dnormal, gt; 13 floats per pixel) from pinned host memory on a copy stream, one step
-    ahead into the other of two plane sets, and reads the mean transmittance back."""
+    ahead into the other of two plane sets, and reads every step's mean transmittance back
+    (through a pinned slot, one step later, so the host does not stall the stream)."""
     import torch
     from svraster_b200.step import BatchedTrainStep
     step = BatchedTrainStep(scene, cams, device=dev, lambda_R_concen=0.1)
@@ -279,6 +280,12 @@ def run_e2e_batched(args, scene, cams, dev):
                 ddst.copy_(hsrc, non_blocking=True)
         filled[i].record(copy_stream)
 
+    # each step's result (mean transmittance) goes to a pinned host slot and is read one step
+    # later, once its event has completed, so the host never stalls the stream on it
+    res_host = torch.zeros(2, dtype=torch.float32).pin_memory()
+    res_ready = [torch.cuda.Event(), torch.cuda.Event()]
+    results = []
+
     def one_step():
         i = k[0] % 2
         compute = torch.cuda.current_stream(dev)
@@ -287,22 +294,34 @@ def run_e2e_batched(args, scene, cams, dev):
         compute.wait_event(filled[i])
         _, T = step.replay_backward(i)
         done[i].record(compute)
+        res_host[i:i + 1].copy_(T.mean().reshape(1), non_blocking=True)
+        res_ready[i].record(compute)
+        if k[0] > 0:                              # device -> host read of the previous step's result
+            res_ready[1 - i].synchronize()
+            results.append(float(res_host[1 - i]))
         k[0] += 1
-        return float(T.mean().item())             # device -> host read of the step's result
+
+    def drain():
+        last = (k[0] - 1) % 2
+        res_ready[last].synchronize()
+        results.append(float(res_host[last]))
 
     for e in done:
         e.record(torch.cuda.current_stream(dev))
     fill(0)
     for _ in range(3):
         one_step()
+    drain()
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
     for _ in range(args.steps):
         one_step()
+    drain()
     ev1.record()
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1) / args.steps
+    assert len(results) == 4 + args.steps and all(np.isfinite(results))
     status = step.graph_status()
     del step
     torch.cuda.empty_cache()
