@@ -107,6 +107,23 @@ SVR_API int svr_bin_and_sort(const svr_view_t* views_host, int n_views, int N, i
  * 16 flags a path with bits the trimmed key would drop).  svr_workspace_query returns the
  * geom, binning and image buffer sizes {sizes[0], sizes[1], sizes[2]} for a capacity. */
 SVR_API int svr_binning_count(const void* binning_buffer, int64_t* count_host, void* stream);
+
+/* Dense ranks (no counterpart in the reference): svr_rank_table_build sorts the trimmed rank
+ * (octpath ^ octant pattern, low groups dropped as for path_or) of every (voxel, octant) pair
+ * once per octree and writes table u32[8N] (index voxel * 8 + octant) = the pair's index
+ * among the distinct ranks, and *rank_bits_host = the bits that index needs (synchronises;
+ * workspace from svr_rank_table_workspace_bytes).  svr_bin_and_sort_ranked is
+ * svr_bin_and_sort with the table's index in place of the rank in the sort key: the same
+ * order and ties (the index orders as the rank does), a key narrower by up to
+ * 3 * levels - rank_bits bits, so fewer radix passes.  path_or must be the one the table was
+ * built with (it sets the trimming). */
+SVR_API int svr_rank_table_workspace_bytes(int64_t N, size_t* bytes);
+SVR_API int svr_rank_table_build(int64_t N, const int64_t* octpaths, uint64_t path_or, uint32_t* table,
+                                 int* rank_bits_host, void* ws, size_t ws_bytes, void* stream);
+SVR_API int svr_bin_and_sort_ranked(const svr_view_t* views_host, int n_views, int N, int64_t num_rendered,
+                                    uint64_t path_or, const int64_t* octpaths, const uint32_t* rank_table,
+                                    int rank_table_bits, void* geom_buffer, void* binning_buffer,
+                                    size_t binning_bytes, void* image_buffer, void* stream);
 SVR_API int svr_workspace_query(int n_views, int N, int64_t capacity, int64_t total_pixels,
                                 int total_tiles, size_t* sizes_host);
 

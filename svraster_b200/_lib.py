@@ -61,6 +61,9 @@ _SIGS = {
     "svr_binning_buffer_bytes": (_SZ, [_I64, _I]),
     "svr_image_buffer_bytes": (_SZ, [_I64, _I]),
     "svr_bin_and_sort": (_I, [_P, _I, _I, _I64, _U64, _P, _P, _P, _SZ, _P, _P]),
+    "svr_bin_and_sort_ranked": (_I, [_P, _I, _I, _I64, _U64, _P, _P, _I, _P, _P, _SZ, _P, _P]),
+    "svr_rank_table_workspace_bytes": (_I, [_I64, C.POINTER(C.c_size_t)]),
+    "svr_rank_table_build": (_I, [_I64, _P, _U64, _P, C.POINTER(C.c_int), _P, _SZ, _P]),
     "svr_unpack_binning": (_I, [_P, _I64, _I, _P, _I64, _P, _P, _P, _P, _P]),
     "svr_render_fwd": (_I, [_P, _I, _I, _I64, _I, _I, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P,
                             _P, _P, _P, _P, _P, _P]),

@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(256) duplicate_kernel(
     const uint32_t* __restrict__ ndup, const uint32_t* __restrict__ scan, const uint2* __restrict__ bboxes,
     const uint32_t* __restrict__ bitsets, KeyT* __restrict__ keys, uint32_t* __restrict__ vals,
     int rank_shift, int rank_bits, const GeomMeta* __restrict__ gmeta, int64_t cap, BinMeta* __restrict__ meta,
-    unsigned* status)
+    unsigned* status, const uint32_t* __restrict__ rank_table)
 {
     const int64_t item = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (item == 0) {
@@ -394,7 +394,8 @@ __global__ void __launch_bounds__(256) duplicate_kernel(
     const uint32_t qb = bitsets[item];
     for (uint32_t q = 0; q < 8; ++q) {
         if (!(qb & (1u << q))) continue;
-        const uint64_t rank = (path ^ rep3(q)) >> rank_shift;
+        // the dense rank of (voxel, octant) when a table is given: same order, fewer bits
+        const uint64_t rank = rank_table ? (uint64_t)rank_table[8 * (size_t)i + q] : (path ^ rep3(q)) >> rank_shift;
         for (int y = ty0; y <= ty1; ++y)
             for (int x = tx0; x <= tx1; ++x) {
                 if (off >= end) { atomicOr(status, ERR_COUNT_MISMATCH); return; }
@@ -443,7 +444,7 @@ __global__ void tile_ranges_kernel(const BinMeta* __restrict__ meta, const KeyT*
 template <typename KeyT>
 static int bin_sort_typed(const Views& V, int N, int64_t R, const KeyFmt& kf, int T, const int64_t* octpaths,
                           char* g, const GeomLayout& GL, char* b, const BinLayout& BL, char* im, const ImgLayout& IL,
-                          unsigned* status, cudaStream_t st)
+                          unsigned* status, cudaStream_t st, const uint32_t* rank_table = nullptr)
 {
     const int64_t M = (int64_t)N * V.n;
     const int nb = (int)((M + 255) / 256);
@@ -453,7 +454,7 @@ static int bin_sort_typed(const Views& V, int N, int64_t R, const KeyFmt& kf, in
     uint32_t* vals_in = (uint32_t*)(b + BL.vals_in);
     duplicate_kernel<KeyT><<<nb, 256, 0, st>>>(V, N, octpaths, (const uint32_t*)(g + GL.ndup),
         (const uint32_t*)(g + GL.scan), (const uint2*)(g + GL.bbox), (const uint32_t*)(g + GL.bits),
-        keys_in, vals_in, kf.rank_shift, kf.rank_bits, (const GeomMeta*)g, R, meta, status);
+        keys_in, vals_in, kf.rank_shift, kf.rank_bits, (const GeomMeta*)g, R, meta, status, rank_table);
     LAUNCH_CHECK();
     const KeyT sentinel = kf.key_bits >= (int)(8 * sizeof(KeyT)) ? (KeyT)~(KeyT)0
                                                                     : (KeyT)((((KeyT)1) << kf.key_bits) - 1);
@@ -517,9 +518,10 @@ extern "C" int svr_workspace_query(int n_views, int N, int64_t capacity, int64_t
     return SVR_OK;
 }
 
-extern "C" int svr_bin_and_sort(const svr_view_t* views_host, int n_views, int N, int64_t R, uint64_t path_or,
-                                const int64_t* octpaths, void* geom_buffer, void* binning_buffer,
-                                size_t binning_bytes, void* image_buffer, void* stream)
+static int bin_and_sort_impl(const svr_view_t* views_host, int n_views, int N, int64_t R, uint64_t path_or,
+                             const int64_t* octpaths, const uint32_t* rank_table, int rank_table_bits,
+                             void* geom_buffer, void* binning_buffer, size_t binning_bytes, void* image_buffer,
+                             void* stream)
 {
     Views V;
     int T; int64_t P;
@@ -538,12 +540,133 @@ extern "C" int svr_bin_and_sort(const svr_view_t* views_host, int n_views, int N
     CUDA_TRY(cudaMemsetAsync(im + IL.ranges, 0, 8 * (size_t)T, st));
     CUDA_TRY(cudaMemsetAsync(status, 0, 4, st));
     if (R == 0) return tile_launch_order(T, im, IL, st);
-    const KeyFmt kf = key_format(path_or, T);
+    KeyFmt kf = key_format(path_or, T);
+    if (rank_table) {
+        if (rank_table_bits < 1 || rank_table_bits > 32) return svr_fail(SVR_ERR_ARG, "rank table bits");
+        kf.key_bits = kf.key_bits - kf.rank_bits + rank_table_bits;
+        kf.rank_bits = rank_table_bits;
+    }
     if (kf.key_bits > 64) return svr_fail(SVR_ERR_UNSUPPORTED, "sort key wider than 64 bits");
-    rc = kf.key_bits <= 32 ? bin_sort_typed<uint32_t>(V, N, R, kf, T, octpaths, g, GL, b, BL, im, IL, status, st)
-                           : bin_sort_typed<uint64_t>(V, N, R, kf, T, octpaths, g, GL, b, BL, im, IL, status, st);
+    rc = kf.key_bits <= 32
+             ? bin_sort_typed<uint32_t>(V, N, R, kf, T, octpaths, g, GL, b, BL, im, IL, status, st, rank_table)
+             : bin_sort_typed<uint64_t>(V, N, R, kf, T, octpaths, g, GL, b, BL, im, IL, status, st, rank_table);
     if (rc) return rc;
     return tile_launch_order(T, im, IL, st);
+}
+
+extern "C" int svr_bin_and_sort(const svr_view_t* views_host, int n_views, int N, int64_t R, uint64_t path_or,
+                                const int64_t* octpaths, void* geom_buffer, void* binning_buffer,
+                                size_t binning_bytes, void* image_buffer, void* stream)
+{
+    return bin_and_sort_impl(views_host, n_views, N, R, path_or, octpaths, nullptr, 0, geom_buffer, binning_buffer,
+                             binning_bytes, image_buffer, stream);
+}
+
+extern "C" int svr_bin_and_sort_ranked(const svr_view_t* views_host, int n_views, int N, int64_t R,
+                                       uint64_t path_or, const int64_t* octpaths, const uint32_t* rank_table,
+                                       int rank_table_bits, void* geom_buffer, void* binning_buffer,
+                                       size_t binning_bytes, void* image_buffer, void* stream)
+{
+    if (!rank_table) return svr_fail(SVR_ERR_ARG, "rank table");
+    return bin_and_sort_impl(views_host, n_views, N, R, path_or, octpaths, rank_table, rank_table_bits, geom_buffer,
+                             binning_buffer, binning_bytes, image_buffer, stream);
+}
+
+// ------------------------------------------------------------------ dense rank table
+// Once per octree and trimming: the trimmed rank (path ^ rep3(q)) >> shift of every (voxel,
+// octant) pair, sorted; equal ranks share one dense index, so the dense index orders and ties
+// exactly as the rank does and the binning key narrows from 3 * MAX_LEVELS - shift bits to
+// the bits of the number of distinct ranks.
+struct RankWs { size_t keys_in, keys_out, vals_in, vals_out, flags, tmp, tmp_bytes, total; };
+static int rank_ws(int64_t n8, RankWs& w)
+{
+    const int n = (int)(n8 > 0 ? n8 : 1);
+    size_t ts = 0, tc = 0;
+    if (cub::DeviceRadixSort::SortPairs(nullptr, ts, (const uint64_t*)nullptr, (uint64_t*)nullptr,
+                                        (const uint32_t*)nullptr, (uint32_t*)nullptr, n) != cudaSuccess ||
+        cub::DeviceScan::InclusiveSum(nullptr, tc, (const uint32_t*)nullptr, (uint32_t*)nullptr, n) != cudaSuccess)
+        return svr_fail(SVR_ERR_CUDA, "rank table: size query");
+    size_t off = 0;
+    w.keys_in = off; off = align_up(off + 8 * (size_t)n, 256);
+    w.keys_out = off; off = align_up(off + 8 * (size_t)n, 256);
+    w.vals_in = off; off = align_up(off + 4 * (size_t)n, 256);
+    w.vals_out = off; off = align_up(off + 4 * (size_t)n, 256);
+    w.flags = off; off = align_up(off + 4 * (size_t)n, 256);
+    w.tmp = off; w.tmp_bytes = ts > tc ? ts : tc; off = align_up(off + w.tmp_bytes, 256);
+    w.total = off;
+    return SVR_OK;
+}
+
+extern "C" int svr_rank_table_workspace_bytes(int64_t N, size_t* bytes)
+{
+    if (!bytes || N < 0 || 8 * N >= (1ll << 31)) return svr_fail(SVR_ERR_ARG, "rank table: N");
+    RankWs w;
+    if (int rc = rank_ws(8 * N, w)) return rc;
+    *bytes = w.total;
+    return SVR_OK;
+}
+
+__global__ void rank_key_kernel(int64_t N, const int64_t* __restrict__ octpaths, int shift, uint64_t* __restrict__ keys,
+                                uint32_t* __restrict__ vals)
+{
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= 8 * N) return;
+    const uint32_t q = (uint32_t)(s & 7);
+    keys[s] = ((uint64_t)octpaths[s >> 3] ^ rep3(q)) >> shift;
+    vals[s] = (uint32_t)s;
+}
+
+__global__ void rank_flag_kernel(int64_t n, const uint64_t* __restrict__ keys, uint32_t* __restrict__ flags)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    flags[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+}
+
+__global__ void rank_scatter_kernel(int64_t n, const uint32_t* __restrict__ vals, const uint32_t* __restrict__ incl,
+                                    uint32_t* __restrict__ table)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    table[vals[i]] = incl[i] - 1u;
+}
+
+extern "C" int svr_rank_table_build(int64_t N, const int64_t* octpaths, uint64_t path_or, uint32_t* table,
+                                    int* rank_bits_host, void* ws, size_t ws_bytes, void* stream)
+{
+    size_t need = 0;
+    if (int rc = svr_rank_table_workspace_bytes(N, &need)) return rc;
+    if (N <= 0 || !octpaths || !table || !rank_bits_host || !ws || ws_bytes < need)
+        return svr_fail(SVR_ERR_ARG, "rank table: bad argument or workspace too small");
+    RankWs w;
+    if (int rc = rank_ws(8 * N, w)) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    char* base = (char*)ws;
+    uint64_t* kin = (uint64_t*)(base + w.keys_in);
+    uint64_t* kout = (uint64_t*)(base + w.keys_out);
+    uint32_t* vin = (uint32_t*)(base + w.vals_in);
+    uint32_t* vout = (uint32_t*)(base + w.vals_out);
+    uint32_t* flags = (uint32_t*)(base + w.flags);
+    const KeyFmt kf = key_format(path_or, 1);
+    const int64_t n = 8 * N;
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    rank_key_kernel<<<nb, 256, 0, st>>>(N, octpaths, kf.rank_shift, kin, vin);
+    LAUNCH_CHECK();
+    size_t tb = w.tmp_bytes;
+    CUDA_TRY(cub::DeviceRadixSort::SortPairs(base + w.tmp, tb, kin, kout, vin, vout, (int)n, 0, kf.rank_bits, st));
+    rank_flag_kernel<<<nb, 256, 0, st>>>(n, kout, flags);
+    LAUNCH_CHECK();
+    tb = w.tmp_bytes;
+    CUDA_TRY(cub::DeviceScan::InclusiveSum(base + w.tmp, tb, flags, flags, (int)n, st));
+    rank_scatter_kernel<<<nb, 256, 0, st>>>(n, vout, flags, table);
+    LAUNCH_CHECK();
+    uint32_t n_unique = 0;
+    CUDA_TRY(cudaMemcpyAsync(&n_unique, flags + (n - 1), 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    int bits = 1;
+    while (bits < 32 && (1ull << bits) < (unsigned long long)n_unique) ++bits;
+    *rank_bits_host = bits;
+    return SVR_OK;
 }
 
 extern "C" int svr_unpack_binning(const void* binning_buffer, int64_t R, int T, const void* image_buffer,

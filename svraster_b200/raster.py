@@ -50,12 +50,14 @@ class RasterState:
         return n_dup
 
     # -------------------------------------------------------------- binning
-    def bin(self, octpaths, capacity=None, path_or=None):
+    def bin(self, octpaths, capacity=None, path_or=None, rank_table=None):
         """Duplicate, sort and range the records.  By default the record total is read back
         (one host synchronisation, as the reference does).  With ``capacity`` (and ``path_or``,
         the OR of every voxel's octree path) nothing is read back: the buffers hold
         ``capacity`` records and the device bins min(total, capacity) of them (status bit 8
-        if any were dropped), which lets the call be captured into a CUDA graph."""
+        if any were dropped), which lets the call be captured into a CUDA graph.
+        ``rank_table`` (a ``RankTable``) narrows the sort key to dense ranks when it was built
+        for the same trimming as this call's path_or (same order, fewer radix passes)."""
         L = _lib.load()
         M = self.N * self.n_views
         if capacity is None:
@@ -71,9 +73,15 @@ class RasterState:
         nb = L.svr_binning_buffer_bytes(self.num_rendered, self.total_tiles)
         self.binning = _empty_bytes(nb, self.device)
         self.image = _empty_bytes(L.svr_image_buffer_bytes(self.total_pix, self.total_tiles), self.device)
-        check(L.svr_bin_and_sort(self.views, self.n_views, self.N, self.num_rendered, self.path_or, ptr(octpaths),
-                                 ptr(self.geom), ptr(self.binning), nb, ptr(self.image), stream_ptr(self.device)),
-              "svr_bin_and_sort")
+        if rank_table is not None and rank_table.matches(self.path_or):
+            check(L.svr_bin_and_sort_ranked(self.views, self.n_views, self.N, self.num_rendered, self.path_or,
+                                            ptr(octpaths), ptr(rank_table.table), rank_table.bits, ptr(self.geom),
+                                            ptr(self.binning), nb, ptr(self.image), stream_ptr(self.device)),
+                  "svr_bin_and_sort_ranked")
+        else:
+            check(L.svr_bin_and_sort(self.views, self.n_views, self.N, self.num_rendered, self.path_or,
+                                     ptr(octpaths), ptr(self.geom), ptr(self.binning), nb, ptr(self.image),
+                                     stream_ptr(self.device)), "svr_bin_and_sort")
         return self.num_rendered
 
     # -------------------------------------------------------------- render
@@ -141,3 +149,35 @@ class RasterState:
                                              self.total_pix, ptr(vals), ptr(ranges), ptr(tl), ptr(nc),
                                              stream_ptr(self.device)), "svr_unpack_binning")
         return vals[: self.num_rendered], ranges, tl, nc
+
+
+def rank_shift(path_or):
+    """Low rank bits the binning key drops for this path OR (raster.cu key_format): all 3-bit
+    level groups below the lowest non-zero one but one."""
+    path_or = int(path_or)
+    g = 16 if path_or == 0 else ((path_or & -path_or).bit_length() - 1) // 3
+    return 3 * (g - 1) if g > 0 else 0
+
+
+class RankTable:
+    """Dense ranks of every (voxel, octant) pair of an octree (svr_rank_table_build), for
+    ``RasterState.bin(rank_table=...)``.  Valid for the octree it was built from and for
+    binning calls whose path_or trims as ``path_or`` does."""
+
+    def __init__(self, octpaths, path_or):
+        L = _lib.load()
+        dev = octpaths.device
+        paths = octpaths.reshape(-1).to(torch.int64).contiguous()
+        N = paths.numel()
+        nbytes = C.c_size_t(0)
+        check(L.svr_rank_table_workspace_bytes(N, C.byref(nbytes)), "svr_rank_table_workspace_bytes")
+        ws = _empty_bytes(nbytes.value, dev)
+        self.table = torch.empty(8 * N, dtype=torch.int32, device=dev)
+        bits = C.c_int(0)
+        check(L.svr_rank_table_build(N, ptr(paths), int(path_or), ptr(self.table), C.byref(bits), ptr(ws),
+                                     nbytes.value, stream_ptr(dev)), "svr_rank_table_build")
+        self.bits = int(bits.value)
+        self.shift = rank_shift(path_or)
+
+    def matches(self, path_or):
+        return rank_shift(path_or) == self.shift

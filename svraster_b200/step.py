@@ -18,7 +18,7 @@ import torch
 
 from . import _lib
 from ._lib import check, ptr, stream_ptr
-from .raster import RasterState
+from .raster import RankTable, RasterState
 from . import utils
 
 
@@ -26,14 +26,16 @@ class BatchedTrainStep:
 
     def __init__(self, scene, cams, device="cuda", lr=(1e-3, 1e-3, 1e-4), betas=(0.1, 0.99), eps=1e-15,
                  lambda_ls=1e-3, lambda_ge=1e-3, lambda_R_concen=0.0, sh_degree=3, seed=0, fused_smoothness=True,
-                 sh_dtype="f32", normal_losses=None):
+                 sh_dtype="f32", normal_losses=None, dense_ranks=True):
         """``sh_dtype="bf16"`` stores the SH coefficients in bf16 (the precision configuration):
         colours, compositing, transmittance and every gradient stay f32, Adam keeps f32 moments
         and rounds the updated coefficients to nearest bf16.  ``normal_losses`` (a dict with
         any of lambda_dmean, dmean_ks, dmean_tol_deg, lambda_dmed; train.py:159-166, 418-425)
         adds the normal-from-depth consistency losses of the rendered batch: one launch each
         between the render forward and the adjoint, their gradients added to the upstream
-        depth / normal planes the adjoint reads."""
+        depth / normal planes the adjoint reads.  ``dense_ranks`` bins with the octree's dense
+        (voxel, octant) ranks (``raster.RankTable``, built here once): the same record order
+        with a narrower sort key."""
         dev = torch.device(device)
         self.dev = dev
         t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
@@ -124,6 +126,7 @@ class BatchedTrainStep:
         # per-group Adam coefficient tables
         leaf_paths = np.asarray(scene.octpath, dtype=np.int64)[np.asarray(scene.is_leaf).astype(bool).reshape(-1)]
         self.path_or_all = int(np.bitwise_or.reduce(leaf_paths.view(np.uint64))) if leaf_paths.size else 0
+        self.rank_table = RankTable(self.octpath, self.path_or_all) if dense_ranks else None
         self.graph = None
         self.graph_b = None
         self.graph_out = None
@@ -173,9 +176,9 @@ class BatchedTrainStep:
         state.preprocess(self.octpath, self.centers, self.lengths, self.is_leaf)
         mark("preprocess")
         if graph:
-            state.bin(self.octpath, capacity=self.capacity, path_or=self.path_or_all)
+            state.bin(self.octpath, capacity=self.capacity, path_or=self.path_or_all, rank_table=self.rank_table)
         else:
-            state.bin(self.octpath)
+            state.bin(self.octpath, rank_table=self.rank_table)
         mark("count+sort")
         color, depth, normal, T, _ = state.render(3, True, True, self.centers, self.lengths, self.geos, self.rgbs,
                                                   self.s_val, rgb_per_view=True)
