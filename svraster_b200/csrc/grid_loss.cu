@@ -553,7 +553,7 @@ __device__ __forceinline__ void add8(float* dvox, int ld, bool vec4, int v, cons
 }
 
 template <bool LS, bool GE>
-__global__ void __launch_bounds__(256) smooth_vox_kernel(VoxCtx c, int A, const int32_t* __restrict__ active,
+__global__ void __launch_bounds__(256, 5) smooth_vox_kernel(VoxCtx c, int A, const int32_t* __restrict__ active,
                                                          const uint8_t* __restrict__ mask, float w_ls, float w_ge,
                                                          float vox_size_inv, int seed,
                                                          const int64_t* __restrict__ seed_step,

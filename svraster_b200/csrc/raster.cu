@@ -160,7 +160,7 @@ static int build_views(const svr_view_t* vh, int n, Views& V, int& total_tiles, 
 // Grid-stride over the voxels of view blockIdx.y with a bounded grid: the running total and
 // path OR are reduced over the block and leave with one atomic each (one per warp put tens
 // of millions of same-address atomics on one L2 slice for a 64-view batch).
-__global__ void __launch_bounds__(256) preprocess_kernel(
+__global__ void __launch_bounds__(256, 4) preprocess_kernel(
     const __grid_constant__ Views V, int N, const float3* __restrict__ centers,
     const float* __restrict__ lengths, const uint8_t* __restrict__ is_leaf,
     const int64_t* __restrict__ octpaths, int32_t* __restrict__ out_ndup,
