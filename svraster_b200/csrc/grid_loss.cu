@@ -280,6 +280,28 @@ __device__ __forceinline__ void scatter8(const SampleCtx& c, int v, const float*
     for (int i = 0; i < 8; ++i) atomicAdd(grad + c.vox_key[8 * (int64_t)v + i], d * w[i]);
 }
 
+// Sums acc[0:8] over each run of lanes [head, next head) of a warp into the run's head
+// lane (a segmented shuffle reduction).  The rounds stop at the warp's longest run: a
+// further round would add nothing to any head, so each head's sum, and its order, is the
+// one all five rounds give.  Warps whose runs are all single lanes skip the shuffles.
+__device__ __forceinline__ void run_sum8(float acc[8], unsigned heads, bool head, int lane) {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned upto = FULL >> (31 - lane);            // lanes 0..lane
+    const int my_head = 31 - __clz(heads & upto);
+    const unsigned later = heads & ~upto;                 // heads after this lane
+    const unsigned run = head ? (unsigned)((later ? __ffs(later) - 1 : 32) - lane) : 0u;
+    const int longest = (int)__reduce_max_sync(FULL, run);
+    for (int off = 1; off < longest; off <<= 1) {
+        const int other_head = __shfl_down_sync(FULL, my_head, off);
+        const bool same = (lane + off < 32) && other_head == my_head;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float v = __shfl_down_sync(FULL, acc[i], off);
+            if (same) acc[i] += v;
+        }
+    }
+}
+
 // Gradient scatter of one key's samples with two levels of aggregation before the atomics:
 // samples whose owner voxel equals the primary sample's are merged in registers, then lanes
 // of a warp holding the same primary voxel in a contiguous run (consecutive keys inside one
@@ -308,18 +330,7 @@ __device__ __forceinline__ void scatter_samples(const SampleCtx& c, bool valid, 
     const int prev = __shfl_up_sync(FULL, primary, 1);
     const bool head = lane == 0 || prev != primary;
     const unsigned heads = __ballot_sync(FULL, head);
-    // segment of each lane = [its head, next head)
-    const int my_head = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        const int other_head = __shfl_down_sync(FULL, my_head, off);
-        const bool same = (lane + off < 32) && other_head == my_head;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const float v = __shfl_down_sync(FULL, acc[i], off);
-            if (same) acc[i] += v;
-        }
-    }
+    run_sum8(acc, heads, head, lane);
     if (head && primary >= 0) {
 #pragma unroll
         for (int i = 0; i < 8; ++i) atomicAdd(grad + c.vox_key[8 * (int64_t)primary + i], acc[i]);
@@ -654,17 +665,7 @@ __global__ void __launch_bounds__(256, 5) smooth_vox_kernel(VoxCtx c, int A, con
     const int prev = __shfl_up_sync(FULL, primary, 1);
     const bool head = lane == 0 || prev != primary;
     const unsigned heads = __ballot_sync(FULL, head);
-    const int my_head = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        const int other_head = __shfl_down_sync(FULL, my_head, off);
-        const bool same = (lane + off < 32) && other_head == my_head;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const float v = __shfl_down_sync(FULL, acc[i], off);
-            if (same) acc[i] += v;
-        }
-    }
+    run_sum8(acc, heads, head, lane);
     if (head && primary >= 0) add8(dvox, ld, vec4, primary, acc);
 }
 
