@@ -515,6 +515,16 @@ struct VoxCtx {
     const float4* geos;   // [N][2] float4 = 8 corner values
 };
 
+// Weight clamp to [0, 1] in two NaN-propagating min/max instructions.  It equals
+// `w < 0 ? 0 : (w > 1 ? 1 : w)` for every input but -0.0, which becomes +0.0 (a zero
+// weight either way).
+__device__ __forceinline__ float clamp01(float w) {
+    float r;
+    asm("max.NaN.f32 %0, %1, 0f00000000;" : "=f"(r) : "f"(w));
+    asm("min.NaN.f32 %0, %1, 0f3F800000;" : "=f"(r) : "f"(r));
+    return r;
+}
+
 // Owner voxel of table row `id` and the sample at cell (x,y,z) + rv: returns the SDF value,
 // writes the owner (-1 if absent) and the local coordinate q used for the weights.
 __device__ __forceinline__ float sample_vox(const VoxCtx& c, int id, int x, int y, int z, float3 rv, int& v,
@@ -535,8 +545,7 @@ __device__ __forceinline__ float sample_vox(const VoxCtx& c, int id, int x, int 
     float s = 0.f;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        if (w[i] < 0) w[i] = 0;
-        if (w[i] > 1) w[i] = 1;
+        w[i] = clamp01(w[i]);
         s += g[i] * w[i];
     }
     v = vv;
@@ -546,10 +555,7 @@ __device__ __forceinline__ float sample_vox(const VoxCtx& c, int id, int x, int 
 __device__ __forceinline__ void clamped_weights(float3 q, float w[8]) {
     tri_weights(q, w);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        if (w[i] < 0) w[i] = 0;
-        if (w[i] > 1) w[i] = 1;
-    }
+    for (int i = 0; i < 8; ++i) w[i] = clamp01(w[i]);
 }
 
 __device__ __forceinline__ void add8(float* dvox, int ld, bool vec4, int v, const float* a) {
