@@ -686,13 +686,27 @@ extern "C" int svr_unpack_binning(const void* binning_buffer, int64_t R, int T, 
 }
 
 // ------------------------------------------------------------------ record packing
+// Centre and edge length of every voxel as one float4 (x, y, z, length): record packing
+// then gathers one 16-byte piece per record instead of four scalars from two arrays (the
+// gathers miss L2 on large batches, so this is one DRAM sector per record instead of two
+// or three).  Written into the unsorted-key region of the binning buffer, which is dead
+// once the records are sorted.
+__global__ void center_len_kernel(int N, const float* __restrict__ centers, const float* __restrict__ lengths,
+                                  float4* __restrict__ center_len)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) center_len[i] = make_float4(centers[3 * (size_t)i], centers[3 * (size_t)i + 1],
+                                           centers[3 * (size_t)i + 2], lengths[i]);
+}
+
 // Gather each sorted record's voxel data into one 80-byte record.  The record's view is
 // the view of its tile, read from the sorted key.
 __global__ void __launch_bounds__(256) pack_records_kernel(
     const __grid_constant__ Views V, int N, int64_t R, const BinMeta* __restrict__ meta,
     const void* __restrict__ keys, const uint32_t* __restrict__ vals, const uint2* __restrict__ bboxes,
     const float* __restrict__ centers, const float* __restrict__ lengths, const float4* __restrict__ geos,
-    const float* __restrict__ rgbs, int rgb_per_view, Rec* __restrict__ recs, unsigned* status)
+    const float* __restrict__ rgbs, int rgb_per_view, const float4* __restrict__ center_len,
+    Rec* __restrict__ recs, unsigned* status)
 {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= R || k >= meta->count) return;
@@ -703,8 +717,13 @@ __global__ void __launch_bounds__(256) pack_records_kernel(
     const uint32_t vid = val & 0x1FFFFFFFu;
     if (vid >= (uint32_t)N) { atomicOr(status, ERR_BAD_INDEX); return; }
     Rec r;
-    r.cx = centers[3 * (size_t)vid]; r.cy = centers[3 * (size_t)vid + 1]; r.cz = centers[3 * (size_t)vid + 2];
-    r.len = lengths[vid];
+    if (center_len) {
+        const float4 c = center_len[vid];
+        r.cx = c.x; r.cy = c.y; r.cz = c.z; r.len = c.w;
+    } else {
+        r.cx = centers[3 * (size_t)vid]; r.cy = centers[3 * (size_t)vid + 1]; r.cz = centers[3 * (size_t)vid + 2];
+        r.len = lengths[vid];
+    }
     const float4 g0 = geos[2 * (size_t)vid], g1 = geos[2 * (size_t)vid + 1];
     r.g[0] = g0.x; r.g[1] = g0.y; r.g[2] = g0.z; r.g[3] = g0.w;
     r.g[4] = g1.x; r.g[5] = g1.y; r.g[6] = g1.z; r.g[7] = g1.w;
@@ -890,9 +909,17 @@ static int render_fwd_impl(const svr_view_t* views_host, int n_views, int N, int
     const uint32_t* order = (const uint32_t*)(im + IL.order);
     Rec* recs = (Rec*)(b + BL.recs);
     if (R > 0) {
+        // the unsorted keys (8 bytes per record slot) hold the N float4 when R >= 2N
+        float4* cl = nullptr;
+        if (N > 0 && R >= 2 * (int64_t)N) {
+            cl = (float4*)(b + BL.keys_in);
+            center_len_kernel<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(N, centers, lengths, cl);
+            LAUNCH_CHECK();
+        }
         pack_records_kernel<<<(unsigned)((R + 255) / 256), 256, 0, st>>>(
             V, N, R, (const BinMeta*)b, b + BL.keys_out, (const uint32_t*)(b + BL.vals_out),
-            (const uint2*)(g + GL.bbox), centers, lengths, (const float4*)geos, rgbs, n_rgb_views > 1, recs, status);
+            (const uint2*)(g + GL.bbox), centers, lengths, (const float4*)geos, rgbs, n_rgb_views > 1, cl, recs,
+            status);
         LAUNCH_CHECK();
     }
     uint32_t* tl = (uint32_t*)(im + IL.tile_last);
