@@ -541,9 +541,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_kernel(
                     }
                     const float dL_dalpha = T * (dL_dpt_w - last_dT);
                     last_dT += alpha * (dL_dpt_w - last_dT);
+                    const float pe = s_val * phi_entry * (1.f - phi_entry);
                     {
                         // backward.cu:650-671
-                        const float pe = s_val * phi_entry * (1.f - phi_entry);
                         const float pxv = s_val * phi_exit * (1.f - phi_exit);
                         const float dae = (pe * (1.f - alpha)) / denom;
                         const float dax = -pxv / denom;
@@ -561,9 +561,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_kernel(
                         // sub-segment end points are evaluated once; each point's weight
                         // gradient collects both segments it bounds
                         const float3 qt_step = ((bb - a) * ray.rd / 3.0f) * vox_l_inv;
+                        // the first end point is the entry point: its phi and phi' are
+                        // phi_entry and pe, bit for bit (same weights, same summation order)
                         float ph[4], dph[4];
+                        ph[0] = phi_entry;
+                        dph[0] = pe;
 #pragma unroll
-                        for (int k2 = 0; k2 < 4; ++k2) {
+                        for (int k2 = 1; k2 < 4; ++k2) {
                             const float3 qk = qt_entry + qt_step * (float)k2;
                             float wk[8];
                             tri_weights(qk, wk);
