@@ -45,16 +45,32 @@ WORKLOAD = CONFIGS["mid"]["workload"]
 N_VIEWS, W, H = 8, 800, 800
 
 
-def make_workload(rank=0, n_views=None, config="mid"):
+def rank_cameras(rank=0, n_views=None, config="mid"):
+    """The views of one rank (data parallel over views, weak scaling): rank r takes the r-th
+    block of the workload's views-per-GPU from a camera set of (r + 1) blocks."""
     from svraster_b200 import synthetic as S
     n = CONFIGS[config]["views"]
     if config == "batched":
-        scene = S.scene_batched(seed=0)
         cams = S.mixed_resolution_cameras(n * (rank + 1), 3.0, seed=0)[n * rank:n * (rank + 1)]
     else:
-        scene = S.scene_mid(seed=0)
         cams = S.fibonacci_cameras(n * (rank + 1), 3.0, W, H, fovx_deg=50.0)[n * rank:n * (rank + 1)]
-    return scene, cams[:n_views or n]
+    return cams[:n_views or n]
+
+
+def make_workload(rank=0, n_views=None, config="mid"):
+    from svraster_b200 import synthetic as S
+    scene = S.scene_batched(seed=0) if config == "batched" else S.scene_mid(seed=0)
+    return scene, rank_cameras(rank, n_views, config)
+
+
+def max_over_ranks(ms, device):
+    """The slowest rank's time: every rank's timed region ends at the same barrier, so the
+    job's step time is the maximum (one all-reduce, the same collective on every rank)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def measured_peaks():
@@ -204,9 +220,7 @@ def run_ours(args, rank, world):
                       "eager_ms_per_step": round(eager_ms / args.steps, 3)}
 
     if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = max_over_ranks(total_ms, dev)
         dist.barrier()
     ms_per_step = total_ms / args.steps
     rays = step.rays * world

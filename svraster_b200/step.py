@@ -22,6 +22,19 @@ from .raster import RankTable, RasterState
 from . import utils
 
 
+def flat_views(shapes, device, align=64):
+    """One zeroed float32 buffer holding a view of each shape, every view starting on a
+    multiple of ``align`` elements (256 bytes): one fill zeroes them all and one collective
+    exchanges them all.  The padding between views stays zero.  Returns (flat, views)."""
+    offs, total = [], 0
+    for shape in shapes:
+        n = int(np.prod(shape)) if len(shape) else 1
+        offs.append((total, n))
+        total += (n + align - 1) // align * align
+    flat = torch.zeros(max(total, 1), dtype=torch.float32, device=device)
+    return flat, [flat[o:o + n].view(shape) for (o, n), shape in zip(offs, shapes)]
+
+
 class BatchedTrainStep:
 
     def __init__(self, scene, cams, device="cuda", lr=(1e-3, 1e-3, 1e-4), betas=(0.1, 0.99), eps=1e-15,
@@ -109,15 +122,9 @@ class BatchedTrainStep:
         self.dvox = torch.zeros(self.N, 12, device=dev)
         self.drgbs = torch.zeros(self.V * self.N, 3, device=dev)
         self.ds = torch.zeros(1, device=dev)
-        # the gradients are views into one flat buffer (each view 256-byte aligned), so that a
-        # step zeroes them with one fill and a data-parallel step exchanges them with one
-        # all-reduce (``grad_flat``)
-        offs, total = [], 0
-        for p in self.params:
-            offs.append(total)
-            total += (p.numel() + 63) // 64 * 64
-        self.grad_flat = torch.zeros(total, dtype=torch.float32, device=dev)
-        self.grads = [self.grad_flat[o:o + p.numel()].view(p.shape) for o, p in zip(offs, self.params)]
+        # the gradients are views into one flat buffer, so that a step zeroes them with one
+        # fill and a data-parallel step exchanges them with one all-reduce (``grad_flat``)
+        self.grad_flat, self.grads = flat_views([p.shape for p in self.params], dev)
         self.all_idx = torch.arange(self.N, dtype=torch.int64, device=dev)
         self.state = None
         self.ev = None

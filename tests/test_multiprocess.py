@@ -1,6 +1,8 @@
 """Host logic of the data-parallel step on CPU ranks (gloo, world size 2): each rank owns
-its own views, the gradients are summed across ranks between the adjoints and Adam, and the
-parameters stay replicated.  Also the rank-failure path: a rank that raises before the
+its own views (``bench.rank_cameras``), the gradients live in one flat buffer
+(``svraster_b200.step.flat_views``) that one all-reduce sums across ranks between the
+adjoints and Adam, the parameters stay replicated, and the job time is the slowest rank's
+(``bench.max_over_ranks``).  Also the rank-failure path: a rank that raises before the
 exchange makes the others' collective end with an error instead of hanging."""
 import os
 import sys
@@ -25,20 +27,37 @@ def _worker_allreduce(rank, world, port, out):
     sys.path.insert(0, ROOT)
     _init(rank, world, port)
     import bench
-    from svraster_b200 import synthetic as S
-    # views of rank r are the r-th block of the Fibonacci set (bench.make_workload)
-    cams = S.fibonacci_cameras(2 * (rank + 1), 3.0, 8, 8)[2 * rank:2 * (rank + 1)]
-    # stand-in per-rank gradients: a deterministic function of the rank's cameras
-    g = [torch.full((5,), float(sum(c.position.sum() for c in cams)), dtype=torch.float32),
-         torch.arange(3, dtype=torch.float32) * (rank + 1)]
-    for t in g:
-        dist.all_reduce(t)
-    # Adam on replicated params gives identical params on every rank
-    p = torch.zeros(5)
-    p -= 0.1 * g[0]
-    gathered = [torch.zeros(5) for _ in range(world)]
+    from svraster_b200.step import flat_views
+    # the rank's views: bench.rank_cameras, as the data-parallel bench assigns them
+    cams = bench.rank_cameras(rank, 2)
+    positions = torch.tensor(np.stack([c.position for c in cams]), dtype=torch.float64)
+    gathered_pos = [torch.zeros_like(positions) for _ in range(world)]
+    dist.all_gather(gathered_pos, positions)
+    # gradients of the three parameter groups (grid, sh0, shs shapes of a small scene) as
+    # views of one flat buffer, filled with a per-rank pattern; one all-reduce of the flat
+    # buffer is the exchange the bench's gradient hook makes
+    shapes = [(37, 1), (11, 3), (11, 45)]
+    flat, grads = flat_views(shapes, "cpu")
+    for gi, gv in enumerate(grads):
+        gv.copy_(torch.arange(gv.numel(), dtype=torch.float32).view(gv.shape) * (rank + 1) + gi)
+    dist.all_reduce(flat)
+    # Adam-like update on replicated parameters stays identical on every rank
+    p = torch.zeros(11, 45)
+    p -= 0.1 * grads[2]
+    gathered = [torch.zeros_like(p) for _ in range(world)]
     dist.all_gather(gathered, p)
-    out[rank] = (g[0][0].item(), g[1].tolist(), all(torch.equal(gathered[0], x) for x in gathered))
+    # the job time is the slowest rank's
+    job_ms = bench.max_over_ranks(10.0 + rank, "cpu")
+    pad_zero = True
+    off = 0
+    for gv in grads:
+        n = gv.numel()
+        end = (n + 63) // 64 * 64
+        pad_zero &= bool((flat[off + n:off + end] == 0).all())
+        off += end
+    out[rank] = dict(grads=[g.clone().numpy() for g in grads], same_params=all(torch.equal(gathered[0], x) for x in gathered),
+                     positions=[x.numpy() for x in gathered_pos], job_ms=job_ms, pad_zero=pad_zero,
+                     aligned=[(g.data_ptr() - flat.data_ptr()) % 256 == 0 for g in grads])
     dist.barrier()
     dist.destroy_process_group()
 
@@ -79,9 +98,21 @@ def _run(fn, world=2):
 def test_data_parallel_gradient_allreduce_gloo():
     out = _run(_worker_allreduce)
     assert len(out) == 2
-    a, b = out[0], out[1]
-    assert a[0] == pytest.approx(b[0]) and a[1] == b[1] == [0.0, 3.0, 6.0]
-    assert a[2] and b[2]
+    world = 2
+    shapes = [(37, 1), (11, 3), (11, 45)]
+    for r in range(world):
+        o = out[r]
+        # every view holds the sum over ranks of rank-scaled patterns: arange * (1 + 2) + 2 * gi
+        for gi, (g, shape) in enumerate(zip(o["grads"], shapes)):
+            expect = np.arange(int(np.prod(shape)), dtype=np.float32).reshape(shape) * 3 + 2 * gi
+            assert np.array_equal(g, expect)
+        assert o["pad_zero"] and all(o["aligned"])
+        assert o["same_params"]
+        assert o["job_ms"] == 11.0
+    # ranks own different views (weak scaling over views)
+    p0, p1 = out[0]["positions"]
+    assert p0.shape == p1.shape == (2, 3)
+    assert not np.allclose(p0, p1)
 
 
 def test_failed_rank_does_not_hang_the_others():
