@@ -9,7 +9,8 @@ by the tests from the same seeds and checked against the stored input digest.
 The reference backward reads the depth and normal gradient planes unconditionally
 (backward.cu:180-184), so every case renders with need_depth and need_normal on.
 
-Usage (GPU machine):  python tests/golden/make_golden.py --out gpurun_out/golden [--only reg ...]
+Usage (GPU machine):  python tests/golden/make_golden.py [--out DIR] [--only reg ...]
+(default DIR: tests/golden/_new; the fixtures that pass review are copied into tests/golden/)
 """
 from __future__ import annotations
 
@@ -200,7 +201,7 @@ def run_reg_case(R_, case, dev):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden", "_new"))
     ap.add_argument("--only", nargs="*", default=None,
                     help="fixtures to (re)write, e.g. reg table; default all")
     args = ap.parse_args()
