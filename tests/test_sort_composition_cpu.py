@@ -7,7 +7,8 @@ forward.cu:749-829 + stable sort):
   rank gives the same order (stable composition: lexicographic order with emission-order
   ties), the property a two-level sort (tile passes, then one block per tile) relies on;
 * dense ranks (the sorted distinct ranks renumbered 0, 1, ...) order and tie exactly as the
-  48-bit ranks do.
+  48-bit ranks do;
+* so do the trimmed ranks of the binning key (``raster.rank_shift``).
 """
 import numpy as np
 
@@ -78,3 +79,24 @@ def test_sort_composition_matches_the_oracle_order():
         assert np.array_equal(np.argsort(dkeys, kind="stable"), one)
         checked += len(keys)
     assert checked > 1000
+
+
+def test_trimmed_rank_keeps_order_and_ties():
+    """raster.rank_shift drops the low 3-bit level groups that are zero in every path but
+    one: the kept group still carries the octant, so the trimmed ranks order and tie the
+    (voxel, octant) pairs exactly as the full 48-bit ranks do."""
+    from svraster_b200.raster import rank_shift
+    rng = np.random.default_rng(3)
+    for max_level in (1, 4, 9, 10, 15, 16):
+        zero_groups = 16 - max_level
+        paths = rng.integers(0, 1 << (3 * max_level), size=300, dtype=np.int64).astype(np.uint64)
+        paths <<= np.uint64(3 * zero_groups)
+        paths[:20] = paths[20:40]                        # repeated paths give ties
+        path_or = int(np.bitwise_or.reduce(paths))
+        shift = rank_shift(path_or)
+        assert shift == (3 * (zero_groups - 1) if zero_groups > 0 else 0) or path_or & (7 << (3 * zero_groups)) == 0
+        q = rng.integers(0, 8, size=paths.size)
+        full = paths ^ np.array([rep3(int(x)) for x in q], np.uint64)
+        trimmed = full >> np.uint64(shift)
+        assert np.array_equal(np.argsort(full, kind="stable"), np.argsort(trimmed, kind="stable"))
+        assert np.array_equal(full[:, None] == full[None, :], trimmed[:, None] == trimmed[None, :])
