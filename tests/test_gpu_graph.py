@@ -63,6 +63,23 @@ def test_capacity_binning_matches_exact_count(extra):
     assert torch.equal(c0, c1) and torch.equal(d0, d1) and torch.equal(T0, T1)
 
 
+def test_record_packing_sources_agree():
+    """Record packing takes centre and length from a per-voxel float4 when the record
+    capacity is at least twice the voxel count, and from the two arrays otherwise: the same
+    records either way, so the same binning and images, bit for bit."""
+    dev = torch.device("cuda")
+    sc, cams = scene_and_cams("small", n_cams=1, W=160, H=120)
+    ref, c0, d0, T0 = _render(sc, cams, dev)
+    R = ref.num_rendered
+    assert 0 < R < 2 * sc.n_vox                      # exact count: the two-array source
+    cap, c1, d1, T1 = _render(sc, cams, dev, capacity=2 * sc.n_vox + 5, path_or=_path_or_all(sc))
+    assert cap.binned_count() == R and cap.status() == 0
+    v0, r0, _, _ = ref.binning_fields()
+    v1, r1, _, _ = cap.binning_fields()
+    assert torch.equal(v0.cpu(), v1[:R].cpu()) and torch.equal(r0.cpu(), r1.cpu())
+    assert torch.equal(c0, c1) and torch.equal(d0, d1) and torch.equal(T0, T1)
+
+
 def test_capacity_overflow_is_flagged_not_faulted():
     dev = torch.device("cuda")
     sc, cams = scene_and_cams("small", n_cams=2, W=128, H=96)
