@@ -184,7 +184,9 @@ SVR_API int svr_render_fwd_max_w_views(const svr_view_t* views_host, int n_views
 
 /* Device status word of the raster launches that used this image buffer (0 = clean;
  * bit 1 wait timeout, bit 2 index out of range, bit 4 duplicate count mismatch, bit 8
- * records beyond the binning capacity, bit 16 sort-key format).
+ * records beyond the binning capacity, bit 16 sort-key format, bit 64 a render CTA that had
+ * timed out exited while one of its bulk copies had not been seen to land: the launch's
+ * outputs are undefined and the process should not trust the device afterwards).
  * Synchronises `stream`.  Replaces the reference's __trap() sanity checks
  * (preprocess.cu:141-146, forward.cu:796-801, backward.cu:126-137). */
 SVR_API int svr_read_status(const void* image_buffer, int64_t total_pixels, int total_tiles,
@@ -343,11 +345,13 @@ SVR_API int svr_smoothness_bw_vox(int G, int A, const int32_t* active, const int
  * memory (a host that reserves all device memory in a fixed arena at start-up and forbids
  * later cudaMalloc calls).  It has no counterpart in the reference.  The direct-mapped key
  * index lives in a static 8 MiB device array inside the library instead of caller memory,
- * so grid_res must be at most 128 (larger grids return SVR_ERR_CAPACITY).  Inputs, outputs
- * and the status word are the caller's, as for svr_laplacian_bw, and no device memory is
- * allocated.  The first call on each device resolves the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share
- * the one array and rebuild it each time, so calls that overlap on the GPU race. */
+ * so grid_res must be at most 128 (larger grids return SVR_ERR_CAPACITY; grid_res <= 0 is
+ * SVR_ERR_ARG).  Inputs, outputs and the status word are the caller's, as for
+ * svr_laplacian_bw, and no device memory is allocated.  The first call on each device
+ * resolves the array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  The address is cached per device and context: after cudaDeviceReset
+ * the next call resolves it again.  All calls share the one array and rebuild it each time,
+ * so calls that overlap on the GPU race. */
 SVR_API int svr_laplacian_bw_noalloc(int G, int A, const int32_t* active, const int32_t* grid_keys,
                                      const int32_t* grid2voxel, int grid_res, const uint8_t* grid_mask,
                                      const float* voxel_coords, const float* voxel_sizes, int N,

@@ -25,7 +25,10 @@ SOURCES = [
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SVR_REFERENCE_DIR")
+    if not ref:
+        print("no reference checkout given (argument or SVR_REFERENCE_DIR); nothing to build")
+        return 0
     cuda_dir = os.path.join(ref, "cuda")
     if not os.path.isdir(cuda_dir):
         print(f"reference sources not found at {cuda_dir}; nothing to build")

@@ -13,7 +13,9 @@ import sys
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SVR_REFERENCE_DIR")
+    if not ref:
+        sys.exit("usage: give the reference checkout as the first argument or in SVR_REFERENCE_DIR")
     src = open(os.path.join(ref, "cuda", "svraster_cuda", "marching_cubes.py")).read()
     start = src.index("tri_table = torch.tensor(")
     end = src.index("], dtype=torch.long", start)

@@ -9,6 +9,7 @@
 #include <mutex>
 #include <string>
 
+#include <cuda.h>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
@@ -176,6 +177,8 @@ extern "C" int svr_grid_index_build(int G, const int32_t* grid_keys, int grid_re
                                     uint32_t* status, void* stream)
 {
     if (grid_res <= 0 || grid_res > 1024) return svr_fail(SVR_ERR_ARG, "grid index: resolution");
+    if (!dense_index || (G > 0 && (!grid_keys || !status)))
+        return svr_fail(SVR_ERR_ARG, "grid index: null argument");
     cudaStream_t st = (cudaStream_t)stream;
     const int cells = grid_res * grid_res * grid_res;
     CUDA_TRY(cudaMemsetAsync(dense_index, 0xFF, 4 * (size_t)cells, st));
@@ -839,19 +842,41 @@ static __device__ __align__(256) int32_t g_noalloc_grid_index[SVR_NOALLOC_MAX_RE
 
 // Device address of g_noalloc_grid_index per device.  The host-side name of the array is a
 // stand-in, not a device address, so the address comes from cudaGetSymbolAddress, resolved
-// once per device with that device current.
+// once per device with that device current.  The cached address belongs to the context that
+// was current when it was resolved: after cudaDeviceReset (or any teardown of the primary
+// context) the module is loaded again, possibly elsewhere, so the cache is keyed on the
+// context as well and resolved again when the context changes.
 static int32_t* g_noalloc_index_ptr[64];
+static CUcontext g_noalloc_index_ctx[64];
 static std::mutex g_noalloc_mutex;
+
+// cuCtxGetCurrent through the runtime's driver entry point (the library links only cudart)
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+static CUcontext current_context() {
+    static CtxGetCurrentFn fn = []() -> CtxGetCurrentFn {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return (CtxGetCurrentFn)f;
+    }();
+    CUcontext ctx = nullptr;
+    if (!fn || fn(&ctx) != CUDA_SUCCESS) return nullptr;
+    return ctx;
+}
 
 static int noalloc_index_ptr(int32_t** out) {
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return svr_fail(SVR_ERR_UNSUPPORTED, "noalloc: device ordinal above 63");
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_index_ptr[dev]) {
+    CUcontext ctx = current_context();
+    if (!g_noalloc_index_ptr[dev] || ctx == nullptr || g_noalloc_index_ctx[dev] != ctx) {
         void* p = nullptr;
-        CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_grid_index));
+        CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_grid_index));   // makes the primary context current
         g_noalloc_index_ptr[dev] = (int32_t*)p;
+        g_noalloc_index_ctx[dev] = current_context();
     }
     *out = g_noalloc_index_ptr[dev];
     return SVR_OK;
@@ -864,9 +889,15 @@ extern "C" int svr_laplacian_bw_noalloc(int G, int A, const int32_t* active, con
                                         float vox_size_inv, int seed, float* grid_grad, uint32_t* status,
                                         void* stream)
 {
-    if (grid_res <= 0 || grid_res > SVR_NOALLOC_MAX_RES)
+    if (grid_res <= 0) return svr_fail(SVR_ERR_ARG, "svr_laplacian_bw_noalloc: grid_res must be positive");
+    if (grid_res > SVR_NOALLOC_MAX_RES)
         return svr_fail(SVR_ERR_CAPACITY, "svr_laplacian_bw_noalloc: grid_res exceeds the static index capacity "
                                           "(maximum 128)");
+    if (A <= 0) return SVR_OK;
+    // every pointer the adjoint reads is checked before the index build launches anything
+    if (!active || !grid_keys || !grid2voxel || !grid_mask || !voxel_coords || !voxel_sizes || !vox_key ||
+        !grid_pts || !grid_grad || !status)
+        return svr_fail(SVR_ERR_ARG, "svr_laplacian_bw_noalloc: null argument");
     int32_t* index = nullptr;
     int rc = noalloc_index_ptr(&index);
     if (rc) return rc;

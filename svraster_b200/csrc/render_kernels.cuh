@@ -78,6 +78,7 @@ struct alignas(128) FwdSmem {
     Rec buf[RING][BATCH];
     uint64_t full[RING];
     uint32_t arrived[RING];
+    uint32_t armed[RING];      // phases armed on each slot (bulk copies and end-of-stream arrivals)
     uint32_t octl[NWARP][8];
     uint32_t warps_done;
     int32_t stop;              // first batch not issued once every warp is done (INT_MAX before)
@@ -89,6 +90,7 @@ struct alignas(128) BwdSmem {
     Rec buf[RING][BATCH];
     uint64_t full[RING];
     uint32_t arrived[RING];
+    uint32_t armed[RING];      // phases armed on each slot (bulk copies)
     uint32_t octl[NWARP][8];
     float red[NWARP];
 };
@@ -135,6 +137,22 @@ __device__ __forceinline__ void warp_octant_lanes(uint32_t* octl, bool inside, u
     __syncwarp();
 }
 
+// Before a CTA exits: wait (bounded) for the last phase armed on every ring slot, so no bulk
+// copy is still writing this CTA's shared memory when the next CTA on the SM takes it over.
+// On the normal path every armed phase has been consumed and each wait returns at once; it
+// matters after a timed-out wait, when warps left the stream with copies in flight.  A slot
+// whose phase does not complete within the bound keeps its mbarrier and flags ERR_DRAIN:
+// that path is bounded, not provably drained.
+template <int RING>
+__device__ __forceinline__ void drain_ring(uint64_t* full, const uint32_t* armed, unsigned* status) {
+#pragma unroll
+    for (int k = 0; k < RING; ++k) {
+        const uint32_t a = armed[k];
+        if (a == 0u || mbar_wait(&full[k], (a - 1u) & 1u)) mbar_inval(&full[k]);
+        else atomicOr(status, ERR_DRAIN | ERR_WAIT_TIMEOUT);
+    }
+}
+
 // ============================================================================ forward
 // RING (ring slots) and MINB (CTAs per SM asked of the register allocator) change only the
 // schedule, never the arithmetic: every (RING, MINB) instance produces the same outputs.
@@ -170,7 +188,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_kernel(
     const int nbatch = (n + BATCH - 1) / BATCH;
     if (tid == 0) {
 #pragma unroll
-        for (int k = 0; k < RING; ++k) { mbar_init(&S.full[k], 1); S.arrived[k] = 0; }
+        for (int k = 0; k < RING; ++k) { mbar_init(&S.full[k], 1); S.arrived[k] = 0; S.armed[k] = 0; }
         S.warps_done = 0;
         S.stop = INT_MAX;
         fence_mbar_init();
@@ -179,6 +197,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_kernel(
     auto issue = [&](int b) {
         const int slot = b % RING;
         const uint32_t bytes = (uint32_t)min(BATCH, n - b * BATCH) * (uint32_t)sizeof(Rec);
+        ++S.armed[slot];
         mbar_arrive_tx(&S.full[slot], bytes);
         bulk_g2s(S.buf[slot], recs + range.x + (size_t)b * BATCH, bytes, &S.full[slot]);
     };
@@ -298,6 +317,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_kernel(
                 if (nb2 < nbatch) {
                     if (*(volatile uint32_t*)&S.warps_done == NWARP) {
                         atomicMin(&S.stop, nb2);
+                        ++S.armed[slot];
                         __threadfence_block();
                         mbar_arrive(&S.full[slot]);          // wakes waiters without data
                     } else {
@@ -374,8 +394,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_kernel(
 #pragma unroll
         for (int w = 0; w < NWARP; ++w) m = max(m, S.red[w]);
         tile_last[tile] = range.x + m;
-#pragma unroll
-        for (int k = 0; k < RING; ++k) mbar_inval(&S.full[k]);
+        drain_ring<RING>(S.full, S.armed, status);
     }
 }
 
@@ -415,7 +434,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_kernel(
     const int nbatch = (n + BATCH - 1) / BATCH;
     if (tid == 0) {
 #pragma unroll
-        for (int k = 0; k < RING; ++k) { mbar_init(&S.full[k], 1); S.arrived[k] = 0; }
+        for (int k = 0; k < RING; ++k) { mbar_init(&S.full[k], 1); S.arrived[k] = 0; S.armed[k] = 0; }
         fence_mbar_init();
     }
     __syncthreads();
@@ -425,6 +444,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_kernel(
         const int hi = n - b * BATCH;
         const int c = min(BATCH, hi);
         const uint32_t bytes = (uint32_t)c * (uint32_t)sizeof(Rec);
+        ++S.armed[slot];
         mbar_arrive_tx(&S.full[slot], bytes);
         bulk_g2s(S.buf[slot], recs + r0 + (hi - c), bytes, &S.full[slot]);
     };
@@ -654,8 +674,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_kernel(
 #pragma unroll
         for (int w = 0; w < NWARP; ++w) s += S.red[w];
         if (s != 0.f) atomicAdd(dL_ds, s);
-#pragma unroll
-        for (int k = 0; k < RING; ++k) mbar_inval(&S.full[k]);
+        drain_ring<RING>(S.full, S.armed, status);
     }
 }
 

@@ -25,6 +25,7 @@ constexpr unsigned ERR_BAD_INDEX = 2u;
 constexpr unsigned ERR_COUNT_MISMATCH = 4u;
 constexpr unsigned ERR_CAPACITY = 8u;      // more records than the binning buffer holds
 constexpr unsigned ERR_KEY_FORMAT = 16u;   // a rendered path has bits the trimmed key drops
+constexpr unsigned ERR_DRAIN = 64u;        // a timed-out CTA exited with a bulk copy not seen to land
 
 struct Views {
     int n;

@@ -35,7 +35,9 @@ def load_on_cpu(path, name, extra=None):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SVR_REFERENCE_DIR")
+    if not ref:
+        sys.exit("usage: give the reference checkout as the first argument or in SVR_REFERENCE_DIR")
     import svraster_b200
     svraster_b200.install_as_svraster_cuda()   # cameras.py imports svraster_cuda (unused here)
     cams_mod = load_on_cpu(os.path.join(ref, "src", "cameras.py"), "ref_cameras")

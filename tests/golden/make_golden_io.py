@@ -28,7 +28,9 @@ from tests.golden.make_golden_extract import load_on_cpu  # noqa: E402
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SVR_REFERENCE_DIR")
+    if not ref:
+        sys.exit("usage: give the reference checkout as the first argument or in SVR_REFERENCE_DIR")
     import svraster_b200
     svraster_b200.install_as_svraster_cuda()
     for name in ("src", "src.utils"):

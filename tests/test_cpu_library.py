@@ -39,3 +39,21 @@ def test_buffer_size_queries_are_monotone():
 def test_view_descriptor_layout():
     import ctypes as C
     assert C.sizeof(_lib.ViewDesc) == 80
+
+
+def test_null_arguments_are_rejected_before_any_cuda_call():
+    """Null pointers come back as SVR_ERR_ARG (-1) from the argument checks, before the entry
+    point reaches the CUDA runtime (without a GPU any runtime call would fail with -2)."""
+    lib = _lib.load()
+    # svr_grid_index_build(G, grid_keys, grid_res, dense_index, status, stream)
+    assert lib.svr_grid_index_build(10, None, 64, None, None, None) == -1
+    # svr_laplacian_bw_noalloc(G, A, active, grid_keys, grid2voxel, grid_res, grid_mask, voxel_coords,
+    #     voxel_sizes, N, vox_key, grid_pts, M, weight, vox_size_inv, seed, grid_grad, status, stream)
+    # with A > 0 and every pointer null
+    args = [10, 5, None, None, None, 64, None, None, None, 0, None, None, 0, 0.01, 1.0, 1, None, None, None]
+    assert len(args) == 19
+    assert lib.svr_laplacian_bw_noalloc(*args) == -1
+    args[5] = 0                        # grid_res <= 0: a bad argument
+    assert lib.svr_laplacian_bw_noalloc(*args) == -1
+    args[5] = 256                      # above the static index: capacity
+    assert lib.svr_laplacian_bw_noalloc(*args) == -3

@@ -53,11 +53,24 @@ def _run(fn_name, d, seed, with_index):
     return grad.cpu().numpy()
 
 
+def _half_table(d):
+    """Every second key of the grid table with its voxel row, and a fresh active set over it:
+    if the shared index kept entries of an earlier call, they would point at wrong rows."""
+    out = dict(d)
+    out["keys"] = d["keys"][::2].contiguous()
+    out["g2v"] = d["g2v"][::2].contiguous()
+    rng = np.random.default_rng(12)
+    G = out["keys"].numel()
+    out["active"] = torch.as_tensor(rng.permutation(G)[: G // 2].astype(np.int32), device=d["grid"].device)
+    return out
+
+
 def test_noalloc_laplacian_matches_regular_entry_point_twice():
     d = _inputs()
-    for seed in (123, 456):     # two calls in a row: the shared index must be rebuilt each time
-        got = _run("svr_laplacian_bw_noalloc", d, seed, with_index=False)
-        ref = _run("svr_laplacian_bw", d, seed, with_index=True)
+    # two calls in a row, the second on a smaller key table: the shared index must be rebuilt
+    for inputs, seed in ((d, 123), (_half_table(d), 456)):
+        got = _run("svr_laplacian_bw_noalloc", inputs, seed, with_index=False)
+        ref = _run("svr_laplacian_bw", inputs, seed, with_index=True)
         scale = np.abs(ref).max()
         assert scale > 0
         # same arithmetic; only the order of the float atomics differs
@@ -75,3 +88,22 @@ def test_noalloc_rejects_grid_beyond_static_capacity():
                                     ptr(grad), ptr(status), stream_ptr())
     assert rc == -3
     assert b"capacity" in L.svr_last_error()
+
+
+def test_noalloc_rejects_null_arguments_before_any_launch():
+    d = _inputs()
+    L = _lib.load()
+    grad = torch.zeros_like(d["grid"])
+    status = torch.zeros(1, dtype=torch.int32, device=grad.device)
+    args = [d["keys"].numel(), d["active"].numel(), ptr(d["active"]), ptr(d["keys"]), ptr(d["g2v"]), d["res"],
+            ptr(d["mask"]), ptr(d["coord"]), ptr(d["vsize"]), d["sc"].n_vox, ptr(d["vox_key"]), ptr(d["grid"]),
+            d["grid"].numel(), 0.01, 1.0, 1, ptr(grad), ptr(status), stream_ptr()]
+    for i in (3, 4, 16, 17):            # grid_keys, grid2voxel, grid_grad, status
+        bad = list(args)
+        bad[i] = None
+        assert L.svr_laplacian_bw_noalloc(*bad) == -1
+    bad = list(args)
+    bad[5] = 0                          # grid_res <= 0 is a bad argument, not a capacity problem
+    assert L.svr_laplacian_bw_noalloc(*bad) == -1
+    torch.cuda.synchronize()
+    assert float(grad.abs().sum()) == 0.0
