@@ -1,22 +1,29 @@
 """Throughput benchmark of the sm_100a sparse-voxel SDF rasterizer training step.
 
-Workload (mid-size plain method): ~1.4M voxels at octree levels 6-10 around three spheres and
-a torus, SH degree 3, 8 views of 800x800 on a Fibonacci sphere of radius 3.  One step renders
-all 8 views forward and backward and runs the SDF regularisers and Adam (svraster_b200.step).
+Headline workload (batched): a sphere with 64 Gaussian bumps, octree levels 7-11 (~4.2M
+voxels), SH degree 3, 64 views of mixed resolution (16 each of 480x360, 960x540, 1280x720,
+1920x1080, shuffled; 58.9M rays) in one step: gather, SH, preprocess, binning (sort
+included), render forward and adjoint, smoothness adjoints and Adam, captured as one CUDA
+graph (svraster_b200.step).  ``--config mid`` is the plain mid-size workload (3 spheres and a
+torus, levels 6-10, 8 views of 800x800); the default line carries it as ``mid_size``.
 
   value : forward+backward Mrays/s of the batched step, inputs resident in HBM
-  e2e   : the same metric through the batched C-ABI training step (BatchedTrainStep, two
-          CUDA graphs), that step's upstream gradient planes and target image copied from
-          pinned host memory every step (overlapping the forward graph) and the mean
-          transmittance read back; ``e2e_dropin_per_view`` is the same through the drop-in
-          per-view API (svraster_b200.renderer with autograd, grid_loss_bw, SparseAdam)
+  per_view : the same work through the plain per-view kernels (the drop-in API one view at
+          a time, as the reference's train.py drives it), same device-resident inputs
+  e2e   : the batched step through the C-ABI training step (two CUDA graphs) with each
+          step's upstream gradient planes and target image copied from pinned host memory
+          and the mean transmittance read back; ``e2e_per_view`` is the same through the
+          per-view API
+  reference_cuda : the reference's own CUDA extension (built from its unmodified sources)
+          on the same views, per view, timed after our timed regions (a baseline leg)
   roofline : the dominant kernel's algorithmic bytes / CUDA-event duration vs the measured
-          HBM copy bandwidth (MEASURED_PEAKS.json)
-  cpu_baseline : the CPU oracle (single thread) on one view of the same workload
+          HBM copy bandwidth (MEASURED_PEAKS.json), and its FP32 / MUFU issue ceiling from
+          measured pair counts (``compute``)
+  cpu_baseline : the CPU oracle (single thread) on a sample of the same workload
 
 ``--impl reference`` times the CPU restatement of the reference algorithm (the reference's
 only implementation of this path is CUDA) with all host threads on a bounded sample.
-Multi-GPU (torchrun): every rank renders its own 8 views (weak scaling) and the gradients are
+Multi-GPU (torchrun): every rank renders its own views (weak scaling) and the gradients are
 all-reduced over NCCL before Adam.
 """
 from __future__ import annotations
@@ -34,18 +41,31 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 CONFIGS = {
-    # the headline: plain method, mid-size scene
-    "mid": dict(workload="mid-size: 3 spheres + torus, levels 6-10, SH deg 3, 8 views 800x800", views=8,
-                image="800x800"),
-    # batched: one step over 64 views of four resolutions
+    # the headline: one step over 64 views of four resolutions
     "batched": dict(workload="batched: sphere with 64 bumps, levels 7-11, SH deg 3, 64 views (16 each of "
                              "480x360, 960x540, 1280x720, 1920x1080, shuffled)", views=64, image="mixed"),
+    # plain method, mid-size scene
+    "mid": dict(workload="mid-size: 3 spheres + torus, levels 6-10, SH deg 3, 8 views 800x800", views=8,
+                image="800x800"),
 }
-WORKLOAD = CONFIGS["mid"]["workload"]
-N_VIEWS, W, H = 8, 800, 800
+DEFAULT_CONFIG = "batched"
+WORKLOAD = CONFIGS[DEFAULT_CONFIG]["workload"]
+W, H = 800, 800          # mid-size view size
+
+# Per-pair operation model of the render kernels (three sub-samples, depth and normal on),
+# counted from the kernel source: an IEEE division is one MUFU reciprocal and 4 FP32 ops,
+# expf one MUFU ex2 and 3 FP32 ops, rsqrtf one MUFU op; FFMA, FADD, FMUL and FMNMX one FP32
+# op each.  "eval": a (pixel, record) pair that reaches the SDF evaluation (slab test twice,
+# entry point and three sub-steps of trilinear SDF and logistic CDF, local and total alpha);
+# "acc": the extra work of a pair with alpha >= MIN_ALPHA (compositing, depth, normal; in the
+# adjoint the transmittance recovery, normal chain rule, alpha and depth sub-segment
+# derivatives over four re-evaluated points, and the colour terms).
+OPS_PER_PAIR = {"fwd": {"eval": (269, 16), "acc": (53, 1)},
+                "bwd": {"eval": (157, 6), "acc": (527, 24)}}
+SMS, FP32_LANES, MUFU_LANES = 148, 128, 16
 
 
-def rank_cameras(rank=0, n_views=None, config="mid"):
+def rank_cameras(rank=0, n_views=None, config=DEFAULT_CONFIG):
     """The views of one rank (data parallel over views, weak scaling): rank r takes the r-th
     block of the workload's views-per-GPU from a camera set of (r + 1) blocks."""
     from svraster_b200 import synthetic as S
@@ -57,7 +77,7 @@ def rank_cameras(rank=0, n_views=None, config="mid"):
     return cams[:n_views or n]
 
 
-def make_workload(rank=0, n_views=None, config="mid"):
+def make_workload(rank=0, n_views=None, config=DEFAULT_CONFIG):
     from svraster_b200 import synthetic as S
     scene = S.scene_batched(seed=0) if config == "batched" else S.scene_mid(seed=0)
     return scene, rank_cameras(rank, n_views, config)
@@ -132,25 +152,32 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def load_traffic(kernel, workload):
-    """DRAM bytes per launch of `kernel` on `workload` from the ncu summary table in
-    profiles/traffic.md (None when the workload was not captured)."""
-    path = os.path.join(ROOT, "profiles", "traffic.md")
-    if not os.path.exists(path):
-        return None
-    with open(path) as f:
-        for line in f:
-            cells = [c.strip() for c in line.strip().strip("|").split("|")]
-            if len(cells) == 3 and cells[0] == kernel and cells[1] == workload:
-                try:
-                    return int(cells[2])
-                except ValueError:
-                    return None
-    return None
-
-
 # ----------------------------------------------------------------------------- our arm
-def run_ours(args, rank, world):
+def compute_ceiling(state, s_val, kname, kms, sm_mhz):
+    """FP32 / MUFU issue ceiling of the dominant render kernel: the pairs it evaluates and
+    accepts (counted on the device by the counting instance of the forward), times the
+    per-pair operation model OPS_PER_PAIR, over the B200's FP32 lanes (148 SMs x 128) and MUFU
+    lanes (148 SMs x 16) at the sampled SM clock."""
+    n_eval, n_acc, n_eval_last = state.count_pairs(s_val)
+    pas = "bwd" if kname == "render_bwd_kernel" else "fwd"
+    ev = n_eval_last if pas == "bwd" else n_eval
+    m = OPS_PER_PAIR[pas]
+    fp32 = ev * m["eval"][0] + n_acc * m["acc"][0]
+    mufu = ev * m["eval"][1] + n_acc * m["acc"][1]
+    hz = (sm_mhz or 1965.0) * 1e6
+    t_fp32 = fp32 / (SMS * FP32_LANES * hz) * 1e3
+    t_mufu = mufu / (SMS * MUFU_LANES * hz) * 1e3
+    t_bound = max(t_fp32, t_mufu)
+    return {"pairs_evaluated": int(ev), "pairs_accepted": int(n_acc),
+            "pairs_evaluated_forward": int(n_eval),
+            "fp32_ops": int(fp32), "mufu_ops": int(mufu),
+            "fp32_peak_ops_per_s": SMS * FP32_LANES * hz, "mufu_peak_ops_per_s": SMS * MUFU_LANES * hz,
+            "sm_mhz": sm_mhz, "t_fp32_ms": round(t_fp32, 4), "t_mufu_ms": round(t_mufu, 4),
+            "binding": "fp32" if t_fp32 >= t_mufu else "mufu", "frac": round(t_bound / kms, 4),
+            "model": "OPS_PER_PAIR in bench.py (per-pair FP32 and MUFU operations counted from the kernel source)"}
+
+
+def run_ours(args, rank, world, config):
     from svraster_b200.step import BatchedTrainStep
     import torch
     import torch.distributed as dist
@@ -158,8 +185,8 @@ def run_ours(args, rank, world):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    scene, cams = make_workload(rank, args.views, args.config)
-    workload = CONFIGS[args.config]["workload"]
+    scene, cams = make_workload(rank, args.views, config)
+    workload = CONFIGS[config]["workload"]
     step = BatchedTrainStep(scene, cams, device=dev, lambda_R_concen=0.1)
     L = _lib.load()
 
@@ -168,9 +195,7 @@ def run_ours(args, rank, world):
     def allreduce_grads(grads):
         dist.all_reduce(step.grad_flat)           # grid, sh0 and shs gradients in one call
     hook = allreduce_grads if world > 1 else None
-    # one GPU: the timed steps replay one CUDA graph holding the whole step (the record count
-    # stays on the device); several GPUs: eager steps with the all-reduce between them
-    use_graph = world == 1 and not args.no_graph
+    use_graph = not args.no_graph
     for _ in range(args.warmup):
         step.step(grad_hook=hook)
     # the render launch configuration is chosen on this batch before anything is timed
@@ -182,13 +207,13 @@ def run_ours(args, rank, world):
     if world > 1:
         dist.barrier()
 
-    def timed(fn):
+    def timed(fn, n):
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         n0 = L.svr_kernel_launches()
         with ClockSampler(dev.index) as clk:
             torch.cuda.synchronize()
             ev0.record()
-            for _ in range(args.steps):
+            for _ in range(n):
                 fn()
             ev1.record()
             torch.cuda.synchronize()
@@ -200,24 +225,28 @@ def run_ours(args, rank, world):
     def eager():
         step.step(time_render=True, grad_hook=hook)
         step_events.append(step.ev)
-    eager_ms, launches, clocks = timed(eager)
+    n_eager = max(3, min(args.steps, 10))
+    eager_ms, launches, clocks = timed(eager, n_eager)
     stages = [BatchedTrainStep.stage_ms(m) for m in step_events]
     stage_avg = {k: float(np.mean([s_[k] for s_ in stages])) for k in stages[0]}
     fwd_ms = [s_["render_fwd"] for s_ in stages]
     bwd_ms = [s_["render_bwd"] for s_ in stages]
-    total_ms = eager_ms
+    total_ms = eager_ms * args.steps / n_eager
     graph_info = None
     if use_graph:
-        per_step = step.capture()
+        # the whole step, all-reduce included when several ranks run, as one CUDA graph
+        per_step = step.capture(grad_hook=hook)
         for _ in range(args.warmup):
             step.replay()
-        total_ms, _, clocks = timed(step.replay)
+        total_ms, _, clocks = timed(step.replay, args.steps)
         launches = per_step * args.steps
         st_raster, st_misc = step.graph_status()
         if st_raster or st_misc:
             raise RuntimeError(f"graph replay status raster={st_raster} misc={st_misc}")
         graph_info = {"captured": True, "kernels_per_step": per_step, "record_capacity": step.capacity,
-                      "eager_ms_per_step": round(eager_ms / args.steps, 3)}
+                      "allreduce_in_graph": world > 1, "eager_ms_per_step": round(eager_ms / n_eager, 3)}
+    else:
+        launches = launches * args.steps // n_eager
 
     if world > 1:
         total_ms = max_over_ranks(total_ms, dev)
@@ -240,17 +269,23 @@ def run_ours(args, rank, world):
         kname, kbytes, kms = "render_fwd_kernel", fwd_bytes, fwd_avg
     peak, peak_src = measured_peaks()
     achieved = kbytes / (kms * 1e-3) / 1e9
+    compute = compute_ceiling(step.state, step.s_val, kname, kms, clocks.get("sm_mhz"))
     roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak,
                 "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": load_traffic(kname, workload), "algorithmic_bytes": int(kbytes),
-                "launch_ms": round(kms, 4)}
+                "traffic": None,
+                "traffic_note": "DRAM bytes per launch are taken by ncu outside the bench run (the ncu "
+                                "summaries of the render kernels); none is measured in this run",
+                "algorithmic_bytes": int(kbytes), "launch_ms": round(kms, 4),
+                "launch_ms_source": "CUDA events around the kernel in eager steps, on its stream",
+                "compute": compute}
 
     result = {"metric": "fwd+bwd Mrays/s", "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
               "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
+              "iters_per_s": round(1e3 / ms_per_step, 3),
               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
               "data": "synthetic (seeded procedural scene, N(0,1) upstream gradients)",
               "config": {"workload": workload, "n_voxels": scene.n_vox, "n_grid_pts": int(step.grid.numel()),
-                         "views_per_gpu": len(cams), "image": CONFIGS[args.config]["image"], "rays_per_step": rays,
+                         "views_per_gpu": len(cams), "image": CONFIGS[config]["image"], "rays_per_step": rays,
                          "records_R": R, "records_R_prime": R_prime, "visible_voxels": V_vis,
                          "l2": "inputs larger than L2 (records + SH state > 126 MB)",
                          "parallelism": f"dp{world} over views" if world > 1 else "single GPU"},
@@ -345,12 +380,19 @@ def run_e2e_batched(args, scene, cams, dev):
                     "upstream planes from pinned host memory every step, mean T read back"}
 
 
-def run_e2e(args, scene, cams, dev):
-    """The same metric through the drop-in per-view API with host-resident upstream gradients."""
+def run_per_view(args, scene, cams, dev, host_inputs, steps=None, warmup=None):
+    """The same step through the plain per-view path: the drop-in API (renderer.rasterize_voxels
+    with autograd, GatherGeoParams, SH_eval) one view at a time, as the reference's train.py
+    drives its extension, then grid_loss_bw and SparseAdam.  ``host_inputs``: every step copies
+    all views' upstream planes and target images from pinned host memory (view v's render waits
+    only for its own planes) and reads the step's result back; otherwise the planes stay
+    resident on the device, as for the batched ``value``."""
     import torch
     from svraster_b200 import renderer, grid_loss_bw
     from svraster_b200.sparse_adam import SparseAdam
 
+    steps = steps or args.steps
+    warmup = warmup or args.warmup
     t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
     octpath = t(scene.octpath, torch.int64)
     centers = t(scene.vox_center)
@@ -374,8 +416,10 @@ def run_e2e(args, scene, cams, dev):
     host = []
     for c in cams:
         P = c.width * c.height
-        planes = [torch.from_numpy(rng.normal(size=n * P).astype(np.float32)).pin_memory() for n in (3, 4, 3)]
-        gt = torch.from_numpy(rng.uniform(size=3 * P).astype(np.float32)).pin_memory()
+        planes = [torch.from_numpy(rng.normal(size=n * P).astype(np.float32)) for n in (3, 4, 3)]
+        gt = torch.from_numpy(rng.uniform(size=3 * P).astype(np.float32))
+        if host_inputs:
+            planes, gt = [p_.pin_memory() for p_ in planes], gt.pin_memory()
         host.append((planes, gt))
     mats = [(t(c.w2c), t(c.c2w)) for c in cams]
     bg = torch.zeros(3, device=dev)
@@ -390,30 +434,31 @@ def run_e2e(args, scene, cams, dev):
                        * np.float32(res)))
     vsize = t(np.round(scene.vox_size / ext * np.float32(res))).reshape(-1)
     active = torch.arange(keys.numel(), dtype=torch.int32, device=dev)
-    h2d = sum(sum(p.numel() for p in planes) * 4 + gt.numel() * 4 for planes, gt in host) + 2 * 64 * len(cams)
+    h2d = sum(sum(p_.numel() for p_ in planes) * 4 + gt.numel() * 4 for planes, gt in host) + 2 * 64 * len(cams)
 
-    # every step copies all views' upstream planes from pinned host memory on a copy stream;
-    # view v's render waits only for its own planes, so the copies overlap earlier views
-    dev_bufs = [([torch.empty_like(p, device=dev) for p in planes], torch.empty_like(gt, device=dev))
-                for planes, gt in host]
+    # device buffers of the upstream planes; with host inputs they are refilled every step on a
+    # copy stream, otherwise filled once
+    dev_bufs = [([p_.to(dev) for p_ in planes], gt.to(dev)) for planes, gt in host]
     copy_stream = torch.cuda.Stream(device=dev)
 
     def one_step(it):
         opt.zero_grad(set_to_none=False) if grid.grad is not None else None
         tot = torch.zeros((), device=dev)
         compute = torch.cuda.current_stream(dev)
-        copy_stream.wait_stream(compute)          # buffers are free once the last step used them
-        ready = []
-        with torch.cuda.stream(copy_stream):
-            for (planes, gt_h), (dplanes, dgt) in zip(host, dev_bufs):
-                for hp, dp in zip(planes, dplanes):
-                    dp.copy_(hp, non_blocking=True)
-                dgt.copy_(gt_h, non_blocking=True)
-                ev = torch.cuda.Event()
-                ev.record(copy_stream)
-                ready.append(ev)
+        ready = [None] * len(cams)
+        if host_inputs:
+            copy_stream.wait_stream(compute)      # buffers are free once the last step used them
+            with torch.cuda.stream(copy_stream):
+                for v, ((planes, gt_h), (dplanes, dgt)) in enumerate(zip(host, dev_bufs)):
+                    for hp, dp in zip(planes, dplanes):
+                        dp.copy_(hp, non_blocking=True)
+                    dgt.copy_(gt_h, non_blocking=True)
+                    ev = torch.cuda.Event()
+                    ev.record(copy_stream)
+                    ready[v] = ev
         for (dplanes, dgt), ev, (w2c, c2w), c in zip(dev_bufs, ready, mats, cams):
-            compute.wait_event(ev)
+            if ev is not None:
+                compute.wait_event(ev)
             dc, dd, dn = dplanes
             gt = dgt.view(3, c.height, c.width)
             rs = renderer.RasterSettings(color_mode="sh", vox_geo_mode="triinterp3", density_mode="sdf",
@@ -430,23 +475,124 @@ def run_e2e(args, scene, cams, dev):
             fn(grid, vox_key, coord, vsize, res, mask, keys, g2v, active, 1e-3, float(res) / scene.scene_extent,
                True, False, grid.grad, seed=it)
         opt.step()
-        return float(tot.item())   # device -> host read of the step's result
+        return float(tot.item()) if host_inputs else tot   # device -> host read of the step's result
 
-    for i in range(args.warmup):
+    for i in range(warmup):
         one_step(i)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
-    for i in range(args.steps):
+    for i in range(steps):
         one_step(1000 + i)
     ev1.record()
     torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = ev0.elapsed_time(ev1) / steps
     rays = sum(c.width * c.height for c in cams)
-    return {"value": round(rays / (ms * 1e-3) / 1e6, 3), "unit": "Mrays/s", "ms_per_step": round(ms, 3),
-            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4,
-            "path": "svraster_b200.renderer.rasterize_voxels per view + autograd + grid_loss_bw + SparseAdam"}
+    out = {"value": round(rays / (ms * 1e-3) / 1e6, 3), "unit": "Mrays/s", "ms_per_step": round(ms, 3),
+           "iters_per_s": round(1e3 / ms, 3), "steps": steps,
+           "path": "svraster_b200.renderer.rasterize_voxels per view + autograd + grid_loss_bw + SparseAdam"}
+    if host_inputs:
+        out.update({"h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4})
+    del opt, grid, sh0, shs, dev_bufs
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_reference_cuda(scene, cams, dev, steps=3, warmup=1):
+    """The reference's own CUDA extension (oracle/_ref, built from its unmodified sources by
+    oracle/build_ref.py) on the same scene and views, one view at a time on the default stream
+    as the reference's train.py drives it (train.py:316-709): per view rasterize_preprocess,
+    gather and SH on the in-frustum voxels, rasterize_voxels, rasterize_voxels_backward and
+    the gather / SH adjoints; per step the Laplacian and grid-Eikonal adjoints over every
+    dense-grid key and Adam on grid / sh0 / shs.  A baseline leg, timed after our own timed
+    regions with CUDA events (median step).  Returns {"unavailable": why} when the built
+    extension is not present."""
+    import importlib.util
+    import torch
+    so = os.path.join(ROOT, "oracle", "_ref", "svraster_ref_C.so")
+    if not os.path.exists(so):
+        return {"unavailable": "the reference extension was not built (oracle/build_ref.py needs the reference "
+                               "sources on the build machine)"}
+    spec = importlib.util.spec_from_file_location("svraster_ref_C", so)
+    R_ = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(R_)
+    t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
+    octpath, centers, lengths = t(scene.octpath, torch.int64), t(scene.vox_center), t(scene.vox_size)
+    is_leaf = t(scene.is_leaf, torch.uint8)
+    vox_key, grid = t(scene.vox_key, torch.int64), t(scene.geo_grid_pts)
+    sh0, shs = t(scene.sh0), t(scene.shs)
+    s_val = torch.exp(torch.tensor([scene.log_s], dtype=torch.float32, device=dev) * 10.0)
+    views = [(t(c.w2c), t(c.c2w), c) for c in cams]
+    bg = torch.zeros(3, device=dev)
+    g = torch.Generator(device=dev).manual_seed(0)
+    ups = [(torch.randn(3, c.height, c.width, device=dev, generator=g),
+            torch.randn(4, c.height, c.width, device=dev, generator=g),
+            torch.randn(3, c.height, c.width, device=dev, generator=g),
+            torch.zeros(1, c.height, c.width, device=dev),
+            torch.rand(3, c.height, c.width, device=dev, generator=g)) for c in cams]
+    res_pow2 = min(int(scene.octlevel.max()), 9)
+    res = 1 << res_pow2
+    mask, keys, g2v = R_.valid_gradient_table(centers, lengths, torch.zeros(3, device=dev),
+                                              float(scene.scene_extent), res_pow2, is_leaf.bool())
+    order = torch.argsort(keys)
+    keys, g2v = keys[order].contiguous(), g2v[order].contiguous()
+    ext = np.float32(scene.scene_extent)
+    coord = t(np.round(((scene.vox_center - scene.vox_size * np.float32(0.5)) + ext * np.float32(0.5)) / ext
+                       * np.float32(res)))
+    vsize = t(np.round(scene.vox_size / ext * np.float32(res))).reshape(-1)
+    active = torch.arange(keys.numel(), dtype=torch.int32, device=dev)
+    params = [grid, sh0, shs]
+    ms_ = [torch.zeros_like(p_) for p_ in params]
+    vs_ = [torch.zeros_like(p_) for p_ in params]
+
+    def one_step(it):
+        dgrid = torch.zeros_like(grid)
+        dsh0 = torch.zeros_like(sh0)
+        dshs = torch.zeros_like(shs)
+        for (w2c, c2w, c), (dc, dd, dn, dT, gt) in zip(views, ups):
+            ndup, geom = R_.rasterize_preprocess(c.width, c.height, c.tanfovx, c.tanfovy, c.cx, c.cy, w2c, c2w, 0,
+                                                 c.near, octpath, centers, lengths, is_leaf, False)
+            care = torch.where(ndup > 0)[0]
+            geos = R_.gather_triinterp_geo_params(vox_key, care, grid)
+            cam_pos = c2w[:3, 3].contiguous()
+            rgbs = R_.sh_compute(3, care, centers, cam_pos, sh0, shs)
+            out = R_.rasterize_voxels(3, 1, c.width, c.height, c.tanfovx, c.tanfovy, c.cx, c.cy, w2c, c2w, bg, 0,
+                                      True, False, True, False, octpath, centers, lengths, geos, rgbs,
+                                      torch.empty(scene.n_vox, 0, device=dev), geom, False, s_val)
+            nr, binning, img, color, depth, normal, T = out[:7]
+            dgeos, drgbs, _, ds = R_.rasterize_voxels_backward(
+                nr, 3, 1, c.width, c.height, c.tanfovx, c.tanfovy, c.cx, c.cy, w2c, c2w, bg, octpath, centers,
+                lengths, geos, rgbs, geom, binning, img, T, dc, dd, dn, dT, 0.1, gt, 0.0, 0.0, True, True, depth,
+                normal, False, s_val, out[8])
+            dgrid += R_.gather_triinterp_geo_params_bw(vox_key, care, grid.numel(), dgeos.contiguous())
+            a0, a1 = R_.sh_compute_bw(3, 16, care, centers, cam_pos, rgbs, drgbs.contiguous())
+            dsh0 += a0
+            dshs += a1
+        R_.laplacian_smoothness_bw(grid, vox_key, coord, vsize, res, mask, keys, g2v, active, 1e-3,
+                                   float(res) / scene.scene_extent, True, False, dgrid)
+        R_.grid_eikonal_bw(grid, vox_key, coord, vsize, res, mask, keys, g2v, active, 1e-3,
+                           float(res) / scene.scene_extent, True, False, dgrid)
+        for p_, gr, m, v, lr in zip(params, (dgrid, dsh0, dshs), ms_, vs_, (1e-3, 1e-3, 1e-4)):
+            R_.unbiased_adam_step(False, p_, gr, m, v, it + 1, lr, 0.1, 0.99, 1e-15)
+
+    for i in range(warmup):
+        one_step(i)
+    torch.cuda.synchronize()
+    times = []
+    for i in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        one_step(warmup + i)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = float(np.median(times))
+    rays = sum(c.width * c.height for c in cams)
+    del params, ms_, vs_, ups
+    torch.cuda.empty_cache()
+    return {"value": round(rays / ms / 1e3, 3), "unit": "Mrays/s", "ms_per_step": round(ms, 3),
+            "iters_per_s": round(1e3 / ms, 4), "steps": steps,
+            "path": "reference svraster_cuda._C built from its unmodified sources, per view, default stream"}
 
 
 def run_extraction(step, scene, cams, dev):
@@ -775,39 +921,62 @@ def oracle_view_step(scene, cam, threads):
     return Hc * Wc
 
 
+def sample_views(cams):
+    """The CPU sample of a workload: the first view of each distinct resolution, in order."""
+    seen, out = set(), []
+    for c in cams:
+        if (c.width, c.height) not in seen:
+            seen.add((c.width, c.height))
+            out.append(c)
+    return out
+
+
 def cpu_baseline(scene, cams):
+    views = sample_views(cams)
     t0 = time.perf_counter()
-    rays = oracle_view_step(scene, cams[0], threads=1)
+    rays = sum(oracle_view_step(scene, c, threads=1) for c in views)
     dt = time.perf_counter() - t0
+    sizes = ", ".join(f"{c.width}x{c.height}" for c in views)
     return {"value": round(rays / dt / 1e6, 5), "unit": "Mrays/s", "cores": 1, "kind": "port",
-            "sample": f"1 of {len(cams)} views ({cams[0].width}x{cams[0].height}) preprocess+binning+fwd+bwd, "
+            "sample": f"{len(views)} of {len(cams)} views ({sizes}) preprocess+binning+fwd+bwd, "
                       f"single thread, {dt:.1f} s"}
 
 
 # ----------------------------------------------------------------------------- reference arm
 def run_reference(args):
-    scene, cams = make_workload(0)
+    config = getattr(args, "config", DEFAULT_CONFIG)
+    scene, cams = make_workload(0, config=config)
+    views = sample_views(cams)
     threads = os.cpu_count() or 1
-    oracle_view_step(scene, cams[0], threads)  # warm caches / page in
+    oracle_view_step(scene, views[0], threads)  # warm caches / page in
     for i in range(max(0, args.warmup - 1)):
-        oracle_view_step(scene, cams[(i + 1) % len(cams)], threads)
+        oracle_view_step(scene, views[(i + 1) % len(views)], threads)
     times, rays = [], 0
     for i in range(args.steps):
         t0 = time.perf_counter()
-        rays_i = oracle_view_step(scene, cams[i % len(cams)], threads)
+        rays_i = oracle_view_step(scene, views[i % len(views)], threads)
         times.append(time.perf_counter() - t0)
         rays += rays_i
     total = sum(times)
     value = rays / total / 1e6
+    sizes = ", ".join(f"{c.width}x{c.height}" for c in views)
     return {"metric": "fwd+bwd Mrays/s", "value": round(value, 5), "unit": "Mrays/s", "impl": "reference",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_voxels": scene.n_vox,
-                       "sample": "one view per step (rotating), preprocess+binning+fwd+bwd"},
+            "config": {"workload": CONFIGS[config]["workload"], "n_voxels": scene.n_vox,
+                       "sample": f"one view per step, rotating over the workload's resolutions ({sizes}); "
+                                 "preprocess+binning+fwd+bwd"},
             "cpu_baseline": {"value": round(value, 5), "unit": "Mrays/s", "cores": threads, "kind": "port",
-                             "sample": "one 800x800 view per step of the 8-view workload"},
+                             "sample": f"one view per step ({sizes}, rotating) of the {len(cams)}-view workload"},
             "e2e": {"value": round(value, 5), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def secondary_summary(res):
+    """The fields of a secondary workload's line kept in the headline line."""
+    keep = ("value", "unit", "ms_per_step", "iters_per_s", "config", "stages_ms", "roofline", "clocks", "cuda_graph",
+            "autotuned_render", "gpu_launches")
+    return {k: res[k] for k in keep if k in res}
 
 
 def main():
@@ -816,11 +985,15 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="mid", choices=sorted(CONFIGS), help="workload (mid = the headline)")
+    ap.add_argument("--config", default=DEFAULT_CONFIG, choices=sorted(CONFIGS),
+                    help=f"workload ({DEFAULT_CONFIG} = the headline)")
     ap.add_argument("--views", type=int, default=None, help="views per GPU (default: the workload's)")
+    ap.add_argument("--per-view-steps", type=int, default=5, help="timed steps of the per-view legs")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-extract", action="store_true")
+    ap.add_argument("--no-extract", action="store_true", help="skip the extraction / regulariser / format legs")
+    ap.add_argument("--no-per-view", action="store_true", help="skip the per-view and reference-CUDA legs")
+    ap.add_argument("--no-mid", action="store_true", help="skip the secondary mid-size workload")
     ap.add_argument("--no-graph", action="store_true", help="time eager steps instead of graph replays")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default render launch configuration")
     args = ap.parse_args()
@@ -833,40 +1006,73 @@ def main():
             print(json.dumps(run_reference(args)), flush=True)
         return
 
+    import torch
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     if world > 1:
         import datetime
         import torch.distributed as dist
-        import torch
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        torch.cuda.set_device(dev)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    result, step, scene, cams = run_ours(args, rank, world)
-    if rank == 0:
-        import torch
-        if not args.no_extract:
-            result["extraction"] = run_extraction(step, scene, cams,
-                                                  torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
-            result["adaptive"] = run_adaptive(step, scene, cams,
-                                              torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
-            result["regularisers"] = run_regularisers(step, scene,
-                                                      torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
-            result["checkpoint"] = run_checkpoint(scene, torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
-            result["normal_losses"] = run_normal_losses(step, cams,
-                                                        torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
-            result["normal_losses"]["step_with_losses"] = run_step_with_normal_losses(
-                scene, cams, torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
-        if not args.no_e2e:
-            del step
-            torch.cuda.empty_cache()
-            dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
-            result["e2e"] = run_e2e_batched(args, scene, cams, dev)
-            result["e2e_dropin_per_view"] = run_e2e(args, scene, cams, dev)
-        if not args.no_cpu:
-            result["cpu_baseline"] = cpu_baseline(scene, cams)
-        print(json.dumps(result), flush=True)
+    result, step, scene, cams = run_ours(args, rank, world, args.config)
     if world > 1:
+        # several ranks: the headline line only (the other legs are single-GPU measurements)
+        if rank == 0:
+            print(json.dumps(result), flush=True)
         import torch.distributed as dist
+        step.graph = step.graph_b = None   # graphs holding NCCL calls go before the group does
+        del step
         dist.barrier()
         dist.destroy_process_group()
+        return
+    if rank == 0:
+        # everything below runs after the headline's timed region
+        step.graph = step.graph_b = None
+        del step
+        torch.cuda.empty_cache()
+        if not args.no_e2e:
+            result["e2e"] = run_e2e_batched(args, scene, cams, dev)
+        if not args.no_per_view:
+            pv = run_per_view(args, scene, cams, dev, host_inputs=False, steps=args.per_view_steps)
+            result["per_view"] = pv
+            result["batched_vs_per_view"] = {"value": round(result["value"] / pv["value"], 3)}
+            if not args.no_e2e:
+                pve = run_per_view(args, scene, cams, dev, host_inputs=True, steps=args.per_view_steps)
+                result["e2e_per_view"] = pve
+                result["batched_vs_per_view"]["e2e"] = round(result["e2e"]["value"] / pve["value"], 3)
+            result["reference_cuda"] = run_reference_cuda(scene, cams, dev)
+            if "value" in result["reference_cuda"]:
+                result["vs_reference_cuda"] = {"value": round(result["value"] / result["reference_cuda"]["value"], 3)}
+                if "e2e" in result:
+                    result["vs_reference_cuda"]["e2e"] = round(result["e2e"]["value"] /
+                                                               result["reference_cuda"]["value"], 3)
+        if not args.no_cpu:
+            result["cpu_baseline"] = cpu_baseline(scene, cams)
+        if args.config != "mid" and not args.no_mid:
+            # the plain mid-size workload: its own step, e2e, per-view and reference legs, and the
+            # extraction / regulariser / format legs on its scene
+            margs = argparse.Namespace(**vars(args))
+            margs.views = None
+            mres, mstep, mscene, mcams = run_ours(margs, rank, world, "mid")
+            mid = secondary_summary(mres)
+            if not args.no_extract:
+                mid["extraction"] = run_extraction(mstep, mscene, mcams, dev)
+                mid["adaptive"] = run_adaptive(mstep, mscene, mcams, dev)
+                mid["regularisers"] = run_regularisers(mstep, mscene, dev)
+                mid["checkpoint"] = run_checkpoint(mscene, dev)
+                mid["normal_losses"] = run_normal_losses(mstep, mcams, dev)
+                mid["normal_losses"]["step_with_losses"] = run_step_with_normal_losses(mscene, mcams, dev)
+            mstep.graph = mstep.graph_b = None
+            del mstep
+            torch.cuda.empty_cache()
+            if not args.no_e2e:
+                mid["e2e"] = run_e2e_batched(margs, mscene, mcams, dev)
+            if not args.no_per_view:
+                mid["per_view"] = run_per_view(margs, mscene, mcams, dev, host_inputs=False)
+                if not args.no_e2e:
+                    mid["e2e_per_view"] = run_per_view(margs, mscene, mcams, dev, host_inputs=True)
+                mid["reference_cuda"] = run_reference_cuda(mscene, mcams, dev, steps=5, warmup=2)
+            result["mid_size"] = mid
+        print(json.dumps(result), flush=True)
 
 
 if __name__ == "__main__":

@@ -182,6 +182,17 @@ SVR_API int svr_render_fwd_max_w_views(const svr_view_t* views_host, int n_views
                                        float* out_normal, float* out_T, float* max_w_views,
                                        void* stream);
 
+/* Work measurement, no counterpart in the reference: the forward render of
+ * svr_render_fwd (three sub-samples, depth and normal on) on records already packed by an
+ * earlier svr_render_fwd on the same buffers, with the same outputs, that also writes to
+ * pair_count (device u64[3]) the (pixel, record) pairs that reached the SDF evaluation, those
+ * with alpha >= MIN_ALPHA, and those up to each pixel's last contributor (the pairs the adjoint
+ * evaluates).  A separate kernel instance: the plain forward does not count. */
+SVR_API int svr_render_fwd_count_pairs(const svr_view_t* views_host, int n_views, int N, int64_t R,
+                                       const float* s_val, void* binning_buffer, void* image_buffer,
+                                       float* out_color, float* out_depth, float* out_normal, float* out_T,
+                                       unsigned long long* pair_count, void* stream);
+
 /* Device status word of the raster launches that used this image buffer (0 = clean;
  * bit 1 wait timeout, bit 2 index out of range, bit 4 duplicate count mismatch, bit 8
  * records beyond the binning capacity, bit 16 sort-key format, bit 64 a render CTA that had

@@ -65,6 +65,7 @@ _SIGS = {
     "svr_rank_table_workspace_bytes": (_I, [_I64, C.POINTER(C.c_size_t)]),
     "svr_rank_table_build": (_I, [_I64, _P, _U64, _P, C.POINTER(C.c_int), _P, _SZ, _P]),
     "svr_unpack_binning": (_I, [_P, _I64, _I, _P, _I64, _P, _P, _P, _P, _P]),
+    "svr_render_fwd_count_pairs": (_I, [_P, _I, _I, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "svr_render_fwd": (_I, [_P, _I, _I, _I64, _I, _I, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P,
                             _P, _P, _P, _P, _P, _P]),
     "svr_render_bwd": (_I, [_P, _I, _I, _I64, _I, _I, _F, _P, _P, _P, _P, _P, _P, _P, _P, _P,

@@ -821,7 +821,7 @@ static int launch_fwd_cfg(int T, cudaStream_t st, const Views& V, const uint32_t
     int rc = ensure_smem(k, smem, done);
     if (rc) return rc;
     k<<<T, BLOCK, smem, st>>>(V, order, ranges, recs, s_val, tile_last, n_contrib, color,
-                              depth, normal, outT, max_w, mw_stride, status);
+                              depth, normal, outT, max_w, mw_stride, status, nullptr);
     LAUNCH_CHECK();
     return SVR_OK;
 }
@@ -941,6 +941,38 @@ static int render_fwd_impl(const svr_view_t* views_host, int n_views, int N, int
     FWD_CASE(3)
 #undef FWD_CASE
     return svr_fail(SVR_ERR_UNSUPPORTED, "n_samp");
+}
+
+// The pair-counting instance of the forward (three sub-samples, depth and normal on, the
+// default launch configuration): the same outputs as svr_render_fwd plus the pair counts.
+extern "C" int svr_render_fwd_count_pairs(const svr_view_t* views_host, int n_views, int N, int64_t R,
+                                          const float* s_val, void* binning_buffer, void* image_buffer,
+                                          float* out_color, float* out_depth, float* out_normal, float* out_T,
+                                          unsigned long long* pair_count, void* stream)
+{
+    Views V;
+    int T; int64_t P;
+    int rc = build_views(views_host, n_views, V, T, P);
+    if (rc) return rc;
+    if (!out_color || !out_depth || !out_normal || !out_T || !s_val || !pair_count)
+        return svr_fail(SVR_ERR_ARG, "render_fwd_count_pairs: null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    BinLayout BL = bin_layout(R);
+    ImgLayout IL = img_layout(P, T);
+    char* b = (char*)binning_buffer;
+    char* im = (char*)image_buffer;
+    auto k = render_fwd_kernel<3, true, true, false, SVR_NSLOT, SVR_FWD_MINB, true>;
+    const int smem = (int)sizeof(FwdSmem<SVR_NSLOT>);
+    static std::atomic<unsigned long long> done{0};
+    rc = ensure_smem(k, smem, done);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemsetAsync(pair_count, 0, 3 * sizeof(unsigned long long), st));
+    k<<<T, BLOCK, smem, st>>>(V, (const uint32_t*)(im + IL.order), (const uint2*)(im + IL.ranges),
+                              (const Rec*)(b + BL.recs), s_val, (uint32_t*)(im + IL.tile_last),
+                              (uint32_t*)(im + IL.n_contrib), out_color, out_depth, out_normal, out_T, nullptr, 0,
+                              (unsigned*)(im + IL.status), pair_count);
+    LAUNCH_CHECK();
+    return SVR_OK;
 }
 
 template <bool DEPTH, bool NORMAL, bool RCONC, int RING, int MINB>

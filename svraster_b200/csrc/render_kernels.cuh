@@ -156,13 +156,18 @@ __device__ __forceinline__ void drain_ring(uint64_t* full, const uint32_t* armed
 // ============================================================================ forward
 // RING (ring slots) and MINB (CTAs per SM asked of the register allocator) change only the
 // schedule, never the arithmetic: every (RING, MINB) instance produces the same outputs.
-template <int NS, bool DEPTH, bool NORMAL, bool MAXW, int RING = NSLOT, int MINB = SVR_FWD_MINB>
+// COUNT (a separate instance, used only to measure the work) also adds to pair_count[0..2]
+// the (pixel, record) pairs that reached the SDF evaluation, those accepted (alpha >=
+// MIN_ALPHA), and those evaluated up to the pixel's last contributor (the pairs the adjoint
+// evaluates).
+template <int NS, bool DEPTH, bool NORMAL, bool MAXW, int RING = NSLOT, int MINB = SVR_FWD_MINB, bool COUNT = false>
 __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_kernel(
     const __grid_constant__ Views V, const uint32_t* __restrict__ order, const uint2* __restrict__ ranges,
     const Rec* __restrict__ recs, const float* __restrict__ s_ptr, uint32_t* __restrict__ tile_last,
     uint32_t* __restrict__ n_contrib,
     float* __restrict__ out_color, float* __restrict__ out_depth, float* __restrict__ out_normal,
-    float* __restrict__ out_T, float* __restrict__ max_w, int64_t max_w_stride, unsigned* __restrict__ status)
+    float* __restrict__ out_T, float* __restrict__ max_w, int64_t max_w_stride, unsigned* __restrict__ status,
+    unsigned long long* __restrict__ pair_count = nullptr)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     FwdSmem<RING>& S = *reinterpret_cast<FwdSmem<RING>*>(smem_raw);
@@ -213,6 +218,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_kernel(
     bool reported = false;
     uint32_t parity = 0;
     bool failed = false;
+    uint32_t n_eval = 0, n_acc = 0, n_eval_last = 0;   // COUNT only
 
     for (int b = 0; b < nbatch; ++b) {
         const int slot = b % RING;
@@ -267,7 +273,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_kernel(
                         phi_former = phi_curr;
                     }
                     const float alpha = fmaxf((phi_entry - phi_former) / (phi_entry + 1e-6f), 0.f);
+                    if (COUNT) ++n_eval;
                     if (alpha < MIN_ALPHA) continue;
+                    if (COUNT) { ++n_acc; n_eval_last = n_eval; }
                     const float pt_w = T * alpha;
                     C = C + pt_w * f3(r.r, r.gr, r.b);
                     if (DEPTH) {
@@ -385,6 +393,16 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_kernel(
             on[pix] = Nn.x; on[HW + pix] = Nn.y; on[2 * HW + pix] = Nn.z;
         }
         my_last = last;
+    }
+    if (COUNT) {
+        const unsigned long long e = __reduce_add_sync(0xffffffffu, n_eval);
+        const unsigned long long a = __reduce_add_sync(0xffffffffu, n_acc);
+        const unsigned long long l = __reduce_add_sync(0xffffffffu, n_eval_last);
+        if (lane == 0) {
+            atomicAdd(pair_count, e);
+            atomicAdd(pair_count + 1, a);
+            atomicAdd(pair_count + 2, l);
+        }
     }
     const uint32_t wl = __reduce_max_sync(0xffffffffu, my_last);
     if (lane == 0) S.red[warp] = wl;

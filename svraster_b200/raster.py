@@ -101,6 +101,21 @@ class RasterState:
                                stream_ptr(dev)), "svr_render_fwd")
         return color, depth, normal, T, max_w
 
+    def count_pairs(self, s_val, return_planes=False):
+        """(evaluated, accepted, adjoint) (pixel, record) pair counts of this batch's forward
+        (three sub-samples, depth and normal on), by the counting instance of the forward
+        kernel; call after ``render`` packed the records.  Synchronises.  With
+        ``return_planes`` also returns that instance's (color, depth, normal, T)."""
+        L = _lib.load()
+        P, dev = self.total_pix, self.device
+        out = [torch.empty(n * P, dtype=torch.float32, device=dev) for n in (3, 4, 3, 1)]
+        cnt = torch.zeros(3, dtype=torch.int64, device=dev)
+        check(L.svr_render_fwd_count_pairs(self.views, self.n_views, self.N, self.num_rendered, ptr(s_val),
+                                           ptr(self.binning), ptr(self.image), *[ptr(o) for o in out], ptr(cnt),
+                                           stream_ptr(dev)), "svr_render_fwd_count_pairs")
+        counts = tuple(int(x) for x in cnt.cpu().tolist())
+        return (counts, tuple(out)) if return_planes else counts
+
     def render_backward(self, need_depth, need_normal, s_val, out_T, dcolor, ddepth, dnormal, dT,
                         lambda_R_concen=0.0, gt_color=None, drgbs=None, dvox=None, ds=None):
         L = _lib.load()

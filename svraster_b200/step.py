@@ -303,7 +303,7 @@ class BatchedTrainStep:
         torch.cuda.synchronize(self.dev)
         return self.tuned
 
-    def capture(self, capacity=None, rows=1 << 20, split=False, upstream_sets=1):
+    def capture(self, capacity=None, rows=1 << 20, split=False, upstream_sets=1, grad_hook=None):
         """Capture one whole step (gather, SH, preprocess, scan, duplicate, sort, pack, render
         forward and adjoint, scatter, SH adjoint, smoothness adjoints, Adam) into a CUDA graph.
         ``capacity`` bounds the records per step (default: this batch's record total, found by
@@ -315,6 +315,9 @@ class BatchedTrainStep:
         ``upstream_sets=2`` (split only) one backward graph is captured per set of upstream
         planes (``upstream(i)``); ``replay_backward(i)`` reads set i, so the next step's
         planes can be copied into the other set during the whole current step.
+        ``grad_hook(grads)`` is captured between the adjoints and Adam, like ``step``'s (the
+        data-parallel NCCL all-reduce of ``grad_flat`` is captured into the graph with it; a
+        graph holding NCCL calls must be released before the process group is destroyed).
         Returns the number of this library's kernels in the graph(s)."""
         L = _lib.load()
         if capacity is None:
@@ -355,7 +358,7 @@ class BatchedTrainStep:
                     setattr(self, n, t)
                 g = torch.cuda.CUDAGraph()
                 with torch.cuda.graph(g, pool=self.graph.pool()):
-                    self.graph_out = self._backward_part(True, nomark, None, self._graph_fw, [], False)
+                    self.graph_out = self._backward_part(True, nomark, grad_hook, self._graph_fw, [], False)
                 self.graph_bs.append(g)
             for n, t in zip(names, sets[0]):
                 setattr(self, n, t)
@@ -364,7 +367,7 @@ class BatchedTrainStep:
             self.graph = torch.cuda.CUDAGraph()
             self.graph_b = None
             with torch.cuda.graph(self.graph):
-                self.graph_out = self._body(True)
+                self.graph_out = self._body(True, grad_hook=grad_hook)
         self.graph_launches = int(L.svr_kernel_launches() - n0)
         torch.cuda.synchronize(self.dev)
         self._dev_step_synced = True

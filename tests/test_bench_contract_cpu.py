@@ -17,13 +17,15 @@ import bench  # noqa: E402
 
 
 def test_reference_arm_line():
-    line = bench.run_reference(types.SimpleNamespace(steps=1, warmup=3))
+    assert bench.DEFAULT_CONFIG == "batched" and bench.WORKLOAD == bench.CONFIGS["batched"]["workload"]
+    # the mid-size workload keeps this CPU test short; the default run times the batched one
+    line = bench.run_reference(types.SimpleNamespace(steps=1, warmup=3, config="mid"))
     for key in ("metric", "value", "unit", "impl", "n_gpus", "steps", "warmup", "ms_per_step",
                 "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
         assert key in line, key
     assert line["impl"] == "reference" and line["metric"] == "fwd+bwd Mrays/s" and line["unit"] == "Mrays/s"
     assert line["higher_is_better"] is True and line["steps"] == 1 and line["value"] > 0
-    assert line["config"]["workload"] == bench.WORKLOAD
+    assert line["config"]["workload"] == bench.CONFIGS["mid"]["workload"]
     cb = line["cpu_baseline"]
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == line["value"] and cb["sample"]
     assert line["e2e"] == {"value": line["value"], "unit": "Mrays/s", "h2d_bytes_per_step": 0,

@@ -130,3 +130,18 @@ def test_empty_view_and_all_culled():
     c = out["color"].cpu().numpy().reshape(3, -1)
     assert np.allclose(c[0], 0.5) and np.allclose(c[1], 0.25) and np.allclose(c[2], 0.125)
     assert float(out["dvox"].abs().sum()) == 0.0
+
+
+def test_pair_counting_instance_matches_forward():
+    """The counting instance of the forward writes the same images bit for bit, and its pair
+    counts are ordered: accepted <= evaluated up to the last contributor <= evaluated."""
+    sc, cams = scene_and_cams("small", 2, 160, 120, seed=7)
+    geos, _ = oracle_inputs(sc, cams[0])
+    rgbs = [oracle_inputs(sc, c)[1] for c in cams]
+    out = cuda_views(sc, cams, geos, rgbs)
+    st = out["state"]
+    s_val = torch.tensor([sc.s_val], dtype=torch.float32, device="cuda")
+    (n_eval, n_acc, n_last), planes = st.count_pairs(s_val, return_planes=True)
+    assert 0 < n_acc <= n_last <= n_eval
+    for a, k in zip(planes, ("color", "depth", "normal", "T")):
+        assert torch.equal(a, out[k]), k
