@@ -182,6 +182,22 @@ SVR_API int svr_render_fwd_max_w_views(const svr_view_t* views_host, int n_views
                                        float* out_normal, float* out_T, float* max_w_views,
                                        void* stream);
 
+/* Binning without a global radix sort (no counterpart in the reference; same result as
+ * svr_bin_and_sort, whose order is the one of cuda/src/forward.cu:749-829, 882-939).
+ * svr_pair_order_build (once per octree): pair_pos u32[8N] = the position of every (voxel,
+ * octant) pair in the order of the full octree rank, ties by voxel id then octant;
+ * *key_bits_host = bits of a position.  The workspace is svr_rank_table_workspace_bytes(N).
+ * svr_bin_tiles (per step, after svr_preprocess): counts the records of every tile, scans
+ * the counts into tile ranges and the heavy-first launch order, scatters every record into
+ * its tile's range, and sorts each tile by pair position with one CTA.  R is the record
+ * capacity (the device bins min(total, R) records and sets status bit 8 beyond it); no host
+ * synchronisation, so it can be captured into a CUDA graph. */
+SVR_API int svr_pair_order_build(int64_t N, const int64_t* octpaths, uint32_t* pair_pos, int* key_bits_host,
+                                 void* ws, size_t ws_bytes, void* stream);
+SVR_API int svr_bin_tiles(const svr_view_t* views_host, int n_views, int N, int64_t R, const uint32_t* pair_pos,
+                          int key_bits, void* geom_buffer, void* binning_buffer, size_t binning_bytes,
+                          void* image_buffer, void* stream);
+
 /* Work measurement, no counterpart in the reference: the forward render of
  * svr_render_fwd (three sub-samples, depth and normal on) on records already packed by an
  * earlier svr_render_fwd on the same buffers, with the same outputs, that also writes to

@@ -21,6 +21,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include "svr_common.cuh"
+#include "tile_sort.cuh"
 
 using namespace svr;
 
@@ -46,6 +47,21 @@ int svr_fail(int code, const char* what) {
 #define LAUNCH_CHECK() do { svr_note_launch(1); CUDA_TRY(cudaGetLastError()); } while (0)
 
 static inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Raise a kernel's dynamic shared-memory limit once per device (kept out of the launch
+// path so that launches can be captured into a graph without extra API calls).
+template <typename K>
+static int ensure_smem(K k, int smem, std::atomic<unsigned long long>& done)
+{
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return SVR_OK;
+    CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    done.fetch_or(bit, std::memory_order_acq_rel);
+    return SVR_OK;
+}
+
 
 // ------------------------------------------------------------------ buffer layouts
 // geom buffer: meta | n_dup u32[M] | scan u32[M] | bbox uint2[M] | bits u32[M] | scan tmp
@@ -107,7 +123,8 @@ static BinLayout bin_layout(int64_t R) {
 // image buffer: ranges uint2[T] | tile_last u32[T] | n_contrib u32[P] | status |
 //               launch order u32[T] | order sort keys / values / scratch
 struct ImgLayout {
-    size_t ranges, tile_last, n_contrib, status, order, okeys_in, okeys_out, ovals_in, otmp, otmp_bytes, total;
+    size_t ranges, tile_last, n_contrib, status, order, okeys_in, okeys_out, ovals_in, otmp, otmp_bytes;
+    size_t tile_cnt, cursor, blk_sum, blk_hist, total;   // tile binning (svr_bin_tiles)
 };
 static ImgLayout img_layout(int64_t P, int T) {
     ImgLayout L{};
@@ -125,6 +142,11 @@ static ImgLayout img_layout(int64_t P, int T) {
     cub::DeviceRadixSort::SortPairs(nullptr, tb, (const uint32_t*)nullptr, (uint32_t*)nullptr,
                                     (const uint32_t*)nullptr, (uint32_t*)nullptr, nt);
     L.otmp = off; L.otmp_bytes = tb; off = align_up(off + tb, 256);
+    const size_t nblk = (size_t)(nt + TS_BLK - 1) / TS_BLK;
+    L.tile_cnt = off; off = align_up(off + 4 * (size_t)nt, 256);
+    L.cursor = off; off = align_up(off + 4 * (size_t)nt, 256);
+    L.blk_sum = off; off = align_up(off + 4 * nblk, 256);
+    L.blk_hist = off; off = align_up(off + 4 * 256 * nblk, 256);
     L.total = off;
     return L;
 }
@@ -572,6 +594,90 @@ extern "C" int svr_bin_and_sort_ranked(const svr_view_t* views_host, int n_views
                              binning_buffer, binning_bytes, image_buffer, stream);
 }
 
+// ------------------------------------------------------------------ tile binning
+// Per step: count, scan, scatter and per-tile sort of the batch's records (tile_sort.cuh).
+// R is the record capacity of the binning buffer; the device bins min(total, R) records.
+extern "C" int svr_bin_tiles(const svr_view_t* views_host, int n_views, int N, int64_t R, const uint32_t* pair_pos,
+                             int key_bits, void* geom_buffer, void* binning_buffer, size_t binning_bytes,
+                             void* image_buffer, void* stream)
+{
+    Views V;
+    int T; int64_t P;
+    int rc = build_views(views_host, n_views, V, T, P);
+    if (rc) return rc;
+    if (N < 0 || (N > 0 && (!pair_pos || !geom_buffer || !binning_buffer || !image_buffer)))
+        return svr_fail(SVR_ERR_ARG, "bin_tiles: null argument");
+    if (key_bits < 1 || key_bits > 32) return svr_fail(SVR_ERR_ARG, "bin_tiles: key bits");
+    if (R >= (1ll << 32)) return svr_fail(SVR_ERR_CAPACITY, "bin_tiles: capacity above 2^32 records");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t M = (int64_t)N * n_views;
+    GeomLayout GL = geom_layout(M);
+    BinLayout BL = bin_layout(R);
+    ImgLayout IL = img_layout(P, T);
+    if (binning_bytes < BL.total) return svr_fail(SVR_ERR_CAPACITY, "binning buffer too small");
+    char* g = (char*)geom_buffer;
+    char* b = (char*)binning_buffer;
+    char* im = (char*)image_buffer;
+    unsigned* status = (unsigned*)(im + IL.status);
+    BinMeta* meta = (BinMeta*)b;
+    uint32_t* tile_cnt = (uint32_t*)(im + IL.tile_cnt);
+    uint32_t* cursor = (uint32_t*)(im + IL.cursor);
+    CUDA_TRY(cudaMemsetAsync(status, 0, 4, st));
+    CUDA_TRY(cudaMemsetAsync(tile_cnt, 0, 4 * (size_t)T, st));
+    const int n_rec = (int)(R > 0 ? R : 1);
+    const uint32_t* ndup = (const uint32_t*)(g + GL.ndup);
+    const uint2* bbox = (const uint2*)(g + GL.bbox);
+    const uint32_t* bits = (const uint32_t*)(g + GL.bits);
+    // per-view histograms in shared memory when the largest view's tiles fit in 96 KB
+    int max_nt = 0;
+    for (int v = 0; v < n_views; ++v) max_nt = std::max(max_nt, V.v[v].tiles_x * V.v[v].tiles_y);
+    const bool smem_hist = max_nt <= 24576;
+    const int hist_bytes = smem_hist ? 4 * max_nt : 0;
+    // about 8 CTAs per SM in all, split over the views (as preprocess)
+    const int per_view = std::max(1, std::min((N + 255) / 256, (8 * 148 + n_views - 1) / n_views));
+    dim3 grid(per_view, n_views);
+    if (N > 0) {
+        if (smem_hist) {
+            static std::atomic<unsigned long long> d1{0}, d2{0};
+            if ((rc = ensure_smem(tile_count_kernel<true>, hist_bytes, d1))) return rc;
+            if ((rc = ensure_smem(tile_scatter_kernel<true>, hist_bytes, d2))) return rc;
+            tile_count_kernel<true><<<grid, 256, hist_bytes, st>>>(V, N, ndup, bbox, bits, tile_cnt);
+        } else {
+            tile_count_kernel<false><<<grid, 256, 0, st>>>(V, N, ndup, bbox, bits, tile_cnt);
+        }
+        LAUNCH_CHECK();
+    }
+    const int nblk = (T + TS_BLK - 1) / TS_BLK;
+    tile_sum_kernel<<<nblk, 256, 0, st>>>(T, tile_cnt, (uint32_t*)(im + IL.blk_sum), (uint32_t*)(im + IL.blk_hist));
+    LAUNCH_CHECK();
+    tile_offsets_kernel<<<nblk, 256, 0, st>>>(T, nblk, tile_cnt, (const uint32_t*)(im + IL.blk_sum),
+                                              (const uint32_t*)(im + IL.blk_hist), R, (uint2*)(im + IL.ranges), cursor,
+                                              (uint32_t*)(im + IL.order), &meta->count, &meta->rank_bits, status);
+    LAUNCH_CHECK();
+    if (N == 0 || R == 0) return SVR_OK;
+    // record keys and values: (A) keys_in[0, R) / vals_in, (B) keys_in[R, 2R) / keys_out[R, 2R);
+    // results: vals_out and the tile id of every record in keys_out[0, R)
+    uint32_t* ka = (uint32_t*)(b + BL.keys_in);
+    uint32_t* kb = ka + n_rec;
+    uint32_t* va = (uint32_t*)(b + BL.vals_in);
+    uint32_t* tile_out = (uint32_t*)(b + BL.keys_out);
+    uint32_t* vb = tile_out + n_rec;
+    if (smem_hist)
+        tile_scatter_kernel<true><<<grid, 256, hist_bytes, st>>>(V, N, ndup, bbox, bits, pair_pos, cursor, R, ka, va,
+                                                                 status);
+    else
+        tile_scatter_kernel<false><<<grid, 256, 0, st>>>(V, N, ndup, bbox, bits, pair_pos, cursor, R, ka, va, status);
+    LAUNCH_CHECK();
+    static std::atomic<unsigned long long> d3{0};
+    const int ts_smem = (int)sizeof(TileSortSmem);
+    if ((rc = ensure_smem(tile_sort_kernel, ts_smem, d3))) return rc;
+    tile_sort_kernel<<<T, TS_THREADS, ts_smem, st>>>(T, (const uint32_t*)(im + IL.order),
+                                                      (const uint2*)(im + IL.ranges), key_bits, ka, va, kb, vb,
+                                                      (uint32_t*)(b + BL.vals_out), tile_out, status);
+    LAUNCH_CHECK();
+    return SVR_OK;
+}
+
 // ------------------------------------------------------------------ dense rank table
 // Once per octree and trimming: the trimmed rank (path ^ rep3(q)) >> shift of every (voxel,
 // octant) pair, sorted; equal ranks share one dense index, so the dense index orders and ties
@@ -669,6 +775,35 @@ extern "C" int svr_rank_table_build(int64_t N, const int64_t* octpaths, uint64_t
     return SVR_OK;
 }
 
+extern "C" int svr_pair_order_build(int64_t N, const int64_t* octpaths, uint32_t* pair_pos, int* key_bits_host,
+                                    void* ws, size_t ws_bytes, void* stream)
+{
+    size_t need = 0;
+    if (int rc = svr_rank_table_workspace_bytes(N, &need)) return rc;
+    if (N <= 0 || !octpaths || !pair_pos || !key_bits_host || !ws || ws_bytes < need)
+        return svr_fail(SVR_ERR_ARG, "pair order: bad argument or workspace too small");
+    RankWs w;
+    if (int rc = rank_ws(8 * N, w)) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    char* base = (char*)ws;
+    uint64_t* kin = (uint64_t*)(base + w.keys_in);
+    uint64_t* kout = (uint64_t*)(base + w.keys_out);
+    uint32_t* vin = (uint32_t*)(base + w.vals_in);
+    uint32_t* vout = (uint32_t*)(base + w.vals_out);
+    const int64_t n = 8 * N;
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    pair_rank_kernel<<<nb, 256, 0, st>>>(N, octpaths, kin, vin);
+    LAUNCH_CHECK();
+    size_t tb = w.tmp_bytes;
+    CUDA_TRY(cub::DeviceRadixSort::SortPairs(base + w.tmp, tb, kin, kout, vin, vout, (int)n, 0, RANK_BITS, st));
+    pair_pos_kernel<<<nb, 256, 0, st>>>(n, vout, pair_pos);
+    LAUNCH_CHECK();
+    int bits = 1;
+    while (bits < 32 && (1ll << bits) < n) ++bits;
+    *key_bits_host = bits;
+    return SVR_OK;
+}
+
 extern "C" int svr_unpack_binning(const void* binning_buffer, int64_t R, int T, const void* image_buffer,
                                   int64_t P, uint32_t* vals, uint32_t* ranges, uint32_t* tile_last,
                                   uint32_t* n_contrib, void* stream)
@@ -742,20 +877,6 @@ __global__ void __launch_bounds__(256) pack_records_kernel(
 
 // ------------------------------------------------------------------ render kernels
 #include "render_kernels.cuh"
-
-// Raise a kernel's dynamic shared-memory limit once per device (kept out of the launch
-// path so that launches can be captured into a graph without extra API calls).
-template <typename K>
-static int ensure_smem(K k, int smem, std::atomic<unsigned long long>& done)
-{
-    int dev = 0;
-    CUDA_TRY(cudaGetDevice(&dev));
-    const unsigned long long bit = 1ull << (dev & 63);
-    if (done.load(std::memory_order_acquire) & bit) return SVR_OK;
-    CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    done.fetch_or(bit, std::memory_order_acq_rel);
-    return SVR_OK;
-}
 
 // Launch configurations (ring slots, CTAs per SM) the tuner chooses between for the
 // common flag sets (three sub-samples, depth and normal on; with or without the

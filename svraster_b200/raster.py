@@ -50,14 +50,17 @@ class RasterState:
         return n_dup
 
     # -------------------------------------------------------------- binning
-    def bin(self, octpaths, capacity=None, path_or=None, rank_table=None):
+    def bin(self, octpaths, capacity=None, path_or=None, rank_table=None, pair_order=None):
         """Duplicate, sort and range the records.  By default the record total is read back
         (one host synchronisation, as the reference does).  With ``capacity`` (and ``path_or``,
         the OR of every voxel's octree path) nothing is read back: the buffers hold
         ``capacity`` records and the device bins min(total, capacity) of them (status bit 8
         if any were dropped), which lets the call be captured into a CUDA graph.
         ``rank_table`` (a ``RankTable``) narrows the sort key to dense ranks when it was built
-        for the same trimming as this call's path_or (same order, fewer radix passes)."""
+        for the same trimming as this call's path_or (same order, fewer radix passes).
+        ``pair_order`` (a ``PairOrder`` of the same octree) bins with the per-tile sort
+        (svr_bin_tiles: count, scan, scatter, one CTA per tile) instead of the global radix
+        sort; the record order is the same."""
         L = _lib.load()
         M = self.N * self.n_views
         if capacity is None:
@@ -73,7 +76,11 @@ class RasterState:
         nb = L.svr_binning_buffer_bytes(self.num_rendered, self.total_tiles)
         self.binning = _empty_bytes(nb, self.device)
         self.image = _empty_bytes(L.svr_image_buffer_bytes(self.total_pix, self.total_tiles), self.device)
-        if rank_table is not None and rank_table.matches(self.path_or):
+        if pair_order is not None:
+            check(L.svr_bin_tiles(self.views, self.n_views, self.N, self.num_rendered, ptr(pair_order.pos),
+                                  pair_order.bits, ptr(self.geom), ptr(self.binning), nb, ptr(self.image),
+                                  stream_ptr(self.device)), "svr_bin_tiles")
+        elif rank_table is not None and rank_table.matches(self.path_or):
             check(L.svr_bin_and_sort_ranked(self.views, self.n_views, self.N, self.num_rendered, self.path_or,
                                             ptr(octpaths), ptr(rank_table.table), rank_table.bits, ptr(self.geom),
                                             ptr(self.binning), nb, ptr(self.image), stream_ptr(self.device)),
@@ -196,3 +203,39 @@ class RankTable:
 
     def matches(self, path_or):
         return rank_shift(path_or) == self.shift
+
+
+class PairOrder:
+    """Position of every (voxel, octant) pair of an octree in the reference's record order
+    (full octree rank, ties by voxel id then octant; svr_pair_order_build), for
+    ``RasterState.bin(pair_order=...)``.  Valid for the octree it was built from."""
+
+    def __init__(self, octpaths):
+        L = _lib.load()
+        dev = octpaths.device
+        paths = octpaths.reshape(-1).to(torch.int64).contiguous()
+        N = paths.numel()
+        nbytes = C.c_size_t(0)
+        check(L.svr_rank_table_workspace_bytes(N, C.byref(nbytes)), "svr_rank_table_workspace_bytes")
+        ws = _empty_bytes(nbytes.value, dev)
+        self.pos = torch.empty(8 * N, dtype=torch.int32, device=dev)
+        bits = C.c_int(0)
+        check(L.svr_pair_order_build(N, ptr(paths), ptr(self.pos), C.byref(bits), ptr(ws), nbytes.value,
+                                     stream_ptr(dev)), "svr_pair_order_build")
+        self.bits = int(bits.value)
+        self.N = N
+
+
+_PAIR_ORDER_CACHE = {}
+
+
+def pair_order_for(octpaths):
+    """The PairOrder of an octree, cached on the path tensor's storage and version (a new
+    octree after pruning or subdivision gets a new table)."""
+    key = (octpaths.data_ptr(), octpaths.numel(), octpaths._version, str(octpaths.device))
+    po = _PAIR_ORDER_CACHE.get(key)
+    if po is None:
+        _PAIR_ORDER_CACHE.clear()
+        po = PairOrder(octpaths)
+        _PAIR_ORDER_CACHE[key] = po
+    return po

@@ -18,7 +18,7 @@ import torch
 
 from . import _lib
 from ._lib import check, ptr, stream_ptr
-from .raster import RankTable, RasterState
+from .raster import PairOrder, RankTable, RasterState
 from . import utils
 
 
@@ -39,7 +39,7 @@ class BatchedTrainStep:
 
     def __init__(self, scene, cams, device="cuda", lr=(1e-3, 1e-3, 1e-4), betas=(0.1, 0.99), eps=1e-15,
                  lambda_ls=1e-3, lambda_ge=1e-3, lambda_R_concen=0.0, sh_degree=3, seed=0, fused_smoothness=True,
-                 sh_dtype="f32", normal_losses=None, dense_ranks=True):
+                 sh_dtype="f32", normal_losses=None, dense_ranks=True, binning="tiles"):
         """``sh_dtype="bf16"`` stores the SH coefficients in bf16 (the precision configuration):
         colours, compositing, transmittance and every gradient stay f32, Adam keeps f32 moments
         and rounds the updated coefficients to nearest bf16.  ``normal_losses`` (a dict with
@@ -48,7 +48,9 @@ class BatchedTrainStep:
         between the render forward and the adjoint, their gradients added to the upstream
         depth / normal planes the adjoint reads.  ``dense_ranks`` bins with the octree's dense
         (voxel, octant) ranks (``raster.RankTable``, built here once): the same record order
-        with a narrower sort key."""
+        with a narrower sort key.  ``binning="tiles"`` (default) bins with the per-tile sort
+        (``raster.PairOrder``, built here once; svr_bin_tiles), ``"radix"`` with the global
+        radix sort of svr_bin_and_sort; both give the same record order."""
         dev = torch.device(device)
         self.dev = dev
         t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
@@ -133,7 +135,11 @@ class BatchedTrainStep:
         # per-group Adam coefficient tables
         leaf_paths = np.asarray(scene.octpath, dtype=np.int64)[np.asarray(scene.is_leaf).astype(bool).reshape(-1)]
         self.path_or_all = int(np.bitwise_or.reduce(leaf_paths.view(np.uint64))) if leaf_paths.size else 0
-        self.rank_table = RankTable(self.octpath, self.path_or_all) if dense_ranks else None
+        if binning not in ("tiles", "radix"):
+            raise ValueError("binning is 'tiles' or 'radix'")
+        self.binning = binning
+        self.pair_order = PairOrder(self.octpath) if binning == "tiles" else None
+        self.rank_table = RankTable(self.octpath, self.path_or_all) if dense_ranks and binning == "radix" else None
         self.graph = None
         self.graph_b = None
         self.graph_out = None
@@ -183,9 +189,10 @@ class BatchedTrainStep:
         state.preprocess(self.octpath, self.centers, self.lengths, self.is_leaf)
         mark("preprocess")
         if graph:
-            state.bin(self.octpath, capacity=self.capacity, path_or=self.path_or_all, rank_table=self.rank_table)
+            state.bin(self.octpath, capacity=self.capacity, path_or=self.path_or_all, rank_table=self.rank_table,
+                      pair_order=self.pair_order)
         else:
-            state.bin(self.octpath, rank_table=self.rank_table)
+            state.bin(self.octpath, rank_table=self.rank_table, pair_order=self.pair_order)
         mark("count+sort")
         color, depth, normal, T, _ = state.render(3, True, True, self.centers, self.lengths, self.geos, self.rgbs,
                                                   self.s_val, rgb_per_view=True)
