@@ -498,7 +498,30 @@ def run_per_view(args, scene, cams, dev, host_inputs, steps=None, warmup=None):
     return out
 
 
+class StdoutToStderr:
+    """Sends everything written to file descriptor 1 (C printf included) to descriptor 2 while
+    active, so that the bench's JSON line stays the only thing on stdout."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *a):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
 def run_reference_cuda(scene, cams, dev, steps=3, warmup=1):
+    """See _run_reference_cuda; the reference extension prints to stdout (valid_gradient_table),
+    which is kept off the bench's stdout."""
+    with StdoutToStderr():
+        return _run_reference_cuda(scene, cams, dev, steps, warmup)
+
+
+def _run_reference_cuda(scene, cams, dev, steps=3, warmup=1):
     """The reference's own CUDA extension (oracle/_ref, built from its unmodified sources by
     oracle/build_ref.py) on the same scene and views, one view at a time on the default stream
     as the reference's train.py drives it (train.py:316-709): per view rasterize_preprocess,

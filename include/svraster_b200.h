@@ -198,6 +198,14 @@ SVR_API int svr_bin_tiles(const svr_view_t* views_host, int n_views, int N, int6
                           int key_bits, void* geom_buffer, void* binning_buffer, size_t binning_bytes,
                           void* image_buffer, void* stream);
 
+/* Which render kernels later launches use (no counterpart in the reference; a process-wide
+ * choice read when a launch is issued).  Forward: 1 = record-parallel filter with dense pair
+ * evaluation (the default), 0 = per-warp filter with one pixel per lane.  Adjoint: the same
+ * choice.  Every choice gives the same forward outputs bit for bit and the same gradients up
+ * to the order of their float atomics. */
+SVR_API int svr_render_set_impl(int fwd_impl, int bwd_impl);
+SVR_API int svr_render_get_impl(int* fwd_impl, int* bwd_impl);
+
 /* Work measurement, no counterpart in the reference: the forward render of
  * svr_render_fwd (three sub-samples, depth and normal on) on records already packed by an
  * earlier svr_render_fwd on the same buffers, with the same outputs, that also writes to

@@ -877,6 +877,71 @@ __global__ void __launch_bounds__(256) pack_records_kernel(
 
 // ------------------------------------------------------------------ render kernels
 #include "render_kernels.cuh"
+#include "render_pairs.cuh"
+
+// Which forward render kernel the launches use: 1 = record-parallel filter with dense pair
+// evaluation (render_fwd_pairs_kernel, the default), 0 = the warp-filter kernel
+// (render_fwd_kernel).  Both give the same outputs bit for bit.
+static std::atomic<int> g_fwd_impl{1}, g_bwd_impl{1};
+extern "C" int svr_render_set_impl(int fwd_impl, int bwd_impl)
+{
+    if (fwd_impl < 0 || fwd_impl > 1 || bwd_impl < 0 || bwd_impl > 1) return svr_fail(SVR_ERR_ARG, "render impl");
+    g_fwd_impl.store(fwd_impl);
+    g_bwd_impl.store(bwd_impl);
+    return SVR_OK;
+}
+extern "C" int svr_render_get_impl(int* fwd_impl, int* bwd_impl)
+{
+    if (fwd_impl) *fwd_impl = g_fwd_impl.load();
+    if (bwd_impl) *bwd_impl = g_bwd_impl.load();
+    return SVR_OK;
+}
+
+#ifndef SVR_PBWD_RING
+#define SVR_PBWD_RING 3
+#endif
+#ifndef SVR_PBWD_MINB
+#define SVR_PBWD_MINB 3
+#endif
+template <bool DEPTH, bool NORMAL, bool RCONC>
+static int launch_bwd_pairs(int T, int N, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
+                            const uint32_t* tl, const uint32_t* nc, const Rec* recs, const float* s_val,
+                            const float* out_T, const float* dc, const float* dd, const float* dn, const float* dT,
+                            float lam, const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status)
+{
+    auto k = render_bwd_pairs_kernel<DEPTH, NORMAL, RCONC, SVR_PBWD_RING, SVR_PBWD_MINB>;
+    const int smem = (int)sizeof(PairBwdSmem<SVR_PBWD_RING>);
+    static std::atomic<unsigned long long> done{0};
+    int rc = ensure_smem(k, smem, done);
+    if (rc) return rc;
+    k<<<T, BLOCK, smem, st>>>(V, N, order, ranges, tl, nc, recs, s_val, out_T, dc, dd, dn, dT, lam, gt, dvox, drgbs, ds,
+                               status);
+    LAUNCH_CHECK();
+    return SVR_OK;
+}
+
+#ifndef SVR_PFWD_RING
+#define SVR_PFWD_RING 3
+#endif
+#ifndef SVR_PFWD_MINB
+#define SVR_PFWD_MINB 4
+#endif
+template <int NS, bool DEPTH, bool NORMAL, bool MAXW, bool COUNT>
+static int launch_fwd_pairs(int T, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
+                            const Rec* recs, const float* s_val, uint32_t* tile_last, uint32_t* n_contrib,
+                            float* color, float* depth, float* normal, float* outT, float* max_w, int64_t mw_stride,
+                            unsigned* status, unsigned long long* pair_count)
+{
+    auto k = render_fwd_pairs_kernel<NS, DEPTH, NORMAL, MAXW, SVR_PFWD_RING, SVR_PFWD_MINB, COUNT>;
+    const int smem = (int)sizeof(PairFwdSmem<SVR_PFWD_RING>);
+    static std::atomic<unsigned long long> done{0};
+    int rc = ensure_smem(k, smem, done);
+    if (rc) return rc;
+    k<<<T, BLOCK, smem, st>>>(V, order, ranges, recs, s_val, tile_last, n_contrib, color, depth, normal, outT, max_w,
+                              mw_stride, status, pair_count);
+    LAUNCH_CHECK();
+    return SVR_OK;
+}
 
 // Launch configurations (ring slots, CTAs per SM) the tuner chooses between for the
 // common flag sets (three sub-samples, depth and normal on; with or without the
@@ -953,6 +1018,10 @@ static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint32_t* or
                       const float* s_val, uint32_t* tile_last, uint32_t* n_contrib, float* color, float* depth,
                       float* normal, float* outT, float* max_w, int64_t mw_stride, unsigned* status)
 {
+    if (g_fwd_impl.load() == 1)
+        return launch_fwd_pairs<NS, DEPTH, NORMAL, MAXW, false>(T, st, V, order, ranges, recs, s_val, tile_last,
+                                                                n_contrib, color, depth, normal, outT, max_w,
+                                                                mw_stride, status, nullptr);
 #define FWD_CFG_ARGS T, st, V, order, ranges, recs, s_val, tile_last, n_contrib, color, depth, normal, outT, max_w, mw_stride, status
     if constexpr (NS == 3 && DEPTH && NORMAL && !MAXW) {
         int cfg = g_fwd_cfg.load();
@@ -1082,12 +1151,19 @@ extern "C" int svr_render_fwd_count_pairs(const svr_view_t* views_host, int n_vi
     ImgLayout IL = img_layout(P, T);
     char* b = (char*)binning_buffer;
     char* im = (char*)image_buffer;
+    CUDA_TRY(cudaMemsetAsync(pair_count, 0, 3 * sizeof(unsigned long long), st));
+    if (g_fwd_impl.load() == 1)
+        return launch_fwd_pairs<3, true, true, false, true>(T, st, V, (const uint32_t*)(im + IL.order),
+                                                            (const uint2*)(im + IL.ranges), (const Rec*)(b + BL.recs),
+                                                            s_val, (uint32_t*)(im + IL.tile_last),
+                                                            (uint32_t*)(im + IL.n_contrib), out_color, out_depth,
+                                                            out_normal, out_T, nullptr, 0,
+                                                            (unsigned*)(im + IL.status), pair_count);
     auto k = render_fwd_kernel<3, true, true, false, SVR_NSLOT, SVR_FWD_MINB, true>;
     const int smem = (int)sizeof(FwdSmem<SVR_NSLOT>);
     static std::atomic<unsigned long long> done{0};
     rc = ensure_smem(k, smem, done);
     if (rc) return rc;
-    CUDA_TRY(cudaMemsetAsync(pair_count, 0, 3 * sizeof(unsigned long long), st));
     k<<<T, BLOCK, smem, st>>>(V, (const uint32_t*)(im + IL.order), (const uint2*)(im + IL.ranges),
                               (const Rec*)(b + BL.recs), s_val, (uint32_t*)(im + IL.tile_last),
                               (uint32_t*)(im + IL.n_contrib), out_color, out_depth, out_normal, out_T, nullptr, 0,
@@ -1121,6 +1197,7 @@ static int launch_bwd(int T, int N, cudaStream_t st, const Views& V, const uint3
                       const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status)
 {
 #define BWD_CFG_ARGS T, N, st, V, order, ranges, tl, nc, recs, s_val, out_T, dc, dd, dn, dT, lam, gt, dvox, drgbs, ds, status
+    if (g_bwd_impl.load() == 1) return launch_bwd_pairs<DEPTH, NORMAL, RCONC>(BWD_CFG_ARGS);
     if constexpr (DEPTH && NORMAL) {
         int cfg = g_bwd_cfg.load();
         if (cfg == 0 && T < SMALL_LAUNCH_TILES) cfg = 2;          // 4 x 2
