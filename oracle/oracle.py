@@ -92,6 +92,40 @@ def set_pixel_mask(mask, bits=32):
 
 
 _mask_keep = None
+_trace_keep = None
+
+
+def set_trace(pixel_trace, voxel_trace=None, bits=32):
+    """Record decision flags in later render_fwd / render_bwd calls of that build:
+    ``pixel_trace`` uint8[H*W] (flags ORed in: 1 alpha near MIN_ALPHA, 2 transmittance near the
+    early stop, 4 a median-depth decision near T = 0.5, 8 an adjoint alpha or depth-derivative
+    switch near its threshold), ``voxel_trace`` uint8[N] (set for voxels that a flagged pixel
+    sends gradient to).  None stops recording.  The arrays are written in place."""
+    global _trace_keep
+    if pixel_trace is None:
+        _trace_keep = None
+        lib(bits).svo_set_trace(None, None)
+        return
+    assert pixel_trace.dtype == np.uint8 and pixel_trace.flags.c_contiguous
+    assert voxel_trace is None or (voxel_trace.dtype == np.uint8 and voxel_trace.flags.c_contiguous)
+    _trace_keep = (pixel_trace, voxel_trace)
+    lib(bits).svo_set_trace(_p(pixel_trace), _p(voxel_trace))
+
+
+_abs_keep = None
+
+
+def set_abs_sum(abs_sum, bits=32):
+    """Accumulate |term| of every adjoint pair term into ``abs_sum`` ([N,12], the build's float
+    type) in later render_bwd calls; None stops."""
+    global _abs_keep
+    if abs_sum is None:
+        _abs_keep = None
+        lib(bits).svo_set_abs_sum(None)
+        return
+    assert abs_sum.dtype == (np.float64 if bits == 64 else np.float32) and abs_sum.flags.c_contiguous
+    _abs_keep = abs_sum
+    lib(bits).svo_set_abs_sum(_p(abs_sum))
 
 
 def render_fwd(cam, bg, n_samp, need_depth, need_normal, ranges, vals, bboxes, centers, lengths, geos, rgbs,

@@ -48,6 +48,33 @@ void svo_set_threads(int n) { g_threads = n > 0 ? n : 1; }
  * them; they contribute no gradient).  NULL renders every pixel. */
 static const uint8_t* g_pixel_mask = NULL;
 void svo_set_pixel_mask(const uint8_t* mask) { g_pixel_mask = mask; }
+
+/* Optional decision trace for the parity tests (uint8[H*W] per pixel, uint8[N] per voxel).
+ * The forward ORs into the pixel trace: TR_ALPHA an evaluated pair whose alpha lies within
+ * TR_ALPHA_BAND of MIN_ALPHA (kept in one precision, dropped in another); TR_STOP an accepted
+ * pair that left T within TR_STOP_BAND of the early-stop threshold; TR_MEDIAN a median-depth
+ * decision with T within TR_MED_BAND of 0.5.  The adjoint ORs TR_ADJ for a pair whose
+ * recomputed alpha lies within TR_ALPHA_BAND of MIN_ALPHA or whose depth sub-segment raw
+ * alpha lies within TR_RAW_BAND of 0 (the derivative switch), and marks in the voxel trace
+ * every voxel that a traced pixel contributes gradient to.  The bands are a few float32
+ * ulps of the quantity compared, scaled up by the cancellation in alpha. */
+#define TR_ALPHA 1
+#define TR_STOP 2
+#define TR_MEDIAN 4
+#define TR_ADJ 8
+#define TR_ALPHA_BAND 5e-7
+#define TR_STOP_BAND 1e-7
+#define TR_MED_BAND 5e-6
+#define TR_RAW_BAND 1e-6
+static uint8_t* g_trace = NULL;
+static uint8_t* g_vox_trace = NULL;
+void svo_set_trace(uint8_t* pixel_trace, uint8_t* voxel_trace) { g_trace = pixel_trace; g_vox_trace = voxel_trace; }
+/* Optional: the adjoint also adds |term| of every pair's 12 gradient terms into abs_sum[N,12]
+ * (the scale against which a sum of those terms computed in another order or precision is
+ * compared).  Same type as the build's render math; NULL switches it off. */
+static void* g_abs_sum = NULL;
+void svo_set_abs_sum(void* abs_sum) { g_abs_sum = abs_sum; }
+static inline double dabs(double x) { return x < 0 ? -x : x; }
 int svo_get_threads(void) { return g_threads; }
 
 typedef struct { float x, y, z; } f3;
@@ -327,7 +354,9 @@ void svo_render_fwd(int W, int H, float tanfovx, float tanfovy, float cx, float 
                     phi_f = phi_c; sdf_f = sdf_c;
                 }
                 real alpha = rmax((phi_e - phi_f) / (phi_e + (real)1e-6f), 0.f);
+                if (g_trace && dabs((double)alpha - (double)MIN_ALPHA) <= TR_ALPHA_BAND) g_trace[py * W + px] |= TR_ALPHA;
                 if (alpha < MIN_ALPHA) continue;
+                if (g_trace && need_depth && dabs((double)T - 0.5) <= TR_MED_BAND) g_trace[py * W + px] |= TR_MEDIAN;
                 real pw = T * alpha;
                 Cc = radd(Cc, rmuls(rk(rgbs[3 * vid], rgbs[3 * vid + 1], rgbs[3 * vid + 2]), pw));
                 if (need_depth) {
@@ -354,6 +383,7 @@ void svo_render_fwd(int W, int H, float tanfovx, float tanfovy, float cx, float 
                     Nn = radd(Nn, rmuls(rk(nx, ny, nz), pw * rl));
                 }
                 T *= (1.f - alpha);
+                if (g_trace && dabs((double)T - (double)EARLY_STOP_T) <= TR_STOP_BAND) g_trace[py * W + px] |= TR_STOP;
                 last = k - r0 + 1;
                 if (max_w && pw > max_w[vid]) max_w[vid] = pw;
                 if (T < EARLY_STOP_T) break;
@@ -381,6 +411,7 @@ void svo_render_fwd(int W, int H, float tanfovx, float tanfovy, float cx, float 
                     real phi_c = (real)1 / ((real)1 + EXPR(-s_val * rinterp8(g, w)));
                     real ak = (phi_p - phi_c) / (phi_p + (real)1e-6f);
                     med_T *= (1.f - ak);
+                    if (g_trace && dabs((double)med_T - 0.5) <= TR_MED_BAND) g_trace[py * W + px] |= TR_MEDIAN;
                     phi_p = phi_c;
                 }
             }
@@ -487,6 +518,7 @@ void svo_render_bwd(int W, int H, float tanfovx, float tanfovy, float cx, float 
                         real dk = pk + (real)1e-6f;
                         real raw = (pk - pk1) / dk;
                         real allow = raw > 0.f ? 1.f : 0.f;
+                        if (g_trace && dabs((double)raw) <= TR_RAW_BAND && !(alpha < MIN_ALPHA)) g_trace[pid] |= TR_ADJ;
                         la[s] = rmax(raw, 0.f);
                         real d0 = allow * (pk1 / (dk * dk));
                         real d1 = allow * (-(real)1 / dk);
@@ -495,7 +527,9 @@ void svo_render_bwd(int W, int H, float tanfovx, float tanfovy, float cx, float 
                         for (int i = 0; i < 8; ++i) eg[s][i] += d0 * p0 * wk[i] + d1 * p1 * wk1[i];
                     }
                 }
+                if (g_trace && dabs((double)alpha - (double)MIN_ALPHA) <= TR_ALPHA_BAND) g_trace[pid] |= TR_ADJ;
                 if (alpha < MIN_ALPHA) continue;   /* lambda_ascending = 0 */
+                if (g_vox_trace && g_trace && g_trace[pid]) g_vox_trace[vid] = 1;
                 T = T / (1.f - alpha);
                 real pw = alpha * T;
                 r3 c = rk(rgbs[3 * vid], rgbs[3 * vid + 1], rgbs[3 * vid + 2]);
@@ -557,12 +591,18 @@ void svo_render_bwd(int W, int H, float tanfovx, float tanfovy, float cx, float 
                 for (int i = 0; i < 8; ++i) pack[i] = dg[i];
                 pack[8] = drgb[0]; pack[9] = drgb[1]; pack[10] = drgb[2];
                 pack[11] = FABSR(dalpha * alpha);
+                real* oa = g_abs_sum ? (real*)g_abs_sum + 12 * (size_t)vid : NULL;
                 if (nth == 1) {
                     for (int i = 0; i < 12; ++i) o[i] += pack[i];
+                    if (oa) for (int i = 0; i < 12; ++i) oa[i] += FABSR(pack[i]);
                 } else {
                     for (int i = 0; i < 12; ++i) {
                         #pragma omp atomic update
                         o[i] += pack[i];
+                    }
+                    if (oa) for (int i = 0; i < 12; ++i) {
+                        #pragma omp atomic update
+                        oa[i] += FABSR(pack[i]);
                     }
                 }
             }

@@ -631,7 +631,8 @@ extern "C" int svr_bin_tiles(const svr_view_t* views_host, int n_views, int N, i
     // per-view histograms in shared memory when the largest view's tiles fit in 96 KB
     int max_nt = 0;
     for (int v = 0; v < n_views; ++v) max_nt = std::max(max_nt, V.v[v].tiles_x * V.v[v].tiles_y);
-    const bool smem_hist = max_nt <= 24576;
+    constexpr int MAX_HIST_TILES = 24576;     // 96 KB of shared memory
+    const bool smem_hist = max_nt <= MAX_HIST_TILES;
     const int hist_bytes = smem_hist ? 4 * max_nt : 0;
     // about 8 CTAs per SM in all, split over the views (as preprocess)
     const int per_view = std::max(1, std::min((N + 255) / 256, (8 * 148 + n_views - 1) / n_views));
@@ -639,8 +640,9 @@ extern "C" int svr_bin_tiles(const svr_view_t* views_host, int n_views, int N, i
     if (N > 0) {
         if (smem_hist) {
             static std::atomic<unsigned long long> d1{0}, d2{0};
-            if ((rc = ensure_smem(tile_count_kernel<true>, hist_bytes, d1))) return rc;
-            if ((rc = ensure_smem(tile_scatter_kernel<true>, hist_bytes, d2))) return rc;
+            // the limit is raised once per device, to the largest histogram this path uses
+            if ((rc = ensure_smem(tile_count_kernel<true>, 4 * MAX_HIST_TILES, d1))) return rc;
+            if ((rc = ensure_smem(tile_scatter_kernel<true>, 4 * MAX_HIST_TILES, d2))) return rc;
             tile_count_kernel<true><<<grid, 256, hist_bytes, st>>>(V, N, ndup, bbox, bits, tile_cnt);
         } else {
             tile_count_kernel<false><<<grid, 256, 0, st>>>(V, N, ndup, bbox, bits, tile_cnt);

@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(256) tile_offsets_kernel(
         const unsigned long long s1 = s0 + c[k];
         const uint32_t a = (uint32_t)min(s0, (unsigned long long)cap);
         const uint32_t e = (uint32_t)min(s1, (unsigned long long)cap);
-        ranges[t] = make_uint2(a, e);
+        ranges[t] = e > a ? make_uint2(a, e) : make_uint2(0u, 0u);   // empty tiles: [0, 0), as the reference
         cursor[t] = (uint32_t)min(s0, (unsigned long long)0xFFFFFFFFull);
     }
     // stable rank of the tiles by launch bucket (warp multisplit, then across warps)

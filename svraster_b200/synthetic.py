@@ -135,7 +135,7 @@ class Scene:
 
 
 def build_scene(sdf, lv_min, lv_max, seed=0, scene_extent=2.0, band=2.0, keep=None,
-                kept_parent_frac=0.0, sh_degree=3):
+                kept_parent_frac=0.0, sh_degree=3, lv_max_fn=None, region=None):
     """Recursively subdivide cells with ``|sdf(centre)| < band * size`` from ``lv_min`` to ``lv_max``.
 
     Cells that are not subdivided stay as leaves when ``|sdf(centre)| < keep * size``
@@ -145,6 +145,10 @@ def build_scene(sdf, lv_min, lv_max, seed=0, scene_extent=2.0, band=2.0, keep=No
     ``kept_parent_frac`` re-inserts that fraction of the parents of finest-level leaves as
     non-leaf voxels, like the reference keeps deep parents on subdivision
     (src/sparse_voxel_gears/adaptive.py:59-63); those are culled by the preprocess.
+
+    ``lv_max_fn(centres) -> int levels`` gives a finest level per region (clipped to
+    [lv_min, lv_max]): a cell stops subdividing at its region's level.  ``region`` (lo, hi)
+    keeps only the cells whose cube meets that box (a block of the same octree).
     """
     rng = np.random.default_rng(seed)
     smin = -0.5 * scene_extent
@@ -154,6 +158,10 @@ def build_scene(sdf, lv_min, lv_max, seed=0, scene_extent=2.0, band=2.0, keep=No
     leaf_ijk, leaf_lv, parents = [], [], []
     while True:
         size = scene_extent * 2.0 ** -cur_lv
+        if region is not None:
+            c = smin + (cur_ijk + 0.5) * size
+            meet = np.all((c + 0.5 * size >= np.asarray(region[0])) & (c - 0.5 * size <= np.asarray(region[1])), axis=1)
+            cur_ijk = cur_ijk[meet]
         c = smin + (cur_ijk + 0.5) * size
         d = np.abs(sdf(c))
         if cur_lv == lv_max:
@@ -161,6 +169,8 @@ def build_scene(sdf, lv_min, lv_max, seed=0, scene_extent=2.0, band=2.0, keep=No
             leaf_ijk.append(kept); leaf_lv.append(np.full(len(kept), cur_lv))
             break
         near = d < band * size
+        if lv_max_fn is not None:
+            near &= np.clip(lv_max_fn(c), lv_min, lv_max) > cur_lv
         stay = ~near if keep is None else (~near) & (d < keep * size)
         leaf_ijk.append(cur_ijk[stay]); leaf_lv.append(np.full(int(stay.sum()), cur_lv))
         sub = cur_ijk[near]
@@ -302,6 +312,113 @@ def scene_precision(seed=0):
 def scene_batched(seed=0):
     """Sphere with 64 Gaussian bumps (amplitude 0.05) at levels 7-11, about 4M voxels."""
     return build_scene(make_bumpy_sphere(seed=seed), 7, 11, seed=seed, band=0.42, keep=1.1, kept_parent_frac=0.02)
+
+
+ROOM_HALF = (2.0, 1.5, 1.25)          # 4 x 3 x 2.5 room
+
+
+def sdf_box(p, c, half):
+    q = np.abs(p - np.asarray(c, dtype=np.float64)) - np.asarray(half, dtype=np.float64)
+    outside = np.linalg.norm(np.maximum(q, 0.0), axis=-1)
+    return outside + np.minimum(q.max(axis=-1), 0.0)
+
+
+def make_room(n_objects=20, n_fine=4, seed=0):
+    """An indoor-like SDF: the inside of an axis-aligned 4 x 3 x 2.5 box room (walls solid)
+    with ``n_objects`` seeded boxes and spheres standing inside it.  Returns (sdf, objects_sdf,
+    fine_sdf): the scene, the union of the objects, and the union of the first ``n_fine``
+    objects (the ones refined to the finest level)."""
+    rng = np.random.default_rng(seed)
+    hx, hy, hz = ROOM_HALF
+    objs = []
+    for k in range(n_objects):
+        r = rng.uniform(0.12, 0.35)
+        c = rng.uniform([-hx + 0.5, -hy + 0.5, -hz + r], [hx - 0.5, hy - 0.5, hz - 0.5])
+        if k % 2 == 0:
+            objs.append(("sphere", c, r))
+        else:
+            objs.append(("box", c, rng.uniform(0.1, 0.35, size=3)))
+
+    def one(p, o):
+        kind, c, sz = o
+        return sdf_sphere(p, sz, c) if kind == "sphere" else sdf_box(p, c, sz)
+
+    cache = {}
+
+    def union(p, sel):
+        # the octree builder asks for the scene and the objects at the same centres in a row
+        key = (id(p), p.shape, len(sel))
+        if cache.get("key") == key:
+            return cache["val"]
+        q = np.asarray(p, dtype=np.float64)
+        d = np.full(q.shape[:-1], np.inf)
+        for o in sel:
+            d = np.minimum(d, one(q, o))
+        cache["key"], cache["val"] = key, d
+        return d
+
+    def room(p):
+        q = np.asarray(p, dtype=np.float64)
+        walls = np.minimum(np.minimum(hx - np.abs(q[..., 0]), hy - np.abs(q[..., 1])), hz - np.abs(q[..., 2]))
+        return np.minimum(walls, union(p, objs))
+
+    return room, (lambda p: union(p, objs)), (lambda p: union(p, objs[:n_fine]))
+
+
+def scene_full(seed=0):
+    """Full reconstruction workload: the 4 x 3 x 2.5 room with 20 boxes and spheres in the
+    scene cube [-2, 2]^3 (inside extent 4), levels 8-12: walls refined to level 10, objects to
+    level 11, four of them to level 12; empty space pruned; about 12M voxels."""
+    room, objs, fine = make_room(seed=seed)
+
+    def lv_max(c):
+        lv = np.full(len(c), 10)
+        lv[np.abs(objs(c)) < 0.03] = 11
+        lv[np.abs(fine(c)) < 0.02] = 12
+        return lv
+    return build_scene(room, 8, 12, seed=seed, scene_extent=4.0, band=0.46, keep=1.1, kept_parent_frac=0.02,
+                       lv_max_fn=lv_max)
+
+
+def full_block_region(seed=0, margin=0.08):
+    """A box around the first of the objects refined to level 12 in scene_full."""
+    rng = np.random.default_rng(seed)
+    hx, hy, hz = ROOM_HALF
+    r = rng.uniform(0.12, 0.35)
+    c = rng.uniform([-hx + 0.5, -hy + 0.5, -hz + r], [hx - 0.5, hy - 0.5, hz - 0.5])
+    lo = c - r - margin
+    return (lo, lo + np.array([r + margin, 2 * (r + margin), 2 * (r + margin)]))
+
+
+def scene_full_block(seed=0):
+    """A block of the full reconstruction workload's octree (scene_full's procedure restricted
+    to a box that cuts through one level-12 object and its surroundings), small enough for
+    reference checks on the CPU."""
+    room, objs, fine = make_room(seed=seed)
+
+    def lv_max(c):
+        lv = np.full(len(c), 10)
+        lv[np.abs(objs(c)) < 0.03] = 11
+        lv[np.abs(fine(c)) < 0.02] = 12
+        return lv
+    return build_scene(room, 8, 12, seed=seed, scene_extent=4.0, band=0.46, keep=1.1, kept_parent_frac=0.02,
+                       lv_max_fn=lv_max, region=full_block_region(seed))
+
+
+def room_cameras(n, width=1024, height=768, fovx_deg=70.0, seed=0):
+    """n views from inside the room: positions on an ellipse at mid height (clear of the
+    objects' extent in z only where they stand low), each looking at a seeded point on the far
+    walls or floor."""
+    rng = np.random.default_rng(seed)
+    hx, hy, hz = ROOM_HALF
+    cams = []
+    for i in range(n):
+        az = 2 * math.pi * i / n
+        pos = np.array([0.55 * hx * math.cos(az), 0.55 * hy * math.sin(az), rng.uniform(0.3, 0.8) * hz])
+        tgt = np.array([rng.uniform(-hx, hx), rng.uniform(-hy, hy), rng.uniform(-hz, 0.2 * hz)])
+        tgt[0] = -np.sign(pos[0] + 1e-9) * abs(tgt[0])
+        cams.append(look_at_camera(pos, width, height, fovx_deg, target=tuple(tgt)))
+    return cams
 
 
 MIXED_RESOLUTIONS = ((480, 360), (960, 540), (1280, 720), (1920, 1080))

@@ -16,7 +16,23 @@ TSDF_CASES = {
 MC_CASES = {
     "mc_a": dict(kind="tiny", seed=0, iso=0.0, subset=1, specials=False),
     "mc_b": dict(kind="small", seed=1, iso=0.01, subset=2, specials=True),
+    # the full reconstruction workload's procedure on a block: the level-12 voxels only
+    "mc_full_block": dict(kind="full_block", seed=0, iso=0.0, subset=1, specials=False, level=12, compact=True),
 }
+
+
+def mesh_digest(verts, faces, n_sample=2048, seed=0):
+    """Compact golden of a large mesh: SHA-256 of the exact bytes of the vertices (float32
+    [V,3]) and faces (int64 [F,3]), the counts, and a seeded sample of rows for diagnostics."""
+    verts = np.ascontiguousarray(verts, dtype=np.float32)
+    faces = np.ascontiguousarray(faces, dtype=np.int64)
+    rng = np.random.default_rng(seed)
+    vi = np.sort(rng.choice(len(verts), min(n_sample, len(verts)), replace=False))
+    fi = np.sort(rng.choice(len(faces), min(n_sample, len(faces)), replace=False))
+    return dict(verts_sha256=hashlib.sha256(verts.tobytes()).hexdigest(),
+                faces_sha256=hashlib.sha256(faces.tobytes()).hexdigest(),
+                n_verts=len(verts), n_faces=len(faces), vert_rows=vi, verts_sample=verts[vi], face_rows=fi,
+                faces_sample=faces[fi])
 
 
 def _digest(arrays):
@@ -54,13 +70,19 @@ def tsdf_inputs(case):
 
 
 def mc_inputs(case):
-    sc = S.scene_tiny(seed=case["seed"]) if case["kind"] == "tiny" else S.scene_small(seed=case["seed"])
+    if case["kind"] == "full_block":
+        sc = S.scene_full_block(seed=case["seed"])
+    else:
+        sc = S.scene_tiny(seed=case["seed"]) if case["kind"] == "tiny" else S.scene_small(seed=case["seed"])
     val = sc.geo_grid_pts.reshape(-1).astype(np.float32).copy()
     if case["specials"]:
         rng = np.random.default_rng(case["seed"] + 9)
         k = len(val)
         val[rng.choice(k, k // 200, replace=False)] = np.float32(case["iso"])        # exact iso hits
         val[rng.choice(k, k // 500, replace=False)] = np.nan                          # NaN corners
-    vox_key = sc.vox_key[:: case["subset"]].astype(np.int64).copy()
+    vox_key = sc.vox_key
+    if "level" in case:
+        vox_key = vox_key[sc.octlevel.reshape(-1) == case["level"]]
+    vox_key = vox_key[:: case["subset"]].astype(np.int64).copy()
     xyz = sc.grid_pts_xyz.astype(np.float32)
     return dict(val=val, xyz=xyz, vox_key=vox_key, digest=_digest([val, xyz, vox_key]))

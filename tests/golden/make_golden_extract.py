@@ -7,7 +7,7 @@ into this repository) and writes tests/golden/extract_*.npz.  Inputs are seeded 
 scenes; the depth / transmittance maps fused here come from the C oracle's renderer.
 
 Usage (this machine, with the reference sources):
-    python tests/golden/make_golden_extract.py [/path/to/reference]
+    python tests/golden/make_golden_extract.py [/path/to/reference] [--only CASE ...]
 """
 from __future__ import annotations
 
@@ -21,7 +21,7 @@ import torch
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
 
-from tests.golden.extract_cases import TSDF_CASES, MC_CASES, tsdf_inputs, mc_inputs  # noqa: E402
+from tests.golden.extract_cases import TSDF_CASES, MC_CASES, tsdf_inputs, mc_inputs, mesh_digest  # noqa: E402
 
 
 def load_on_cpu(path, name, extra=None):
@@ -35,7 +35,11 @@ def load_on_cpu(path, name, extra=None):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SVR_REFERENCE_DIR")
+    args = sys.argv[1:]
+    only = set(args[args.index("--only") + 1:]) if "--only" in args else None
+    if "--only" in args:
+        args = args[:args.index("--only")]
+    ref = args[0] if args else os.environ.get("SVR_REFERENCE_DIR")
     if not ref:
         sys.exit("usage: give the reference checkout as the first argument or in SVR_REFERENCE_DIR")
     import svraster_b200
@@ -46,6 +50,8 @@ def main():
     out_dir = os.path.dirname(os.path.abspath(__file__))
 
     for name, case in TSDF_CASES.items():
+        if only is not None and name not in only:
+            continue
         inp = tsdf_inputs(case)
         cams = []
         for c in inp["cams"]:
@@ -67,11 +73,17 @@ def main():
         print(name, "fused points", int((fuser.weight > 0).sum()))
 
     for name, case in MC_CASES.items():
+        if only is not None and name not in only:
+            continue
         inp = mc_inputs(case)
         verts, faces = mc_mod.torch_marching_cubes_grid(torch.from_numpy(inp["val"]), torch.from_numpy(inp["xyz"]),
                                                         torch.from_numpy(inp["vox_key"]), case["iso"])
-        np.savez_compressed(os.path.join(out_dir, f"extract_{name}.npz"), digest=inp["digest"],
-                            verts=verts.numpy(), faces=faces.numpy())
+        if case.get("compact"):
+            np.savez_compressed(os.path.join(out_dir, f"extract_{name}.npz"), digest=inp["digest"],
+                                **mesh_digest(verts.numpy(), faces.numpy()))
+        else:
+            np.savez_compressed(os.path.join(out_dir, f"extract_{name}.npz"), digest=inp["digest"],
+                                verts=verts.numpy(), faces=faces.numpy())
         print(name, "verts", len(verts), "faces", len(faces))
 
 

@@ -1,0 +1,229 @@
+"""Parity at the benchmark workloads' own sizes.
+
+Mid-size workload (1.45M voxels, 8 views of 800x800): for every view, the per-view
+duplicate counts, bboxes, octant bits, the sorted record order (13.6M records in all) and the
+tile ranges of the batched launch equal the oracle's bit for bit; for two full views the images
+and the adjoint are compared with the oracle pixel by pixel and voxel by voxel.
+
+Batched workload (4.2M voxels, 64 views of four resolutions): one view of each resolution
+out of the real 64-view launch: the batch's records restricted to the view equal the
+oracle's records of the view alone, and its images equal the oracle's.
+
+Threshold flips are separated from error with the oracle's decision trace: pixels where a
+pair's alpha sits within a few ulps of MIN_ALPHA, where T lands at the early-stop threshold or
+a median-depth decision meets T = 0.5 (and, for gradients, voxels such pixels send gradient
+to, or where an adjoint switch is near its threshold) are counted and reported; every other
+pixel and voxel must meet the tight bound.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+REPORT = {}
+
+
+def _report(key, value):
+    REPORT[key] = value
+    print("SCALE_PARITY", key, json.dumps(value))
+    out = os.environ.get("SVR_PARITY_OUT")
+    if out:
+        with open(out, "w") as f:
+            json.dump(REPORT, f, indent=1)
+
+
+@pytest.fixture(scope="module")
+def oracle():
+    from oracle import oracle as O
+    O.set_threads(os.cpu_count() or 1)
+    yield O
+    O.set_threads(1)
+    O.set_trace(None)
+    O.set_abs_sum(None)
+
+
+def _batched_state(sc, cams):
+    from svraster_b200.raster import PairOrder, RasterState
+    from tests.helpers import cam_dict, torch_scene
+    ts = torch_scene(sc)
+    st = RasterState([cam_dict(c) for c in cams], sc.n_vox, torch.device("cuda"))
+    st.preprocess(ts["octpath"], ts["centers"], ts["lengths"], ts["is_leaf"])
+    st.bin(ts["octpath"], pair_order=PairOrder(ts["octpath"]))
+    return st, ts
+
+
+def _view_slices(cams):
+    tiles, pix = [], []
+    t0 = p0 = 0
+    for c in cams:
+        nt = ((c.width + 15) // 16) * ((c.height + 15) // 16)
+        tiles.append((t0, t0 + nt))
+        pix.append((p0, p0 + c.width * c.height))
+        t0 += nt
+        p0 += c.width * c.height
+    return tiles, pix
+
+
+def _check_binning(O, sc, cam, v, st_fields, tiles, N):
+    nd_all, bb_all, bits_all, vals_all, ranges_all = st_fields
+    nd, bb, bits = O.preprocess(cam, sc.vox_center, sc.vox_size, sc.is_leaf)
+    keys, vals, ranges = O.binning(cam, sc.octpath, nd, bb, bits)
+    g_nd = nd_all[v * N:(v + 1) * N]
+    assert np.array_equal(g_nd, nd.astype(np.uint32)), f"view {v}: duplicate counts differ"
+    r = nd > 0
+    assert np.array_equal(bb_all[v * N:(v + 1) * N][r], bb[r]), f"view {v}: bboxes differ"
+    assert np.array_equal(bits_all[v * N:(v + 1) * N][r], bits[r]), f"view {v}: octant bits differ"
+    rg = ranges_all[tiles[0]:tiles[1]]
+    nonempty = ranges[:, 1] > ranges[:, 0]
+    base = int(rg[nonempty][0, 0]) if nonempty.any() else 0
+    assert np.array_equal(rg[nonempty] - base, ranges[nonempty]), f"view {v}: tile ranges differ"
+    assert np.array_equal(vals_all[base:base + len(vals)], vals), f"view {v}: sorted records differ"
+    return nd, bb, bits, vals, ranges
+
+
+def _image_errors(name, got, ref, flagged, rtol):
+    """Per-element relative error |got - ref| / |ref| on unflagged pixels, with entries of
+    |ref| below 1e-3 of the plane's largest compared absolutely at that scale."""
+    got = got.astype(np.float64).reshape(got.shape[0], -1)
+    ref = ref.astype(np.float64).reshape(ref.shape[0], -1)
+    ok = ~flagged.reshape(-1)
+    scale = np.maximum(np.abs(ref), 1e-3 * np.abs(ref).max(axis=1, keepdims=True) + 1e-30)
+    rel = (np.abs(got - ref) / scale)[:, ok]
+    stats = {"max": float(rel.max()) if rel.size else 0.0, "p999": float(np.quantile(rel, 0.999)) if rel.size else 0.0,
+             "bitwise_equal_frac": float((got[:, ok] == ref[:, ok]).mean()) if rel.size else 1.0,
+             "n_over": int((rel > rtol).sum())}
+    return stats
+
+
+FLIP_FWD = 1 | 2 | 4
+
+
+@pytest.mark.parametrize("views_checked", [(0, 5)])
+def test_mid_size_workload_all_views(oracle, views_checked):
+    import bench
+    from tests.helpers import upstream_grads
+    O = oracle
+    sc, cams = bench.make_workload(0, config="mid")
+    N = sc.n_vox
+    st, ts = _batched_state(sc, cams)
+    nd_all, bb_all, bits_all = [x.cpu().numpy() for x in st.geom_fields()]
+    vals, ranges, _, _ = st.binning_fields()
+    fields = (nd_all.view(np.uint32), bb_all.view(np.uint32).reshape(-1, 2), bits_all.view(np.uint32),
+              vals.cpu().numpy().view(np.uint32), ranges.cpu().numpy().view(np.uint32))
+    tiles, pix = _view_slices(cams)
+    geos = O.gather_geo(np.arange(N), sc.vox_key, sc.geo_grid_pts, N)
+    rgbs = [O.sh_eval(3, None, sc.vox_center, c.position, sc.sh0, sc.shs) for c in cams]
+    per_view = []
+    for v, cam in enumerate(cams):
+        per_view.append(_check_binning(O, sc, cam, v, fields, tiles[v], N))
+    _report("mid_binning", {"views": len(cams), "records": int(st.num_rendered), "bit_exact": True})
+    # images of the batched launch
+    s_val = torch.tensor([sc.s_val], dtype=torch.float32, device="cuda")
+    color, depth, normal, T, _ = st.render(3, True, True, ts["centers"], ts["lengths"], torch.as_tensor(geos).cuda(),
+                                           torch.as_tensor(np.concatenate(rgbs, 0)).cuda(), s_val, rgb_per_view=True)
+    planes = {k: x.cpu().numpy() for k, x in (("color", color), ("depth", depth), ("normal", normal), ("T", T))}
+    _, _, tl_all, nc_all = [x.cpu().numpy().view(np.uint32) for x in st.binning_fields()]
+    for v in views_checked:
+        cam = cams[v]
+        nd, bb, bits, vals_v, ranges_v = per_view[v]
+        H, W = cam.height, cam.width
+        tr = np.zeros(H * W, np.uint8)
+        O.set_trace(tr)
+        f = O.render_fwd(cam, np.zeros(3, np.float32), 3, True, True, ranges_v, vals_v, bb, sc.vox_center,
+                         sc.vox_size, geos, rgbs[v], sc.s_val)
+        O.set_trace(None)
+        flagged = (tr & FLIP_FWD) > 0
+        p0, p1 = pix[v]
+        stats = {}
+        for key, ch in (("color", 3), ("depth", 4), ("normal", 3), ("T", 1)):
+            got = planes[key][ch * p0: ch * p1].reshape(ch, H, W)
+            stats[key] = _image_errors(key, got, f[key], flagged, 1e-5)
+        nc = nc_all[p0:p1]
+        stats["n_contrib_differs"] = int((nc != f["n_contrib"]).sum())
+        stats["n_contrib_differs_unflagged"] = int(((nc != f["n_contrib"]) & ~flagged).sum())
+        stats["flagged_pixels"] = int(flagged.sum())
+        stats["pixels"] = H * W
+        _report(f"mid_view{v}_images", stats)
+        # the adjoint of this view alone (single-view launch: its gradients only)
+        g = upstream_grads(H, W, seed=40 + v)[0]
+        from tests.helpers import cuda_views
+        out = cuda_views(sc, [cam], geos, [rgbs[v]], grads_list=[g])
+        dv = out["dvox"].cpu().numpy().astype(np.float64)
+        vt = np.zeros(N, np.uint8)
+        O.set_trace(tr)
+        ref, ds_ref = O.render_bwd(cam, np.zeros(3, np.float32), True, True, ranges_v, f["tile_last"], vals_v, bb,
+                                   sc.vox_center, sc.vox_size, geos, rgbs[v], sc.s_val, f["T"], f["n_contrib"],
+                                   g["color"], g["depth"], g["normal"], g["T"])
+        absum = np.zeros((N, 12), np.float32)
+        O.set_trace(tr, vt)
+        O.set_abs_sum(absum)
+        O.render_bwd(cam, np.zeros(3, np.float32), True, True, ranges_v, f["tile_last"], vals_v, bb, sc.vox_center,
+                     sc.vox_size, geos, rgbs[v], sc.s_val, f["T"], f["n_contrib"], g["color"], g["depth"],
+                     g["normal"], g["T"])
+        O.set_trace(None)
+        O.set_abs_sum(None)
+        touched = np.abs(absum).sum(1) > 0
+        flagged_v = vt > 0
+        scale = absum.astype(np.float64) + 1e-30
+        rel = np.abs(dv - ref) / scale
+        ok = touched & ~flagged_v
+        bad = touched & flagged_v
+        gstats = {"voxels": int(touched.sum()), "flagged_voxels": int(bad.sum()),
+                  "rel_to_abs_sum_max_unflagged": float(rel[ok].max()) if ok.any() else 0.0,
+                  "rel_to_abs_sum_p9999_unflagged": float(np.quantile(rel[ok], 0.9999)) if ok.any() else 0.0,
+                  "rel_to_abs_sum_max_flagged": float(rel[bad].max()) if bad.any() else 0.0,
+                  "rel_elementwise_p99_unflagged": float(np.quantile(
+                      (np.abs(dv - ref) / (np.abs(ref) + 1e-30))[ok][np.abs(ref[ok]) > 1e-3 * np.abs(ref).max()], 0.99)),
+                  "ds": [float(out["ds"].item()), float(ds_ref)],
+                  "trace_pixels": {str(b): int(((tr & b) > 0).sum()) for b in (1, 2, 4, 8)}}
+        _report(f"mid_view{v}_adjoint", gstats)
+
+
+def test_batched_workload_one_view_per_resolution(oracle):
+    import bench
+    from svraster_b200 import synthetic as S
+    O = oracle
+    sc, cams = bench.make_workload(0, config="batched")
+    N = sc.n_vox
+    st, ts = _batched_state(sc, cams)
+    nd_all, bb_all, bits_all = [x.cpu().numpy() for x in st.geom_fields()]
+    vals, ranges, _, _ = st.binning_fields()
+    fields = (nd_all.view(np.uint32), bb_all.view(np.uint32).reshape(-1, 2), bits_all.view(np.uint32),
+              vals.cpu().numpy().view(np.uint32), ranges.cpu().numpy().view(np.uint32))
+    tiles, pix = _view_slices(cams)
+    pick = []
+    for res in S.MIXED_RESOLUTIONS:
+        pick.append(next(i for i, c in enumerate(cams) if (c.width, c.height) == res))
+    geos = O.gather_geo(np.arange(N), sc.vox_key, sc.geo_grid_pts, N)
+    rgbs = np.zeros((len(cams) * N, 3), np.float32)
+    for v in pick:
+        rgbs[v * N:(v + 1) * N] = O.sh_eval(3, None, sc.vox_center, cams[v].position, sc.sh0, sc.shs)
+    s_val = torch.tensor([sc.s_val], dtype=torch.float32, device="cuda")
+    color, depth, normal, T, _ = st.render(3, True, True, ts["centers"], ts["lengths"], torch.as_tensor(geos).cuda(),
+                                           torch.as_tensor(rgbs).cuda(), s_val, rgb_per_view=True)
+    planes = {k: x.cpu().numpy() for k, x in (("color", color), ("depth", depth), ("normal", normal), ("T", T))}
+    del color, depth, normal, T
+    summary = {"records": int(st.num_rendered), "views": len(cams), "checked": pick}
+    for v in pick:
+        cam = cams[v]
+        nd, bb, bits, vals_v, ranges_v = _check_binning(O, sc, cam, v, fields, tiles[v], N)
+        H, W = cam.height, cam.width
+        tr = np.zeros(H * W, np.uint8)
+        O.set_trace(tr)
+        f = O.render_fwd(cam, np.zeros(3, np.float32), 3, True, True, ranges_v, vals_v, bb, sc.vox_center,
+                         sc.vox_size, geos, rgbs[v * N:(v + 1) * N], sc.s_val)
+        O.set_trace(None)
+        flagged = (tr & FLIP_FWD) > 0
+        p0, p1 = pix[v]
+        stats = {"records": int(len(vals_v)), "flagged_pixels": int(flagged.sum()), "pixels": H * W}
+        for key, ch in (("color", 3), ("depth", 4), ("normal", 3), ("T", 1)):
+            got = planes[key][ch * p0: ch * p1].reshape(ch, H, W)
+            stats[key] = _image_errors(key, got, f[key], flagged, 1e-5)
+        summary[f"{W}x{H}"] = stats
+    _report("batched_views", summary)
