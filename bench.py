@@ -47,6 +47,10 @@ CONFIGS = {
     # plain method, mid-size scene
     "mid": dict(workload="mid-size: 3 spheres + torus, levels 6-10, SH deg 3, 8 views 800x800", views=8,
                 image="800x800"),
+    # full reconstruction step: room scene, 128 training views, TSDF of 200 maps, MC at level 12
+    "full": dict(workload="full reconstruction: 4x3x2.5 room + 20 boxes/spheres, levels 8-12, SH deg 3, "
+                          "128 views 1024x768; TSDF of 200 depth maps 1024x768 (trunc 3 voxels), MC at level 12",
+                 views=128, image="1024x768"),
 }
 DEFAULT_CONFIG = "batched"
 WORKLOAD = CONFIGS[DEFAULT_CONFIG]["workload"]
@@ -72,6 +76,8 @@ def rank_cameras(rank=0, n_views=None, config=DEFAULT_CONFIG):
     n = CONFIGS[config]["views"]
     if config == "batched":
         cams = S.mixed_resolution_cameras(n * (rank + 1), 3.0, seed=0)[n * rank:n * (rank + 1)]
+    elif config == "full":
+        cams = S.room_cameras(n * (rank + 1), 1024, 768, seed=0)[n * rank:n * (rank + 1)]
     else:
         cams = S.fibonacci_cameras(n * (rank + 1), 3.0, W, H, fovx_deg=50.0)[n * rank:n * (rank + 1)]
     return cams[:n_views or n]
@@ -79,7 +85,7 @@ def rank_cameras(rank=0, n_views=None, config=DEFAULT_CONFIG):
 
 def make_workload(rank=0, n_views=None, config=DEFAULT_CONFIG):
     from svraster_b200 import synthetic as S
-    scene = S.scene_batched(seed=0) if config == "batched" else S.scene_mid(seed=0)
+    scene = {"batched": S.scene_batched, "mid": S.scene_mid, "full": S.scene_full}[config](seed=0)
     return scene, rank_cameras(rank, n_views, config)
 
 
@@ -944,6 +950,112 @@ def oracle_view_step(scene, cam, threads):
     return Hc * Wc
 
 
+def run_full(args):
+    """The full reconstruction workload on one GPU: the training step over 128 views of
+    1024x768 (graph-captured; the views rendered 32 at a time, their gradients summed before
+    Adam), then the extraction: the median depth and transmittance of 200 views rendered in
+    two batches and fused into every grid point (FP64 running sums, truncation 3 finest
+    voxels), and marching cubes over the level-12 voxels of the fused field.  CUDA events."""
+    import torch
+    from svraster_b200 import _lib
+    from svraster_b200 import synthetic as S
+    from svraster_b200._lib import check, ptr, stream_ptr
+    from svraster_b200.marching_cubes import torch_marching_cubes_grid
+    from svraster_b200.raster import RasterState
+    from svraster_b200.step import BatchedTrainStep
+    dev = torch.device("cuda", 0)
+    t0 = time.perf_counter()
+    scene, cams = make_workload(0, None, "full")
+    gen_s = time.perf_counter() - t0
+    step = BatchedTrainStep(scene, cams, device=dev, lambda_R_concen=0.1, view_chunk=args.view_chunk)
+    L = _lib.load()
+    for _ in range(args.warmup):
+        step.step()
+    torch.cuda.synchronize()
+    per_step = step.capture()
+    for _ in range(args.warmup):
+        step.replay()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(args.steps):
+            step.replay()
+        ev1.record()
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    st_raster, st_misc = step.graph_status()
+    if st_raster or st_misc:
+        raise RuntimeError(f"graph replay status raster={st_raster} misc={st_misc}")
+    rays = step.rays
+    records = [int(c) for c in step.capacity]
+    step.step(time_render=True)
+    torch.cuda.synchronize()
+    stages = {k: round(v, 3) for k, v in BatchedTrainStep.stage_ms(step.ev).items()}
+    grid, centers, lengths, octpath, is_leaf = step.grid, step.centers, step.lengths, step.octpath, step.is_leaf
+    geos, s_val = step.geos, step.s_val
+    step.graph = None
+    del step
+    torch.cuda.empty_cache()
+    # ---------------------------------------------------------------- extraction
+    tcams = S.room_cameras(200, 1024, 768, seed=1)
+    xyz = torch.as_tensor(scene.grid_pts_xyz).to(dev).contiguous()
+    M = xyz.shape[0]
+    h = scene.scene_extent * 2.0 ** -int(scene.octlevel.max())
+    wacc = torch.zeros(M, dtype=torch.float64, device=dev)
+    sacc = torch.zeros(M, dtype=torch.float64, device=dev)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32)).to(dev)
+
+    def view_dicts(cs):
+        return [dict(width=c.width, height=c.height, tanfovx=c.tanfovx, tanfovy=c.tanfovy, cx=c.cx, cy=c.cy,
+                     near=c.near, w2c=t(c.w2c), c2w=t(c.c2w), bg=torch.zeros(3, device=dev)) for c in cs]
+    rgb0 = torch.zeros(100 * scene.n_vox, 3, device=dev)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    render_ms = fuse_ms = 0.0
+    for a in range(0, len(tcams), 100):
+        vc = tcams[a:a + 100]
+        views = view_dicts(vc)
+        e[0].record()
+        st_ = RasterState(views, scene.n_vox, dev)
+        st_.preprocess(octpath, centers, lengths, is_leaf)
+        st_.bin(octpath)
+        _, depth, _, T, _ = st_.render(3, True, False, centers, lengths, geos, rgb0[:len(vc) * scene.n_vox], s_val,
+                                       rgb_per_view=True)
+        e[1].record()
+        proj = []
+        for c in vc:
+            proj += [c.tanfovx, c.tanfovy, 0.5, 0.5]
+        proj_h = (len(proj) * _lib.C.c_double)(*proj)
+        check(L.svr_tsdf_integrate(st_.views, proj_h, len(vc), M, ptr(xyz), ptr(depth), 4, 2, ptr(T), 1, 0, 1, None,
+                                   3.0 * h, 0.01, 0.5, 1, 0, 0, 10.0, 1, ptr(wacc), ptr(sacc), stream_ptr(dev)),
+              "tsdf")
+        e[2].record()
+        torch.cuda.synchronize()
+        render_ms += e[0].elapsed_time(e[1])
+        fuse_ms += e[1].elapsed_time(e[2])
+        del st_, depth, T
+    tsdf = torch.where(wacc > 0, sacc / wacc, torch.full_like(wacc, float("nan"))).float()
+    lv12 = torch.as_tensor(scene.octlevel.reshape(-1) == int(scene.octlevel.max())).to(dev)
+    key12 = torch.as_tensor(scene.vox_key).to(dev)[lv12].contiguous()
+    torch_marching_cubes_grid(tsdf, xyz, key12[:1024], 0.0)   # warm up
+    e[0].record()
+    verts, faces = torch_marching_cubes_grid(tsdf, xyz, key12, 0.0)
+    e[1].record()
+    torch.cuda.synchronize()
+    mc_ms = e[0].elapsed_time(e[1])
+    return {"metric": "fwd+bwd Mrays/s", "value": round(rays / ms / 1e3, 3), "unit": "Mrays/s",
+            "ms_per_step": round(ms, 3), "iters_per_s": round(1e3 / ms, 3), "steps": args.steps,
+            "config": {"workload": CONFIGS["full"]["workload"], "n_voxels": scene.n_vox, "n_grid_pts": M,
+                       "views": len(cams), "view_chunk": args.view_chunk, "rays_per_step": rays,
+                       "records_per_chunk": records, "scene_generation_s": round(gen_s, 1)},
+            "stages_ms_eager": stages, "kernels_per_step": per_step, "clocks": clk.summary(),
+            "extraction": {"views": len(tcams), "render_ms": round(render_ms, 3), "tsdf_fp64_ms": round(fuse_ms, 3),
+                           "fused_points": int((wacc > 0).sum().item()), "grid_points": M,
+                           "mc_level": int(scene.octlevel.max()), "mc_voxels": int(lv12.sum().item()),
+                           "mc_ms": round(mc_ms, 3), "mc_faces": int(faces.shape[0]),
+                           "mc_verts": int(verts.shape[0])}}
+
+
 def sample_views(cams):
     """The CPU sample of a workload: the first view of each distinct resolution, in order."""
     seen, out = set(), []
@@ -1012,6 +1124,7 @@ def main():
                     help=f"workload ({DEFAULT_CONFIG} = the headline)")
     ap.add_argument("--views", type=int, default=None, help="views per GPU (default: the workload's)")
     ap.add_argument("--per-view-steps", type=int, default=5, help="timed steps of the per-view legs")
+    ap.add_argument("--view-chunk", type=int, default=32, help="views per chunk of the full workload's step")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extract", action="store_true", help="skip the extraction / regulariser / format legs")
@@ -1029,6 +1142,10 @@ def main():
             print(json.dumps(run_reference(args)), flush=True)
         return
 
+    if args.config == "full":
+        if rank == 0:
+            print(json.dumps(run_full(args)), flush=True)
+        return
     import torch
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     if world > 1:

@@ -258,6 +258,11 @@ SVR_API int svr_sh_eval_views(int N, int n_views, int degree, int M, const float
 SVR_API int svr_sh_eval_views_bw(int N, int n_views, int degree, int M, const float* centers,
                                  const float* cam_pos, const float* drgbs, float* dL_dsh0,
                                  float* dL_dshs, void* stream);
+/* The same adjoint added to dL_dsh0 / dL_dshs (a step that renders its views in several
+ * chunks sums every chunk's contribution); no counterpart in the reference. */
+SVR_API int svr_sh_eval_views_bw_add(int N, int n_views, int degree, int M, const float* centers,
+                                     const float* cam_pos, const float* drgbs, float* dL_dsh0,
+                                     float* dL_dshs, void* stream);
 
 /* ---------------------------------------------------------------- grid regularisers
  * Replace _C.valid_gradient_table (cuda/src/utils.cu:362-408) + the key sort of

@@ -40,6 +40,7 @@ _SIGS = {
     "svr_scatter_vox_grads": (_I, [_I64, _I, _P, _P, _P, _P]),
     "svr_sh_eval_views": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P]),
     "svr_sh_eval_views_bw": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P]),
+    "svr_sh_eval_views_bw_add": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P]),
     "svr_geom_buffer_bytes": (_SZ, [_I64]),
     "svr_preprocess": (_I, [_P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
     "svr_unpack_geom": (_I, [_P, _I64, _P, _P, _P, _P]),

@@ -371,7 +371,7 @@ __global__ void sh_views_kernel(int N, int V, int M, const float3* __restrict__ 
     }
 }
 
-template <int DEG>
+template <int DEG, bool ADD = false>
 __global__ void sh_views_bw_kernel(int N, int V, int M, const float3* __restrict__ centers,
                                    const float3* __restrict__ cam_pos, const float3* __restrict__ drgbs,
                                    float3* __restrict__ dsh0, float3* __restrict__ dshs)
@@ -393,15 +393,18 @@ __global__ void sh_views_bw_kernel(int N, int V, int M, const float3* __restrict
 #pragma unroll
         for (int k = 0; k < NB; ++k) acc[k] = acc[k] + B[k] * d;
     }
-    dsh0[i] = acc[0];
+    dsh0[i] = ADD ? dsh0[i] + acc[0] : acc[0];
 #pragma unroll
-    for (int k = 1; k < NB; ++k) dshs[i * (M - 1) + k - 1] = acc[k];
+    for (int k = 1; k < NB; ++k) {
+        float3& o = dshs[i * (M - 1) + k - 1];
+        o = ADD ? o + acc[k] : acc[k];
+    }
 }
 
 // Same adjoint with coalesced stores when every coefficient row is full (NB == M): the block's
 // rows are staged in shared memory and written back as one contiguous range (one thread per
 // voxel writing its 180-byte row left 32 scattered sectors per warp store).
-template <int DEG>
+template <int DEG, bool ADD = false>
 __global__ void __launch_bounds__(128) sh_views_bw_full_kernel(int N, int V, const float3* __restrict__ centers,
                                                                const float3* __restrict__ cam_pos,
                                                                const float3* __restrict__ drgbs,
@@ -440,9 +443,9 @@ __global__ void __launch_bounds__(128) sh_views_bw_full_kernel(int N, int V, con
     __syncthreads();
     const int nv = (int)min((int64_t)128, (int64_t)N - base);
     float* o0 = dsh0 + 3 * base;
-    for (int j = t; j < 3 * nv; j += 128) o0[j] = dc[j];
+    for (int j = t; j < 3 * nv; j += 128) o0[j] = ADD ? o0[j] + dc[j] : dc[j];
     float* o1 = dshs + (int64_t)ROW * base;
-    for (int j = t; j < ROW * nv; j += 128) o1[j] = rows[j];
+    for (int j = t; j < ROW * nv; j += 128) o1[j] = ADD ? o1[j] + rows[j] : rows[j];
 }
 
 template <typename Coef>
@@ -483,15 +486,33 @@ extern "C" int svr_sh_eval_views_bf16(int N, int n_views, int degree, int M, con
                            ShBF16{(const __nv_bfloat16*)sh0, (const __nv_bfloat16*)shs}, o, stream);
 }
 
+template <bool ADD>
+static int sh_views_bw_impl(int N, int n_views, int degree, int M, const float* centers, const float* cam_pos,
+                            const float* drgbs, float* dsh0, float* dshs, void* stream);
+
 extern "C" int svr_sh_eval_views_bw(int N, int n_views, int degree, int M, const float* centers,
                                     const float* cam_pos, const float* drgbs, float* dsh0, float* dshs, void* stream)
+{
+    return sh_views_bw_impl<false>(N, n_views, degree, M, centers, cam_pos, drgbs, dsh0, dshs, stream);
+}
+
+extern "C" int svr_sh_eval_views_bw_add(int N, int n_views, int degree, int M, const float* centers,
+                                        const float* cam_pos, const float* drgbs, float* dsh0, float* dshs,
+                                        void* stream)
+{
+    return sh_views_bw_impl<true>(N, n_views, degree, M, centers, cam_pos, drgbs, dsh0, dshs, stream);
+}
+
+template <bool ADD>
+static int sh_views_bw_impl(int N, int n_views, int degree, int M, const float* centers, const float* cam_pos,
+                            const float* drgbs, float* dsh0, float* dshs, void* stream)
 {
     if (degree < 0 || degree > 3 || M < (degree + 1) * (degree + 1) || n_views <= 0)
         return svr_fail(SVR_ERR_ARG, "sh views bw: bad degree / view count");
     if (N <= 0) return SVR_OK;
     cudaStream_t st = (cudaStream_t)stream;
     if (degree == 3 && M == 16) {
-        sh_views_bw_full_kernel<3><<<nblk(N, 128), 128, 0, st>>>(N, n_views, (const float3*)centers,
+        sh_views_bw_full_kernel<3, ADD><<<nblk(N, 128), 128, 0, st>>>(N, n_views, (const float3*)centers,
                                                                  (const float3*)cam_pos, (const float3*)drgbs,
                                                                  dsh0, dshs);
         LAUNCHED();
@@ -501,10 +522,10 @@ extern "C" int svr_sh_eval_views_bw(int N, int n_views, int degree, int M, const
     auto c = (const float3*)centers; auto cp = (const float3*)cam_pos; auto d = (const float3*)drgbs;
     auto o0 = (float3*)dsh0; auto o1 = (float3*)dshs;
     switch (degree) {
-        case 0: sh_views_bw_kernel<0><<<g, 128, 0, st>>>(N, n_views, M, c, cp, d, o0, o1); break;
-        case 1: sh_views_bw_kernel<1><<<g, 128, 0, st>>>(N, n_views, M, c, cp, d, o0, o1); break;
-        case 2: sh_views_bw_kernel<2><<<g, 128, 0, st>>>(N, n_views, M, c, cp, d, o0, o1); break;
-        default: sh_views_bw_kernel<3><<<g, 128, 0, st>>>(N, n_views, M, c, cp, d, o0, o1); break;
+        case 0: sh_views_bw_kernel<0, ADD><<<g, 128, 0, st>>>(N, n_views, M, c, cp, d, o0, o1); break;
+        case 1: sh_views_bw_kernel<1, ADD><<<g, 128, 0, st>>>(N, n_views, M, c, cp, d, o0, o1); break;
+        case 2: sh_views_bw_kernel<2, ADD><<<g, 128, 0, st>>>(N, n_views, M, c, cp, d, o0, o1); break;
+        default: sh_views_bw_kernel<3, ADD><<<g, 128, 0, st>>>(N, n_views, M, c, cp, d, o0, o1); break;
     }
     LAUNCHED();
     return SVR_OK;

@@ -39,7 +39,7 @@ class BatchedTrainStep:
 
     def __init__(self, scene, cams, device="cuda", lr=(1e-3, 1e-3, 1e-4), betas=(0.1, 0.99), eps=1e-15,
                  lambda_ls=1e-3, lambda_ge=1e-3, lambda_R_concen=0.0, sh_degree=3, seed=0, fused_smoothness=True,
-                 sh_dtype="f32", normal_losses=None, dense_ranks=True, binning="tiles"):
+                 sh_dtype="f32", normal_losses=None, dense_ranks=True, binning="tiles", view_chunk=None):
         """``sh_dtype="bf16"`` stores the SH coefficients in bf16 (the precision configuration):
         colours, compositing, transmittance and every gradient stay f32, Adam keeps f32 moments
         and rounds the updated coefficients to nearest bf16.  ``normal_losses`` (a dict with
@@ -50,7 +50,10 @@ class BatchedTrainStep:
         (voxel, octant) ranks (``raster.RankTable``, built here once): the same record order
         with a narrower sort key.  ``binning="tiles"`` (default) bins with the per-tile sort
         (``raster.PairOrder``, built here once; svr_bin_tiles), ``"radix"`` with the global
-        radix sort of svr_bin_and_sort; both give the same record order."""
+        radix sort of svr_bin_and_sort; both give the same record order.  ``view_chunk=k`` renders
+        the step's views k at a time (forward and adjoint of each chunk, then the smoothness
+        adjoint and Adam once), so that the per-(view, voxel) state of a large batch is held for
+        one chunk at a time; the gradients of all chunks are summed before Adam."""
         dev = torch.device(device)
         self.dev = dev
         t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
@@ -75,6 +78,14 @@ class BatchedTrainStep:
                       for c in cams]
         self.V = len(cams)
         self.cam_pos = torch.stack([v["c2w"][:3, 3] for v in self.views]).contiguous()
+        self.view_chunk = int(view_chunk) if view_chunk else None
+        if self.view_chunk and normal_losses:
+            raise ValueError("view_chunk does not take the normal-from-depth losses")
+        k = self.view_chunk or self.V
+        self.chunks = [(a, min(a + k, self.V)) for a in range(0, self.V, k)]
+        offs = np.concatenate([[0], np.cumsum([c.width * c.height for c in cams])]).astype(np.int64)
+        self.chunk_pix = [(int(offs[a]), int(offs[b])) for a, b in self.chunks]
+        self.V_buf = max(b - a for a, b in self.chunks)     # views held per chunk
         self.P = sum(c.width * c.height for c in cams)
         self.rays = self.P
         self.lr, self.betas, self.eps = lr, betas, eps
@@ -120,9 +131,9 @@ class BatchedTrainStep:
             self.nd_loss = torch.zeros(self.V, dtype=torch.float64, device=dev)
         # per-step buffers
         self.geos = torch.empty(self.N, 8, device=dev)
-        self.rgbs = torch.empty(self.V * self.N, 3, device=dev)
+        self.rgbs = torch.empty(self.V_buf * self.N, 3, device=dev)
         self.dvox = torch.zeros(self.N, 12, device=dev)
-        self.drgbs = torch.zeros(self.V * self.N, 3, device=dev)
+        self.drgbs = torch.zeros(self.V_buf * self.N, 3, device=dev)
         self.ds = torch.zeros(1, device=dev)
         # the gradients are views into one flat buffer, so that a step zeroes them with one
         # fill and a data-parallel step exchanges them with one all-reduce (``grad_flat``)
@@ -171,8 +182,68 @@ class BatchedTrainStep:
                 marks.append((name, e))
 
         mark("start")
+        if self.view_chunk:
+            return self._body_chunked(graph, mark, grad_hook, marks, time_render)
         fw = self._forward_part(graph, mark)
         return self._backward_part(graph, mark, grad_hook, fw, marks, time_render)
+
+    def _body_chunked(self, graph, mark, grad_hook, marks, time_render):
+        """One step over the views chunk by chunk: per chunk SH, preprocess, binning, render
+        forward and adjoint and the SH adjoint (added up); then smoothness, the gradient
+        scatter and Adam once."""
+        L = _lib.load()
+        st = stream_ptr(self.dev)
+        N = self.N
+        check(L.svr_gather_geo(N, ptr(self.all_idx), ptr(self.vox_key), ptr(self.grid), ptr(self.geos), st),
+              "gather")
+        self.dvox.zero_()
+        self.ds.zero_()
+        self.grad_flat.zero_()
+        mark("gather+zero")
+        sh_eval = L.svr_sh_eval_views_bf16 if self.sh_bf16 else L.svr_sh_eval_views
+        gt = self.gt
+        for k, ((a, b), (pa, pb)) in enumerate(zip(self.chunks, self.chunk_pix)):
+            nv = b - a
+            cam_pos = self.cam_pos[a:b]
+            rgbs = self.rgbs[: nv * N]
+            check(sh_eval(N, nv, self.sh_degree, self.M_sh, ptr(self.centers), ptr(cam_pos), ptr(self.sh0),
+                          ptr(self.shs), ptr(rgbs), st), "sh views")
+            state = RasterState(self.views[a:b], N, self.dev)
+            state.preprocess(self.octpath, self.centers, self.lengths, self.is_leaf)
+            if graph:
+                state.bin(self.octpath, capacity=self.capacity[k], path_or=self.path_or_all,
+                          rank_table=self.rank_table, pair_order=self.pair_order)
+            else:
+                state.bin(self.octpath, rank_table=self.rank_table, pair_order=self.pair_order)
+            color, depth, normal, T, _ = state.render(3, True, True, self.centers, self.lengths, self.geos, rgbs,
+                                                      self.s_val, rgb_per_view=True)
+            drgbs = self.drgbs[: nv * N]
+            drgbs.zero_()
+            state.render_backward(True, True, self.s_val, T, self.dcolor[3 * pa:3 * pb], self.ddepth[4 * pa:4 * pb],
+                                  self.dnormal[3 * pa:3 * pb], self.dT[pa:pb], lambda_R_concen=self.lambda_R,
+                                  gt_color=None if gt is None else gt[3 * pa:3 * pb], drgbs=drgbs, dvox=self.dvox,
+                                  ds=self.ds)
+            check(L.svr_sh_eval_views_bw_add(N, nv, self.sh_degree, self.M_sh, ptr(self.centers), ptr(cam_pos),
+                                             ptr(drgbs), ptr(self.grads[1]), ptr(self.grads[2]), st), "sh views bw")
+            self.state = state
+            mark(f"chunk{k}")
+        G = self.grid_keys.numel()
+        seed = self.seed if graph else self.seed + self.adam_step
+        step_ptr = ptr(self.step_dev) if graph else None
+        check(L.svr_smoothness_bw_vox(G, G, None, ptr(self.grid_keys), ptr(self.grid2voxel), 1 << self.res_pow2,
+                                      ptr(self.grid_mask), ptr(self.grid_index), ptr(self.grid_voxel_coord),
+                                      ptr(self.grid_voxel_size), N, ptr(self.geos), float(self.lambda_ls),
+                                      float(self.lambda_ge), self.vox_size_min_inv, seed, step_ptr,
+                                      ptr(self.dvox), 12, ptr(self.status), st), "smoothness")
+        check(L.svr_scatter_vox_grads(N, 12, ptr(self.vox_key), ptr(self.dvox), ptr(self.grads[0]), st), "scatter")
+        mark("smoothness+scatter")
+        if grad_hook is not None:
+            grad_hook(self.grads)
+            mark("allreduce")
+        self._adam(graph)
+        mark("adam")
+        self.ev = marks if time_render else None
+        return color, T
 
     def _forward_part(self, graph, mark):
         """Gather, SH, preprocess, binning and the render forward of the batch."""
@@ -267,6 +338,17 @@ class BatchedTrainStep:
         if grad_hook is not None:
             grad_hook(self.grads)
             mark("allreduce")
+        self._adam(graph)
+        mark("adam")
+        self.state = state
+        self.ev = marks if time_render else None
+        return color, T
+
+    def _adam(self, graph):
+        """Adam on grid / sh0 / shs: in a graph the step number comes from the device counter
+        and the bias corrections from the captured tables."""
+        L = _lib.load()
+        st = stream_ptr(self.dev)
         if graph:
             check(L.svr_counter_add(ptr(self.step_dev), 1, st), "counter")
             for p, g, m, v, tab, bf in zip(self.params, self.grads, self.adam_m, self.adam_v, self.coef_tables,
@@ -279,10 +361,6 @@ class BatchedTrainStep:
                 fn = L.svr_adam_step_bf16 if bf else L.svr_adam_step
                 check(fn(p.numel(), 0, 0, ptr(p), ptr(g), ptr(m), ptr(v), float(self.adam_step + 1),
                          float(lr), self.betas[0], self.betas[1], self.eps, st), "adam")
-        mark("adam")
-        self.state = state
-        self.ev = marks if time_render else None
-        return color, T
 
     # ------------------------------------------------------------------ CUDA graph
     def autotune(self, reps=3, cache=None):
@@ -327,15 +405,23 @@ class BatchedTrainStep:
         graph holding NCCL calls must be released before the process group is destroyed).
         Returns the number of this library's kernels in the graph(s)."""
         L = _lib.load()
-        if capacity is None:
-            probe = RasterState(self.views, self.N, self.dev)
+        if self.view_chunk and split:
+            raise ValueError("a step with view_chunk is captured whole (split=False)")
+
+        def count(views):
+            probe = RasterState(views, self.N, self.dev)
             probe.preprocess(self.octpath, self.centers, self.lengths, self.is_leaf)
             R, por = C.c_int64(0), C.c_uint64(0)
-            check(L.svr_count_rendered(self.N * self.V, ptr(probe.geom), C.byref(R), C.byref(por),
+            check(L.svr_count_rendered(self.N * len(views), ptr(probe.geom), C.byref(R), C.byref(por),
                                        stream_ptr(self.dev)), "count")
-            capacity = int(R.value)
-            del probe
-        self.capacity = max(int(capacity), 1)
+            return int(R.value)
+        if self.view_chunk:
+            self.capacity = [max(count(self.views[a:b]), 1) if capacity is None else int(capacity)
+                             for a, b in self.chunks]
+        else:
+            if capacity is None:
+                capacity = count(self.views)
+            self.capacity = max(int(capacity), 1)
         self.coef_rows = int(rows)
         self.coef_tables = []
         for lr in self.lr:
