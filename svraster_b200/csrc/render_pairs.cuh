@@ -188,9 +188,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
         }
         __syncthreads();
         // ---------------------------------------------------------------- P + C, per warp
-        uint32_t m[4];
+        uint32_t m[4], mc[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) { m[k] = S.mask[p_own][k]; S.mask[p_own][k] = 0u; }
+        for (int k = 0; k < 4; ++k) { m[k] = mc[k] = S.mask[p_own][k]; S.mask[p_own][k] = 0u; }
         const int cnt_own = __popc(m[0]) + __popc(m[1]) + __popc(m[2]) + __popc(m[3]);
         int incl = cnt_own;
 #pragma unroll
@@ -276,14 +276,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
                 S.res[warp][lane] = make_float2(alpha, dval);
             }
             __syncwarp();
-            // C: this pixel's pairs of the window, in record order
+            // C: this pixel's pairs of the window, in record order (popped from a copy: the
+            // pair numbering above reads every lane's whole mask in each window)
             const int e = min(base + 32, pre + cnt_own);
             for (int ii = max(base, pre); ii < e && !done; ++ii) {
                 int j2;
-                if (m[0]) { j2 = __ffs(m[0]) - 1; m[0] &= m[0] - 1; }
-                else if (m[1]) { j2 = __ffs(m[1]) + 31; m[1] &= m[1] - 1; }
-                else if (m[2]) { j2 = __ffs(m[2]) + 63; m[2] &= m[2] - 1; }
-                else { j2 = __ffs(m[3]) + 95; m[3] &= m[3] - 1; }
+                if (mc[0]) { j2 = __ffs(mc[0]) - 1; mc[0] &= mc[0] - 1; }
+                else if (mc[1]) { j2 = __ffs(mc[1]) + 31; mc[1] &= mc[1] - 1; }
+                else if (mc[2]) { j2 = __ffs(mc[2]) + 63; mc[2] &= mc[2] - 1; }
+                else { j2 = __ffs(mc[3]) + 95; mc[3] &= mc[3] - 1; }
                 const float2 rv = S.res[warp][ii - base];
                 const float alpha = rv.x;
                 if (COUNT) ++n_eval;

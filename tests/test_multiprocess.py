@@ -62,6 +62,53 @@ def _worker_allreduce(rank, world, port, out):
     dist.destroy_process_group()
 
 
+def _view_gradients(sc, cams, views):
+    """The oracle's adjoint over views ``views`` of ``cams``, summed, as the step's gradient groups: grid-point
+    gradients (corner terms scattered by vox_key) and the sh0 / shs gradients of the SH
+    adjoint, in one flat float64 vector."""
+    from oracle import oracle as O
+    N = sc.n_vox
+    geos = O.gather_geo(np.arange(N), sc.vox_key, sc.geo_grid_pts, N)
+    dgrid = np.zeros(len(sc.geo_grid_pts), np.float64)
+    dsh0 = np.zeros((N, 3), np.float64)
+    dshs = np.zeros((N, 15, 3), np.float64)
+    for k in views:
+        cam = cams[k]
+        rgbs = O.sh_eval(3, None, sc.vox_center, cam.position, sc.sh0, sc.shs)
+        nd, bb, bits = O.preprocess(cam, sc.vox_center, sc.vox_size, sc.is_leaf)
+        keys, vals, ranges = O.binning(cam, sc.octpath, nd, bb, bits)
+        f = O.render_fwd(cam, np.zeros(3, np.float32), 3, True, True, ranges, vals, bb, sc.vox_center, sc.vox_size,
+                         geos, rgbs, sc.s_val)
+        rng = np.random.default_rng(100 + k)          # view k's own upstream gradients
+        g = [rng.normal(size=(c, cam.height, cam.width)).astype(np.float32) for c in (3, 4, 3)]
+        dvox, _ = O.render_bwd(cam, np.zeros(3, np.float32), True, True, ranges, f["tile_last"], vals, bb,
+                               sc.vox_center, sc.vox_size, geos, rgbs, sc.s_val, f["T"], f["n_contrib"], g[0], g[1],
+                               g[2], np.zeros((1, cam.height, cam.width), np.float32))
+        np.add.at(dgrid, sc.vox_key.reshape(-1), dvox[:, :8].reshape(-1).astype(np.float64))
+        d0, d1 = O.sh_eval_bw(3, None, sc.vox_center, cam.position, dvox[:, 8:11].copy(), 16)
+        dsh0 += d0
+        dshs += d1.reshape(N, 15, 3)
+    return np.concatenate([dgrid, dsh0.reshape(-1), dshs.reshape(-1)])
+
+
+def _scene_and_views():
+    from svraster_b200 import synthetic as S
+    sc = S.scene_tiny(seed=4)
+    return sc, S.ring_cameras(4, 3.0, 64, 48, fovx_deg=50.0, phase=0.1)
+
+
+def _worker_view_adjoint(rank, world, port, out):
+    sys.path.insert(0, ROOT)
+    _init(rank, world, port)
+    sc, cams = _scene_and_views()
+    mine = list(range(rank, len(cams), world))    # disjoint views per rank
+    local = torch.from_numpy(_view_gradients(sc, cams, mine))
+    dist.all_reduce(local)                        # the step's one exchange
+    out[rank] = local.numpy()
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def _worker_fail(rank, world, port, out):
     _init(rank, world, port)
     try:
@@ -119,3 +166,19 @@ def test_failed_rank_does_not_hang_the_others():
     out = _run(_worker_fail)
     assert out[1].startswith("error")
     assert out[0].startswith("error") or out[0] == "completed"
+
+
+def test_data_parallel_adjoint_equals_single_process():
+    """Two ranks, each running the oracle's adjoint on its own views and summing the ranks'
+    gradients with one all-reduce, get the gradients one process computes over all the views
+    (the property the data-parallel step rests on), up to the order of the summation."""
+    sys.path.insert(0, ROOT)
+    out = _run(_worker_view_adjoint)
+    sc, cams = _scene_and_views()
+    ref = _view_gradients(sc, cams, range(len(cams)))
+    assert np.abs(ref).max() > 0
+    for r in (0, 1):
+        got = out[r]
+        assert got.shape == ref.shape
+        np.testing.assert_allclose(got, ref, rtol=0, atol=1e-9 * np.abs(ref).max() + 1e-12)
+    assert np.array_equal(out[0], out[1]), "the ranks' reduced gradients differ"
