@@ -142,6 +142,11 @@ static inline float rnorm3(float x, float y, float z) { return 1.f / sqrtf(x * x
 
 /* ------------------------------------------------------------------ preprocess
  * cuda/src/preprocess.cu:36-154 (perspective camera); host derivations :196-198. */
+/* The projection is spelled out operation by operation, with contraction off for this
+ * function and the bbox step fused explicitly, the same rounding the library's preprocess
+ * spells out: integer bboxes sit on pixel rounding boundaries, so both sides fix it rather
+ * than leave it to a compiler. */
+__attribute__((optimize("fp-contract=off")))
 void svo_preprocess(int P, int W, int H, float tanfovx, float tanfovy, float cx, float cy,
                     const float* w2c, const float* c2w, float near,
                     const float* centers, const float* lengths, const uint8_t* is_leaf,
@@ -150,30 +155,35 @@ void svo_preprocess(int P, int W, int H, float tanfovx, float tanfovy, float cx,
     const int gx = (W + TILE - 1) / TILE, gy = (H + TILE - 1) / TILE;
     const float focal_x = 0.5f * W / tanfovx;
     const float focal_y = 0.5f * H / tanfovy;
-    const f3 ro = mk(c2w[3], c2w[7], c2w[11]);
+    const float rox = c2w[3], roy = c2w[7], roz = c2w[11];
+    const float* m = w2c;
     for (int i = 0; i < P; ++i) {
         out_ndup[i] = 0; bboxes[2 * i] = 0; bboxes[2 * i + 1] = 0; bits[i] = 0;
         if (is_leaf[i] == 0) continue;
-        f3 c = mk(centers[3 * i], centers[3 * i + 1], centers[3 * i + 2]);
-        float r = 0.5f * lengths[i];
-        f3 rel = sub(c, ro);
-        if (dot(rel, rel) < near * near) continue;
+        const float cxv = centers[3 * i], cyv = centers[3 * i + 1], czv = centers[3 * i + 2];
+        const float r = 0.5f * lengths[i];
+        const float dxr = cxv - rox, dyr = cyv - roy, dzr = czv - roz;
+        const float d2 = (dxr * dxr + dyr * dyr) + dzr * dzr;
+        if (d2 < near * near) continue;
         uint32_t qb = 0;
         float mnx = 1e9f, mny = 1e9f, mxx = -1e9f, mxy = -1e9f;
         for (int k = 0; k < 8; ++k) {
-            f3 sh = mk((float)(((k & 4) >> 2) * 2 - 1), (float)(((k & 2) >> 1) * 2 - 1), (float)((k & 1) * 2 - 1));
-            f3 wc = add(c, muls(sh, r));
-            f3 cc = transform_3x4(w2c, wc);
-            if (cc.z < near) continue;
-            float iz = 1.0f / cc.z;
-            float u = cc.x * iz, v = cc.y * iz;
-            int q = ((wc.x < ro.x) << 2) | ((wc.y < ro.y) << 1) | (wc.z < ro.z);
+            const float sx = (float)(((k & 4) >> 2) * 2 - 1), sy = (float)(((k & 2) >> 1) * 2 - 1);
+            const float sz = (float)((k & 1) * 2 - 1);
+            const float wx = cxv + r * sx, wy = cyv + r * sy, wz = czv + r * sz;   /* exact: s = +-1 */
+            const float X = ((m[0] * wx + m[1] * wy) + m[2] * wz) + m[3];
+            const float Y = ((m[4] * wx + m[5] * wy) + m[6] * wz) + m[7];
+            const float Z = ((m[8] * wx + m[9] * wy) + m[10] * wz) + m[11];
+            if (Z < near) continue;
+            const float iz = 1.0f / Z;
+            const float u = X * iz, v = Y * iz;
+            const int q = ((wx < rox) << 2) | ((wy < roy) << 1) | (wz < roz);
             mnx = minf(mnx, u); mny = minf(mny, v); mxx = maxf(mxx, u); mxy = maxf(mxy, v);
             qb |= 1u << q;
         }
-        float cxh = cx - 0.5f, cyh = cy - 0.5f;
-        float bminx = maxf(focal_x * mnx + cxh, 0.0f), bminy = maxf(focal_y * mny + cyh, 0.0f);
-        float bmaxx = minf(focal_x * mxx + cxh, (float)W), bmaxy = minf(focal_y * mxy + cyh, (float)H);
+        const float cxh = cx - 0.5f, cyh = cy - 0.5f;
+        const float bminx = maxf(fmaf(focal_x, mnx, cxh), 0.0f), bminy = maxf(fmaf(focal_y, mny, cyh), 0.0f);
+        const float bmaxx = minf(fmaf(focal_x, mxx, cxh), (float)W), bmaxy = minf(fmaf(focal_y, mxy, cyh), (float)H);
         if (bminx > bmaxx || bminy > bmaxy) continue;
         uint32_t b0 = (((uint32_t)lrintf(bminx)) << 16) | ((uint32_t)lrintf(bminy));
         uint32_t b1 = (((uint32_t)lrintf(bmaxx)) << 16) | ((uint32_t)lrintf(bmaxy));

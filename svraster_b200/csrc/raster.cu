@@ -99,7 +99,7 @@ struct BinMeta {
 };
 static_assert(sizeof(BinMeta) == 256, "bin meta block");
 struct BinLayout {
-    size_t keys_in, keys_out, vals_in, vals_out, tmp, tmp_bytes, recs, total;
+    size_t keys_in, keys_out, vals_in, vals_out, tmp, tmp_bytes, recs, pairs_b, total;
 };
 static BinLayout bin_layout(int64_t R) {
     BinLayout L{};
@@ -116,6 +116,7 @@ static BinLayout bin_layout(int64_t R) {
     L.vals_out = off; off = align_up(off + 4 * (size_t)n, 256);
     L.tmp = off; L.tmp_bytes = t64 > t32 ? t64 : t32; off = align_up(off + L.tmp_bytes, 256);
     L.recs = off; off = align_up(off + sizeof(Rec) * (size_t)n, 256);
+    L.pairs_b = off; off = align_up(off + 8 * (size_t)n, 256);   // per-tile sort: second (key, value) array
     L.total = off;
     return L;
 }
@@ -212,7 +213,9 @@ __global__ void __launch_bounds__(256, 4) preprocess_kernel(
             const float3 vox_c = centers[i];
             const float vox_r = 0.5f * lengths[i];
             const float3 rel = vox_c - ro;
-            if (!(dot3(rel, rel) < near * near)) {
+            const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(rel.x, rel.x), __fmul_rn(rel.y, rel.y)),
+                                       __fmul_rn(rel.z, rel.z));
+            if (!(d2 < near * near)) {
                 float2 cmin = make_float2(1e9f, 1e9f), cmax = make_float2(-1e9f, -1e9f);
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
@@ -228,10 +231,11 @@ __global__ void __launch_bounds__(256, 4) preprocess_kernel(
                     cmax = make_float2(fmaxf(cmax.x, u), fmaxf(cmax.y, v));
                     qbits |= (1u << q);
                 }
-                const float bminx = fmaxf(focal_x * cmin.x + cx_h, 0.0f);
-                const float bminy = fmaxf(focal_y * cmin.y + cy_h, 0.0f);
-                const float bmaxx = fminf(focal_x * cmax.x + cx_h, (float)view.width);
-                const float bmaxy = fminf(focal_y * cmax.y + cy_h, (float)view.height);
+                // fused (one rounding), as the C oracle spells it
+                const float bminx = fmaxf(fmaf(focal_x, cmin.x, cx_h), 0.0f);
+                const float bminy = fmaxf(fmaf(focal_y, cmin.y, cy_h), 0.0f);
+                const float bmaxx = fminf(fmaf(focal_x, cmax.x, cx_h), (float)view.width);
+                const float bmaxy = fminf(fmaf(focal_y, cmax.y, cy_h), (float)view.height);
                 if (!(bminx > bmaxx || bminy > bmaxy)) {
                     bbox = make_uint2((((uint32_t)lrintf(bminx)) << 16) | ((uint32_t)lrintf(bminy)),
                                       (((uint32_t)lrintf(bmaxx)) << 16) | ((uint32_t)lrintf(bmaxy)));
@@ -624,7 +628,6 @@ extern "C" int svr_bin_tiles(const svr_view_t* views_host, int n_views, int N, i
     uint32_t* cursor = (uint32_t*)(im + IL.cursor);
     CUDA_TRY(cudaMemsetAsync(status, 0, 4, st));
     CUDA_TRY(cudaMemsetAsync(tile_cnt, 0, 4 * (size_t)T, st));
-    const int n_rec = (int)(R > 0 ? R : 1);
     const uint32_t* ndup = (const uint32_t*)(g + GL.ndup);
     const uint2* bbox = (const uint2*)(g + GL.bbox);
     const uint32_t* bits = (const uint32_t*)(g + GL.bits);
@@ -657,24 +660,22 @@ extern "C" int svr_bin_tiles(const svr_view_t* views_host, int n_views, int N, i
                                               (uint32_t*)(im + IL.order), &meta->count, &meta->rank_bits, status);
     LAUNCH_CHECK();
     if (N == 0 || R == 0) return SVR_OK;
-    // record keys and values: (A) keys_in[0, R) / vals_in, (B) keys_in[R, 2R) / keys_out[R, 2R);
-    // results: vals_out and the tile id of every record in keys_out[0, R)
-    uint32_t* ka = (uint32_t*)(b + BL.keys_in);
-    uint32_t* kb = ka + n_rec;
-    uint32_t* va = (uint32_t*)(b + BL.vals_in);
+    // (key, value) pairs: A in keys_in, B (large tiles' passes) in pairs_b; results: vals_out
+    // and the tile id of every record in keys_out (read by the record packing)
+    uint2* pa = (uint2*)(b + BL.keys_in);
+    uint2* pb = (uint2*)(b + BL.pairs_b);
     uint32_t* tile_out = (uint32_t*)(b + BL.keys_out);
-    uint32_t* vb = tile_out + n_rec;
     if (smem_hist)
-        tile_scatter_kernel<true><<<grid, 256, hist_bytes, st>>>(V, N, ndup, bbox, bits, pair_pos, cursor, R, ka, va,
+        tile_scatter_kernel<true><<<grid, 256, hist_bytes, st>>>(V, N, ndup, bbox, bits, pair_pos, cursor, R, pa,
                                                                  status);
     else
-        tile_scatter_kernel<false><<<grid, 256, 0, st>>>(V, N, ndup, bbox, bits, pair_pos, cursor, R, ka, va, status);
+        tile_scatter_kernel<false><<<grid, 256, 0, st>>>(V, N, ndup, bbox, bits, pair_pos, cursor, R, pa, status);
     LAUNCH_CHECK();
     static std::atomic<unsigned long long> d3{0};
     const int ts_smem = (int)sizeof(TileSortSmem);
     if ((rc = ensure_smem(tile_sort_kernel, ts_smem, d3))) return rc;
     tile_sort_kernel<<<T, TS_THREADS, ts_smem, st>>>(T, (const uint32_t*)(im + IL.order),
-                                                      (const uint2*)(im + IL.ranges), key_bits, ka, va, kb, vb,
+                                                      (const uint2*)(im + IL.ranges), key_bits, pa, pb,
                                                       (uint32_t*)(b + BL.vals_out), tile_out, status);
     LAUNCH_CHECK();
     return SVR_OK;
@@ -881,13 +882,15 @@ __global__ void __launch_bounds__(256) pack_records_kernel(
 #include "render_kernels.cuh"
 #include "render_pairs.cuh"
 
-// Which forward render kernel the launches use: 1 = record-parallel filter with dense pair
-// evaluation (render_fwd_pairs_kernel, the default), 0 = the warp-filter kernel
-// (render_fwd_kernel).  Both give the same outputs bit for bit.
+// Which render kernels the launches use: 0 = the warp-filter kernels (render_fwd_kernel /
+// render_bwd_kernel), 1 = record-parallel filter with dense pair evaluation
+// (render_fwd_pairs_kernel / render_bwd_pairs_kernel) with warps on 8x4 pixel blocks, 2 = the
+// same with every warp on a lattice spread over the tile.  All give the same forward outputs
+// bit for bit and the same gradients up to the order of their float atomics.
 static std::atomic<int> g_fwd_impl{1}, g_bwd_impl{1};
 extern "C" int svr_render_set_impl(int fwd_impl, int bwd_impl)
 {
-    if (fwd_impl < 0 || fwd_impl > 1 || bwd_impl < 0 || bwd_impl > 1) return svr_fail(SVR_ERR_ARG, "render impl");
+    if (fwd_impl < 0 || fwd_impl > 2 || bwd_impl < 0 || bwd_impl > 2) return svr_fail(SVR_ERR_ARG, "render impl");
     g_fwd_impl.store(fwd_impl);
     g_bwd_impl.store(bwd_impl);
     return SVR_OK;
@@ -905,13 +908,13 @@ extern "C" int svr_render_get_impl(int* fwd_impl, int* bwd_impl)
 #ifndef SVR_PBWD_MINB
 #define SVR_PBWD_MINB 3
 #endif
-template <bool DEPTH, bool NORMAL, bool RCONC>
+template <bool DEPTH, bool NORMAL, bool RCONC, bool LATTICE = true>
 static int launch_bwd_pairs(int T, int N, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
                             const uint32_t* tl, const uint32_t* nc, const Rec* recs, const float* s_val,
                             const float* out_T, const float* dc, const float* dd, const float* dn, const float* dT,
                             float lam, const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status)
 {
-    auto k = render_bwd_pairs_kernel<DEPTH, NORMAL, RCONC, SVR_PBWD_RING, SVR_PBWD_MINB>;
+    auto k = render_bwd_pairs_kernel<DEPTH, NORMAL, RCONC, SVR_PBWD_RING, SVR_PBWD_MINB, LATTICE>;
     const int smem = (int)sizeof(PairBwdSmem<SVR_PBWD_RING>);
     static std::atomic<unsigned long long> done{0};
     int rc = ensure_smem(k, smem, done);
@@ -928,13 +931,13 @@ static int launch_bwd_pairs(int T, int N, cudaStream_t st, const Views& V, const
 #ifndef SVR_PFWD_MINB
 #define SVR_PFWD_MINB 4
 #endif
-template <int NS, bool DEPTH, bool NORMAL, bool MAXW, bool COUNT>
+template <int NS, bool DEPTH, bool NORMAL, bool MAXW, bool COUNT, bool LATTICE = true>
 static int launch_fwd_pairs(int T, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
                             const Rec* recs, const float* s_val, uint32_t* tile_last, uint32_t* n_contrib,
                             float* color, float* depth, float* normal, float* outT, float* max_w, int64_t mw_stride,
                             unsigned* status, unsigned long long* pair_count)
 {
-    auto k = render_fwd_pairs_kernel<NS, DEPTH, NORMAL, MAXW, SVR_PFWD_RING, SVR_PFWD_MINB, COUNT>;
+    auto k = render_fwd_pairs_kernel<NS, DEPTH, NORMAL, MAXW, SVR_PFWD_RING, SVR_PFWD_MINB, COUNT, LATTICE>;
     const int smem = (int)sizeof(PairFwdSmem<SVR_PFWD_RING>);
     static std::atomic<unsigned long long> done{0};
     int rc = ensure_smem(k, smem, done);
@@ -1021,9 +1024,13 @@ static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint32_t* or
                       float* normal, float* outT, float* max_w, int64_t mw_stride, unsigned* status)
 {
     if (g_fwd_impl.load() == 1)
-        return launch_fwd_pairs<NS, DEPTH, NORMAL, MAXW, false>(T, st, V, order, ranges, recs, s_val, tile_last,
-                                                                n_contrib, color, depth, normal, outT, max_w,
-                                                                mw_stride, status, nullptr);
+        return launch_fwd_pairs<NS, DEPTH, NORMAL, MAXW, false, false>(T, st, V, order, ranges, recs, s_val,
+                                                                       tile_last, n_contrib, color, depth, normal,
+                                                                       outT, max_w, mw_stride, status, nullptr);
+    if (g_fwd_impl.load() == 2)
+        return launch_fwd_pairs<NS, DEPTH, NORMAL, MAXW, false, true>(T, st, V, order, ranges, recs, s_val,
+                                                                      tile_last, n_contrib, color, depth, normal,
+                                                                      outT, max_w, mw_stride, status, nullptr);
 #define FWD_CFG_ARGS T, st, V, order, ranges, recs, s_val, tile_last, n_contrib, color, depth, normal, outT, max_w, mw_stride, status
     if constexpr (NS == 3 && DEPTH && NORMAL && !MAXW) {
         int cfg = g_fwd_cfg.load();
@@ -1154,7 +1161,7 @@ extern "C" int svr_render_fwd_count_pairs(const svr_view_t* views_host, int n_vi
     char* b = (char*)binning_buffer;
     char* im = (char*)image_buffer;
     CUDA_TRY(cudaMemsetAsync(pair_count, 0, 3 * sizeof(unsigned long long), st));
-    if (g_fwd_impl.load() == 1)
+    if (g_fwd_impl.load() >= 1)
         return launch_fwd_pairs<3, true, true, false, true>(T, st, V, (const uint32_t*)(im + IL.order),
                                                             (const uint2*)(im + IL.ranges), (const Rec*)(b + BL.recs),
                                                             s_val, (uint32_t*)(im + IL.tile_last),
@@ -1199,7 +1206,8 @@ static int launch_bwd(int T, int N, cudaStream_t st, const Views& V, const uint3
                       const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status)
 {
 #define BWD_CFG_ARGS T, N, st, V, order, ranges, tl, nc, recs, s_val, out_T, dc, dd, dn, dT, lam, gt, dvox, drgbs, ds, status
-    if (g_bwd_impl.load() == 1) return launch_bwd_pairs<DEPTH, NORMAL, RCONC>(BWD_CFG_ARGS);
+    if (g_bwd_impl.load() == 1) return launch_bwd_pairs<DEPTH, NORMAL, RCONC, false>(BWD_CFG_ARGS);
+    if (g_bwd_impl.load() == 2) return launch_bwd_pairs<DEPTH, NORMAL, RCONC, true>(BWD_CFG_ARGS);
     if constexpr (DEPTH && NORMAL) {
         int cfg = g_bwd_cfg.load();
         if (cfg == 0 && T < SMALL_LAUNCH_TILES) cfg = 2;          // 4 x 2

@@ -15,7 +15,8 @@
 //    arithmetic runs on full warps however unevenly the pixels' candidates are spread;
 //  * C (compositing, per pixel): each pixel folds its own pairs in record order with the
 //    forward's expressions, so every output is bit-identical to render_fwd_kernel's.
-// Two CTA barriers per slot: after F, and after C (the slot and the masks are then free).
+// Two CTA barriers per slot: when the slot has arrived (every warp is then through the previous
+// slot, which is refilled), and after F.
 #pragma once
 
 #include <climits>
@@ -52,6 +53,20 @@ __device__ __forceinline__ int kth_set_bit(uint32_t w, int k) {
     return pos;
 }
 
+// Pixel (dx, dy) of lane `lane` of warp `warp` in a 16x16 tile.  LATTICE: every warp owns a
+// stride-4 x stride-2 lattice spread over the whole tile, so the warps' pair counts are alike
+// and the CTA barriers wait less on the warp holding the silhouette; else 8x4 blocks.
+template <bool LATTICE>
+__device__ __forceinline__ void pair_pixel(int warp, int lane, int& dx, int& dy) {
+    if (LATTICE) {
+        dx = (warp & 3) + 4 * (lane & 3);
+        dy = (warp >> 2) + 2 * (lane >> 2);
+    } else {
+        dx = (warp & 1) * 8 + (lane & 7);
+        dy = (warp >> 1) * 4 + (lane >> 3);
+    }
+}
+
 // Filter test of one (record, pixel): live pixel, matching octant, slab test passed.
 __device__ __forceinline__ bool filter_hit(const float4 pr, uint32_t q, float3 c, float l, float3 ro) {
     const uint32_t f = __float_as_uint(pr.w);
@@ -60,7 +75,8 @@ __device__ __forceinline__ bool filter_hit(const float4 pr, uint32_t q, float3 c
     return !(ab.x > ab.y);
 }
 
-template <int NS, bool DEPTH, bool NORMAL, bool MAXW, int RING = 3, int MINB = 4, bool COUNT = false>
+template <int NS, bool DEPTH, bool NORMAL, bool MAXW, int RING = 3, int MINB = 4, bool COUNT = false,
+          bool LATTICE = true>
 __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
     const __grid_constant__ Views V, const uint32_t* __restrict__ order, const uint2* __restrict__ ranges,
     const Rec* __restrict__ recs, const float* __restrict__ s_ptr, uint32_t* __restrict__ tile_last,
@@ -79,7 +95,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
     const int lt = tile - view.tile_offset;
     const int tx = lt % view.tiles_x, ty = lt / view.tiles_x;
     int dx, dy;
-    tile_pixel(tid, dx, dy);
+    pair_pixel<LATTICE>(warp, lane, dx, dy);
     const uint32_t px = tx * TILE + dx, py = ty * TILE + dy;
     const bool inside = (px < (uint32_t)W) && (py < (uint32_t)H);
     const Ray ray = pixel_ray(view, px, py);
@@ -91,8 +107,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
     S.pdir[p_own] = make_float4(ray.rd.x, ray.rd.y, ray.rd.z, ray.rd_norm_inv);
 #pragma unroll
     for (int k = 0; k < 4; ++k) S.mask[p_own][k] = 0u;
-    // pixel of lane l of this warp: its 8x4 block, row-major inside the tile
-    const int wx0 = (warp & 1) * 8, wy0 = (warp >> 1) * 4;
 
     const uint2 range = ranges[tile];
     const int n = (int)(range.y - range.x);
@@ -131,6 +145,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
         // every thread must reach the barriers below: a timed-out wait is agreed on by all
         if (__syncthreads_or(failed)) { failed = true; break; }
         parity ^= 1u << slot;
+        // every warp is through the previous slot: refill it with the batch RING ahead
+        if (tid == 0 && b >= 1 && b - 1 + RING < nbatch) {
+            fence_proxy_async_smem();
+            issue(b - 1 + RING);
+        }
         const int cnt = min(BATCH, n - b * BATCH);
         const Rec* buf = S.buf[slot];
         // ---------------------------------------------------------------- F: filter
@@ -186,7 +205,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
                 }
             }
         }
-        __syncthreads();
+        // the masks are complete; stop streaming once every pixel is done (as of the last slot)
+        if (__syncthreads_and(done)) break;
         // ---------------------------------------------------------------- P + C, per warp
         uint32_t m[4], mc[4];
 #pragma unroll
@@ -226,7 +246,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
                     }
                 }
                 const int j = jb + kth_set_bit(wsel, k);
-                const int p = (wy0 + (ol >> 3)) * TILE + wx0 + (ol & 7);
+                int odx, ody;
+                pair_pixel<LATTICE>(warp, ol, odx, ody);
+                const int p = ody * TILE + odx;
                 const float4 pr = S.pray[p], pd = S.pdir[p];
                 const float3 rd = f3(pd.x, pd.y, pd.z);
                 const Rec& r = buf[j];
@@ -313,14 +335,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
         if (done && inside) {
             const float4 pr = S.pray[p_own];
             S.pray[p_own].w = __uint_as_float(__float_as_uint(pr.w) & ~PIX_LIVE);
-        }
-        // the slot and the masks are free once every pixel composited; stop streaming once
-        // every pixel is done
-        const bool all_done = __syncthreads_and(done);
-        if (all_done) break;
-        if (tid == 0 && b + RING < nbatch) {
-            fence_proxy_async_smem();
-            issue(b + RING);
         }
     }
     if (failed && tid == 0) atomicOr(status, ERR_WAIT_TIMEOUT);
@@ -462,7 +476,7 @@ __device__ __forceinline__ int kth_highest_bit(const uint32_t (&m)[4], int k) {
     return jb + 31 - kth_set_bit(__brev(wsel), k);
 }
 
-template <bool DEPTH, bool NORMAL, bool RCONC, int RING = 3, int MINB = 3>
+template <bool DEPTH, bool NORMAL, bool RCONC, int RING = 3, int MINB = 3, bool LATTICE = true>
 __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
     const __grid_constant__ Views V, int N, const uint32_t* __restrict__ order, const uint2* __restrict__ ranges,
     const uint32_t* __restrict__ tile_last,
@@ -482,14 +496,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
     const int lt = tile - view.tile_offset;
     const int tx = lt % view.tiles_x, ty = lt / view.tiles_x;
     int dx, dy;
-    tile_pixel(tid, dx, dy);
+    pair_pixel<LATTICE>(warp, lane, dx, dy);
     const uint32_t px = tx * TILE + dx, py = ty * TILE + dy;
     const bool inside = (px < (uint32_t)W) && (py < (uint32_t)H);
     const Ray ray = pixel_ray(view, px, py);
     const uint32_t pq = ray_octant(ray.rd);
     const float s_val = *s_ptr;
     const int p_own = dy * TILE + dx;
-    const int wx0 = (warp & 1) * 8, wy0 = (warp >> 1) * 4;
 
     // per-pixel adjoint state (backward.cu:156-216)
     const int64_t HW = (int64_t)W * H;
@@ -561,6 +574,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
         if (!mbar_wait(&S.full[slot], (parity >> slot) & 1)) failed = true;
         if (__syncthreads_or(failed)) { failed = true; break; }
         parity ^= 1u << slot;
+        // every warp is through the previous slot: refill it with the batch RING ahead
+        if (tid == 0 && b >= 1 && b - 1 + RING < nbatch) {
+            fence_proxy_async_smem();
+            issue(b - 1 + RING);
+        }
         const int hi = n - b * BATCH;
         const int cnt = min(BATCH, hi);
         const int lo = hi - cnt;                      // relative index of slot entry 0
@@ -648,7 +666,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
             for (int k = 0; k < 4; ++k) om[k] = __shfl_sync(0xffffffffu, m[k], ol);
             const bool has = i < total;
             const int j = has ? kth_highest_bit(om, i - opre) : 0;
-            const int p = (wy0 + (ol >> 3)) * TILE + wx0 + (ol & 7);
+            int odx, ody;
+            pair_pixel<LATTICE>(warp, ol, odx, ody);
+            const int p = ody * TILE + odx;
             PairBwdRes& R = S.res[warp][lane];
             // ---------------------------------------------------------- A
             if (has) {
@@ -838,12 +858,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
                 }
             }
             __syncwarp();
-        }
-        // the slot and the masks are free once every warp is through
-        __syncthreads();
-        if (tid == 0 && b + RING < nbatch) {
-            fence_proxy_async_smem();
-            issue(b + RING);
         }
     }
     if (failed && tid == 0) atomicOr(status, ERR_WAIT_TIMEOUT);

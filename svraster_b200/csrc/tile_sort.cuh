@@ -132,15 +132,15 @@ __device__ __forceinline__ void block_rank(const uint32_t (&key)[TS_K], int coun
 }
 
 // Sort of one tile's records [start, start + n) by key (pair position), values along.
-// Input in (ka, va); the sorted values go to vals_out and the tile id of every record to
-// tile_out.  Passes over bits [0, key_bits) eight at a time.  Large tiles ping-pong through
-// (ka, va) and (kb, vb) in global memory.
+// Input in A as (key, value) pairs; the sorted values go to vals_out and the tile id of every
+// record to tile_out.  Passes over bits [0, key_bits) eight at a time.  Large tiles ping-pong
+// through A and B in global memory.
 #ifndef SVR_TS_MINB
 #define SVR_TS_MINB 2
 #endif
 __global__ void __launch_bounds__(TS_THREADS, SVR_TS_MINB) tile_sort_kernel(
     int T, const uint32_t* __restrict__ order, const uint2* __restrict__ ranges, int key_bits,
-    uint32_t* __restrict__ ka, uint32_t* __restrict__ va, uint32_t* __restrict__ kb, uint32_t* __restrict__ vb,
+    uint2* __restrict__ A, uint2* __restrict__ B,
     uint32_t* __restrict__ vals_out, uint32_t* __restrict__ tile_out, unsigned* __restrict__ status)
 {
     extern __shared__ __align__(16) unsigned char ts_smem[];
@@ -160,8 +160,9 @@ __global__ void __launch_bounds__(TS_THREADS, SVR_TS_MINB) tile_sort_kernel(
 #pragma unroll
         for (int k = 0; k < TS_K; ++k) {
             const int i = w * 32 * TS_K + k * 32 + lane;
-            key[k] = i < n ? ka[start + i] : 0u;
-            val[k] = i < n ? va[start + i] : 0u;
+            const uint2 kv = i < n ? A[start + i] : make_uint2(0u, 0u);
+            key[k] = kv.x;
+            val[k] = kv.y;
         }
         for (int p = 0; p < npass; ++p) {
             block_rank(key, n, 8 * p, true, S, pos);
@@ -191,7 +192,7 @@ __global__ void __launch_bounds__(TS_THREADS, SVR_TS_MINB) tile_sort_kernel(
 
     // large tile: each pass counts the digits over the whole range, then ranks and scatters
     // it block-tile by block-tile with a running digit base
-    uint32_t *src_k = ka, *src_v = va, *dst_k = kb, *dst_v = vb;
+    uint2 *src = A, *dst = B;
     for (int p = 0; p < npass; ++p) {
         const int sh = 8 * p;
         const bool last = p == npass - 1;
@@ -203,7 +204,7 @@ __global__ void __launch_bounds__(TS_THREADS, SVR_TS_MINB) tile_sort_kernel(
             for (int k = 0; k < TS_K; ++k) {
                 const int i = w * 32 * TS_K + k * 32 + lane;
                 const bool valid = i < cnt;
-                const uint32_t d = valid ? (src_k[start + c0 + i] >> sh) & 255u : 0u;
+                const uint32_t d = valid ? (src[start + c0 + i].x >> sh) & 255u : 0u;
                 const uint32_t peers = digit_peers(d, valid);
                 if (valid && lane == 31 - __clz(peers)) atomicAdd(&S.base[d], (uint32_t)__popc(peers));
             }
@@ -221,8 +222,9 @@ __global__ void __launch_bounds__(TS_THREADS, SVR_TS_MINB) tile_sort_kernel(
 #pragma unroll
             for (int k = 0; k < TS_K; ++k) {
                 const int i = w * 32 * TS_K + k * 32 + lane;
-                key[k] = i < cnt ? src_k[start + c0 + i] : 0u;
-                val[k] = i < cnt ? src_v[start + c0 + i] : 0u;
+                const uint2 kv = i < cnt ? src[start + c0 + i] : make_uint2(0u, 0u);
+                key[k] = kv.x;
+                val[k] = kv.y;
             }
             block_rank(key, cnt, sh, false, S, pos);
 #pragma unroll
@@ -234,15 +236,13 @@ __global__ void __launch_bounds__(TS_THREADS, SVR_TS_MINB) tile_sort_kernel(
                         vals_out[start + pos[k]] = val[k];
                         tile_out[start + pos[k]] = (uint32_t)tile;
                     } else {
-                        dst_k[start + pos[k]] = key[k];
-                        dst_v[start + pos[k]] = val[k];
+                        dst[start + pos[k]] = make_uint2(key[k], val[k]);
                     }
                 }
             }
             __syncthreads();
         }
-        uint32_t* t = src_k; src_k = dst_k; dst_k = t;
-        t = src_v; src_v = dst_v; dst_v = t;
+        uint2* t = src; src = dst; dst = t;
     }
 }
 
@@ -448,12 +448,12 @@ __global__ void __launch_bounds__(256) tile_offsets_kernel(
 // tile_count_kernel: the CTA counts its records per tile, reserves one contiguous run per
 // touched tile with a global atomic on the tile's cursor, then places every record inside
 // its run with a shared-memory atomic.  Key = the (voxel, octant) pair's position in the
-// reference order (pair-order table), value = octant << 29 | voxel id.
+// reference order (pair-order table), value = octant << 29 | voxel id, stored together.
 template <bool SMEM>
 __global__ void __launch_bounds__(256) tile_scatter_kernel(
     const __grid_constant__ Views V, int N, const uint32_t* __restrict__ ndup, const uint2* __restrict__ bboxes,
     const uint32_t* __restrict__ bits, const uint32_t* __restrict__ pair_pos, uint32_t* __restrict__ cursor,
-    int64_t cap, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, unsigned* __restrict__ status)
+    int64_t cap, uint2* __restrict__ kv, unsigned* __restrict__ status)
 {
     extern __shared__ __align__(16) uint32_t hist[];
     const int vi = blockIdx.y;
@@ -499,10 +499,7 @@ __global__ void __launch_bounds__(256) tile_scatter_kernel(
 #pragma unroll
                 for (uint32_t q = 0; q < 8; ++q) {
                     if (!(qb & (1u << q))) continue;
-                    if ((int64_t)p < cap) {
-                        keys[p] = pp[q];
-                        vals[p] = (q << 29) | (uint32_t)i;
-                    }
+                    if ((int64_t)p < cap) kv[p] = make_uint2(pp[q], (q << 29) | (uint32_t)i);
                     ++p;
                 }
             }

@@ -37,7 +37,7 @@ def _render_both(sc, cams, track_max_w=False, grads=None):
     saved = _impl()
     outs = []
     try:
-        for impl in (0, 1):
+        for impl in (0, 1, 2):
             assert L.svr_render_set_impl(impl, saved[1]) == 0
             o = st.render(3, True, True, ts["centers"], ts["lengths"], geos, rgbs, s_val, track_max_w=track_max_w,
                           rgb_per_view=len(cams) > 1)
@@ -54,19 +54,21 @@ def _render_both(sc, cams, track_max_w=False, grads=None):
 def test_pair_forward_is_bit_identical(kind, n_cams, W, H, seed):
     sc = S.scene_small(seed=seed) if kind == "small" else S.scene_tiny(seed=seed)
     cams = S.ring_cameras(n_cams, 3.0, W, H, fovx_deg=50.0, phase=0.4 * seed)
-    a, b = _render_both(sc, cams, track_max_w=True)
+    a, *others = _render_both(sc, cams, track_max_w=True)
     names = ("color", "depth", "normal", "T", "max_w", "tile_last", "n_contrib")
-    for name, x, y in zip(names, a, b):
-        assert torch.equal(x, y), f"{name} differs between the kernels"
+    for impl, b in enumerate(others, 1):
+        for name, x, y in zip(names, a, b):
+            assert torch.equal(x, y), f"{name} differs between the kernels (impl {impl})"
 
 
 def test_pair_forward_bit_identical_mid_size_workload():
     import bench
     sc, cams = bench.make_workload(0, config="mid")
-    a, b = _render_both(sc, cams[:4])
-    for name, x, y in zip(("color", "depth", "normal", "T", "max_w", "tile_last", "n_contrib"), a, b):
-        if x is not None:
-            assert torch.equal(x, y), f"{name} differs between the kernels"
+    a, *others = _render_both(sc, cams[:4])
+    for impl, b in enumerate(others, 1):
+        for name, x, y in zip(("color", "depth", "normal", "T", "max_w", "tile_last", "n_contrib"), a, b):
+            if x is not None:
+                assert torch.equal(x, y), f"{name} differs between the kernels (impl {impl})"
 
 
 def _adjoint_both(sc, cams, lambda_R):
@@ -87,7 +89,7 @@ def _adjoint_both(sc, cams, lambda_R):
     saved = _impl()
     outs = []
     try:
-        for impl in (0, 1):
+        for impl in (0, 1, 2):
             assert L.svr_render_set_impl(saved[0], impl) == 0
             drgbs = torch.zeros(len(cams) * sc.n_vox, 3, device="cuda") if len(cams) > 1 else None
             dvox, ds = st.render_backward(True, True, s_val, T, cat("color"), cat("depth"), cat("normal"), cat("T"),
@@ -113,9 +115,10 @@ def _close_sums(a, b, name):
 def test_pair_adjoint_matches_warp_filter_adjoint(kind, n_cams, W, H, seed, lam):
     sc = S.scene_small(seed=seed) if kind == "small" else S.scene_tiny(seed=seed)
     cams = S.ring_cameras(n_cams, 3.0, W, H, fovx_deg=50.0, phase=0.4 * seed)
-    (d0, s0, r0), (d1, s1, r1) = _adjoint_both(sc, cams, lam)
+    (d0, s0, r0), *others = _adjoint_both(sc, cams, lam)
     assert np.abs(d0).max() > 0
-    _close_sums(d1, d0, "dvox")
-    if r0 is not None:
-        _close_sums(r1, r0, "drgbs")
-    assert abs(s1 - s0) <= 1e-4 * abs(s0) + 1e-9   # per-CTA sums agree; CTA atomics in any order
+    for d1, s1, r1 in others:
+        _close_sums(d1, d0, "dvox")
+        if r0 is not None:
+            _close_sums(r1, r0, "drgbs")
+        assert abs(s1 - s0) <= 1e-4 * abs(s0) + 1e-9   # per-CTA sums agree; CTA atomics in any order
