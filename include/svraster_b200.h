@@ -192,6 +192,11 @@ SVR_API int svr_render_fwd_max_w_views(const svr_view_t* views_host, int n_views
  * its tile's range, and sorts each tile by pair position with one CTA.  R is the record
  * capacity (the device bins min(total, R) records and sets status bit 8 beyond it); no host
  * synchronisation, so it can be captured into a CUDA graph. */
+/* Record total and path OR of a preprocessed batch (one 16-byte read and a stream
+ * synchronisation, no scan): what svr_bin_tiles needs to size its buffers.  No counterpart in
+ * the reference (its count is the scan's last entry, forward.cu:855-880). */
+SVR_API int svr_rendered_total(const void* geom_buffer, int64_t* num_rendered_host, uint64_t* path_or_host,
+                               void* stream);
 SVR_API int svr_pair_order_build(int64_t N, const int64_t* octpaths, uint32_t* pair_pos, int* key_bits_host,
                                  void* ws, size_t ws_bytes, void* stream);
 SVR_API int svr_bin_tiles(const svr_view_t* views_host, int n_views, int N, int64_t R, const uint32_t* pair_pos,
@@ -199,10 +204,11 @@ SVR_API int svr_bin_tiles(const svr_view_t* views_host, int n_views, int N, int6
                           void* image_buffer, void* stream);
 
 /* Which render kernels later launches use (no counterpart in the reference; a process-wide
- * choice read when a launch is issued).  Forward: 1 = record-parallel filter with dense pair
- * evaluation (the default), 0 = per-warp filter with one pixel per lane.  Adjoint: the same
- * choice.  Every choice gives the same forward outputs bit for bit and the same gradients up
- * to the order of their float atomics. */
+ * choice read when a launch is issued), for the forward and the adjoint: 0 = per-warp filter
+ * with one pixel per lane, 1 = record-parallel filter with dense pair evaluation, warps on
+ * 8x4 pixel blocks, 2 (the default) = the same with every warp on a lattice spread over the
+ * tile.  Every choice gives the same forward outputs bit for bit and the same gradients up to
+ * the order of their float atomics. */
 SVR_API int svr_render_set_impl(int fwd_impl, int bwd_impl);
 SVR_API int svr_render_get_impl(int* fwd_impl, int* bwd_impl);
 

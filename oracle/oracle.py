@@ -99,8 +99,8 @@ def set_trace(pixel_trace, voxel_trace=None, bits=32):
     """Record decision flags in later render_fwd / render_bwd calls of that build:
     ``pixel_trace`` uint8[H*W] (flags ORed in: 1 alpha near MIN_ALPHA, 2 transmittance near the
     early stop, 4 a median-depth decision near T = 0.5, 8 an adjoint alpha or depth-derivative
-    switch near its threshold), ``voxel_trace`` uint8[N] (set for voxels that a flagged pixel
-    sends gradient to).  None stops recording.  The arrays are written in place."""
+    switch near its threshold), ``voxel_trace`` uint8[N] (set for voxels that a pixel with a
+    forward flag sends gradient to).  None stops recording.  The arrays are written in place."""
     global _trace_keep
     if pixel_trace is None:
         _trace_keep = None

@@ -56,7 +56,7 @@ void svo_set_pixel_mask(const uint8_t* mask) { g_pixel_mask = mask; }
  * decision with T within TR_MED_BAND of 0.5.  The adjoint ORs TR_ADJ for a pair whose
  * recomputed alpha lies within TR_ALPHA_BAND of MIN_ALPHA or whose depth sub-segment raw
  * alpha lies within TR_RAW_BAND of 0 (the derivative switch), and marks in the voxel trace
- * every voxel that a traced pixel contributes gradient to.  The bands are a few float32
+ * every voxel that a pixel with a forward flag contributes gradient to.  The bands are a few float32
  * ulps of the quantity compared, scaled up by the cancellation in alpha. */
 #define TR_ALPHA 1
 #define TR_STOP 2
@@ -539,7 +539,7 @@ void svo_render_bwd(int W, int H, float tanfovx, float tanfovy, float cx, float 
                 }
                 if (g_trace && dabs((double)alpha - (double)MIN_ALPHA) <= TR_ALPHA_BAND) g_trace[pid] |= TR_ADJ;
                 if (alpha < MIN_ALPHA) continue;   /* lambda_ascending = 0 */
-                if (g_vox_trace && g_trace && g_trace[pid]) g_vox_trace[vid] = 1;
+                if (g_vox_trace && g_trace && (g_trace[pid] & (TR_ALPHA | TR_STOP | TR_MEDIAN))) g_vox_trace[vid] = 1;
                 T = T / (1.f - alpha);
                 real pw = alpha * T;
                 r3 c = rk(rgbs[3 * vid], rgbs[3 * vid + 1], rgbs[3 * vid + 2]);

@@ -350,6 +350,22 @@ extern "C" int svr_count_rendered(int64_t M, void* geom_buffer, int64_t* num_ren
     return SVR_OK;
 }
 
+// Record total and path OR of a preprocessed batch, read without the scan that
+// svr_count_rendered runs for the radix-sort binning (svr_bin_tiles needs no scan).
+extern "C" int svr_rendered_total(const void* geom_buffer, int64_t* num_rendered_host, uint64_t* path_or_host,
+                                  void* stream)
+{
+    if (!geom_buffer) return svr_fail(SVR_ERR_ARG, "rendered_total: null buffer");
+    cudaStream_t st = (cudaStream_t)stream;
+    GeomMeta meta;
+    CUDA_TRY(cudaMemcpyAsync(&meta, geom_buffer, 16, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (meta.total >= (1ull << 32)) return svr_fail(SVR_ERR_CAPACITY, "more than 2^32 duplicated records");
+    if (num_rendered_host) *num_rendered_host = (int64_t)meta.total;
+    if (path_or_host) *path_or_host = meta.path_or;
+    return SVR_OK;
+}
+
 // ------------------------------------------------------------------ binning
 struct KeyFmt {
     int rank_shift;   // low rank bits dropped (all equal to the octant pattern)
@@ -887,7 +903,7 @@ __global__ void __launch_bounds__(256) pack_records_kernel(
 // (render_fwd_pairs_kernel / render_bwd_pairs_kernel) with warps on 8x4 pixel blocks, 2 = the
 // same with every warp on a lattice spread over the tile.  All give the same forward outputs
 // bit for bit and the same gradients up to the order of their float atomics.
-static std::atomic<int> g_fwd_impl{1}, g_bwd_impl{1};
+static std::atomic<int> g_fwd_impl{2}, g_bwd_impl{2};
 extern "C" int svr_render_set_impl(int fwd_impl, int bwd_impl)
 {
     if (fwd_impl < 0 || fwd_impl > 2 || bwd_impl < 0 || bwd_impl > 2) return svr_fail(SVR_ERR_ARG, "render impl");

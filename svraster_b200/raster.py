@@ -65,13 +65,18 @@ class RasterState:
         M = self.N * self.n_views
         if capacity is None:
             R, por = C.c_int64(0), C.c_uint64(0)
-            check(L.svr_count_rendered(M, ptr(self.geom), C.byref(R), C.byref(por), stream_ptr(self.device)),
-                  "svr_count_rendered")
+            if pair_order is not None:     # the per-tile sort needs the total only, no scan
+                check(L.svr_rendered_total(ptr(self.geom), C.byref(R), C.byref(por), stream_ptr(self.device)),
+                      "svr_rendered_total")
+            else:
+                check(L.svr_count_rendered(M, ptr(self.geom), C.byref(R), C.byref(por), stream_ptr(self.device)),
+                      "svr_count_rendered")
             self.num_rendered, self.path_or = int(R.value), int(por.value)
         else:
             if path_or is None:
                 raise ValueError("bin(capacity=...) needs path_or")
-            check(L.svr_scan_rendered(M, ptr(self.geom), stream_ptr(self.device)), "svr_scan_rendered")
+            if pair_order is None:
+                check(L.svr_scan_rendered(M, ptr(self.geom), stream_ptr(self.device)), "svr_scan_rendered")
             self.num_rendered, self.path_or = int(capacity), int(path_or)
         nb = L.svr_binning_buffer_bytes(self.num_rendered, self.total_tiles)
         self.binning = _empty_bytes(nb, self.device)

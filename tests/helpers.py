@@ -44,9 +44,14 @@ def oracle_view(sc, cam, geos, rgbs, n_samp=3, need_depth=True, need_normal=True
     bg = np.asarray(bg, np.float32)
     nd, bb, bits = O.preprocess(cam, sc.vox_center, sc.vox_size, sc.is_leaf)
     keys, vals, ranges = O.binning(cam, sc.octpath, nd, bb, bits)
-    f = O.render_fwd(cam, bg, n_samp, need_depth, need_normal, ranges, vals, bb, sc.vox_center, sc.vox_size,
-                     geos, rgbs, sc.s_val, track_max_w=True)
-    res = dict(n_dup=nd, bbox=bb, bits=bits, keys=keys, vals=vals, ranges=ranges, **f)
+    tr = np.zeros(cam.width * cam.height, np.uint8)
+    O.set_trace(tr)
+    try:
+        f = O.render_fwd(cam, bg, n_samp, need_depth, need_normal, ranges, vals, bb, sc.vox_center, sc.vox_size,
+                         geos, rgbs, sc.s_val, track_max_w=True)
+    finally:
+        O.set_trace(None)
+    res = dict(n_dup=nd, bbox=bb, bits=bits, keys=keys, vals=vals, ranges=ranges, flags=forward_flags(cam, tr), **f)
     if grads is not None:
         dvox, ds = O.render_bwd(cam, bg, need_depth, need_normal, ranges, f["tile_last"], vals, bb, sc.vox_center,
                                 sc.vox_size, geos, rgbs, sc.s_val, f["T"], f["n_contrib"], grads["color"],
@@ -115,3 +120,50 @@ def split_view(arr, views, v, channels):
     n = views[v].width * views[v].height
     a = arr.reshape(-1)[channels * off: channels * (off + n)]
     return a.reshape(channels, views[v].height, views[v].width)
+
+
+# Image parity on the pixels whose forward decisions are not at a threshold (the oracle's
+# trace: alpha within ulps of MIN_ALPHA, T at the early stop or a median-depth decision at
+# T = 0.5): |got - ref| <= 1e-5 of the channel's range everywhere, and <= 1e-5 of |ref| for all
+# but 0.2% of the entries above 1% of the range (float32 evaluations of the same expressions;
+# the device's expf and the host's differ by an ulp, alpha = (phi_e - phi_x) / phi_e cancels).
+IMG_RANGE_TOL, IMG_ELEM_TOL, IMG_ELEM_FRAC = 1e-5, 1e-5, 2e-3
+FLIP_FWD = 1 | 2 | 4
+
+
+def image_parity(got, ref, flagged):
+    """Errors of one plane group [C, ...] on the unflagged pixels: relative to each channel's
+    range, and per element for entries at least 1% of the range."""
+    got = np.asarray(got, np.float64).reshape(np.shape(ref)[0], -1)
+    ref = np.asarray(ref, np.float64).reshape(np.shape(ref)[0], -1)
+    ok = ~np.asarray(flagged).reshape(-1)
+    rng = np.abs(ref).max(axis=1, keepdims=True) + 1e-30
+    err = np.abs(got - ref)[:, ok]
+    r_range = err / rng
+    big = (np.abs(ref) >= 1e-2 * rng)[:, ok]
+    r_elem = (err / (np.abs(ref[:, ok]) + 1e-30))[big]
+    return {"range_rel_max": float(r_range.max()) if r_range.size else 0.0,
+            "elem_rel_max": float(r_elem.max()) if r_elem.size else 0.0,
+            "elem_rel_p999": float(np.quantile(r_elem, 0.999)) if r_elem.size else 0.0,
+            "elem_over_tol": int((r_elem > IMG_ELEM_TOL).sum()), "elements": int(r_elem.size),
+            "bitwise_equal_frac": float((got[:, ok] == ref[:, ok]).mean()) if ok.any() else 1.0}
+
+
+def assert_image_parity(tag, stats):
+    assert stats["range_rel_max"] <= IMG_RANGE_TOL, (tag, stats)
+    assert stats["elem_over_tol"] <= IMG_ELEM_FRAC * max(stats["elements"], 1), (tag, stats)
+
+
+def images_match(got, ref, flagged, tag=""):
+    """Colour, depth, normal and T of one view against a reference render ({name: [C,H,W]})."""
+    out = {}
+    for key in ("color", "depth", "normal", "T"):
+        if key in got and got[key] is not None:
+            out[key] = image_parity(got[key], ref[key], flagged)
+            assert_image_parity(f"{tag} {key}", out[key])
+    return out
+
+
+def forward_flags(cam, trace):
+    """Pixels [H, W] with a forward decision at a threshold, from an oracle pixel trace."""
+    return ((np.asarray(trace) & FLIP_FWD) > 0).reshape(cam.height, cam.width)

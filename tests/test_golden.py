@@ -27,28 +27,46 @@ def _check_inputs(g, inp):
     assert str(g["digest"]) == digest(inp), "synthetic inputs changed; regenerate the golden fixtures"
 
 
-# Reference float32 vs our float32: identical expression shapes; only expf / rsqrtf ulps and
-# atomic summation order differ.
-IMG_RTOL, IMG_ATOL, BAD = 1e-4, 2e-5, 2e-3
+def _flags(case, inp, geos, rgbs):
+    """Pixels whose forward decisions sit at a threshold, from the oracle's trace of this case."""
+    from oracle import oracle as O
+    from tests.helpers import forward_flags
+    sc, cam = inp["scene"], inp["cam"]
+    nd, bb, bits = O.preprocess(cam, sc.vox_center, sc.vox_size, sc.is_leaf)
+    _, vals, ranges = O.binning(cam, sc.octpath, nd, bb, bits)
+    tr = np.zeros(cam.width * cam.height, np.uint8)
+    O.set_trace(tr)
+    try:
+        O.render_fwd(cam, np.asarray(case["bg"], np.float32), case["vox_geo_mode"], True, True, ranges, vals, bb,
+                     sc.vox_center, sc.vox_size, geos, rgbs, sc.s_val)
+    finally:
+        O.set_trace(None)
+    return forward_flags(cam, tr)
 
 
-def _compare_render(res, g, cam):
+def _compare_render(res, g, cam, flagged, tag):
+    """Images against the reference's own extension on the pixels with no decision at a
+    threshold (tests.helpers.image_parity: 1e-5 of the range everywhere, 1e-5 per element for
+    99.8% of the entries); a decision at a threshold may move a pixel's last contributor."""
+    from tests.helpers import images_match
     H, W = cam.height, cam.width
-    from tests.helpers import assert_close
-    assert_close("color", res["color"].reshape(3, H, W), g["color"], IMG_RTOL, IMG_ATOL, BAD)
-    assert_close("T", res["T"].reshape(1, H, W), g["T"], IMG_RTOL, IMG_ATOL, BAD)
-    assert_close("depth", res["depth"].reshape(4, H, W), g["depth"], IMG_RTOL, 1e-4, BAD)
-    assert_close("normal", res["normal"].reshape(3, H, W), g["normal"], IMG_RTOL, 1e-4, BAD)
-    assert (np.asarray(res["n_contrib"]).reshape(-1) != g["n_contrib"]).mean() <= BAD
+    got = {k: np.asarray(res[k]).reshape(ch, H, W) for k, ch in (("color", 3), ("T", 1), ("depth", 4), ("normal", 3))}
+    images_match(got, g, flagged, tag)
+    nc_bad = np.asarray(res["n_contrib"]).reshape(-1) != g["n_contrib"]
+    assert not (nc_bad & ~flagged.reshape(-1)).any()
 
 
 def _compare_grads(dvox, ds, g, n_vox):
+    """Gradients: the same per-pair terms summed in another order (the reference adds with
+    atomics in schedule order): within 1e-5 of the column's largest entry at the 99.9th
+    percentile and 1e-4 everywhere; dL/ds (one sum over every pair) within 2e-5."""
     ref = np.zeros((n_vox, 12), np.float32)
     ref[g["dvox_rows"]] = g["dvox"]
     scale = np.abs(ref).max(0) + 1e-12
     err = np.abs(np.asarray(dvox) - ref) / scale
-    assert np.quantile(err, 0.999) < 1e-3, np.quantile(err, 0.999)
-    assert abs(float(ds) - float(g["ds"][0])) <= 1e-3 * abs(float(g["ds"][0])) + 1e-3
+    assert np.quantile(err, 0.999) <= 1e-5, np.quantile(err, 0.999)
+    assert err.max() <= 1e-4, err.max()
+    assert abs(float(ds) - float(g["ds"][0])) <= 2e-5 * abs(float(g["ds"][0])) + 1e-7
 
 
 @pytest.mark.parametrize("name", list(CASES))
@@ -80,7 +98,7 @@ def test_oracle_matches_reference_goldens(name):
     n_samp = {3: 3, 2: 2, 1: 1}[case["vox_geo_mode"]]
     f = O.render_fwd(cam, bg, n_samp, True, True, ranges, vals, bb, sc.vox_center, sc.vox_size, geos, rgbs,
                      sc.s_val, track_max_w=True)
-    _compare_render(f, g, cam)
+    _compare_render(f, g, cam, _flags(case, inp, geos, rgbs), f"oracle {name}")
     dvox, ds = O.render_bwd(cam, bg, True, True, ranges, g["tile_last"], vals, bb, sc.vox_center, sc.vox_size, geos,
                             rgbs, sc.s_val, g["T"], g["n_contrib"], grads["color"], grads["depth"], grads["normal"],
                             grads["T"], case["lambda_R_concen"], grads["gt"])
@@ -205,5 +223,5 @@ def test_library_matches_reference_goldens(name):
     assert np.array_equal(ranges[ne], g["ranges"][ne])
     res = {k: out[k].cpu().numpy() for k in ("color", "T", "depth", "normal")}
     res["n_contrib"] = nc
-    _compare_render(res, g, cam)
+    _compare_render(res, g, cam, _flags(case, inp, geos, rgbs), f"library {name}")
     _compare_grads(out["dvox"].cpu().numpy(), out["ds"].item(), g, sc.n_vox)

@@ -216,7 +216,13 @@ def test_adjoint_matches_fp64_central_differences_mid():
                 "p95": float(np.quantile(rel, 0.95)), "p99": float(np.quantile(rel, 0.99)),
                 "max": float(rel.max()), "frac_below_1e-4": float((rel < 1e-4).mean()),
                 "frac_below_1e-3": float((rel < 1e-3).mean())}
+    # probes where the exact FP64 adjoint itself disagrees with the central difference sit at a
+    # discrete decision within the step h (alpha at MIN_ALPHA, T at the early stop): excluded
+    fd_scale = np.maximum(np.abs(fd), 1e-3 * np.abs(fd).max())
+    smooth = np.abs(a64 - fd) / fd_scale <= 1e-3
     report = {"probes": int(len(rows)), "grid_probes": int((kinds == "grid").sum()),
+              "probes_at_decisions": int((~smooth).sum()),
+              "gpu_f32_vs_fd_smooth_probes": stats(gpu[smooth], fd[smooth]),
               "sh0_probes": int((kinds == "sh0").sum()), "h": H_STEP,
               "gpu_f32_vs_fd": stats(gpu, fd), "fp64_adjoint_vs_fd": stats(a64, fd),
               "gpu_f32_vs_fp64_adjoint": stats(gpu, a64), "reference_order_f32_vs_fp64_adjoint": stats(a32, a64)}
@@ -230,6 +236,8 @@ def test_adjoint_matches_fp64_central_differences_mid():
     g64, r64 = report["gpu_f32_vs_fp64_adjoint"], report["reference_order_f32_vs_fp64_adjoint"]
     assert g64["median"] < 2e-4, report
     assert g64["p95"] < max(2e-3, 2.0 * r64["p95"]), report
-    # against finite differences the median holds; the far tail is shared with the FP64
-    # adjoint (discrete decisions at the early-stop and MIN_ALPHA thresholds)
-    assert report["gpu_f32_vs_fd"]["median"] < 2e-4, report
+    # against finite differences: median within 1e-4 over all probes; the far tail is shared
+    # with the FP64 adjoint (discrete decisions at the early-stop and MIN_ALPHA thresholds)
+    assert report["gpu_f32_vs_fd"]["median"] <= 1e-4, report
+    assert report["gpu_f32_vs_fd_smooth_probes"]["median"] <= 1e-4, report
+    assert report["probes_at_decisions"] <= 0.2 * report["probes"], report

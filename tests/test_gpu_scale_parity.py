@@ -24,6 +24,8 @@ import numpy as np
 import pytest
 import torch
 
+from tests.helpers import assert_image_parity, image_parity
+
 pytestmark = pytest.mark.gpu
 
 REPORT = {}
@@ -88,17 +90,12 @@ def _check_binning(O, sc, cam, v, st_fields, tiles, N):
 
 
 def _image_errors(name, got, ref, flagged, rtol):
-    """Per-element relative error |got - ref| / |ref| on unflagged pixels, with entries of
-    |ref| below 1e-3 of the plane's largest compared absolutely at that scale."""
-    got = got.astype(np.float64).reshape(got.shape[0], -1)
-    ref = ref.astype(np.float64).reshape(ref.shape[0], -1)
-    ok = ~flagged.reshape(-1)
-    scale = np.maximum(np.abs(ref), 1e-3 * np.abs(ref).max(axis=1, keepdims=True) + 1e-30)
-    rel = (np.abs(got - ref) / scale)[:, ok]
-    stats = {"max": float(rel.max()) if rel.size else 0.0, "p999": float(np.quantile(rel, 0.999)) if rel.size else 0.0,
-             "bitwise_equal_frac": float((got[:, ok] == ref[:, ok]).mean()) if rel.size else 1.0,
-             "n_over": int((rel > rtol).sum())}
-    return stats
+    return image_parity(got, ref, flagged)
+
+
+def _assert_images(tag, stats):
+    for key in ("color", "depth", "normal", "T"):
+        assert_image_parity(f"{tag} {key}", stats[key])
 
 
 FLIP_FWD = 1 | 2 | 4
@@ -150,18 +147,24 @@ def test_mid_size_workload_all_views(oracle, views_checked):
         stats["flagged_pixels"] = int(flagged.sum())
         stats["pixels"] = H * W
         _report(f"mid_view{v}_images", stats)
+        _assert_images(f"mid view {v}", stats)
+        assert stats["n_contrib_differs_unflagged"] == 0
+        assert stats["flagged_pixels"] <= 0.01 * H * W
         # the adjoint of this view alone (single-view launch: its gradients only)
         g = upstream_grads(H, W, seed=40 + v)[0]
         from tests.helpers import cuda_views
         out = cuda_views(sc, [cam], geos, [rgbs[v]], grads_list=[g])
         dv = out["dvox"].cpu().numpy().astype(np.float64)
-        vt = np.zeros(N, np.uint8)
         O.set_trace(tr)
         ref, ds_ref = O.render_bwd(cam, np.zeros(3, np.float32), True, True, ranges_v, f["tile_last"], vals_v, bb,
                                    sc.vox_center, sc.vox_size, geos, rgbs[v], sc.s_val, f["T"], f["n_contrib"],
                                    g["color"], g["depth"], g["normal"], g["T"])
+        # |terms| per voxel, and the voxels that pixels with a forward flag send gradient to
+        # (the adjoint's own derivative switches are counted, not excluded: they change only
+        # small terms)
         absum = np.zeros((N, 12), np.float32)
-        O.set_trace(tr, vt)
+        vt_fwd = np.zeros(N, np.uint8)
+        O.set_trace(tr, vt_fwd)
         O.set_abs_sum(absum)
         O.render_bwd(cam, np.zeros(3, np.float32), True, True, ranges_v, f["tile_last"], vals_v, bb, sc.vox_center,
                      sc.vox_size, geos, rgbs[v], sc.s_val, f["T"], f["n_contrib"], g["color"], g["depth"],
@@ -169,20 +172,23 @@ def test_mid_size_workload_all_views(oracle, views_checked):
         O.set_trace(None)
         O.set_abs_sum(None)
         touched = np.abs(absum).sum(1) > 0
-        flagged_v = vt > 0
-        scale = absum.astype(np.float64) + 1e-30
-        rel = np.abs(dv - ref) / scale
-        ok = touched & ~flagged_v
-        bad = touched & flagged_v
-        gstats = {"voxels": int(touched.sum()), "flagged_voxels": int(bad.sum()),
-                  "rel_to_abs_sum_max_unflagged": float(rel[ok].max()) if ok.any() else 0.0,
-                  "rel_to_abs_sum_p9999_unflagged": float(np.quantile(rel[ok], 0.9999)) if ok.any() else 0.0,
-                  "rel_to_abs_sum_max_flagged": float(rel[bad].max()) if bad.any() else 0.0,
-                  "rel_elementwise_p99_unflagged": float(np.quantile(
-                      (np.abs(dv - ref) / (np.abs(ref) + 1e-30))[ok][np.abs(ref[ok]) > 1e-3 * np.abs(ref).max()], 0.99)),
+        ok = touched & (vt_fwd == 0)
+        big = np.abs(ref) >= 1e-3 * np.abs(ref).max(0, keepdims=True)
+        rel_e = (np.abs(dv - ref) / (np.abs(ref) + 1e-30))[ok[:, None] & big]
+        rel_s = (np.abs(dv - ref) / (absum.astype(np.float64) + 1e-30))[ok]
+        gstats = {"voxels": int(touched.sum()), "voxels_of_flagged_pixels": int((touched & (vt_fwd > 0)).sum()),
+                  "elem_rel_median": float(np.median(rel_e)), "elem_rel_p99": float(np.quantile(rel_e, 0.99)),
+                  "elem_rel_p999": float(np.quantile(rel_e, 0.999)),
+                  "rel_to_abs_sum_p99": float(np.quantile(rel_s, 0.99)),
+                  "rel_to_abs_sum_p9999": float(np.quantile(rel_s, 0.9999)),
                   "ds": [float(out["ds"].item()), float(ds_ref)],
                   "trace_pixels": {str(b): int(((tr & b) > 0).sum()) for b in (1, 2, 4, 8)}}
         _report(f"mid_view{v}_adjoint", gstats)
+        # gradients: sums of many terms in another order and with the transmittance recovered
+        # by division (which amplifies an ulp where alpha is near 1, in the reference as here)
+        assert gstats["elem_rel_median"] <= 1e-5, gstats
+        assert gstats["elem_rel_p99"] <= 1e-3, gstats
+        assert abs(gstats["ds"][0] - gstats["ds"][1]) <= 1e-4 * abs(gstats["ds"][1]) + 1e-6, gstats
 
 
 def test_batched_workload_one_view_per_resolution(oracle):
@@ -226,4 +232,6 @@ def test_batched_workload_one_view_per_resolution(oracle):
             got = planes[key][ch * p0: ch * p1].reshape(ch, H, W)
             stats[key] = _image_errors(key, got, f[key], flagged, 1e-5)
         summary[f"{W}x{H}"] = stats
+        _assert_images(f"batched view {v} {W}x{H}", stats)
+        assert stats["flagged_pixels"] <= 0.01 * H * W
     _report("batched_views", summary)
