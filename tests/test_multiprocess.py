@@ -67,6 +67,7 @@ def _view_gradients(sc, cams, views):
     gradients (corner terms scattered by vox_key) and the sh0 / shs gradients of the SH
     adjoint, in one flat float64 vector."""
     from oracle import oracle as O
+    O.set_threads(1)                              # deterministic sums (other tests may raise it)
     N = sc.n_vox
     geos = O.gather_geo(np.arange(N), sc.vox_key, sc.geo_grid_pts, N)
     dgrid = np.zeros(len(sc.geo_grid_pts), np.float64)
