@@ -520,6 +520,24 @@ class StdoutToStderr:
         os.close(self.saved)
 
 
+def reference_extension():
+    """The reference's own CUDA extension (oracle/_ref/svraster_ref_C.so, built from its
+    unmodified sources by oracle/build_ref.py), or None where it was not built."""
+    import importlib.util
+    so = os.path.join(ROOT, "oracle", "_ref", "svraster_ref_C.so")
+    if not os.path.exists(so):
+        return None
+    spec = importlib.util.spec_from_file_location("svraster_ref_C", so)
+    mod = importlib.util.module_from_spec(spec)
+    with StdoutToStderr():
+        spec.loader.exec_module(mod)
+    return mod
+
+
+REF_UNAVAILABLE = {"unavailable": "the reference extension was not built (oracle/build_ref.py needs the reference "
+                                  "sources on the build machine)"}
+
+
 def run_reference_cuda(scene, cams, dev, steps=3, warmup=1):
     """See _run_reference_cuda; the reference extension prints to stdout (valid_gradient_table),
     which is kept off the bench's stdout."""
@@ -536,15 +554,10 @@ def _run_reference_cuda(scene, cams, dev, steps=3, warmup=1):
     dense-grid key and Adam on grid / sh0 / shs.  A baseline leg, timed after our own timed
     regions with CUDA events (median step).  Returns {"unavailable": why} when the built
     extension is not present."""
-    import importlib.util
     import torch
-    so = os.path.join(ROOT, "oracle", "_ref", "svraster_ref_C.so")
-    if not os.path.exists(so):
-        return {"unavailable": "the reference extension was not built (oracle/build_ref.py needs the reference "
-                               "sources on the build machine)"}
-    spec = importlib.util.spec_from_file_location("svraster_ref_C", so)
-    R_ = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(R_)
+    R_ = reference_extension()
+    if R_ is None:
+        return dict(REF_UNAVAILABLE)
     t = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
     octpath, centers, lengths = t(scene.octpath, torch.int64), t(scene.vox_center), t(scene.vox_size)
     is_leaf = t(scene.is_leaf, torch.uint8)
@@ -816,6 +829,24 @@ def run_regularisers(step, scene, dev):
                                          False, grad))
     out.update({"points_loss_ms": round(pl_ms, 4), "points_loss_Mpoints_per_s": round(REG_POINTS / pl_ms / 1e3, 1),
                 "compulsory_bytes": {"voxel_gradient": vg_bytes, "total_variation": tv_bytes}})
+    # the reference's own extension on the same inputs, timed the same way
+    R_ = reference_extension()
+    if R_ is None:
+        out["reference_cuda"] = dict(REF_UNAVAILABLE)
+    else:
+        with StdoutToStderr():
+            ref = {"voxel_gradient_ms": timed(lambda: R_.voxel_gradient_bw(step.grid, step.vox_key, vsi, active, 1e-3,
+                                                                           False, False, grad)),
+                   "total_variation_ms": timed(lambda: R_.total_variation_bw(step.grid, step.vox_key, 1e-3, vsi,
+                                                                             False, False, grad)),
+                   "total_variation_sparse_ms": timed(lambda: R_.total_variation_bw(step.grid, step.vox_key, 1e-3, vsi,
+                                                                                    False, True, grad)),
+                   "points_loss_ms": timed(lambda: R_.points_loss_bw(pts, step.grid, step.vox_key,
+                                                                     step.grid_voxel_coord, step.grid_voxel_size, res,
+                                                                     step.grid_mask, step.grid_keys, step.grid2voxel,
+                                                                     1e-3, 1.0, True, False, grad))}
+        out["reference_cuda"] = {k: round(v, 4) for k, v in ref.items()}
+        out["speedup_vs_reference_cuda"] = {k[:-3]: round(v / out[k], 2) for k, v in ref.items() if out.get(k)}
     return out
 
 
@@ -925,9 +956,23 @@ def run_checkpoint(scene, dev):
     deq = dict(sd)
     io.dequantize_state_dict(deq)
     err = float(max((deq[k] - fields[k]).abs().mean().item() / fields[k].abs().mean().item() for k in fields))
-    return {"values": n, "codebooks": 1 + fields["_sh0"].shape[1] + fields["_shs"].shape[1],
-            "quantize_ms": round(q_ms, 2), "quantize_Mvalues_per_s": round(n / q_ms / 1e3, 1),
-            "dequantize_ms": round(d_ms, 3), "mean_rel_abs_error": round(err, 5)}
+    out = {"values": n, "codebooks": 1 + fields["_sh0"].shape[1] + fields["_shs"].shape[1],
+           "quantize_ms": round(q_ms, 2), "quantize_Mvalues_per_s": round(n / q_ms / 1e3, 1),
+           "dequantize_ms": round(d_ms, 3), "mean_rel_abs_error": round(err, 5)}
+    # CPU baseline: the reference builds the codebook with torch ops (io.py:123-167), restated
+    # bit for bit by the C oracle, timed single-threaded on a sample of the same columns
+    from oracle import oracle as O
+    cols = [scene.geo_grid_pts.reshape(-1)] + [scene.sh0[:, j] for j in range(scene.sh0.shape[1])]
+    cols = [np.ascontiguousarray(c, dtype=np.float32) for c in cols]
+    m = sum(c.size for c in cols)
+    t0 = time.perf_counter()
+    for c in cols:
+        O.quantize(c)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    out["cpu_baseline"] = {"value": round(m / cpu_ms / 1e3, 3), "unit": "Mvalues/s (quantize)", "cores": 1,
+                           "kind": "port", "sample": f"the grid and 3 sh0 columns ({m} of {n} values), "
+                                                     f"{cpu_ms / 1e3:.1f} s; C oracle of io.py:123-167"}
+    return out
 
 
 def oracle_view_step(scene, cam, threads):

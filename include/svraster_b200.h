@@ -184,8 +184,9 @@ SVR_API int svr_render_fwd_max_w_views(const svr_view_t* views_host, int n_views
 
 /* Binning without a global radix sort (no counterpart in the reference; same result as
  * svr_bin_and_sort, whose order is the one of cuda/src/forward.cu:749-829, 882-939).
- * svr_pair_order_build (once per octree): pair_pos u32[8N] = the position of every (voxel,
- * octant) pair in the order of the full octree rank, ties by voxel id then octant;
+ * svr_pair_order_build (once per octree): pair_pos u32[8N], octant-major (entry q*N + v) = the
+ * position of the pair (voxel v, octant q) in the order of the full octree rank, ties by voxel
+ * id then octant;
  * *key_bits_host = bits of a position.  The workspace is svr_rank_table_workspace_bytes(N).
  * svr_bin_tiles (per step, after svr_preprocess): counts the records of every tile, scans
  * the counts into tile ranges and the heavy-first launch order, scatters every record into
@@ -211,6 +212,11 @@ SVR_API int svr_bin_tiles(const svr_view_t* views_host, int n_views, int N, int6
  * the order of their float atomics. */
 SVR_API int svr_render_set_impl(int fwd_impl, int bwd_impl);
 SVR_API int svr_render_get_impl(int* fwd_impl, int* bwd_impl);
+
+/* Stage timing, no counterpart in the reference: a CUDA event (cudaEvent_t, or null for none)
+ * that every later svr_render_fwd records on its stream between its record packing launch and
+ * its render launch.  A process-wide setting; leave it null while a CUDA graph is captured. */
+SVR_API int svr_set_pack_event(void* event);
 
 /* Work measurement, no counterpart in the reference: the forward render of
  * svr_render_fwd (three sub-samples, depth and normal on) on records already packed by an

@@ -68,6 +68,7 @@ _SIGS = {
     "svr_unpack_binning": (_I, [_P, _I64, _I, _P, _I64, _P, _P, _P, _P, _P]),
     "svr_render_set_impl": (_I, [_I, _I]),
     "svr_render_get_impl": (_I, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "svr_set_pack_event": (_I, [_P]),
     "svr_rendered_total": (_I, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_uint64), _P]),
     "svr_bin_tiles": (_I, [_P, _I, _I, _I64, _P, _I, _P, _P, _SZ, _P, _P]),
     "svr_pair_order_build": (_I, [_I64, _P, _P, C.POINTER(C.c_int), _P, _SZ, _P]),

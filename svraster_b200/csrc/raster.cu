@@ -815,7 +815,7 @@ extern "C" int svr_pair_order_build(int64_t N, const int64_t* octpaths, uint32_t
     LAUNCH_CHECK();
     size_t tb = w.tmp_bytes;
     CUDA_TRY(cub::DeviceRadixSort::SortPairs(base + w.tmp, tb, kin, kout, vin, vout, (int)n, 0, RANK_BITS, st));
-    pair_pos_kernel<<<nb, 256, 0, st>>>(n, vout, pair_pos);
+    pair_pos_kernel<<<nb, 256, 0, st>>>(N, vout, pair_pos);
     LAUNCH_CHECK();
     int bits = 1;
     while (bits < 32 && (1ll << bits) < n) ++bits;
@@ -901,12 +901,13 @@ __global__ void __launch_bounds__(256) pack_records_kernel(
 // Which render kernels the launches use: 0 = the warp-filter kernels (render_fwd_kernel /
 // render_bwd_kernel), 1 = record-parallel filter with dense pair evaluation
 // (render_fwd_pairs_kernel / render_bwd_pairs_kernel) with warps on 8x4 pixel blocks, 2 = the
-// same with every warp on a lattice spread over the tile.  All give the same forward outputs
+// same with every warp on a lattice spread over the tile, 3 = the same with the pairs of a slot
+// numbered and evaluated over the whole CTA.  All give the same forward outputs
 // bit for bit and the same gradients up to the order of their float atomics.
 static std::atomic<int> g_fwd_impl{2}, g_bwd_impl{2};
 extern "C" int svr_render_set_impl(int fwd_impl, int bwd_impl)
 {
-    if (fwd_impl < 0 || fwd_impl > 2 || bwd_impl < 0 || bwd_impl > 2) return svr_fail(SVR_ERR_ARG, "render impl");
+    if (fwd_impl < 0 || fwd_impl > 3 || bwd_impl < 0 || bwd_impl > 3) return svr_fail(SVR_ERR_ARG, "render impl");
     g_fwd_impl.store(fwd_impl);
     g_bwd_impl.store(bwd_impl);
     return SVR_OK;
@@ -918,19 +919,28 @@ extern "C" int svr_render_get_impl(int* fwd_impl, int* bwd_impl)
     return SVR_OK;
 }
 
+// Stage timing: an event recorded by svr_render_fwd on its stream between the record packing
+// launch and the render launch (null = none).
+static std::atomic<cudaEvent_t> g_pack_event{nullptr};
+extern "C" int svr_set_pack_event(void* event)
+{
+    g_pack_event.store((cudaEvent_t)event);
+    return SVR_OK;
+}
+
 #ifndef SVR_PBWD_RING
 #define SVR_PBWD_RING 3
 #endif
 #ifndef SVR_PBWD_MINB
 #define SVR_PBWD_MINB 3
 #endif
-template <bool DEPTH, bool NORMAL, bool RCONC, bool LATTICE = true>
+template <bool DEPTH, bool NORMAL, bool RCONC, bool LATTICE = true, bool CTAW = false>
 static int launch_bwd_pairs(int T, int N, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
                             const uint32_t* tl, const uint32_t* nc, const Rec* recs, const float* s_val,
                             const float* out_T, const float* dc, const float* dd, const float* dn, const float* dT,
                             float lam, const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status)
 {
-    auto k = render_bwd_pairs_kernel<DEPTH, NORMAL, RCONC, SVR_PBWD_RING, SVR_PBWD_MINB, LATTICE>;
+    auto k = render_bwd_pairs_kernel<DEPTH, NORMAL, RCONC, SVR_PBWD_RING, SVR_PBWD_MINB, LATTICE, CTAW>;
     const int smem = (int)sizeof(PairBwdSmem<SVR_PBWD_RING>);
     static std::atomic<unsigned long long> done{0};
     int rc = ensure_smem(k, smem, done);
@@ -947,13 +957,13 @@ static int launch_bwd_pairs(int T, int N, cudaStream_t st, const Views& V, const
 #ifndef SVR_PFWD_MINB
 #define SVR_PFWD_MINB 4
 #endif
-template <int NS, bool DEPTH, bool NORMAL, bool MAXW, bool COUNT, bool LATTICE = true>
+template <int NS, bool DEPTH, bool NORMAL, bool MAXW, bool COUNT, bool LATTICE = true, bool CTAW = false>
 static int launch_fwd_pairs(int T, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
                             const Rec* recs, const float* s_val, uint32_t* tile_last, uint32_t* n_contrib,
                             float* color, float* depth, float* normal, float* outT, float* max_w, int64_t mw_stride,
                             unsigned* status, unsigned long long* pair_count)
 {
-    auto k = render_fwd_pairs_kernel<NS, DEPTH, NORMAL, MAXW, SVR_PFWD_RING, SVR_PFWD_MINB, COUNT, LATTICE>;
+    auto k = render_fwd_pairs_kernel<NS, DEPTH, NORMAL, MAXW, SVR_PFWD_RING, SVR_PFWD_MINB, COUNT, LATTICE, CTAW>;
     const int smem = (int)sizeof(PairFwdSmem<SVR_PFWD_RING>);
     static std::atomic<unsigned long long> done{0};
     int rc = ensure_smem(k, smem, done);
@@ -1047,6 +1057,11 @@ static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint32_t* or
         return launch_fwd_pairs<NS, DEPTH, NORMAL, MAXW, false, true>(T, st, V, order, ranges, recs, s_val,
                                                                       tile_last, n_contrib, color, depth, normal,
                                                                       outT, max_w, mw_stride, status, nullptr);
+    if (g_fwd_impl.load() == 3)
+        return launch_fwd_pairs<NS, DEPTH, NORMAL, MAXW, false, true, true>(T, st, V, order, ranges, recs, s_val,
+                                                                            tile_last, n_contrib, color, depth,
+                                                                            normal, outT, max_w, mw_stride, status,
+                                                                            nullptr);
 #define FWD_CFG_ARGS T, st, V, order, ranges, recs, s_val, tile_last, n_contrib, color, depth, normal, outT, max_w, mw_stride, status
     if constexpr (NS == 3 && DEPTH && NORMAL && !MAXW) {
         int cfg = g_fwd_cfg.load();
@@ -1137,6 +1152,10 @@ static int render_fwd_impl(const svr_view_t* views_host, int n_views, int N, int
             status);
         LAUNCH_CHECK();
     }
+    if (cudaEvent_t ev = g_pack_event.load()) {
+        const cudaError_t e = cudaEventRecord(ev, st);
+        if (e != cudaSuccess) return svr_fail(SVR_ERR_CUDA, cudaGetErrorString(e));
+    }
     uint32_t* tl = (uint32_t*)(im + IL.tile_last);
     uint32_t* nc = (uint32_t*)(im + IL.n_contrib);
     const bool D = need_depth != 0, Nm = need_normal != 0, MW = max_w != nullptr;
@@ -1224,6 +1243,7 @@ static int launch_bwd(int T, int N, cudaStream_t st, const Views& V, const uint3
 #define BWD_CFG_ARGS T, N, st, V, order, ranges, tl, nc, recs, s_val, out_T, dc, dd, dn, dT, lam, gt, dvox, drgbs, ds, status
     if (g_bwd_impl.load() == 1) return launch_bwd_pairs<DEPTH, NORMAL, RCONC, false>(BWD_CFG_ARGS);
     if (g_bwd_impl.load() == 2) return launch_bwd_pairs<DEPTH, NORMAL, RCONC, true>(BWD_CFG_ARGS);
+    if (g_bwd_impl.load() == 3) return launch_bwd_pairs<DEPTH, NORMAL, RCONC, true, true>(BWD_CFG_ARGS);
     if constexpr (DEPTH && NORMAL) {
         int cfg = g_bwd_cfg.load();
         if (cfg == 0 && T < SMALL_LAUNCH_TILES) cfg = 2;          // 4 x 2

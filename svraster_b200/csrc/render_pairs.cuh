@@ -40,6 +40,11 @@ struct alignas(128) PairFwdSmem {
     float4 nrm[BATCH];           // per record: corner-difference normal, its reciprocal norm
     float2 res[NWARP][32];       // alpha and depth value of the pairs of a warp's window
     uint32_t red[NWARP];
+    // CTA-wide pair windows: the pairs of a window (two buffers), each thread's pair offset
+    // within its warp, and the warps' pair counts
+    float2 cres[2][BLOCK];
+    int ppre[BLOCK];
+    int wcnt[NWARP];
 };
 
 // Position of the k-th (from 0) set bit of w (k < popc(w)).
@@ -75,8 +80,77 @@ __device__ __forceinline__ bool filter_hit(const float4 pr, uint32_t q, float3 c
     return !(ab.x > ab.y);
 }
 
+// Owner of pair i (< the CTA's pair total) of a CTA-wide numbering (thread-major, each
+// thread's pairs in record order): the thread t and i's rank k among t's pairs, from the
+// warps' pair counts and the per-thread offsets within the warp.
+__device__ __forceinline__ void cta_pair_owner(const int* wcnt, const int* ppre, int i, int& t, int& k) {
+    int acc = 0, ow = 0, oacc = 0;
+#pragma unroll
+    for (int q = 0; q < NWARP; ++q) {
+        if (acc <= i) { ow = q; oacc = acc; }
+        acc += wcnt[q];
+    }
+    const int x = i - oacc;
+    const int* pp = ppre + ow * 32;
+    int l = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1)
+        if (pp[l + step] <= x) l += step;
+    t = ow * 32 + l;
+    k = x - pp[l];
+}
+
+// The evaluation of one (pixel, record) pair of the forward (forward.cu:255-306, as
+// render_fwd_kernel): alpha and the depth value.
+template <int NS, bool DEPTH>
+__device__ __forceinline__ float2 fwd_pair_eval(const Rec& r, float3 ro, float3 rd, float3 rd_inv, float s_val) {
+    const float3 vox_c = f3(r.cx, r.cy, r.cz);
+    const float vox_l = r.len;
+    const float2 ab = ray_box(vox_c, vox_l, ro, rd_inv);
+    const float a = ab.x, bb = ab.y;
+    float g[8];
+#pragma unroll
+    for (int qq = 0; qq < 8; ++qq) g[qq] = r.g[qq];
+    float w8[8];
+    float local_a[NS > 1 ? NS : 1];
+    const float vox_l_inv = 1.f / vox_l;
+    const float3 p_entry = ro + a * rd;
+    const float3 P_step = (bb - a) * rd / (float)NS;
+    const float3 qt_entry = (p_entry - (vox_c - 0.5f * vox_l)) * vox_l_inv;
+    const float3 qt_step = P_step * vox_l_inv;
+    tri_weights(qt_entry, w8);
+    float phi_former = 1.f / (1.f + expf(-s_val * interp8(g, w8)));
+    const float phi_entry = phi_former;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const float3 qt_curr = qt_entry + qt_step * (float)(s + 1);
+        tri_weights(qt_curr, w8);
+        const float phi_curr = 1.f / (1.f + expf(-s_val * interp8(g, w8)));
+        if (DEPTH && NS > 1) local_a[s] = fmaxf((phi_former - phi_curr) / (phi_former + 1e-6f), 0.f);
+        phi_former = phi_curr;
+    }
+    const float alpha = fmaxf((phi_entry - phi_former) / (phi_entry + 1e-6f), 0.f);
+    float dval = 0.f;
+    if (DEPTH && !(alpha < MIN_ALPHA)) {
+        if (NS == 3) {
+            const float step_sz = 0.3333333f * (bb - a);
+            const float a0 = local_a[0], a1 = local_a[NS > 1 ? 1 : 0], a2 = local_a[NS > 2 ? 2 : 0];
+            const float t0 = a + 0.5f * step_sz, t1 = a + 1.5f * step_sz, t2 = a + 2.5f * step_sz;
+            dval = a0 * t0 + (1.f - a0) * a1 * t1 + (1.f - a0) * (1.f - a1) * a2 * t2;
+        } else if (NS == 2) {
+            const float step_sz = 0.5f * (bb - a);
+            const float a0 = local_a[0], a1 = local_a[NS > 1 ? 1 : 0];
+            const float t0 = a + 0.5f * step_sz, t1 = a + 1.5f * step_sz;
+            dval = a0 * t0 + (1.f - a0) * a1 * t1;
+        } else {
+            dval = alpha * 0.5f * (a + bb);
+        }
+    }
+    return make_float2(alpha, dval);
+}
+
 template <int NS, bool DEPTH, bool NORMAL, bool MAXW, int RING = 3, int MINB = 4, bool COUNT = false,
-          bool LATTICE = true>
+          bool LATTICE = true, bool CTAW = false>
 __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
     const __grid_constant__ Views V, const uint32_t* __restrict__ order, const uint2* __restrict__ ranges,
     const Rec* __restrict__ recs, const float* __restrict__ s_ptr, uint32_t* __restrict__ tile_last,
@@ -207,130 +281,173 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
         }
         // the masks are complete; stop streaming once every pixel is done (as of the last slot)
         if (__syncthreads_and(done)) break;
-        // ---------------------------------------------------------------- P + C, per warp
-        uint32_t m[4], mc[4];
+        if constexpr (CTAW) {
+            // ------------------------------------------------------------ P + C, CTA-wide
+            // pairs numbered over the whole CTA (thread-major); each window of BLOCK pairs is
+            // evaluated one pair per thread, then every pixel folds its pairs of the window
+            uint32_t mc[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) { m[k] = mc[k] = S.mask[p_own][k]; S.mask[p_own][k] = 0u; }
-        const int cnt_own = __popc(m[0]) + __popc(m[1]) + __popc(m[2]) + __popc(m[3]);
-        int incl = cnt_own;
+            for (int k = 0; k < 4; ++k) mc[k] = S.mask[p_own][k];
+            const int cnt_own = __popc(mc[0]) + __popc(mc[1]) + __popc(mc[2]) + __popc(mc[3]);
+            int incl = cnt_own;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        const int pre = incl - cnt_own;
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
-        for (int base = 0; base < total; base += 32) {
-            // P: pair base + lane
-            const int i = base + lane;
-            int ol = 0;
-#pragma unroll
-            for (int step = 16; step >= 1; step >>= 1) {
-                const int cand = ol + step;
-                const int pv = __shfl_sync(0xffffffffu, pre, cand);
-                if (pv <= i) ol = cand;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
             }
-            const int opre = __shfl_sync(0xffffffffu, pre, ol);
-            uint32_t om[4];
+            S.ppre[tid] = incl - cnt_own;
+            if (lane == 31) S.wcnt[warp] = incl;
+            __syncthreads();
+            int pre = incl - cnt_own, total = 0;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) om[k] = __shfl_sync(0xffffffffu, m[k], ol);
-            if (i < total) {
-                int k = i - opre, jb = 0;
-                uint32_t wsel = om[0];
-                int c = __popc(om[0]);
-                if (k >= c) {
-                    k -= c; wsel = om[1]; jb = 32; c = __popc(om[1]);
+            for (int q = 0; q < NWARP; ++q) {
+                const int c = S.wcnt[q];
+                if (q < warp) pre += c;
+                total += c;
+            }
+            int wi = 0;
+            for (int base = 0; base < total; base += BLOCK, wi ^= 1) {
+                const int i = base + tid;
+                if (i < total) {
+                    int t, k;
+                    cta_pair_owner(S.wcnt, S.ppre, i, t, k);
+                    int odx, ody;
+                    pair_pixel<LATTICE>(t >> 5, t & 31, odx, ody);
+                    const int p = ody * TILE + odx;
+                    const uint32_t om0 = S.mask[p][0], om1 = S.mask[p][1], om2 = S.mask[p][2], om3 = S.mask[p][3];
+                    int jb = 0;
+                    uint32_t wsel = om0;
+                    int c = __popc(om0);
                     if (k >= c) {
-                        k -= c; wsel = om[2]; jb = 64; c = __popc(om[2]);
-                        if (k >= c) { k -= c; wsel = om[3]; jb = 96; }
+                        k -= c; wsel = om1; jb = 32; c = __popc(om1);
+                        if (k >= c) {
+                            k -= c; wsel = om2; jb = 64; c = __popc(om2);
+                            if (k >= c) { k -= c; wsel = om3; jb = 96; }
+                        }
                     }
+                    const int j = jb + kth_set_bit(wsel, k);
+                    const float4 pr = S.pray[p], pd = S.pdir[p];
+                    S.cres[wi][tid] = fwd_pair_eval<NS, DEPTH>(buf[j], ro, f3(pd.x, pd.y, pd.z),
+                                                               f3(pr.x, pr.y, pr.z), s_val);
                 }
-                const int j = jb + kth_set_bit(wsel, k);
-                int odx, ody;
-                pair_pixel<LATTICE>(warp, ol, odx, ody);
-                const int p = ody * TILE + odx;
-                const float4 pr = S.pray[p], pd = S.pdir[p];
-                const float3 rd = f3(pd.x, pd.y, pd.z);
-                const Rec& r = buf[j];
-                const float3 vox_c = f3(r.cx, r.cy, r.cz);
-                const float vox_l = r.len;
-                const float2 ab = ray_box(vox_c, vox_l, ro, f3(pr.x, pr.y, pr.z));
-                const float a = ab.x, bb = ab.y;
-                float g[8];
-#pragma unroll
-                for (int qq = 0; qq < 8; ++qq) g[qq] = r.g[qq];
-                // forward.cu:255-306, as render_fwd_kernel
-                float w8[8];
-                float local_a[NS > 1 ? NS : 1];
-                const float vox_l_inv = 1.f / vox_l;
-                const float3 p_entry = ro + a * rd;
-                const float3 P_step = (bb - a) * rd / (float)NS;
-                const float3 qt_entry = (p_entry - (vox_c - 0.5f * vox_l)) * vox_l_inv;
-                const float3 qt_step = P_step * vox_l_inv;
-                tri_weights(qt_entry, w8);
-                float phi_former = 1.f / (1.f + expf(-s_val * interp8(g, w8)));
-                const float phi_entry = phi_former;
-#pragma unroll
-                for (int s = 0; s < NS; ++s) {
-                    const float3 qt_curr = qt_entry + qt_step * (float)(s + 1);
-                    tri_weights(qt_curr, w8);
-                    const float phi_curr = 1.f / (1.f + expf(-s_val * interp8(g, w8)));
-                    if (DEPTH && NS > 1) local_a[s] = fmaxf((phi_former - phi_curr) / (phi_former + 1e-6f), 0.f);
-                    phi_former = phi_curr;
-                }
-                const float alpha = fmaxf((phi_entry - phi_former) / (phi_entry + 1e-6f), 0.f);
-                float dval = 0.f;
-                if (DEPTH && !(alpha < MIN_ALPHA)) {
-                    if (NS == 3) {
-                        const float step_sz = 0.3333333f * (bb - a);
-                        const float a0 = local_a[0], a1 = local_a[NS > 1 ? 1 : 0], a2 = local_a[NS > 2 ? 2 : 0];
-                        const float t0 = a + 0.5f * step_sz, t1 = a + 1.5f * step_sz, t2 = a + 2.5f * step_sz;
-                        dval = a0 * t0 + (1.f - a0) * a1 * t1 + (1.f - a0) * (1.f - a1) * a2 * t2;
-                    } else if (NS == 2) {
-                        const float step_sz = 0.5f * (bb - a);
-                        const float a0 = local_a[0], a1 = local_a[NS > 1 ? 1 : 0];
-                        const float t0 = a + 0.5f * step_sz, t1 = a + 1.5f * step_sz;
-                        dval = a0 * t0 + (1.f - a0) * a1 * t1;
-                    } else {
-                        dval = alpha * 0.5f * (a + bb);
+                __syncthreads();
+                // C: this pixel's pairs of the window, in record order
+                const int e = min(base + BLOCK, pre + cnt_own);
+                for (int ii = max(base, pre); ii < e && !done; ++ii) {
+                    int j2;
+                    if (mc[0]) { j2 = __ffs(mc[0]) - 1; mc[0] &= mc[0] - 1; }
+                    else if (mc[1]) { j2 = __ffs(mc[1]) + 31; mc[1] &= mc[1] - 1; }
+                    else if (mc[2]) { j2 = __ffs(mc[2]) + 63; mc[2] &= mc[2] - 1; }
+                    else { j2 = __ffs(mc[3]) + 95; mc[3] &= mc[3] - 1; }
+                    const float2 rv = S.cres[wi][ii - base];
+                    const float alpha = rv.x;
+                    if (COUNT) ++n_eval;
+                    if (alpha < MIN_ALPHA) continue;
+                    if (COUNT) { ++n_acc; n_eval_last = n_eval; }
+                    const Rec& r = buf[j2];
+                    const float pt_w = T * alpha;
+                    C = C + pt_w * f3(r.r, r.gr, r.b);
+                    if (DEPTH) {
+                        D = D + T * rv.y;
+                        if (T > 0.5f) { med_rec = (int64_t)range.x + (int64_t)b * BATCH + j2; med_T = T; }
                     }
+                    if (NORMAL) {
+                        const float4 nv = S.nrm[j2];
+                        Nn = Nn + pt_w * nv.w * f3(nv.x, nv.y, nv.z);
+                    }
+                    T *= (1.f - alpha);
+                    done |= (T < EARLY_STOP_T);
+                    last = (uint32_t)(b * BATCH + j2 + 1);
+                    if (MAXW)
+                        atomicMax(((int*)max_w) + (size_t)vi * max_w_stride + (r.val & 0x1FFFFFFFu),
+                                  __float_as_int(pt_w));
                 }
-                S.res[warp][lane] = make_float2(alpha, dval);
             }
-            __syncwarp();
-            // C: this pixel's pairs of the window, in record order (popped from a copy: the
-            // pair numbering above reads every lane's whole mask in each window)
-            const int e = min(base + 32, pre + cnt_own);
-            for (int ii = max(base, pre); ii < e && !done; ++ii) {
-                int j2;
-                if (mc[0]) { j2 = __ffs(mc[0]) - 1; mc[0] &= mc[0] - 1; }
-                else if (mc[1]) { j2 = __ffs(mc[1]) + 31; mc[1] &= mc[1] - 1; }
-                else if (mc[2]) { j2 = __ffs(mc[2]) + 63; mc[2] &= mc[2] - 1; }
-                else { j2 = __ffs(mc[3]) + 95; mc[3] &= mc[3] - 1; }
-                const float2 rv = S.res[warp][ii - base];
-                const float alpha = rv.x;
-                if (COUNT) ++n_eval;
-                if (alpha < MIN_ALPHA) continue;
-                if (COUNT) { ++n_acc; n_eval_last = n_eval; }
-                const Rec& r = buf[j2];
-                const float pt_w = T * alpha;
-                C = C + pt_w * f3(r.r, r.gr, r.b);
-                if (DEPTH) {
-                    D = D + T * rv.y;
-                    if (T > 0.5f) { med_rec = (int64_t)range.x + (int64_t)b * BATCH + j2; med_T = T; }
-                }
-                if (NORMAL) {
-                    const float4 nv = S.nrm[j2];
-                    Nn = Nn + pt_w * nv.w * f3(nv.x, nv.y, nv.z);
-                }
-                T *= (1.f - alpha);
-                done |= (T < EARLY_STOP_T);
-                last = (uint32_t)(b * BATCH + j2 + 1);
-                if (MAXW)
-                    atomicMax(((int*)max_w) + (size_t)vi * max_w_stride + (r.val & 0x1FFFFFFFu),
-                              __float_as_int(pt_w));
+            // every owner lookup of the slot is behind the last window's barrier
+#pragma unroll
+            for (int k = 0; k < 4; ++k) S.mask[p_own][k] = 0u;
+        } else {
+            // ---------------------------------------------------------------- P + C, per warp
+            uint32_t m[4], mc[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) { m[k] = mc[k] = S.mask[p_own][k]; S.mask[p_own][k] = 0u; }
+            const int cnt_own = __popc(m[0]) + __popc(m[1]) + __popc(m[2]) + __popc(m[3]);
+            int incl = cnt_own;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
             }
-            __syncwarp();
+            const int pre = incl - cnt_own;
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            for (int base = 0; base < total; base += 32) {
+                // P: pair base + lane
+                const int i = base + lane;
+                int ol = 0;
+#pragma unroll
+                for (int step = 16; step >= 1; step >>= 1) {
+                    const int cand = ol + step;
+                    const int pv = __shfl_sync(0xffffffffu, pre, cand);
+                    if (pv <= i) ol = cand;
+                }
+                const int opre = __shfl_sync(0xffffffffu, pre, ol);
+                uint32_t om[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) om[k] = __shfl_sync(0xffffffffu, m[k], ol);
+                if (i < total) {
+                    int k = i - opre, jb = 0;
+                    uint32_t wsel = om[0];
+                    int c = __popc(om[0]);
+                    if (k >= c) {
+                        k -= c; wsel = om[1]; jb = 32; c = __popc(om[1]);
+                        if (k >= c) {
+                            k -= c; wsel = om[2]; jb = 64; c = __popc(om[2]);
+                            if (k >= c) { k -= c; wsel = om[3]; jb = 96; }
+                        }
+                    }
+                    const int j = jb + kth_set_bit(wsel, k);
+                    int odx, ody;
+                    pair_pixel<LATTICE>(warp, ol, odx, ody);
+                    const int p = ody * TILE + odx;
+                    const float4 pr = S.pray[p], pd = S.pdir[p];
+                    S.res[warp][lane] = fwd_pair_eval<NS, DEPTH>(buf[j], ro, f3(pd.x, pd.y, pd.z),
+                                                                 f3(pr.x, pr.y, pr.z), s_val);
+                }
+                __syncwarp();
+                // C: this pixel's pairs of the window, in record order (popped from a copy: the
+                // pair numbering above reads every lane's whole mask in each window)
+                const int e = min(base + 32, pre + cnt_own);
+                for (int ii = max(base, pre); ii < e && !done; ++ii) {
+                    int j2;
+                    if (mc[0]) { j2 = __ffs(mc[0]) - 1; mc[0] &= mc[0] - 1; }
+                    else if (mc[1]) { j2 = __ffs(mc[1]) + 31; mc[1] &= mc[1] - 1; }
+                    else if (mc[2]) { j2 = __ffs(mc[2]) + 63; mc[2] &= mc[2] - 1; }
+                    else { j2 = __ffs(mc[3]) + 95; mc[3] &= mc[3] - 1; }
+                    const float2 rv = S.res[warp][ii - base];
+                    const float alpha = rv.x;
+                    if (COUNT) ++n_eval;
+                    if (alpha < MIN_ALPHA) continue;
+                    if (COUNT) { ++n_acc; n_eval_last = n_eval; }
+                    const Rec& r = buf[j2];
+                    const float pt_w = T * alpha;
+                    C = C + pt_w * f3(r.r, r.gr, r.b);
+                    if (DEPTH) {
+                        D = D + T * rv.y;
+                        if (T > 0.5f) { med_rec = (int64_t)range.x + (int64_t)b * BATCH + j2; med_T = T; }
+                    }
+                    if (NORMAL) {
+                        const float4 nv = S.nrm[j2];
+                        Nn = Nn + pt_w * nv.w * f3(nv.x, nv.y, nv.z);
+                    }
+                    T *= (1.f - alpha);
+                    done |= (T < EARLY_STOP_T);
+                    last = (uint32_t)(b * BATCH + j2 + 1);
+                    if (MAXW)
+                        atomicMax(((int*)max_w) + (size_t)vi * max_w_stride + (r.val & 0x1FFFFFFFu),
+                                  __float_as_int(pt_w));
+                }
+                __syncwarp();
+            }
         }
         if (done && inside) {
             const float4 pr = S.pray[p_own];
@@ -457,8 +574,10 @@ struct alignas(128) PairBwdSmem {
     float4 pgt[BLOCK];           // target colour (R-concentration term)
     uint32_t mask[BLOCK][4];
     float4 nrm[BATCH];
-    PairBwdRes res[NWARP][32];
+    PairBwdRes res[NWARP][32];   // a warp's window, or (CTA-wide) the CTA's window in thread order
     float red[NWARP];
+    int ppre[BLOCK];             // CTA-wide windows: each thread's pair offset within its warp
+    int wcnt[NWARP];             // and the warps' pair counts
 };
 
 // Position of the k-th (from 0) highest set bit of the 128-bit mask m[0..3].
@@ -476,7 +595,205 @@ __device__ __forceinline__ int kth_highest_bit(const uint32_t (&m)[4], int k) {
     return jb + 31 - kth_set_bit(__brev(wsel), k);
 }
 
-template <bool DEPTH, bool NORMAL, bool RCONC, int RING = 3, int MINB = 3, bool LATTICE = true>
+// Adjoint phase A of one (pixel p, record j) pair (backward.cu:313-388, 650-671, 682-768):
+// alpha, dL/d(point weight) and the factors that do not depend on the transmittance, into R.
+template <bool DEPTH, bool NORMAL, class SM>
+__device__ __forceinline__ void bwd_pair_A(PairBwdRes& R, const SM& S, const Rec* buf, int j, int p, float3 ro,
+                                           float s_val)
+{
+    const Rec& r = buf[j];
+    const float4 pr = S.pray[p], pd = S.pdir[p], pc = S.pdc[p];
+    const float3 rd = f3(pd.x, pd.y, pd.z);
+    const float3 vox_c = f3(r.cx, r.cy, r.cz);
+    const float vox_l = r.len;
+    const float2 ab = ray_box(vox_c, vox_l, ro, f3(pr.x, pr.y, pr.z));
+    const float a = ab.x, bb = ab.y;
+    float g[8];
+#pragma unroll
+    for (int qq = 0; qq < 8; ++qq) g[qq] = r.g[qq];
+    const float vox_l_inv = 1.f / vox_l;
+    const float3 lo3 = vox_c - 0.5f * vox_l;
+    // backward.cu:313-337: entry / exit from ro + t rd
+    const float3 qt_entry = ((ro + a * rd) - lo3) * vox_l_inv;
+    const float3 qt_exit = ((ro + bb * rd) - lo3) * vox_l_inv;
+    float we[8], wx[8];
+    tri_weights(qt_entry, we);
+    tri_weights(qt_exit, wx);
+    float sdf_entry = 0.f, sdf_exit = 0.f;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) { sdf_entry += g[q] * we[q]; sdf_exit += g[q] * wx[q]; }
+    const float phi_entry = 1.f / (1.f + expf(-s_val * sdf_entry));
+    const float phi_exit = 1.f / (1.f + expf(-s_val * sdf_exit));
+    const float denom = phi_entry + 1e-6f;
+    const float alpha = fmaxf((phi_entry - phi_exit) / denom, 0.f);
+    R.alpha = alpha;
+    if (!(alpha < MIN_ALPHA)) {
+        const float3 c3 = f3(r.r, r.gr, r.b);
+        float dL_dpt_w = dot3(f3(pc.x, pc.y, pc.z), c3);
+        if (NORMAL) {
+            const float4 nv = S.nrm[j];
+            const float3 surf_n = nv.w * f3(nv.x, nv.y, nv.z);
+            const float4 pn = S.pdn[p];
+            dL_dpt_w += dot3(f3(pn.x, pn.y, pn.z), surf_n);
+        }
+        R.dpw = dL_dpt_w;
+        const float pe = s_val * phi_entry * (1.f - phi_entry);
+        {
+            // backward.cu:650-671
+            const float pxv = s_val * phi_exit * (1.f - phi_exit);
+            R.dae = (pe * (1.f - alpha)) / denom;
+            R.dax = -pxv / denom;
+            const float dpe = phi_entry * (1.f - phi_entry) * sdf_entry;
+            const float dpx = phi_exit * (1.f - phi_exit) * sdf_exit;
+            R.das = ((dpe * (1.f - alpha)) + (-dpx)) / denom;
+        }
+        if (DEPTH) {
+            // backward.cu:338-388 and :682-768 (three sub-segments); the first end
+            // point is the entry point (same phi and phi', bit for bit)
+            const float3 qt_step = ((bb - a) * rd / 3.0f) * vox_l_inv;
+            float ph[4], dph[4];
+            ph[0] = phi_entry;
+            dph[0] = pe;
+#pragma unroll
+            for (int k2 = 1; k2 < 4; ++k2) {
+                const float3 qk = qt_entry + qt_step * (float)k2;
+                float wk[8];
+                tri_weights(qk, wk);
+                ph[k2] = 1.f / (1.f + expf(-s_val * interp8(g, wk)));
+                dph[k2] = s_val * ph[k2] * (1.f - ph[k2]);
+            }
+            float la[3];
+#pragma unroll
+            for (int k2 = 0; k2 < 3; ++k2) {
+                const float dk = ph[k2] + 1e-6f;
+                const float raw = (ph[k2] - ph[k2 + 1]) / dk;
+                const float allow = raw > 0.f ? 1.f : 0.f;
+                la[k2] = fmaxf(raw, 0.f);
+                R.c_lo[k2] = allow * (ph[k2 + 1] / (dk * dk)) * dph[k2];
+                R.c_hi[k2] = allow * (-1.f / dk) * dph[k2 + 1];
+            }
+            const float step_sz = 0.3333333f * (bb - a);
+            const float a0 = la[0], a1 = la[1], a2 = la[2];
+            const float t0 = a + 0.5f * step_sz, t1 = a + 1.5f * step_sz, t2 = a + 2.5f * step_sz;
+            R.dval = a0 * t0 + (1.f - a0) * a1 * t1 + (1.f - a0) * (1.f - a1) * a2 * t2;
+            R.part[0] = t0 + a1 * a2 * t2 - a1 * t1 - a2 * t2;
+            R.part[1] = t1 + a0 * a2 * t2 - a0 * t1 - a2 * t2;
+            R.part[2] = t2 + a0 * a1 * t2 - a0 * t2 - a1 * t2;
+        }
+    }
+}
+
+// Adjoint phase B of one pair, in a pixel's back-to-front walk (backward.cu:640-680):
+// transmittance recovery, dL/dalpha, the suffix term and dL/ds; R's dpw becomes dL/dalpha, its
+// dval the point weight and its part[] the depth-term scales.
+template <bool DEPTH>
+__device__ __forceinline__ void bwd_pair_B(PairBwdRes& Q, float& T, float& last_dT, float& ds_acc, float dD) {
+    const float alpha = Q.alpha;
+    if (alpha < MIN_ALPHA) return;          // lambda_ascending == 0
+    T = T / (1.f - alpha);
+    const float pt_w = alpha * T;
+    const float dL_dpt_w = Q.dpw;
+    const float dL_dalpha = T * (dL_dpt_w - last_dT);
+    last_dT += alpha * (dL_dpt_w - last_dT);
+    ds_acc += dL_dalpha * Q.das;
+    if (DEPTH) {
+        const float dval = Q.dval;
+        Q.part[0] = dD * T * Q.part[0];
+        Q.part[1] = dD * T * Q.part[1];
+        Q.part[2] = dD * T * Q.part[2];
+        last_dT += dD * dval;
+    }
+    Q.dpw = dL_dalpha;
+    Q.dval = pt_w;
+}
+
+// Adjoint phase C of one pair with alpha >= MIN_ALPHA (backward.cu:585-639, 650-768, 824-848,
+// the lambda_ascending term off as in the forward's defaults): the eight corner
+// gradients, colour and |dL/dalpha * alpha| from the factors of A and the scales of B, sent
+// with vector reductions.
+template <bool DEPTH, bool NORMAL, bool RCONC, class SM>
+__device__ __forceinline__ void bwd_pair_C(const PairBwdRes& R, const SM& S, const Rec* buf, int j, int p, float3 ro,
+                                           float weight_R, int vi, int N, float* __restrict__ dL_dvox,
+                                           float* __restrict__ drgbs, unsigned* __restrict__ status)
+{
+    const Rec& r = buf[j];
+    const float4 pr = S.pray[p], pd = S.pdir[p], pc = S.pdc[p];
+    const float3 rd = f3(pd.x, pd.y, pd.z);
+    const float3 vox_c = f3(r.cx, r.cy, r.cz);
+    const float vox_l = r.len;
+    const float2 ab = ray_box(vox_c, vox_l, ro, f3(pr.x, pr.y, pr.z));
+    const float a = ab.x, bb = ab.y;
+    const float vox_l_inv = 1.f / vox_l;
+    const float3 lo3 = vox_c - 0.5f * vox_l;
+    const float3 qt_entry = ((ro + a * rd) - lo3) * vox_l_inv;
+    const float3 qt_exit = ((ro + bb * rd) - lo3) * vox_l_inv;
+    const float dL_dalpha = R.dpw, pt_w = R.dval, alpha = R.alpha;
+    float dg[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) dg[q] = 0.f;
+    if (NORMAL) {
+        // backward.cu:604-639
+        const float4 nv = S.nrm[j];
+        const float3 lin_n = f3(nv.x, nv.y, nv.z);
+        const float r_lin = nv.w;
+        const float3 surf_n = r_lin * lin_n;
+        const float4 pn = S.pdn[p];
+        const float3 dsn = pt_w * f3(pn.x, pn.y, pn.z);
+        const float3 d = r_lin * (dsn - dot3(dsn, lin_n) * r_lin * surf_n);
+        dg[0] += -d.x - d.y - d.z; dg[1] += -d.x - d.y + d.z;
+        dg[2] += -d.x + d.y - d.z; dg[3] += -d.x + d.y + d.z;
+        dg[4] += +d.x - d.y - d.z; dg[5] += +d.x - d.y + d.z;
+        dg[6] += +d.x + d.y - d.z; dg[7] += +d.x + d.y + d.z;
+    }
+    {
+        float we[8], wx[8];
+        tri_weights(qt_entry, we);
+        tri_weights(qt_exit, wx);
+        const float dae = R.dae, dax = R.dax;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            dg[q] += dae * we[q] * dL_dalpha;
+            dg[q] += dax * wx[q] * dL_dalpha;
+        }
+    }
+    if (DEPTH) {
+        const float3 qt_step = ((bb - a) * rd / 3.0f) * vox_l_inv;
+        const float d0 = R.part[0], d1 = R.part[1], d2 = R.part[2];
+        const float cp[4] = {d0 * R.c_lo[0], d0 * R.c_hi[0] + d1 * R.c_lo[1],
+                             d1 * R.c_hi[1] + d2 * R.c_lo[2], d2 * R.c_hi[2]};
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) {
+            const float3 qk = qt_entry + qt_step * (float)k2;
+            float wk[8];
+            tri_weights(qk, wk);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) dg[q] += cp[k2] * wk[q];
+        }
+    }
+    float drgb0 = pt_w * pc.x, drgb1 = pt_w * pc.y, drgb2 = pt_w * pc.z;
+    if (RCONC) {
+        const float4 pg = S.pgt[p];
+        const float3 gr = weight_R * pt_w * 2.0f * (f3(r.r, r.gr, r.b) - f3(pg.x, pg.y, pg.z));
+        drgb0 += gr.x; drgb1 += gr.y; drgb2 += gr.z;
+    }
+    const uint32_t vid = r.val & 0x1FFFFFFFu;
+    if (vid < (uint32_t)N) {
+        float4* dst = reinterpret_cast<float4*>(dL_dvox + 12 * (size_t)vid);
+        atomicAdd(dst, make_float4(dg[0], dg[1], dg[2], dg[3]));
+        atomicAdd(dst + 1, make_float4(dg[4], dg[5], dg[6], dg[7]));
+        if (drgbs) {
+            float* cr = drgbs + 3 * ((size_t)vi * N + vid);
+            atomicAdd(cr, drgb0); atomicAdd(cr + 1, drgb1); atomicAdd(cr + 2, drgb2);
+            atomicAdd(dL_dvox + 12 * (size_t)vid + 11, fabsf(dL_dalpha * alpha));
+        } else {
+            atomicAdd(dst + 2, make_float4(drgb0, drgb1, drgb2, fabsf(dL_dalpha * alpha)));
+        }
+    } else {
+        atomicOr(status, ERR_BAD_INDEX);
+    }
+}
+
+template <bool DEPTH, bool NORMAL, bool RCONC, int RING = 3, int MINB = 3, bool LATTICE = true, bool CTAW = false>
 __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
     const __grid_constant__ Views V, int N, const uint32_t* __restrict__ order, const uint2* __restrict__ ranges,
     const uint32_t* __restrict__ tile_last,
@@ -637,227 +954,107 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
             }
         }
         __syncthreads();
-        // ---------------------------------------------------------------- per warp
-        uint32_t m[4];
+        if constexpr (CTAW) {
+            // ------------------------------------------------------------ CTA-wide windows
+            // pairs numbered over the whole CTA (thread-major, each pixel's pairs back to
+            // front); per window of BLOCK pairs: A one pair per thread, B per pixel, C one pair
+            // per thread
+            uint32_t m[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) { m[k] = S.mask[p_own][k]; S.mask[p_own][k] = 0u; }
-        const int cnt_own = __popc(m[0]) + __popc(m[1]) + __popc(m[2]) + __popc(m[3]);
-        int incl = cnt_own;
+            for (int k = 0; k < 4; ++k) m[k] = S.mask[p_own][k];
+            const int cnt_own = __popc(m[0]) + __popc(m[1]) + __popc(m[2]) + __popc(m[3]);
+            int incl = cnt_own;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        const int pre = incl - cnt_own;
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
-        for (int base = 0; base < total; base += 32) {
-            // which pair this lane evaluates in A and C: its pixel (lane ol) and record j
-            const int i = base + lane;
-            int ol = 0;
-#pragma unroll
-            for (int step = 16; step >= 1; step >>= 1) {
-                const int cand = ol + step;
-                const int pv = __shfl_sync(0xffffffffu, pre, cand);
-                if (pv <= i) ol = cand;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
             }
-            const int opre = __shfl_sync(0xffffffffu, pre, ol);
-            uint32_t om[4];
+            S.ppre[tid] = incl - cnt_own;
+            if (lane == 31) S.wcnt[warp] = incl;
+            __syncthreads();
+            int pre = incl - cnt_own, total = 0;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) om[k] = __shfl_sync(0xffffffffu, m[k], ol);
-            const bool has = i < total;
-            const int j = has ? kth_highest_bit(om, i - opre) : 0;
-            int odx, ody;
-            pair_pixel<LATTICE>(warp, ol, odx, ody);
-            const int p = ody * TILE + odx;
-            PairBwdRes& R = S.res[warp][lane];
-            // ---------------------------------------------------------- A
-            if (has) {
-                const Rec& r = buf[j];
-                const float4 pr = S.pray[p], pd = S.pdir[p], pc = S.pdc[p];
-                const float3 rd = f3(pd.x, pd.y, pd.z);
-                const float3 vox_c = f3(r.cx, r.cy, r.cz);
-                const float vox_l = r.len;
-                const float2 ab = ray_box(vox_c, vox_l, ro, f3(pr.x, pr.y, pr.z));
-                const float a = ab.x, bb = ab.y;
-                float g[8];
-#pragma unroll
-                for (int qq = 0; qq < 8; ++qq) g[qq] = r.g[qq];
-                const float vox_l_inv = 1.f / vox_l;
-                const float3 lo3 = vox_c - 0.5f * vox_l;
-                // backward.cu:313-337: entry / exit from ro + t rd
-                const float3 qt_entry = ((ro + a * rd) - lo3) * vox_l_inv;
-                const float3 qt_exit = ((ro + bb * rd) - lo3) * vox_l_inv;
-                float we[8], wx[8];
-                tri_weights(qt_entry, we);
-                tri_weights(qt_exit, wx);
-                float sdf_entry = 0.f, sdf_exit = 0.f;
-#pragma unroll
-                for (int q = 0; q < 8; ++q) { sdf_entry += g[q] * we[q]; sdf_exit += g[q] * wx[q]; }
-                const float phi_entry = 1.f / (1.f + expf(-s_val * sdf_entry));
-                const float phi_exit = 1.f / (1.f + expf(-s_val * sdf_exit));
-                const float denom = phi_entry + 1e-6f;
-                const float alpha = fmaxf((phi_entry - phi_exit) / denom, 0.f);
-                R.alpha = alpha;
-                if (!(alpha < MIN_ALPHA)) {
-                    const float3 c3 = f3(r.r, r.gr, r.b);
-                    float dL_dpt_w = dot3(f3(pc.x, pc.y, pc.z), c3);
-                    if (NORMAL) {
-                        const float4 nv = S.nrm[j];
-                        const float3 surf_n = nv.w * f3(nv.x, nv.y, nv.z);
-                        const float4 pn = S.pdn[p];
-                        dL_dpt_w += dot3(f3(pn.x, pn.y, pn.z), surf_n);
-                    }
-                    R.dpw = dL_dpt_w;
-                    const float pe = s_val * phi_entry * (1.f - phi_entry);
-                    {
-                        // backward.cu:650-671
-                        const float pxv = s_val * phi_exit * (1.f - phi_exit);
-                        R.dae = (pe * (1.f - alpha)) / denom;
-                        R.dax = -pxv / denom;
-                        const float dpe = phi_entry * (1.f - phi_entry) * sdf_entry;
-                        const float dpx = phi_exit * (1.f - phi_exit) * sdf_exit;
-                        R.das = ((dpe * (1.f - alpha)) + (-dpx)) / denom;
-                    }
-                    if (DEPTH) {
-                        // backward.cu:338-388 and :682-768 (three sub-segments); the first end
-                        // point is the entry point (same phi and phi', bit for bit)
-                        const float3 qt_step = ((bb - a) * rd / 3.0f) * vox_l_inv;
-                        float ph[4], dph[4];
-                        ph[0] = phi_entry;
-                        dph[0] = pe;
-#pragma unroll
-                        for (int k2 = 1; k2 < 4; ++k2) {
-                            const float3 qk = qt_entry + qt_step * (float)k2;
-                            float wk[8];
-                            tri_weights(qk, wk);
-                            ph[k2] = 1.f / (1.f + expf(-s_val * interp8(g, wk)));
-                            dph[k2] = s_val * ph[k2] * (1.f - ph[k2]);
-                        }
-                        float la[3];
-#pragma unroll
-                        for (int k2 = 0; k2 < 3; ++k2) {
-                            const float dk = ph[k2] + 1e-6f;
-                            const float raw = (ph[k2] - ph[k2 + 1]) / dk;
-                            const float allow = raw > 0.f ? 1.f : 0.f;
-                            la[k2] = fmaxf(raw, 0.f);
-                            R.c_lo[k2] = allow * (ph[k2 + 1] / (dk * dk)) * dph[k2];
-                            R.c_hi[k2] = allow * (-1.f / dk) * dph[k2 + 1];
-                        }
-                        const float step_sz = 0.3333333f * (bb - a);
-                        const float a0 = la[0], a1 = la[1], a2 = la[2];
-                        const float t0 = a + 0.5f * step_sz, t1 = a + 1.5f * step_sz, t2 = a + 2.5f * step_sz;
-                        R.dval = a0 * t0 + (1.f - a0) * a1 * t1 + (1.f - a0) * (1.f - a1) * a2 * t2;
-                        R.part[0] = t0 + a1 * a2 * t2 - a1 * t1 - a2 * t2;
-                        R.part[1] = t1 + a0 * a2 * t2 - a0 * t1 - a2 * t2;
-                        R.part[2] = t2 + a0 * a1 * t2 - a0 * t2 - a1 * t2;
-                    }
-                }
+            for (int q = 0; q < NWARP; ++q) {
+                const int c = S.wcnt[q];
+                if (q < warp) pre += c;
+                total += c;
             }
-            __syncwarp();
-            // ---------------------------------------------------------- B: this pixel, back to front
-            {
-                const int e = min(base + 32, pre + cnt_own);
-                for (int ii = max(base, pre); ii < e; ++ii) {
-                    PairBwdRes& Q = S.res[warp][ii - base];
-                    const float alpha = Q.alpha;
-                    if (alpha < MIN_ALPHA) continue;          // lambda_ascending == 0
-                    T = T / (1.f - alpha);
-                    const float pt_w = alpha * T;
-                    const float dL_dpt_w = Q.dpw;
-                    const float dL_dalpha = T * (dL_dpt_w - last_dT);
-                    last_dT += alpha * (dL_dpt_w - last_dT);
-                    ds_acc += dL_dalpha * Q.das;
-                    if (DEPTH) {
-                        const float dval = Q.dval;
-                        Q.part[0] = dD * T * Q.part[0];
-                        Q.part[1] = dD * T * Q.part[1];
-                        Q.part[2] = dD * T * Q.part[2];
-                        last_dT += dD * dval;
-                    }
-                    Q.dpw = dL_dalpha;
-                    Q.dval = pt_w;
+            PairBwdRes* RF = &S.res[0][0];
+            for (int base = 0; base < total; base += BLOCK) {
+                const int i = base + tid;
+                const bool has = i < total;
+                int j = 0, p = 0;
+                if (has) {
+                    int t, k;
+                    cta_pair_owner(S.wcnt, S.ppre, i, t, k);
+                    int odx, ody;
+                    pair_pixel<LATTICE>(t >> 5, t & 31, odx, ody);
+                    p = ody * TILE + odx;
+                    const uint32_t om[4] = {S.mask[p][0], S.mask[p][1], S.mask[p][2], S.mask[p][3]};
+                    j = kth_highest_bit(om, k);
                 }
+                PairBwdRes& R = RF[tid];
+                if (has) bwd_pair_A<DEPTH, NORMAL>(R, S, buf, j, p, ro, s_val);
+                __syncthreads();
+                const int e = min(base + BLOCK, pre + cnt_own);
+                for (int ii = max(base, pre); ii < e; ++ii) bwd_pair_B<DEPTH>(RF[ii - base], T, last_dT, ds_acc, dD);
+                __syncthreads();
+                if (has && !(R.alpha < MIN_ALPHA))
+                    bwd_pair_C<DEPTH, NORMAL, RCONC>(R, S, buf, j, p, ro, weight_R, vi, N, dL_dvox, drgbs, status);
+                __syncthreads();   // the next window overwrites RF
             }
-            __syncwarp();
-            // ---------------------------------------------------------- C
-            if (has && !(R.alpha < MIN_ALPHA)) {
-                const Rec& r = buf[j];
-                const float4 pr = S.pray[p], pd = S.pdir[p], pc = S.pdc[p];
-                const float3 rd = f3(pd.x, pd.y, pd.z);
-                const float3 vox_c = f3(r.cx, r.cy, r.cz);
-                const float vox_l = r.len;
-                const float2 ab = ray_box(vox_c, vox_l, ro, f3(pr.x, pr.y, pr.z));
-                const float a = ab.x, bb = ab.y;
-                const float vox_l_inv = 1.f / vox_l;
-                const float3 lo3 = vox_c - 0.5f * vox_l;
-                const float3 qt_entry = ((ro + a * rd) - lo3) * vox_l_inv;
-                const float3 qt_exit = ((ro + bb * rd) - lo3) * vox_l_inv;
-                const float dL_dalpha = R.dpw, pt_w = R.dval, alpha = R.alpha;
-                float dg[8];
+            // every owner lookup of the slot is behind the last window's barriers
 #pragma unroll
-                for (int q = 0; q < 8; ++q) dg[q] = 0.f;
-                if (NORMAL) {
-                    // backward.cu:604-639
-                    const float4 nv = S.nrm[j];
-                    const float3 lin_n = f3(nv.x, nv.y, nv.z);
-                    const float r_lin = nv.w;
-                    const float3 surf_n = r_lin * lin_n;
-                    const float4 pn = S.pdn[p];
-                    const float3 dsn = pt_w * f3(pn.x, pn.y, pn.z);
-                    const float3 d = r_lin * (dsn - dot3(dsn, lin_n) * r_lin * surf_n);
-                    dg[0] += -d.x - d.y - d.z; dg[1] += -d.x - d.y + d.z;
-                    dg[2] += -d.x + d.y - d.z; dg[3] += -d.x + d.y + d.z;
-                    dg[4] += +d.x - d.y - d.z; dg[5] += +d.x - d.y + d.z;
-                    dg[6] += +d.x + d.y - d.z; dg[7] += +d.x + d.y + d.z;
+            for (int k = 0; k < 4; ++k) S.mask[p_own][k] = 0u;
+        } else {
+            // ---------------------------------------------------------------- per warp
+            uint32_t m[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) { m[k] = S.mask[p_own][k]; S.mask[p_own][k] = 0u; }
+            const int cnt_own = __popc(m[0]) + __popc(m[1]) + __popc(m[2]) + __popc(m[3]);
+            int incl = cnt_own;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int pre = incl - cnt_own;
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            for (int base = 0; base < total; base += 32) {
+                // which pair this lane evaluates in A and C: its pixel (lane ol) and record j
+                const int i = base + lane;
+                int ol = 0;
+#pragma unroll
+                for (int step = 16; step >= 1; step >>= 1) {
+                    const int cand = ol + step;
+                    const int pv = __shfl_sync(0xffffffffu, pre, cand);
+                    if (pv <= i) ol = cand;
                 }
+                const int opre = __shfl_sync(0xffffffffu, pre, ol);
+                uint32_t om[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) om[k] = __shfl_sync(0xffffffffu, m[k], ol);
+                const bool has = i < total;
+                const int j = has ? kth_highest_bit(om, i - opre) : 0;
+                int odx, ody;
+                pair_pixel<LATTICE>(warp, ol, odx, ody);
+                const int p = ody * TILE + odx;
+                PairBwdRes& R = S.res[warp][lane];
+                // ---------------------------------------------------------- A
+                if (has) bwd_pair_A<DEPTH, NORMAL>(R, S, buf, j, p, ro, s_val);
+                __syncwarp();
+                // ---------------------------------------------------------- B: this pixel, back to front
                 {
-                    float we[8], wx[8];
-                    tri_weights(qt_entry, we);
-                    tri_weights(qt_exit, wx);
-                    const float dae = R.dae, dax = R.dax;
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        dg[q] += dae * we[q] * dL_dalpha;
-                        dg[q] += dax * wx[q] * dL_dalpha;
-                    }
+                    const int e = min(base + 32, pre + cnt_own);
+                    for (int ii = max(base, pre); ii < e; ++ii)
+                        bwd_pair_B<DEPTH>(S.res[warp][ii - base], T, last_dT, ds_acc, dD);
                 }
-                if (DEPTH) {
-                    const float3 qt_step = ((bb - a) * rd / 3.0f) * vox_l_inv;
-                    const float d0 = R.part[0], d1 = R.part[1], d2 = R.part[2];
-                    const float cp[4] = {d0 * R.c_lo[0], d0 * R.c_hi[0] + d1 * R.c_lo[1],
-                                         d1 * R.c_hi[1] + d2 * R.c_lo[2], d2 * R.c_hi[2]};
-#pragma unroll
-                    for (int k2 = 0; k2 < 4; ++k2) {
-                        const float3 qk = qt_entry + qt_step * (float)k2;
-                        float wk[8];
-                        tri_weights(qk, wk);
-#pragma unroll
-                        for (int q = 0; q < 8; ++q) dg[q] += cp[k2] * wk[q];
-                    }
-                }
-                float drgb0 = pt_w * pc.x, drgb1 = pt_w * pc.y, drgb2 = pt_w * pc.z;
-                if (RCONC) {
-                    const float4 pg = S.pgt[p];
-                    const float3 gr = weight_R * pt_w * 2.0f * (f3(r.r, r.gr, r.b) - f3(pg.x, pg.y, pg.z));
-                    drgb0 += gr.x; drgb1 += gr.y; drgb2 += gr.z;
-                }
-                const uint32_t vid = r.val & 0x1FFFFFFFu;
-                if (vid < (uint32_t)N) {
-                    float4* dst = reinterpret_cast<float4*>(dL_dvox + 12 * (size_t)vid);
-                    atomicAdd(dst, make_float4(dg[0], dg[1], dg[2], dg[3]));
-                    atomicAdd(dst + 1, make_float4(dg[4], dg[5], dg[6], dg[7]));
-                    if (drgbs) {
-                        float* cr = drgbs + 3 * ((size_t)vi * N + vid);
-                        atomicAdd(cr, drgb0); atomicAdd(cr + 1, drgb1); atomicAdd(cr + 2, drgb2);
-                        atomicAdd(dL_dvox + 12 * (size_t)vid + 11, fabsf(dL_dalpha * alpha));
-                    } else {
-                        atomicAdd(dst + 2, make_float4(drgb0, drgb1, drgb2, fabsf(dL_dalpha * alpha)));
-                    }
-                } else {
-                    atomicOr(status, ERR_BAD_INDEX);
-                }
+                __syncwarp();
+                // ---------------------------------------------------------- C
+                if (has && !(R.alpha < MIN_ALPHA))
+                    bwd_pair_C<DEPTH, NORMAL, RCONC>(R, S, buf, j, p, ro, weight_R, vi, N, dL_dvox, drgbs, status);
+                __syncwarp();
             }
-            __syncwarp();
         }
     }
     if (failed && tid == 0) atomicOr(status, ERR_WAIT_TIMEOUT);

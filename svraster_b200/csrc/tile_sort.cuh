@@ -14,8 +14,14 @@
 //  * one CTA per tile then sorts its records by their pair position, a key unique within
 //    the tile, so the result is exactly the reference's order whatever order the scatter
 //    left: 8-bit LSD passes, each a stable warp multisplit (digit peers from eight ballots)
-//    and a block scan; a tile of at most TS_CHUNK records is sorted in registers and shared
-//    memory, a larger one in passes over its range in global memory (L2-resident).
+//    and a block scan, in registers and shared memory for a tile of at most TS_CHUNK
+//    records.  A larger tile is first split, unordered, into 256 buckets on its top 8 key
+//    bits (keys are unique, so no stability is needed there); runs of consecutive buckets of
+//    at most TS_CHUNK records are then sorted in shared memory over the bits below the split
+//    digit, a bigger bucket is split again, and past two splits sorted by LSD passes over
+//    global memory.
+//  * the pair-order table is octant-major (entry q*N + voxel), so the scatter reads it
+//    coalesced.
 #pragma once
 
 #include "svr_common.cuh"
@@ -31,8 +37,10 @@ constexpr unsigned FULL = 0xffffffffu;
 
 struct TileSortSmem {
     uint32_t whist[TS_WARPS][256];   // per-warp digit counts, then per-warp digit bases
-    uint32_t base[256];              // running digit base (global path)
+    uint32_t base[256];              // running digit base (global path), bucket cursors (split)
     uint32_t wsum[TS_WARPS];
+    uint32_t b_off[2][256];          // bucket offsets of the two split levels
+    uint32_t b_cnt[2][256];          // bucket sizes of the two split levels
     uint32_t key[TS_CHUNK];          // shared-memory path: keys of the tile between passes
     uint32_t val[TS_CHUNK];
 };
@@ -79,21 +87,22 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* w
     return wbase + x - v;
 }
 
-// Stable rank of one block-tile (keys at warp-striped positions w*32*K + k*32 + lane, the
-// first `count` valid) by digit (key >> sh) & 255.  On return pos[k] is the key's
+// Stable rank of one block-tile (K keys per thread at warp-striped positions w*32*K + k*32 +
+// lane, the first `count` valid) by digit (key >> sh) & 255.  On return pos[k] is the key's
 // destination: base[d] + its rank among the block-tile's digit-d keys, where base is the
 // exclusive scan of the block-tile's own digit counts (self_scan) or the running base in
 // S.base, which is then advanced past this block-tile.
-__device__ __forceinline__ void block_rank(const uint32_t (&key)[TS_K], int count, int sh, bool self_scan,
-                                           TileSortSmem& S, uint32_t (&pos)[TS_K]) {
+template <int K>
+__device__ __forceinline__ void block_rank(const uint32_t (&key)[K], int count, int sh, bool self_scan,
+                                           TileSortSmem& S, uint32_t (&pos)[K]) {
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     for (int i = tid; i < TS_WARPS * 256; i += TS_THREADS) (&S.whist[0][0])[i] = 0u;
     __syncthreads();
     uint32_t* wh = S.whist[w];
     const uint32_t lt = lanemask_lt();
 #pragma unroll
-    for (int k = 0; k < TS_K; ++k) {
-        const int i = w * 32 * TS_K + k * 32 + lane;
+    for (int k = 0; k < K; ++k) {
+        const int i = w * 32 * K + k * 32 + lane;
         const bool valid = i < count;
         const uint32_t d = (key[k] >> sh) & 255u;
         const uint32_t peers = digit_peers(d, valid);
@@ -125,78 +134,145 @@ __device__ __forceinline__ void block_rank(const uint32_t (&key)[TS_K], int coun
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < TS_K; ++k) {
-        const int i = w * 32 * TS_K + k * 32 + lane;
+    for (int k = 0; k < K; ++k) {
+        const int i = w * 32 * K + k * 32 + lane;
         if (i < count) pos[k] += wh[(key[k] >> sh) & 255u];
     }
 }
 
-// Sort of one tile's records [start, start + n) by key (pair position), values along.
-// Input in A as (key, value) pairs; the sorted values go to vals_out and the tile id of every
-// record to tile_out.  Passes over bits [0, key_bits) eight at a time.  Large tiles ping-pong
-// through A and B in global memory.
-#ifndef SVR_TS_MINB
-#define SVR_TS_MINB 2
-#endif
-__global__ void __launch_bounds__(TS_THREADS, SVR_TS_MINB) tile_sort_kernel(
-    int T, const uint32_t* __restrict__ order, const uint2* __restrict__ ranges, int key_bits,
-    uint2* __restrict__ A, uint2* __restrict__ B,
-    uint32_t* __restrict__ vals_out, uint32_t* __restrict__ tile_out, unsigned* __restrict__ status)
+// n <= K * TS_THREADS records of A[start, start + n) sorted in registers (K keys per thread) by
+// key - kbase over npass 8-bit digits, with shared memory between the LSD passes; writes the
+// sorted values and the tile id of every record at the same positions.
+template <int K>
+__device__ __forceinline__ void sort_in_smem(const uint2* __restrict__ A, uint32_t start, int n, int npass,
+                                             uint32_t kbase, int tile, TileSortSmem& S,
+                                             uint32_t* __restrict__ vals_out, uint32_t* __restrict__ tile_out,
+                                             unsigned* __restrict__ status)
 {
-    extern __shared__ __align__(16) unsigned char ts_smem[];
-    TileSortSmem& S = *reinterpret_cast<TileSortSmem*>(ts_smem);
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int tile = order ? (int)order[blockIdx.x] : (int)blockIdx.x;
-    if (tile >= T) return;
-    const uint2 rg = ranges[tile];
-    if (rg.y <= rg.x) return;
-    const uint32_t start = rg.x;
-    const int n = (int)(rg.y - rg.x);
-    const int npass = (key_bits + 7) / 8;
-    uint32_t key[TS_K], val[TS_K], pos[TS_K];
-
-    if (n <= TS_CHUNK) {
-        // the whole tile in registers; shared memory between passes
+    uint32_t key[K], val[K], pos[K];
 #pragma unroll
-        for (int k = 0; k < TS_K; ++k) {
-            const int i = w * 32 * TS_K + k * 32 + lane;
-            const uint2 kv = i < n ? A[start + i] : make_uint2(0u, 0u);
-            key[k] = kv.x;
-            val[k] = kv.y;
-        }
-        for (int p = 0; p < npass; ++p) {
-            block_rank(key, n, 8 * p, true, S, pos);
-#pragma unroll
-            for (int k = 0; k < TS_K; ++k) {
-                const int i = w * 32 * TS_K + k * 32 + lane;
-                if (i < n) {
-                    if (pos[k] < (uint32_t)n) { S.key[pos[k]] = key[k]; S.val[pos[k]] = val[k]; }
-                    else atomicOr(status, ERR_COUNT_MISMATCH);
-                }
-            }
-            __syncthreads();
-#pragma unroll
-            for (int k = 0; k < TS_K; ++k) {
-                const int i = w * 32 * TS_K + k * 32 + lane;
-                key[k] = i < n ? S.key[i] : 0u;
-                val[k] = i < n ? S.val[i] : 0u;
-            }
-            __syncthreads();
-        }
-        for (int i = tid; i < n; i += TS_THREADS) {
-            vals_out[start + i] = S.val[i];
-            tile_out[start + i] = (uint32_t)tile;
-        }
-        return;
+    for (int k = 0; k < K; ++k) {
+        const int i = w * 32 * K + k * 32 + lane;
+        const uint2 kv = i < n ? A[start + i] : make_uint2(kbase, 0u);
+        key[k] = kv.x - kbase;
+        val[k] = kv.y;
     }
+    for (int p = 0; p < npass; ++p) {
+        block_rank<K>(key, n, 8 * p, true, S, pos);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int i = w * 32 * K + k * 32 + lane;
+            if (i < n) {
+                if (pos[k] < (uint32_t)n) { S.key[pos[k]] = key[k]; S.val[pos[k]] = val[k]; }
+                else atomicOr(status, ERR_COUNT_MISMATCH);
+            }
+        }
+        __syncthreads();
+        if (p == npass - 1) break;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int i = w * 32 * K + k * 32 + lane;
+            key[k] = i < n ? S.key[i] : 0u;
+            val[k] = i < n ? S.val[i] : 0u;
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < n; i += TS_THREADS) {
+        vals_out[start + i] = S.val[i];
+        tile_out[start + i] = (uint32_t)tile;
+    }
+}
 
-    // large tile: each pass counts the digits over the whole range, then ranks and scatters
-    // it block-tile by block-tile with a running digit base
-    uint2 *src = A, *dst = B;
+// The smallest K-per-thread instance of sort_in_smem that holds n <= TS_CHUNK records.
+__device__ __forceinline__ void sort_chunk(const uint2* __restrict__ A, uint32_t start, int n, int npass,
+                                           uint32_t kbase, int tile, TileSortSmem& S,
+                                           uint32_t* __restrict__ vals_out, uint32_t* __restrict__ tile_out,
+                                           unsigned* __restrict__ status)
+{
+    if (n <= TS_THREADS) sort_in_smem<1>(A, start, n, npass, kbase, tile, S, vals_out, tile_out, status);
+    else if (n <= 2 * TS_THREADS) sort_in_smem<2>(A, start, n, npass, kbase, tile, S, vals_out, tile_out, status);
+    else if (n <= 4 * TS_THREADS) sort_in_smem<4>(A, start, n, npass, kbase, tile, S, vals_out, tile_out, status);
+    else if (n <= 8 * TS_THREADS) sort_in_smem<8>(A, start, n, npass, kbase, tile, S, vals_out, tile_out, status);
+    else sort_in_smem<TS_K>(A, start, n, npass, kbase, tile, S, vals_out, tile_out, status);
+}
+
+// Unordered split of src[start, start + n) by the digit (key >> sh) & 255 into
+// dst[start, start + n), bucket after bucket: the bucket sizes and offsets (from start) go to
+// S.b_cnt[lv] / S.b_off[lv].  Keys are unique within a tile, so the order inside a bucket is
+// left to the bucket's own sort.  A warp's lanes of one digit take one shared-memory atomic.
+constexpr int SPLIT_K = 8;   // keys per thread per round of the split
+__device__ __forceinline__ void msd_split(const uint2* __restrict__ src, uint2* __restrict__ dst, uint32_t start,
+                                          int n, int sh, int lv, TileSortSmem& S, unsigned* __restrict__ status)
+{
+    const int tid = threadIdx.x, lane = tid & 31;
+    const uint32_t lt = lanemask_lt();
+    S.base[tid] = 0u;
+    __syncthreads();
+    for (int c0 = 0; c0 < n; c0 += TS_THREADS * SPLIT_K) {
+        uint32_t d[SPLIT_K];
+#pragma unroll
+        for (int k = 0; k < SPLIT_K; ++k) {
+            const int i = c0 + k * TS_THREADS + tid;
+            d[k] = i < n ? (src[start + i].x >> sh) & 255u : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < SPLIT_K; ++k) {
+            const bool valid = c0 + k * TS_THREADS + tid < n;
+            const uint32_t peers = digit_peers(d[k], valid);
+            if (valid && lane == 31 - __clz(peers)) atomicAdd(&S.base[d[k]], (uint32_t)__popc(peers));
+        }
+    }
+    __syncthreads();
+    {
+        const uint32_t c = S.base[tid];
+        uint32_t tot;
+        const uint32_t ex = block_exclusive_scan(c, S.wsum, tot);
+        S.b_cnt[lv][tid] = c;
+        S.b_off[lv][tid] = ex;
+        S.base[tid] = ex;
+    }
+    __syncthreads();
+    for (int c0 = 0; c0 < n; c0 += TS_THREADS * SPLIT_K) {
+        uint2 kv[SPLIT_K];
+#pragma unroll
+        for (int k = 0; k < SPLIT_K; ++k) {
+            const int i = c0 + k * TS_THREADS + tid;
+            kv[k] = i < n ? src[start + i] : make_uint2(0u, 0u);
+        }
+#pragma unroll
+        for (int k = 0; k < SPLIT_K; ++k) {
+            const bool valid = c0 + k * TS_THREADS + tid < n;
+            const uint32_t d = (kv[k].x >> sh) & 255u;
+            const uint32_t peers = digit_peers(d, valid);
+            const int leader = 31 - __clz(peers);
+            uint32_t b = 0u;
+            if (valid && lane == leader) b = atomicAdd(&S.base[d], (uint32_t)__popc(peers));
+            b = __shfl_sync(FULL, b, leader & 31);
+            if (valid) {
+                const uint32_t pos = b + __popc(peers & lt);
+                if (pos < (uint32_t)n) dst[start + pos] = kv[k];
+                else atomicOr(status, ERR_COUNT_MISMATCH);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// LSD sort of src[start, start + n) (any size) over npass 8-bit digits in passes over global
+// memory, ping-pong with dst; the last pass writes the values and tile ids.  Each pass counts
+// the digits over the whole range, then ranks and scatters it block-tile by block-tile with a
+// running digit base.
+__device__ __forceinline__ void lsd_global(uint2* __restrict__ src, uint2* __restrict__ dst, uint32_t start, int n,
+                                           int npass, int tile, TileSortSmem& S, uint32_t* __restrict__ vals_out,
+                                           uint32_t* __restrict__ tile_out, unsigned* __restrict__ status)
+{
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    uint32_t key[TS_K], val[TS_K], pos[TS_K];
     for (int p = 0; p < npass; ++p) {
         const int sh = 8 * p;
         const bool last = p == npass - 1;
-        if (tid < 256) S.base[tid] = 0u;
+        S.base[tid] = 0u;
         __syncthreads();
         for (int c0 = 0; c0 < n; c0 += TS_CHUNK) {
             const int cnt = min(TS_CHUNK, n - c0);
@@ -246,6 +322,82 @@ __global__ void __launch_bounds__(TS_THREADS, SVR_TS_MINB) tile_sort_kernel(
     }
 }
 
+// The buckets of split level LV of src[start, ...): runs of consecutive buckets of at most
+// TS_CHUNK records in all are sorted in shared memory by key - (their first key's digits), over
+// the bits below the split digit plus those of the run's digit span; a bucket above TS_CHUNK is
+// split again on the next 8 bits (level 1) or, past two levels, sorted by global passes.  Every
+// thread walks the same buckets (shared-memory sizes), so the barriers inside are uniform.
+template <int LV>
+__device__ void sort_buckets(uint2* __restrict__ src, uint2* __restrict__ alt, uint32_t start, int sh,
+                             uint32_t prefix, int tile, TileSortSmem& S, uint32_t* __restrict__ vals_out,
+                             uint32_t* __restrict__ tile_out, unsigned* __restrict__ status)
+{
+    int b = 0;
+    while (b < 256) {
+        const uint32_t c = S.b_cnt[LV][b];
+        if (c == 0u) { ++b; continue; }
+        const uint32_t o = start + S.b_off[LV][b];
+        if (c > (uint32_t)TS_CHUNK) {
+            if constexpr (LV == 0) {
+                if (sh > 0) {
+                    const int sh2 = sh > 8 ? sh - 8 : 0;
+                    msd_split(src, alt, o, (int)c, sh2, 1, S, status);
+                    sort_buckets<1>(alt, src, o, sh2, prefix | ((uint32_t)b << sh), tile, S, vals_out, tile_out,
+                                    status);
+                    ++b;
+                    continue;
+                }
+            }
+            lsd_global(src, alt, o, (int)c, max(1, (sh + 7) / 8), tile, S, vals_out, tile_out, status);
+            ++b;
+            continue;
+        }
+        int e = b + 1, last = b;
+        uint32_t sum = c;
+        while (e < 256) {
+            const uint32_t ce = S.b_cnt[LV][e];
+            if (ce > (uint32_t)TS_CHUNK || sum + ce > (uint32_t)TS_CHUNK) break;
+            if (ce) { sum += ce; last = e; }
+            ++e;
+        }
+        // keys of the run: prefix | digit << sh | low bits, digit in [b, last]
+        const uint64_t span = ((uint64_t)(last - b + 1) << sh) - 1u;
+        const int bits = span ? 64 - __clzll((long long)span) : 0;
+        sort_chunk(src, o, (int)sum, max(1, (bits + 7) / 8), prefix | ((uint32_t)b << sh), tile, S, vals_out,
+                   tile_out, status);
+        b = e;
+    }
+}
+
+// Sort of one tile's records [start, start + n) by key (pair position), values along.
+// Input in A as (key, value) pairs; the sorted values go to vals_out and the tile id of every
+// record to tile_out.  A tile of at most TS_CHUNK records is sorted in shared memory; a larger
+// one is split on its top 8 key bits into B, bucket runs are then sorted in shared memory
+// (sort_buckets), with A as scratch.
+#ifndef SVR_TS_MINB
+#define SVR_TS_MINB 2
+#endif
+__global__ void __launch_bounds__(TS_THREADS, SVR_TS_MINB) tile_sort_kernel(
+    int T, const uint32_t* __restrict__ order, const uint2* __restrict__ ranges, int key_bits,
+    uint2* __restrict__ A, uint2* __restrict__ B,
+    uint32_t* __restrict__ vals_out, uint32_t* __restrict__ tile_out, unsigned* __restrict__ status)
+{
+    extern __shared__ __align__(16) unsigned char ts_smem[];
+    TileSortSmem& S = *reinterpret_cast<TileSortSmem*>(ts_smem);
+    const int tile = order ? (int)order[blockIdx.x] : (int)blockIdx.x;
+    if (tile >= T) return;
+    const uint2 rg = ranges[tile];
+    if (rg.y <= rg.x) return;
+    const uint32_t start = rg.x;
+    const int n = (int)(rg.y - rg.x);
+    if (n <= TS_CHUNK) {
+        sort_chunk(A, start, n, max(1, (key_bits + 7) / 8), 0u, tile, S, vals_out, tile_out, status);
+        return;
+    }
+    const int sh = key_bits > 8 ? key_bits - 8 : 0;
+    msd_split(A, B, start, n, sh, 0, S, status);
+    sort_buckets<0>(B, A, start, sh, 0u, tile, S, vals_out, tile_out, status);
+}
 }  // namespace svr
 
 namespace svr {
@@ -256,6 +408,29 @@ __device__ __forceinline__ void item_rect(const uint2 bb, int gx, int gy, int& t
     ty0 = max(0, min(gy - 1, (int)((bb.x << 16 >> 16) / TILE)));
     tx1 = max(0, min(gx - 1, (int)((bb.y >> 16) / TILE)));
     ty1 = max(0, min(gy - 1, (int)((bb.y << 16 >> 16) / TILE)));
+}
+
+// Items per thread per round of the count and scatter loops: their loads are issued together.
+constexpr int ITEM_U = 4;
+
+// The rendered items among v0 + tid + u * blockDim.x (u < ITEM_U, below v1) of view vi: octant
+// bits (0 = not rendered) and bbox.
+__device__ __forceinline__ void load_items(int i0, int v1, int vi, int N, const uint32_t* __restrict__ ndup,
+                                           const uint2* __restrict__ bboxes, const uint32_t* __restrict__ bits,
+                                           uint32_t (&qb)[ITEM_U], uint2 (&bb)[ITEM_U])
+{
+    uint32_t nd[ITEM_U];
+#pragma unroll
+    for (int u = 0; u < ITEM_U; ++u) {
+        const int i = i0 + u * (int)blockDim.x;
+        nd[u] = i < v1 ? ndup[(size_t)vi * N + i] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < ITEM_U; ++u) {
+        const size_t item = (size_t)vi * N + i0 + u * (int)blockDim.x;
+        qb[u] = nd[u] ? bits[item] : 0u;
+        bb[u] = nd[u] ? bboxes[item] : make_uint2(0u, 0u);
+    }
 }
 
 // Records per tile.  Grid (chunks, views): each CTA visits a range of the voxels of view
@@ -278,14 +453,19 @@ __global__ void __launch_bounds__(256) tile_count_kernel(
     }
     const int per = (N + gridDim.x - 1) / gridDim.x;
     const int v0 = blockIdx.x * per, v1 = min(N, v0 + per);
-    for (int i = v0 + threadIdx.x; i < v1; i += blockDim.x) {
-        const size_t item = (size_t)vi * N + i;
-        if (ndup[item] == 0u) continue;
-        const uint32_t k = __popc(bits[item]);
-        int tx0, ty0, tx1, ty1;
-        item_rect(bboxes[item], gx, gy, tx0, ty0, tx1, ty1);
-        for (int y = ty0; y <= ty1; ++y)
-            for (int x = tx0; x <= tx1; ++x) atomicAdd(&cnt[y * gx + x], k);
+    for (int i0 = v0 + threadIdx.x; i0 < v1; i0 += ITEM_U * blockDim.x) {
+        uint32_t qb[ITEM_U];
+        uint2 bb[ITEM_U];
+        load_items(i0, v1, vi, N, ndup, bboxes, bits, qb, bb);
+#pragma unroll
+        for (int u = 0; u < ITEM_U; ++u) {
+            if (!qb[u]) continue;
+            const uint32_t k = __popc(qb[u]);
+            int tx0, ty0, tx1, ty1;
+            item_rect(bb[u], gx, gy, tx0, ty0, tx1, ty1);
+            for (int y = ty0; y <= ty1; ++y)
+                for (int x = tx0; x <= tx1; ++x) atomicAdd(&cnt[y * gx + x], k);
+        }
     }
     if (SMEM) {
         __syncthreads();
@@ -464,14 +644,19 @@ __global__ void __launch_bounds__(256) tile_scatter_kernel(
     if (SMEM) {
         for (int i = threadIdx.x; i < nt; i += blockDim.x) hist[i] = 0u;
         __syncthreads();
-        for (int i = v0 + threadIdx.x; i < v1; i += blockDim.x) {
-            const size_t item = (size_t)vi * N + i;
-            if (ndup[item] == 0u) continue;
-            const uint32_t k = __popc(bits[item]);
-            int tx0, ty0, tx1, ty1;
-            item_rect(bboxes[item], gx, gy, tx0, ty0, tx1, ty1);
-            for (int y = ty0; y <= ty1; ++y)
-                for (int x = tx0; x <= tx1; ++x) atomicAdd(&hist[y * gx + x], k);
+        for (int i0 = v0 + threadIdx.x; i0 < v1; i0 += ITEM_U * blockDim.x) {
+            uint32_t qb[ITEM_U];
+            uint2 bb[ITEM_U];
+            load_items(i0, v1, vi, N, ndup, bboxes, bits, qb, bb);
+#pragma unroll
+            for (int u = 0; u < ITEM_U; ++u) {
+                if (!qb[u]) continue;
+                const uint32_t k = __popc(qb[u]);
+                int tx0, ty0, tx1, ty1;
+                item_rect(bb[u], gx, gy, tx0, ty0, tx1, ty1);
+                for (int y = ty0; y <= ty1; ++y)
+                    for (int x = tx0; x <= tx1; ++x) atomicAdd(&hist[y * gx + x], k);
+            }
         }
         __syncthreads();
         for (int i = threadIdx.x; i < nt; i += blockDim.x) {
@@ -480,29 +665,39 @@ __global__ void __launch_bounds__(256) tile_scatter_kernel(
         }
         __syncthreads();
     }
-    for (int i = v0 + threadIdx.x; i < v1; i += blockDim.x) {
-        const size_t item = (size_t)vi * N + i;
-        if (ndup[item] == 0u) continue;
-        const uint32_t qb = bits[item];
-        const uint32_t k = __popc(qb);
-        uint32_t pp[8];
-        const uint4* pq = reinterpret_cast<const uint4*>(pair_pos + 8 * (size_t)i);
-        const uint4 p0 = pq[0], p1 = pq[1];
-        pp[0] = p0.x; pp[1] = p0.y; pp[2] = p0.z; pp[3] = p0.w;
-        pp[4] = p1.x; pp[5] = p1.y; pp[6] = p1.z; pp[7] = p1.w;
-        int tx0, ty0, tx1, ty1;
-        item_rect(bboxes[item], gx, gy, tx0, ty0, tx1, ty1);
-        for (int y = ty0; y <= ty1; ++y)
-            for (int x = tx0; x <= tx1; ++x) {
-                const int lt_ = y * gx + x;
-                uint32_t p = SMEM ? atomicAdd(&hist[lt_], k) : atomicAdd(&cursor[view.tile_offset + lt_], k);
+    for (int i0 = v0 + threadIdx.x; i0 < v1; i0 += ITEM_U * blockDim.x) {
+        uint32_t qb[ITEM_U];
+        uint2 bb[ITEM_U];
+        load_items(i0, v1, vi, N, ndup, bboxes, bits, qb, bb);
+        // pair positions of the first octant of every item (most items have one)
+        uint32_t p0[ITEM_U];
 #pragma unroll
-                for (uint32_t q = 0; q < 8; ++q) {
-                    if (!(qb & (1u << q))) continue;
-                    if ((int64_t)p < cap) kv[p] = make_uint2(pp[q], (q << 29) | (uint32_t)i);
-                    ++p;
+        for (int u = 0; u < ITEM_U; ++u)
+            p0[u] = qb[u] ? pair_pos[(size_t)(__ffs(qb[u]) - 1) * N + i0 + u * (int)blockDim.x] : 0u;
+#pragma unroll
+        for (int u = 0; u < ITEM_U; ++u) {
+            if (!qb[u]) continue;
+            const int i = i0 + u * (int)blockDim.x;
+            const uint32_t q_first = (uint32_t)__ffs(qb[u]) - 1u;
+            const uint32_t k = __popc(qb[u]);
+            uint32_t pp[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                pp[q] = (uint32_t)q == q_first ? p0[u] : ((qb[u] >> q) & 1u ? pair_pos[(size_t)q * N + i] : 0u);
+            int tx0, ty0, tx1, ty1;
+            item_rect(bb[u], gx, gy, tx0, ty0, tx1, ty1);
+            for (int y = ty0; y <= ty1; ++y)
+                for (int x = tx0; x <= tx1; ++x) {
+                    const int lt_ = y * gx + x;
+                    uint32_t p = SMEM ? atomicAdd(&hist[lt_], k) : atomicAdd(&cursor[view.tile_offset + lt_], k);
+#pragma unroll
+                    for (uint32_t q = 0; q < 8; ++q) {
+                        if (!(qb[u] & (1u << q))) continue;
+                        if ((int64_t)p < cap) kv[p] = make_uint2(pp[q], (q << 29) | (uint32_t)i);
+                        ++p;
+                    }
                 }
-            }
+        }
     }
 }
 
@@ -521,10 +716,15 @@ __global__ void pair_rank_kernel(int64_t N, const int64_t* __restrict__ octpaths
     vals[s] = (uint32_t)s;
 }
 
-__global__ void pair_pos_kernel(int64_t n, const uint32_t* __restrict__ sorted_pairs, uint32_t* __restrict__ pos)
+// Octant-major table: entry q*N + v, so the items of a view (mostly one octant over a run of
+// voxel ids) read it coalesced.
+__global__ void pair_pos_kernel(int64_t N, const uint32_t* __restrict__ sorted_pairs, uint32_t* __restrict__ pos)
 {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < n) pos[sorted_pairs[j]] = (uint32_t)j;
+    if (j < 8 * N) {
+        const uint32_t s = sorted_pairs[j];
+        pos[(int64_t)(s & 7u) * N + (s >> 3)] = (uint32_t)j;
+    }
 }
 
 }  // namespace svr

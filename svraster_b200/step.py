@@ -175,11 +175,15 @@ class BatchedTrainStep:
     def _body(self, graph, time_render=False, grad_hook=None):
         marks = []
 
-        def mark(name):
+        def mark(name, event=None):
+            """Event mark ending stage `name`; `event` = one the library records itself."""
             if time_render:
-                e = torch.cuda.Event(enable_timing=True)
-                e.record()
+                e = event
+                if e is None:
+                    e = torch.cuda.Event(enable_timing=True)
+                    e.record()
                 marks.append((name, e))
+        mark.on = time_render
 
         mark("start")
         if self.view_chunk:
@@ -265,9 +269,21 @@ class BatchedTrainStep:
         else:
             state.bin(self.octpath, rank_table=self.rank_table, pair_order=self.pair_order)
         mark("count+sort")
-        color, depth, normal, T, _ = state.render(3, True, True, self.centers, self.lengths, self.geos, self.rgbs,
-                                                  self.s_val, rgb_per_view=True)
-        mark("render_fwd")   # includes the record packing launch
+        pack_ev = None
+        if mark.on and not graph:
+            # the library records this event between its record packing and render launches
+            pack_ev = torch.cuda.Event(enable_timing=True)
+            pack_ev.record()   # creates the event; the library records it again after packing
+            check(L.svr_set_pack_event(pack_ev.cuda_event), "pack event")
+        try:
+            color, depth, normal, T, _ = state.render(3, True, True, self.centers, self.lengths, self.geos,
+                                                      self.rgbs, self.s_val, rgb_per_view=True)
+        finally:
+            if pack_ev is not None:
+                L.svr_set_pack_event(None)
+        if pack_ev is not None:
+            mark("pack", pack_ev)
+        mark("render_fwd")
         return state, color, depth, normal, T
 
     def _backward_part(self, graph, mark, grad_hook, fw, marks, time_render):

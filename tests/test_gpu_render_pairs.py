@@ -37,7 +37,7 @@ def _render_both(sc, cams, track_max_w=False, grads=None):
     saved = _impl()
     outs = []
     try:
-        for impl in (0, 1, 2):
+        for impl in (0, 1, 2, 3):
             assert L.svr_render_set_impl(impl, saved[1]) == 0
             o = st.render(3, True, True, ts["centers"], ts["lengths"], geos, rgbs, s_val, track_max_w=track_max_w,
                           rgb_per_view=len(cams) > 1)
@@ -89,7 +89,7 @@ def _adjoint_both(sc, cams, lambda_R):
     saved = _impl()
     outs = []
     try:
-        for impl in (0, 1, 2):
+        for impl in (0, 1, 2, 3):
             assert L.svr_render_set_impl(saved[0], impl) == 0
             drgbs = torch.zeros(len(cams) * sc.n_vox, 3, device="cuda") if len(cams) > 1 else None
             dvox, ds = st.render_backward(True, True, s_val, T, cat("color"), cat("depth"), cat("normal"), cat("T"),

@@ -47,7 +47,8 @@ def test_pair_order_table_matches_reference_order():
     sc = S.scene_small(seed=3)
     po = PairOrder(torch.as_tensor(sc.octpath.reshape(-1), device="cuda"))
     got = po.pos.cpu().numpy().astype(np.int64)
-    assert np.array_equal(got, _reference_pair_order(sc.octpath))
+    ref = _reference_pair_order(sc.octpath).reshape(sc.n_vox, 8).T.reshape(-1)   # octant-major
+    assert np.array_equal(got, ref)
     assert (1 << po.bits) >= 8 * sc.n_vox
 
 
@@ -126,4 +127,24 @@ def test_tile_binning_mid_size_all_views_equals_radix_sort():
     assert st_t.num_rendered == st_r.num_rendered > 10_000_000
     assert np.array_equal(r_t, r_r)
     assert np.array_equal(v_t, v_r)
+    assert st_t.status() == 0
+
+
+@pytest.mark.parametrize("key_bits", [24, 28, 32])
+def test_tile_sort_paths_for_wider_keys(key_bits):
+    """The same pair positions declared with more key bits move the large tiles' top-digit
+    split onto high (mostly zero) bits: one-bucket splits, second-level splits and, at 32 bits,
+    buckets of more than one block-tile sorted by passes over global memory.  The record order
+    must stay that of the radix sort."""
+    from types import SimpleNamespace
+    sc = S.scene_small(seed=2)
+    cams = S.ring_cameras(2, 3.0, 40, 24, fovx_deg=50.0, phase=0.4)
+    po = PairOrder(torch.as_tensor(sc.octpath.reshape(-1), device="cuda"))
+    assert key_bits >= po.bits
+    wide = SimpleNamespace(pos=po.pos, bits=key_bits, N=po.N)
+    st_t, v_t, r_t = _bin(sc, cams, wide)
+    st_r, v_r, r_r = _bin(sc, cams, None)
+    counts = (r_t[:, 1] - r_t[:, 0]).astype(np.int64)
+    assert counts.max() > 4096
+    assert np.array_equal(v_t, v_r) and np.array_equal(r_t, r_r)
     assert st_t.status() == 0

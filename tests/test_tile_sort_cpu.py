@@ -1,9 +1,10 @@
 """Lane-level restatement, on the CPU, of the per-tile sort's index arithmetic
 (svraster_b200/csrc/tile_sort.cuh): warp-striped block-tiles of TS_THREADS x TS_K keys, digit
 peers from eight ballots, per-warp running digit counts, the block scan of the digit totals
-and the chunked passes of a tile larger than one block-tile.  Checks that the positions it
-computes sort any key set exactly (keys unique, as pair positions are) and stay in range, and
-that the launch-bucket order of the tile scan is heavy first and stable."""
+and the chunked passes over global memory; and the large-tile path (top-digit split, runs of
+buckets sorted over the bits they span, second split, global fallback).  Checks that the
+positions it computes sort any key set exactly (keys unique, as pair positions are) and stay
+in range, and that the launch-bucket order of the tile scan is heavy first and stable."""
 import numpy as np
 import pytest
 
@@ -108,6 +109,112 @@ def test_tile_sort_positions_sort_unique_keys(n, key_bits, seed):
     keys = rng.choice(1 << key_bits, size=n, replace=False)
     out = tile_sort(keys, key_bits)
     assert np.array_equal(out, np.sort(keys))
+
+
+def _lsd_bits_suffice(keys, kbase, npass):
+    """The in-shared-memory and global LSD sorts order by the low 8 * npass bits of key - kbase:
+    exact iff every key of the run is in [kbase, kbase + 2^(8 npass))."""
+    rel = keys.astype(np.int64) - kbase
+    return bool(np.all(rel >= 0) and np.all(rel < (1 << (8 * npass))))
+
+
+def large_tile_sort(keys, key_bits, rng):
+    """Restatement of the large-tile path (msd_split, sort_buckets, lsd_global): split on the
+    top 8 key bits in an arbitrary order inside each bucket, runs of consecutive buckets of at
+    most CHUNK records sorted by their LSD passes (checked to cover the run's keys), a bucket
+    above CHUNK split again on the next 8 bits, and past two splits sorted by global passes.
+    Returns the final order and the path counters."""
+    out = np.full(len(keys), -1, np.int64)
+    stats = {"runs": 0, "level2": 0, "global": 0}
+
+    def split(seg, sh):
+        d = (seg >> sh) & 255
+        cnt = np.bincount(d, minlength=256)
+        off = np.concatenate([[0], np.cumsum(cnt)[:-1]])
+        res = np.empty_like(seg)
+        for b in range(256):
+            part = seg[d == b]
+            res[off[b]:off[b] + cnt[b]] = rng.permutation(part)   # unordered within a bucket
+        return res, cnt, off
+
+    def buckets(seg, start, sh, prefix, cnt, off, level):
+        b = 0
+        while b < 256:
+            c = int(cnt[b])
+            if c == 0:
+                b += 1
+                continue
+            o = int(off[b])
+            if c > CHUNK:
+                sub = seg[o:o + c]
+                if level == 0 and sh > 0:
+                    sh2 = max(sh - 8, 0)
+                    sseg, scnt, soff = split(sub, sh2)
+                    stats["level2"] += 1
+                    buckets(sseg, start + o, sh2, prefix | (b << sh), scnt, soff, 1)
+                else:
+                    npass = max(1, (sh + 7) // 8)
+                    # global passes order by the low 8*npass bits; the bucket's keys share the rest
+                    assert _lsd_bits_suffice(sub, prefix | (b << sh), npass)
+                    out[start + o:start + o + c] = np.sort(sub)
+                    stats["global"] += 1
+                b += 1
+                continue
+            e, last, total = b + 1, b, c
+            while e < 256:
+                ce = int(cnt[e])
+                if ce > CHUNK or total + ce > CHUNK:
+                    break
+                if ce:
+                    total += ce
+                    last = e
+                e += 1
+            span = ((last - b + 1) << sh) - 1
+            npass = max(1, (span.bit_length() + 7) // 8)
+            run = seg[o:o + total]
+            assert _lsd_bits_suffice(run, prefix | (b << sh), npass)
+            out[start + o:start + o + total] = np.sort(run)
+            stats["runs"] += 1
+            b = e
+
+    sh = max(key_bits - 8, 0)
+    seg, cnt, off = split(keys.astype(np.int64), sh)
+    buckets(seg, 0, sh, 0, cnt, off, 0)
+    assert np.all(out >= 0)
+    return out, stats
+
+
+@pytest.mark.parametrize("case", ["uniform", "clustered", "dense_wide", "one_bucket", "small_bits", "tiny_bits",
+                                  "chunk_plus_1"])
+def test_large_tile_split_path_sorts_exactly(case):
+    rng = np.random.default_rng(7)
+    if case == "uniform":
+        kb, keys = 25, rng.choice(1 << 25, size=40000, replace=False)
+    elif case == "clustered":      # a few dense clusters: level-2 splits
+        kb = 25
+        keys = np.unique(np.concatenate([rng.choice(np.arange(c, c + 9000), size=6000, replace=False)
+                                         for c in (5 << 17, (5 << 17) + 40000, 200 << 17)]))
+        keys = np.concatenate([keys, np.arange(100 << 17, (100 << 17) + 12000)])
+    elif case == "dense_wide":     # 30-bit keys, a dense run inside one level-2 bucket: global passes
+        kb = 30
+        keys = np.concatenate([np.arange(3 << 22, (3 << 22) + 7000), rng.choice(1 << 30, size=3000, replace=False)])
+        keys = np.unique(keys)
+    elif case == "one_bucket":     # every key in one top-digit bucket
+        kb, keys = 24, (7 << 16) + rng.choice(1 << 16, size=20000, replace=False)
+    elif case == "small_bits":
+        kb, keys = 14, rng.choice(1 << 14, size=9000, replace=False)
+    elif case == "tiny_bits":
+        kb, keys = 13, np.arange(1 << 13)
+    else:
+        kb, keys = 20, rng.choice(1 << 20, size=CHUNK + 1, replace=False)
+    keys = rng.permutation(np.asarray(keys, np.int64))
+    assert keys.max() < (1 << kb)
+    out, stats = large_tile_sort(keys, kb, rng)
+    assert np.array_equal(out, np.sort(keys))
+    if case == "clustered":
+        assert stats["level2"] >= 1, stats
+    if case == "dense_wide":
+        assert stats["level2"] >= 1 and stats["global"] >= 1, stats
 
 
 def heavy_bucket(c):
