@@ -158,15 +158,16 @@ SVR_API int svr_render_bwd(const svr_view_t* views_host, int n_views, int N, int
                    const float* dL_dnormal, const float* dL_dT,
                    float* dL_dvox, float* drgbs, float* dL_ds, void* stream);
 
-/* Launch configurations of the render kernels (no counterpart in the reference): ring slots
- * and CTAs per SM, which change the schedule only (every configuration gives the same
- * outputs).  pass 0 = forward, 1 = adjoint; configuration 0 is the default, which follows
- * the launch size: under 8192 tiles the forward takes configuration 2 and the adjoint 2,
- * under 16384 tiles the adjoint takes 4.  The choice is
- * process-wide and read when a launch is issued; svraster_b200.autotune times them on the
- * caller's workload. */
+/* Launch variants of the render kernels (no counterpart in the reference): kernel family (as
+ * svr_render_set_impl numbers them), ring slots and CTAs per SM, which change the schedule
+ * only (every variant gives the same forward outputs and the same gradients up to the order of
+ * float atomics).  pass 0 = forward, 1 = adjoint.  Variant 0 is the family chosen by
+ * svr_render_set_impl (default 3) in its default configuration (for family 0 it follows the
+ * launch size); the others name their family.  svr_render_set_impl resets the choice to 0.
+ * The choice is process-wide and read when a launch is issued; svraster_b200.autotune times
+ * the variants on the caller's workload. */
 SVR_API int svr_render_config_count(int* n_fwd, int* n_bwd);
-SVR_API int svr_render_config_describe(int pass, int index, int* ring, int* ctas_per_sm);
+SVR_API int svr_render_config_describe(int pass, int index, int* impl, int* ring, int* ctas_per_sm);
 SVR_API int svr_render_set_config(int fwd_index, int bwd_index);
 SVR_API int svr_render_get_config(int* fwd_index, int* bwd_index);
 
@@ -207,8 +208,8 @@ SVR_API int svr_bin_tiles(const svr_view_t* views_host, int n_views, int N, int6
 /* Which render kernels later launches use (no counterpart in the reference; a process-wide
  * choice read when a launch is issued), for the forward and the adjoint: 0 = per-warp filter
  * with one pixel per lane, 1 = record-parallel filter with dense pair evaluation, warps on
- * 8x4 pixel blocks, 2 (the default) = the same with every warp on a lattice spread over the
- * tile.  Every choice gives the same forward outputs bit for bit and the same gradients up to
+ * 8x4 pixel blocks, 2 = the same with every warp on a lattice spread over the tile, 3 (the
+ * default) = the same with a slot's pairs numbered and evaluated over the whole CTA.  Every choice gives the same forward outputs bit for bit and the same gradients up to
  * the order of their float atomics. */
 SVR_API int svr_render_set_impl(int fwd_impl, int bwd_impl);
 SVR_API int svr_render_get_impl(int* fwd_impl, int* bwd_impl);

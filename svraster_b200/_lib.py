@@ -54,7 +54,7 @@ _SIGS = {
     "svr_agg_voxel_into_grid_pts": (_I, [_I64, _I, _P, _P, _I64, _P, _P, _P, _P]),
     "svr_training_stat_reduce": (_I, [_I, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "svr_render_config_count": (_I, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),
-    "svr_render_config_describe": (_I, [_I, _I, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "svr_render_config_describe": (_I, [_I, _I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "svr_render_set_config": (_I, [_I, _I]),
     "svr_render_get_config": (_I, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "svr_binning_count": (_I, [_P, C.POINTER(C.c_int64), _P]),

@@ -1,9 +1,10 @@
-"""Autotuner for the render kernels' launch configuration.
+"""Autotuner for the render kernels' launch variant.
 
-The forward and adjoint tile kernels come in several compiled configurations of ring depth
-(shared-memory slots of 128 records) and CTAs per SM (the occupancy the register allocator is
-asked to meet).  These change only the schedule: every configuration produces the same
-outputs.  Which one is fastest depends on the workload (records per tile, image sizes, how
+The forward and adjoint tile kernels come in several compiled variants: the kernel family
+(pairs numbered over the whole CTA, pairs per warp, or the per-warp filter kernels), ring
+depth (shared-memory slots of 128 records) and CTAs per SM (the occupancy the register
+allocator is asked to meet).  These change only the schedule: every variant produces the same
+forward outputs bit for bit and the same gradients up to the order of float atomics.  Which one is fastest depends on the workload (records per tile, image sizes, how
 unevenly the work falls on the tiles), so the tuner times each on the caller's own binned
 batch and keeps the fastest.  Tile shape and samples per voxel are not tuned: the 16x16 tile
 is part of the binning format the buffers share with the reference's, and the number of
@@ -25,7 +26,7 @@ from ._lib import check
 
 
 def configs():
-    """{"fwd": [(index, ring, ctas_per_sm), ...], "bwd": [...]}"""
+    """{"fwd": [(index, impl, ring, ctas_per_sm), ...], "bwd": [...]}"""
     L = _lib.load()
     nf, nb = C.c_int(0), C.c_int(0)
     check(L.svr_render_config_count(C.byref(nf), C.byref(nb)), "config count")
@@ -33,11 +34,16 @@ def configs():
     for name, pass_id, n in (("fwd", 0, nf.value), ("bwd", 1, nb.value)):
         rows = []
         for i in range(n):
-            ring, ctas = C.c_int(0), C.c_int(0)
-            check(L.svr_render_config_describe(pass_id, i, C.byref(ring), C.byref(ctas)), "config describe")
-            rows.append((i, ring.value, ctas.value))
+            impl, ring, ctas = C.c_int(0), C.c_int(0), C.c_int(0)
+            check(L.svr_render_config_describe(pass_id, i, C.byref(impl), C.byref(ring), C.byref(ctas)),
+                  "config describe")
+            rows.append((i, impl.value, ring.value, ctas.value))
         out[name] = rows
     return out
+
+
+def _label(impl, ring, ctas):
+    return f"impl{impl}_ring{ring}_cta{ctas}"
 
 
 def get_config():
@@ -78,18 +84,18 @@ def tune_render(run_fwd, run_bwd, reps=3, key=None, cache=None):
     cfg = configs()
     f0, b0 = get_config()
     ms_f, ms_b = {}, {}
-    for i, ring, ctas in cfg["fwd"]:
+    for i, impl, ring, ctas in cfg["fwd"]:
         set_config(i, b0)
-        ms_f[f"ring{ring}_cta{ctas}"] = (i, _time(run_fwd, reps))
+        ms_f[_label(impl, ring, ctas)] = (i, _time(run_fwd, reps))
     best_f = min(ms_f.values(), key=lambda t: t[1])[0]
-    for i, ring, ctas in cfg["bwd"]:
+    for i, impl, ring, ctas in cfg["bwd"]:
         set_config(best_f, i)
-        ms_b[f"ring{ring}_cta{ctas}"] = (i, _time(run_bwd, reps))
+        ms_b[_label(impl, ring, ctas)] = (i, _time(run_bwd, reps))
     best_b = min(ms_b.values(), key=lambda t: t[1])[0]
     set_config(best_f, best_b)
     res = {"fwd": best_f, "bwd": best_b,
-           "fwd_config": dict(zip(("ring", "ctas_per_sm"), cfg["fwd"][best_f][1:])),
-           "bwd_config": dict(zip(("ring", "ctas_per_sm"), cfg["bwd"][best_b][1:])),
+           "fwd_config": dict(zip(("impl", "ring", "ctas_per_sm"), cfg["fwd"][best_f][1:])),
+           "bwd_config": dict(zip(("impl", "ring", "ctas_per_sm"), cfg["bwd"][best_b][1:])),
            "ms": {"fwd": {k: round(v[1], 4) for k, v in ms_f.items()},
                   "bwd": {k: round(v[1], 4) for k, v in ms_b.items()}}}
     if cache and key:

@@ -901,15 +901,18 @@ __global__ void __launch_bounds__(256) pack_records_kernel(
 // Which render kernels the launches use: 0 = the warp-filter kernels (render_fwd_kernel /
 // render_bwd_kernel), 1 = record-parallel filter with dense pair evaluation
 // (render_fwd_pairs_kernel / render_bwd_pairs_kernel) with warps on 8x4 pixel blocks, 2 = the
-// same with every warp on a lattice spread over the tile, 3 = the same with the pairs of a slot
-// numbered and evaluated over the whole CTA.  All give the same forward outputs
+// same with every warp on a lattice spread over the tile, 3 (the default) = the same with the
+// pairs of a slot numbered and evaluated over the whole CTA.  All give the same forward outputs
 // bit for bit and the same gradients up to the order of their float atomics.
-static std::atomic<int> g_fwd_impl{2}, g_bwd_impl{2};
+static std::atomic<int> g_fwd_impl{3}, g_bwd_impl{3};
+static std::atomic<int> g_fwd_cfg{0}, g_bwd_cfg{0};   // launch variant (kFwdCfgs / kBwdCfgs)
 extern "C" int svr_render_set_impl(int fwd_impl, int bwd_impl)
 {
     if (fwd_impl < 0 || fwd_impl > 3 || bwd_impl < 0 || bwd_impl > 3) return svr_fail(SVR_ERR_ARG, "render impl");
     g_fwd_impl.store(fwd_impl);
     g_bwd_impl.store(bwd_impl);
+    g_fwd_cfg.store(0);            // the family's default configuration
+    g_bwd_cfg.store(0);
     return SVR_OK;
 }
 extern "C" int svr_render_get_impl(int* fwd_impl, int* bwd_impl)
@@ -934,14 +937,15 @@ extern "C" int svr_set_pack_event(void* event)
 #ifndef SVR_PBWD_MINB
 #define SVR_PBWD_MINB 3
 #endif
-template <bool DEPTH, bool NORMAL, bool RCONC, bool LATTICE = true, bool CTAW = false>
+template <bool DEPTH, bool NORMAL, bool RCONC, bool LATTICE = true, bool CTAW = false, int RING = SVR_PBWD_RING,
+          int MINB = SVR_PBWD_MINB>
 static int launch_bwd_pairs(int T, int N, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
                             const uint32_t* tl, const uint32_t* nc, const Rec* recs, const float* s_val,
                             const float* out_T, const float* dc, const float* dd, const float* dn, const float* dT,
                             float lam, const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status)
 {
-    auto k = render_bwd_pairs_kernel<DEPTH, NORMAL, RCONC, SVR_PBWD_RING, SVR_PBWD_MINB, LATTICE, CTAW>;
-    const int smem = (int)sizeof(PairBwdSmem<SVR_PBWD_RING>);
+    auto k = render_bwd_pairs_kernel<DEPTH, NORMAL, RCONC, RING, MINB, LATTICE, CTAW>;
+    const int smem = (int)sizeof(PairBwdSmem<RING>);
     static std::atomic<unsigned long long> done{0};
     int rc = ensure_smem(k, smem, done);
     if (rc) return rc;
@@ -957,14 +961,15 @@ static int launch_bwd_pairs(int T, int N, cudaStream_t st, const Views& V, const
 #ifndef SVR_PFWD_MINB
 #define SVR_PFWD_MINB 4
 #endif
-template <int NS, bool DEPTH, bool NORMAL, bool MAXW, bool COUNT, bool LATTICE = true, bool CTAW = false>
+template <int NS, bool DEPTH, bool NORMAL, bool MAXW, bool COUNT, bool LATTICE = true, bool CTAW = false,
+          int RING = SVR_PFWD_RING, int MINB = SVR_PFWD_MINB>
 static int launch_fwd_pairs(int T, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
                             const Rec* recs, const float* s_val, uint32_t* tile_last, uint32_t* n_contrib,
                             float* color, float* depth, float* normal, float* outT, float* max_w, int64_t mw_stride,
                             unsigned* status, unsigned long long* pair_count)
 {
-    auto k = render_fwd_pairs_kernel<NS, DEPTH, NORMAL, MAXW, SVR_PFWD_RING, SVR_PFWD_MINB, COUNT, LATTICE, CTAW>;
-    const int smem = (int)sizeof(PairFwdSmem<SVR_PFWD_RING>);
+    auto k = render_fwd_pairs_kernel<NS, DEPTH, NORMAL, MAXW, RING, MINB, COUNT, LATTICE, CTAW>;
+    const int smem = (int)sizeof(PairFwdSmem<RING>);
     static std::atomic<unsigned long long> done{0};
     int rc = ensure_smem(k, smem, done);
     if (rc) return rc;
@@ -974,18 +979,20 @@ static int launch_fwd_pairs(int T, cudaStream_t st, const Views& V, const uint32
     return SVR_OK;
 }
 
-// Launch configurations (ring slots, CTAs per SM) the tuner chooses between for the
+// Launch variants (kernel family, ring slots, CTAs per SM) the tuner chooses between for the
 // common flag sets (three sub-samples, depth and normal on; with or without the
-// R-concentration term).  Index 0 is the default build configuration.  The choice is process-
-// wide and read when a launch is issued (so a captured graph keeps the one in force then).
-struct RenderCfg { int ring, minb; };
-static const RenderCfg kFwdCfgs[] = {{SVR_NSLOT, SVR_FWD_MINB}, {3, 4}, {4, 3}, {3, 3}, {3, 5}, {4, 5}};
-static const RenderCfg kBwdCfgs[] = {{SVR_BWD_NSLOT, SVR_BWD_MINB}, {3, 3}, {4, 2}, {3, 2}, {4, 3}, {4, 4}};
+// R-concentration term).  Index 0 = the family selected by svr_render_set_impl (default 3) in
+// its default configuration; the others name their family.  The choice is process-wide and
+// read when a launch is issued (so a captured graph keeps the one in force then).
+struct RenderCfg { int impl, ring, minb; };
+static const RenderCfg kFwdCfgs[] = {{3, SVR_PFWD_RING, SVR_PFWD_MINB}, {3, 3, 3}, {3, 4, 3},
+                                     {2, SVR_PFWD_RING, SVR_PFWD_MINB}, {0, SVR_NSLOT, SVR_FWD_MINB}, {0, 4, 3}};
+static const RenderCfg kBwdCfgs[] = {{3, SVR_PBWD_RING, SVR_PBWD_MINB}, {3, 3, 2}, {3, 4, 2},
+                                     {2, SVR_PBWD_RING, SVR_PBWD_MINB}, {0, SVR_BWD_NSLOT, SVR_BWD_MINB}, {0, 4, 2}};
 constexpr int N_FWD_CFGS = 6, N_BWD_CFGS = 6;
-static std::atomic<int> g_fwd_cfg{0}, g_bwd_cfg{0};
-// The default configuration follows the launch size.  Launches of a few thousand tiles are
-// bound by their heaviest tiles and run best with more registers per thread; measured with
-// the tuner on the mid-size scene (800x800 views, 2500 tiles each):
+// The per-warp filter kernels' default configuration follows the launch size.  Launches of a
+// few thousand tiles are bound by their heaviest tiles and run best with more registers per
+// thread; measured with the tuner on the mid-size scene (800x800 views, 2500 tiles each):
 //   1 view  : forward 4x3 0.954 ms (4x4 1.006); adjoint 4x2 1.085 ms (4x3 1.185, 3x4 1.30)
 //   2 views : forward 4x3 1.089 ms (4x4 1.163); adjoint 4x2 1.139 ms (4x3 1.287)
 //   4 views : forward 4x4 1.382 ms;             adjoint 4x3 1.466 ms (3x4 1.664)
@@ -1000,11 +1007,12 @@ extern "C" int svr_render_config_count(int* n_fwd, int* n_bwd)
     return SVR_OK;
 }
 
-extern "C" int svr_render_config_describe(int pass, int index, int* ring, int* ctas_per_sm)
+extern "C" int svr_render_config_describe(int pass, int index, int* impl, int* ring, int* ctas_per_sm)
 {
     const int n = pass == 0 ? N_FWD_CFGS : N_BWD_CFGS;
     if (index < 0 || index >= n) return svr_fail(SVR_ERR_ARG, "render config index");
     const RenderCfg c = pass == 0 ? kFwdCfgs[index] : kBwdCfgs[index];
+    if (impl) *impl = c.impl;
     if (ring) *ring = c.ring;
     if (ctas_per_sm) *ctas_per_sm = c.minb;
     return SVR_OK;
@@ -1049,34 +1057,28 @@ static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint32_t* or
                       const float* s_val, uint32_t* tile_last, uint32_t* n_contrib, float* color, float* depth,
                       float* normal, float* outT, float* max_w, int64_t mw_stride, unsigned* status)
 {
-    if (g_fwd_impl.load() == 1)
-        return launch_fwd_pairs<NS, DEPTH, NORMAL, MAXW, false, false>(T, st, V, order, ranges, recs, s_val,
-                                                                       tile_last, n_contrib, color, depth, normal,
-                                                                       outT, max_w, mw_stride, status, nullptr);
-    if (g_fwd_impl.load() == 2)
-        return launch_fwd_pairs<NS, DEPTH, NORMAL, MAXW, false, true>(T, st, V, order, ranges, recs, s_val,
-                                                                      tile_last, n_contrib, color, depth, normal,
-                                                                      outT, max_w, mw_stride, status, nullptr);
-    if (g_fwd_impl.load() == 3)
-        return launch_fwd_pairs<NS, DEPTH, NORMAL, MAXW, false, true, true>(T, st, V, order, ranges, recs, s_val,
-                                                                            tile_last, n_contrib, color, depth,
-                                                                            normal, outT, max_w, mw_stride, status,
-                                                                            nullptr);
+#define FWD_PAIR_ARGS T, st, V, order, ranges, recs, s_val, tile_last, n_contrib, color, depth, normal, outT, max_w, mw_stride, status, nullptr
 #define FWD_CFG_ARGS T, st, V, order, ranges, recs, s_val, tile_last, n_contrib, color, depth, normal, outT, max_w, mw_stride, status
     if constexpr (NS == 3 && DEPTH && NORMAL && !MAXW) {
-        int cfg = g_fwd_cfg.load();
-        if (cfg == 0 && T < SMALL_LAUNCH_TILES) cfg = 2;          // 4 x 3
-        switch (cfg) {
-            case 1: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 3, 4>(FWD_CFG_ARGS);
-            case 2: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 4, 3>(FWD_CFG_ARGS);
-            case 3: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 3, 3>(FWD_CFG_ARGS);
-            case 4: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 3, 5>(FWD_CFG_ARGS);
-            case 5: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 4, 5>(FWD_CFG_ARGS);
+        switch (g_fwd_cfg.load()) {       // kFwdCfgs
+            case 1: return launch_fwd_pairs<NS, DEPTH, NORMAL, MAXW, false, true, true, 3, 3>(FWD_PAIR_ARGS);
+            case 2: return launch_fwd_pairs<NS, DEPTH, NORMAL, MAXW, false, true, true, 4, 3>(FWD_PAIR_ARGS);
+            case 3: return launch_fwd_pairs<NS, DEPTH, NORMAL, MAXW, false, true, false>(FWD_PAIR_ARGS);
+            case 4: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, SVR_NSLOT, SVR_FWD_MINB>(FWD_CFG_ARGS);
+            case 5: return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 4, 3>(FWD_CFG_ARGS);
             default: break;
         }
     }
+    const int impl = g_fwd_impl.load();
+    if (impl == 1) return launch_fwd_pairs<NS, DEPTH, NORMAL, MAXW, false, false>(FWD_PAIR_ARGS);
+    if (impl == 2) return launch_fwd_pairs<NS, DEPTH, NORMAL, MAXW, false, true>(FWD_PAIR_ARGS);
+    if (impl == 3) return launch_fwd_pairs<NS, DEPTH, NORMAL, MAXW, false, true, true>(FWD_PAIR_ARGS);
+    if constexpr (NS == 3 && DEPTH && NORMAL && !MAXW) {
+        if (T < SMALL_LAUNCH_TILES) return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, 4, 3>(FWD_CFG_ARGS);
+    }
     return launch_fwd_cfg<NS, DEPTH, NORMAL, MAXW, SVR_NSLOT, SVR_FWD_MINB>(FWD_CFG_ARGS);
 #undef FWD_CFG_ARGS
+#undef FWD_PAIR_ARGS
 }
 
 static int render_fwd_impl(const svr_view_t* views_host, int n_views, int N, int64_t R, int n_samp,
@@ -1241,21 +1243,23 @@ static int launch_bwd(int T, int N, cudaStream_t st, const Views& V, const uint3
                       const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status)
 {
 #define BWD_CFG_ARGS T, N, st, V, order, ranges, tl, nc, recs, s_val, out_T, dc, dd, dn, dT, lam, gt, dvox, drgbs, ds, status
-    if (g_bwd_impl.load() == 1) return launch_bwd_pairs<DEPTH, NORMAL, RCONC, false>(BWD_CFG_ARGS);
-    if (g_bwd_impl.load() == 2) return launch_bwd_pairs<DEPTH, NORMAL, RCONC, true>(BWD_CFG_ARGS);
-    if (g_bwd_impl.load() == 3) return launch_bwd_pairs<DEPTH, NORMAL, RCONC, true, true>(BWD_CFG_ARGS);
     if constexpr (DEPTH && NORMAL) {
-        int cfg = g_bwd_cfg.load();
-        if (cfg == 0 && T < SMALL_LAUNCH_TILES) cfg = 2;          // 4 x 2
-        else if (cfg == 0 && T < MEDIUM_LAUNCH_TILES) cfg = 4;    // 4 x 3
-        switch (cfg) {
-            case 1: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 3, 3>(BWD_CFG_ARGS);
-            case 2: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 4, 2>(BWD_CFG_ARGS);
-            case 3: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 3, 2>(BWD_CFG_ARGS);
-            case 4: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 4, 3>(BWD_CFG_ARGS);
-            case 5: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 4, 4>(BWD_CFG_ARGS);
+        switch (g_bwd_cfg.load()) {       // kBwdCfgs
+            case 1: return launch_bwd_pairs<DEPTH, NORMAL, RCONC, true, true, 3, 2>(BWD_CFG_ARGS);
+            case 2: return launch_bwd_pairs<DEPTH, NORMAL, RCONC, true, true, 4, 2>(BWD_CFG_ARGS);
+            case 3: return launch_bwd_pairs<DEPTH, NORMAL, RCONC, true, false>(BWD_CFG_ARGS);
+            case 4: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, SVR_BWD_NSLOT, SVR_BWD_MINB>(BWD_CFG_ARGS);
+            case 5: return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 4, 2>(BWD_CFG_ARGS);
             default: break;
         }
+    }
+    const int impl = g_bwd_impl.load();
+    if (impl == 1) return launch_bwd_pairs<DEPTH, NORMAL, RCONC, false>(BWD_CFG_ARGS);
+    if (impl == 2) return launch_bwd_pairs<DEPTH, NORMAL, RCONC, true>(BWD_CFG_ARGS);
+    if (impl == 3) return launch_bwd_pairs<DEPTH, NORMAL, RCONC, true, true>(BWD_CFG_ARGS);
+    if constexpr (DEPTH && NORMAL) {
+        if (T < SMALL_LAUNCH_TILES) return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 4, 2>(BWD_CFG_ARGS);
+        if (T < MEDIUM_LAUNCH_TILES) return launch_bwd_cfg<DEPTH, NORMAL, RCONC, 4, 3>(BWD_CFG_ARGS);
     }
     return launch_bwd_cfg<DEPTH, NORMAL, RCONC, SVR_BWD_NSLOT, SVR_BWD_MINB>(BWD_CFG_ARGS);
 #undef BWD_CFG_ARGS

@@ -270,7 +270,7 @@ class BatchedTrainStep:
             state.bin(self.octpath, rank_table=self.rank_table, pair_order=self.pair_order)
         mark("count+sort")
         pack_ev = None
-        if mark.on and not graph:
+        if getattr(mark, "on", False) and not graph:
             # the library records this event between its record packing and render launches
             pack_ev = torch.cuda.Event(enable_timing=True)
             pack_ev.record()   # creates the event; the library records it again after packing

@@ -20,9 +20,10 @@ def test_compiled_configurations():
     assert [r[0] for r in cfg["fwd"]] == list(range(len(cfg["fwd"]))) and len(cfg["fwd"]) == 6
     assert [r[0] for r in cfg["bwd"]] == list(range(len(cfg["bwd"]))) and len(cfg["bwd"]) == 6
     for rows in cfg.values():
-        pairs = [(ring, ctas) for _, ring, ctas in rows]
-        assert len(set(pairs)) == len(pairs)                   # distinct schedules
-        assert all(3 <= ring <= 4 and 2 <= ctas <= 5 for ring, ctas in pairs)
+        variants = [(impl, ring, ctas) for _, impl, ring, ctas in rows]
+        assert len(set(variants)) == len(variants)             # distinct schedules
+        assert all(impl in (0, 1, 2, 3) and 3 <= ring <= 4 and 2 <= ctas <= 5 for impl, ring, ctas in variants)
+        assert variants[0][0] == 3                             # the default family
 
 
 def test_set_and_get_config(restore_config):
@@ -52,7 +53,7 @@ def test_tuner_picks_fastest_and_caches(tmp_path, monkeypatch, restore_config):
     assert res["fwd"] == 1 and res["bwd"] == 4
     assert autotune.get_config() == (1, 4)
     cfg = autotune.configs()
-    assert res["fwd_config"] == {"ring": cfg["fwd"][1][1], "ctas_per_sm": cfg["fwd"][1][2]}
+    assert res["fwd_config"] == {"impl": cfg["fwd"][1][1], "ring": cfg["fwd"][1][2], "ctas_per_sm": cfg["fwd"][1][3]}
     # the adjoint configurations are timed with the chosen forward one in force
     assert all(f == 1 for kind, f, _ in seen if kind == "bwd")
     stored = json.loads(cache.read_text())["gpu|w"]

@@ -1,5 +1,5 @@
-"""Every compiled launch configuration of the render kernels (ring slots x CTAs per SM) gives
-the same results, and the autotuner picks one of them and leaves it in force."""
+"""Every compiled launch variant of the render kernels (kernel family x ring slots x CTAs per
+SM) gives the same results, and the autotuner picks one of them and leaves it in force."""
 from __future__ import annotations
 
 import numpy as np
@@ -44,12 +44,12 @@ def test_all_configurations_agree(step):
     AT.set_config(0, 0)
     ref, T = _fwd(step)
     dv0, dr0, ds0 = _bwd(step, T)
-    for i, _, _ in cfg["fwd"]:
+    for i, *_ in cfg["fwd"]:
         AT.set_config(i, 0)
         out, _ = _fwd(step)
         for a, b in zip(out, ref):
             assert np.array_equal(a, b), f"forward configuration {i} differs"
-    for j, _, _ in cfg["bwd"]:
+    for j, *_ in cfg["bwd"]:
         AT.set_config(0, j)
         dv, dr, ds = _bwd(step, T)
         # float atomics: summation order only
