@@ -853,14 +853,34 @@ __global__ void center_len_kernel(int N, const float* __restrict__ centers, cons
                                            centers[3 * (size_t)i + 2], lengths[i]);
 }
 
+// Per-voxel block of the record packing's gathers: centre and size, then the 8 corner SDF
+// values, in one 64-byte-aligned block (one DRAM burst per gathered voxel instead of two).
+struct __align__(64) VoxBlock {
+    float4 cl, g0, g1, pad;
+};
+__global__ void vox_block_kernel(int N, const float* __restrict__ centers, const float* __restrict__ lengths,
+                                 const float4* __restrict__ geos, VoxBlock* __restrict__ blocks)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    VoxBlock v;
+    v.cl = make_float4(centers[3 * (size_t)i], centers[3 * (size_t)i + 1], centers[3 * (size_t)i + 2], lengths[i]);
+    v.g0 = geos[2 * (size_t)i];
+    v.g1 = geos[2 * (size_t)i + 1];
+    v.pad = make_float4(0.f, 0.f, 0.f, 0.f);
+    blocks[i] = v;
+}
+
 // Gather each sorted record's voxel data into one 80-byte record.  The record's view is
-// the view of its tile, read from the sorted key.
+// the view of its tile, read from the sorted key.  The voxel's centre, size and corner values
+// come from `blocks` when given, else from center_len (when given) or the plain arrays and
+// geos.
 __global__ void __launch_bounds__(256) pack_records_kernel(
     const __grid_constant__ Views V, int N, int64_t R, const BinMeta* __restrict__ meta,
     const void* __restrict__ keys, const uint32_t* __restrict__ vals, const uint2* __restrict__ bboxes,
     const float* __restrict__ centers, const float* __restrict__ lengths, const float4* __restrict__ geos,
     const float* __restrict__ rgbs, int rgb_per_view, const float4* __restrict__ center_len,
-    Rec* __restrict__ recs, unsigned* status)
+    const VoxBlock* __restrict__ blocks, Rec* __restrict__ recs, unsigned* status)
 {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= R || k >= meta->count) return;
@@ -871,14 +891,24 @@ __global__ void __launch_bounds__(256) pack_records_kernel(
     const uint32_t vid = val & 0x1FFFFFFFu;
     if (vid >= (uint32_t)N) { atomicOr(status, ERR_BAD_INDEX); return; }
     Rec r;
-    if (center_len) {
-        const float4 c = center_len[vid];
+    float4 g0, g1;
+    if (blocks) {
+        const float4 c = blocks[vid].cl;
         r.cx = c.x; r.cy = c.y; r.cz = c.z; r.len = c.w;
+        g0 = blocks[vid].g0;
+        g1 = blocks[vid].g1;
     } else {
-        r.cx = centers[3 * (size_t)vid]; r.cy = centers[3 * (size_t)vid + 1]; r.cz = centers[3 * (size_t)vid + 2];
-        r.len = lengths[vid];
+        if (center_len) {
+            const float4 c = center_len[vid];
+            r.cx = c.x; r.cy = c.y; r.cz = c.z; r.len = c.w;
+        } else {
+            r.cx = centers[3 * (size_t)vid]; r.cy = centers[3 * (size_t)vid + 1];
+            r.cz = centers[3 * (size_t)vid + 2];
+            r.len = lengths[vid];
+        }
+        g0 = geos[2 * (size_t)vid];
+        g1 = geos[2 * (size_t)vid + 1];
     }
-    const float4 g0 = geos[2 * (size_t)vid], g1 = geos[2 * (size_t)vid + 1];
     r.g[0] = g0.x; r.g[1] = g0.y; r.g[2] = g0.z; r.g[3] = g0.w;
     r.g[4] = g1.x; r.g[5] = g1.y; r.g[6] = g1.z; r.g[7] = g1.w;
     const size_t cb = 3 * ((rgb_per_view ? (size_t)vi * N : 0) + vid);
@@ -886,8 +916,15 @@ __global__ void __launch_bounds__(256) pack_records_kernel(
     const uint2 bb = bboxes[(size_t)vi * N + vid];
     r.bbox0 = bb.x; r.bbox1 = bb.y;
     r.val = val;
-    r.view = (uint32_t)vi;
-    r.pad = 0;
+    // corner bounds for the render filter's dead-record test (record_dead, render_pairs.cuh):
+    // min / max corner widened by 5% of the spread plus 1e-4 of the largest magnitude
+    {
+        const float lo = fminf(fminf(fminf(g0.x, g0.y), fminf(g0.z, g0.w)), fminf(fminf(g1.x, g1.y), fminf(g1.z, g1.w)));
+        const float hi = fmaxf(fmaxf(fmaxf(g0.x, g0.y), fmaxf(g0.z, g0.w)), fmaxf(fmaxf(g1.x, g1.y), fmaxf(g1.z, g1.w)));
+        const float margin = __fadd_rn(__fmul_rn(0.05f, __fsub_rn(hi, lo)), __fmul_rn(1e-4f, fmaxf(fabsf(lo), fabsf(hi))));
+        r.sdf_lo = __fsub_rn(lo, margin);
+        r.sdf_hi = __fadd_rn(hi, margin);
+    }
     const float4* src = reinterpret_cast<const float4*>(&r);
     float4* dst = reinterpret_cast<float4*>(recs + k);
 #pragma unroll
@@ -1141,16 +1178,24 @@ static int render_fwd_impl(const svr_view_t* views_host, int n_views, int N, int
     const uint32_t* order = (const uint32_t*)(im + IL.order);
     Rec* recs = (Rec*)(b + BL.recs);
     if (R > 0) {
-        // the unsorted keys (8 bytes per record slot) hold the N float4 when R >= 2N
+        // the sort's scratch pairs (8 bytes per record slot, free once sorted) hold the N
+        // 64-byte voxel blocks when R >= 8N, else the unsorted keys hold N float4 of centre and
+        // size when R >= 2N
         float4* cl = nullptr;
-        if (N > 0 && R >= 2 * (int64_t)N) {
+        VoxBlock* vb = nullptr;
+        if (N > 0 && R >= 8 * (int64_t)N) {
+            vb = (VoxBlock*)(b + BL.pairs_b);
+            vox_block_kernel<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(N, centers, lengths, (const float4*)geos,
+                                                                          vb);
+            LAUNCH_CHECK();
+        } else if (N > 0 && R >= 2 * (int64_t)N) {
             cl = (float4*)(b + BL.keys_in);
             center_len_kernel<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(N, centers, lengths, cl);
             LAUNCH_CHECK();
         }
         pack_records_kernel<<<(unsigned)((R + 255) / 256), 256, 0, st>>>(
             V, N, R, (const BinMeta*)b, b + BL.keys_out, (const uint32_t*)(b + BL.vals_out),
-            (const uint2*)(g + GL.bbox), centers, lengths, (const float4*)geos, rgbs, n_rgb_views > 1, cl, recs,
+            (const uint2*)(g + GL.bbox), centers, lengths, (const float4*)geos, rgbs, n_rgb_views > 1, cl, vb, recs,
             status);
         LAUNCH_CHECK();
     }

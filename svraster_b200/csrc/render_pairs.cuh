@@ -36,7 +36,7 @@ struct alignas(128) PairFwdSmem {
     uint32_t armed[RING];
     float4 pray[BLOCK];          // per tile pixel (row-major): rd_inv, octant | PIX_LIVE
     float4 pdir[BLOCK];          // rd, 1 / |camera ray|
-    uint32_t mask[BLOCK][4];     // candidate records of the slot, per pixel
+    alignas(16) uint32_t mask[BLOCK][4];   // candidate records of the slot, per pixel
     float4 nrm[BATCH];           // per record: corner-difference normal, its reciprocal norm
     float2 res[NWARP][32];       // alpha and depth value of the pairs of a warp's window
     uint32_t red[NWARP];
@@ -58,6 +58,16 @@ __device__ __forceinline__ int kth_set_bit(uint32_t w, int k) {
     return pos;
 }
 
+// A pixel's 128-bit candidate mask as one 16-byte shared-memory access.
+__device__ __forceinline__ uint4 load_row(const uint32_t (&m)[4]) { return *reinterpret_cast<const uint4*>(m); }
+__device__ __forceinline__ void store_row(uint32_t (&m)[4], uint4 v) { *reinterpret_cast<uint4*>(m) = v; }
+
+// Shared-memory slot of tile pixel p = dy * 16 + dx in the per-pixel arrays (rays, masks,
+// upstream gradients): bits 3 and 5 of p are folded into its low bits, so that the 8 lanes of a
+// quarter-warp reading their own pixels' 16-byte rows (lattice or 8x4 blocks) hit 8 different
+// bank groups.  An involution, hence a bijection of [0, 256).
+__device__ __forceinline__ int pix_slot(int p) { return p ^ ((((p >> 3) & 1) << 1) | ((p >> 5) & 1)); }
+
 // Pixel (dx, dy) of lane `lane` of warp `warp` in a 16x16 tile.  LATTICE: every warp owns a
 // stride-4 x stride-2 lattice spread over the whole tile, so the warps' pair counts are alike
 // and the CTA barriers wait less on the warp holding the silhouette; else 8x4 blocks.
@@ -70,6 +80,31 @@ __device__ __forceinline__ void pair_pixel(int warp, int lane, int& dx, int& dy)
         dx = (warp & 1) * 8 + (lane & 7);
         dy = (warp >> 1) * 4 + (lane >> 3);
     }
+}
+
+// Corner-difference normal of a record's SDF corners (forward.cu:422-432, backward.cu:
+// 607-618), with its reciprocal norm in .w.
+__device__ __forceinline__ float4 record_normal(const Rec& rec) {
+    const float* g = rec.g;
+    const float lin_nx = (g[4] + g[5] + g[6] + g[7]) - (g[0] + g[1] + g[2] + g[3]);
+    const float lin_ny = (g[2] + g[3] + g[6] + g[7]) - (g[0] + g[1] + g[4] + g[5]);
+    const float lin_nz = (g[1] + g[3] + g[5] + g[7]) - (g[0] + g[2] + g[4] + g[6]);
+    return make_float4(lin_nx, lin_ny, lin_nz, safe_rnorm(lin_nx, lin_ny, lin_nz));
+}
+
+// A record none of whose (pixel, record) pairs can reach MIN_ALPHA, by its SDF corners alone.
+// The packing stores the min / max corner widened by 5% of the corner spread plus 1e-4 of the
+// largest corner (points rounded just outside the voxel); if every point of the voxel then has
+// s * sdf >= 16, the logistic CDF at entry and exit is within 1.2e-7 of 1 and alpha <= 1.2e-7,
+// and if s * sdf <= -30 the CDF at entry is below 1e-13 and alpha < 1e-7 (its denominator
+// keeps 1e-6).  The forward and the adjoint skip a pair with alpha < MIN_ALPHA (1e-5)
+// entirely (forward.cu:304, backward.cu:428), so such a record is given no candidate pixels:
+// the outputs are the same bit for bit.  A NaN corner makes every evaluation NaN (alpha 0),
+// so dropping such a record is exact too; infinite corners give an infinite margin and keep
+// the record.
+__device__ __forceinline__ bool record_dead(const Rec& rec, float s_val) {
+    // rec.sdf_lo / sdf_hi: the min / max corner widened by the margin, set by the packing
+    return s_val > 0.f && (s_val * rec.sdf_lo >= 16.f || s_val * rec.sdf_hi <= -30.f);
 }
 
 // Filter test of one (record, pixel): live pixel, matching octant, slab test passed.
@@ -175,12 +210,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
     const Ray ray = pixel_ray(view, px, py);
     const uint32_t pq = ray_octant(ray.rd);
     const float s_val = *s_ptr;
-    const int p_own = dy * TILE + dx;                       // row-major pixel of the tile
+    const int p_own = pix_slot(dy * TILE + dx);             // the pixel's shared-memory slot
     S.pray[p_own] = make_float4(ray.rd_inv.x, ray.rd_inv.y, ray.rd_inv.z,
                                 __uint_as_float(pq | (inside ? PIX_LIVE : 0u)));
     S.pdir[p_own] = make_float4(ray.rd.x, ray.rd.y, ray.rd.z, ray.rd_norm_inv);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) S.mask[p_own][k] = 0u;
+    store_row(S.mask[p_own], make_uint4(0u, 0u, 0u, 0u));
 
     const uint2 range = ranges[tile];
     const int n = (int)(range.y - range.x);
@@ -229,7 +263,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
         // ---------------------------------------------------------------- F: filter
         {
             const int r = tid >> 1, h = tid & 1;
-            bool big = false;
+            bool big = false, hit = false;
             int c0 = 0, c1 = -1, r0 = 0, r1 = -1;
             uint32_t q = 0;
             float3 vc = f3(0.f, 0.f, 0.f);
@@ -237,7 +271,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
             if (r < cnt) {
                 const Rec& rec = buf[r];
                 c0 = max((int)(rec.bbox0 >> 16) - tx0, 0);
-                c1 = min((int)(rec.bbox1 >> 16) - tx0, TILE - 1);
+                c1 = record_dead(rec, s_val) ? -1 : min((int)(rec.bbox1 >> 16) - tx0, TILE - 1);
                 r0 = max((int)(rec.bbox0 & 0xFFFFu) - ty0, 0);
                 r1 = min((int)(rec.bbox1 & 0xFFFFu) - ty0, TILE - 1);
                 q = rec.val >> 29;
@@ -248,17 +282,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
                 if (!big) {
                     for (int y = r0 + h; y <= r1; y += 2)
                         for (int x = c0; x <= c1; ++x) {
-                            const int p = y * TILE + x;
-                            if (filter_hit(S.pray[p], q, vc, vl, ro)) atomicOr(&S.mask[p][r >> 5], 1u << (r & 31));
+                            const int p = pix_slot(y * TILE + x);
+                            if (filter_hit(S.pray[p], q, vc, vl, ro)) {
+                                atomicOr(&S.mask[p][r >> 5], 1u << (r & 31));
+                                hit = true;
+                            }
                         }
                 }
-                if (NORMAL && h == 0) {
-                    const float* g = rec.g;
-                    const float lin_nx = (g[4] + g[5] + g[6] + g[7]) - (g[0] + g[1] + g[2] + g[3]);
-                    const float lin_ny = (g[2] + g[3] + g[6] + g[7]) - (g[0] + g[1] + g[4] + g[5]);
-                    const float lin_nz = (g[1] + g[3] + g[5] + g[7]) - (g[0] + g[2] + g[4] + g[6]);
-                    S.nrm[r] = make_float4(lin_nx, lin_ny, lin_nz, safe_rnorm(lin_nx, lin_ny, lin_nz));
-                }
+            }
+            // the corner-difference normal, for records with a candidate pixel only
+            if (NORMAL) {
+                // every lane takes the shuffle (no short-circuit around a warp collective)
+                const bool pair_hit = __shfl_xor_sync(0xffffffffu, (int)hit, 1) != 0;
+                if (h == 0 && r < cnt && (hit || pair_hit || big)) S.nrm[r] = record_normal(buf[r]);
             }
             // records with a large rectangle: the whole warp walks its pixels
             uint32_t bigm = __ballot_sync(0xffffffffu, big && h == 0);
@@ -274,7 +310,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
                 const float bl = rec.len;
                 const int wdt = bc1 - bc0 + 1, area = wdt * (br1 - br0 + 1);
                 for (int k = lane; k < area; k += 32) {
-                    const int p = (br0 + k / wdt) * TILE + bc0 + k % wdt;
+                    const int p = pix_slot((br0 + k / wdt) * TILE + bc0 + k % wdt);
                     if (filter_hit(S.pray[p], bq, bc, bl, ro)) atomicOr(&S.mask[p][rr >> 5], 1u << (rr & 31));
                 }
             }
@@ -286,8 +322,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
             // pairs numbered over the whole CTA (thread-major); each window of BLOCK pairs is
             // evaluated one pair per thread, then every pixel folds its pairs of the window
             uint32_t mc[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) mc[k] = S.mask[p_own][k];
+            {
+                const uint4 mv = load_row(S.mask[p_own]);
+                mc[0] = mv.x; mc[1] = mv.y; mc[2] = mv.z; mc[3] = mv.w;
+            }
             const int cnt_own = __popc(mc[0]) + __popc(mc[1]) + __popc(mc[2]) + __popc(mc[3]);
             int incl = cnt_own;
 #pragma unroll
@@ -313,8 +351,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
                     cta_pair_owner(S.wcnt, S.ppre, i, t, k);
                     int odx, ody;
                     pair_pixel<LATTICE>(t >> 5, t & 31, odx, ody);
-                    const int p = ody * TILE + odx;
-                    const uint32_t om0 = S.mask[p][0], om1 = S.mask[p][1], om2 = S.mask[p][2], om3 = S.mask[p][3];
+                    const int p = pix_slot(ody * TILE + odx);
+                    const uint4 omv = load_row(S.mask[p]);
+                    const uint32_t om0 = omv.x, om1 = omv.y, om2 = omv.z, om3 = omv.w;
                     int jb = 0;
                     uint32_t wsel = om0;
                     int c = __popc(om0);
@@ -364,8 +403,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
                 }
             }
             // every owner lookup of the slot is behind the last window's barrier
-#pragma unroll
-            for (int k = 0; k < 4; ++k) S.mask[p_own][k] = 0u;
+            store_row(S.mask[p_own], make_uint4(0u, 0u, 0u, 0u));
         } else {
             // ---------------------------------------------------------------- P + C, per warp
             uint32_t m[4], mc[4];
@@ -408,7 +446,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
                     const int j = jb + kth_set_bit(wsel, k);
                     int odx, ody;
                     pair_pixel<LATTICE>(warp, ol, odx, ody);
-                    const int p = ody * TILE + odx;
+                    const int p = pix_slot(ody * TILE + odx);
                     const float4 pr = S.pray[p], pd = S.pdir[p];
                     S.res[warp][lane] = fwd_pair_eval<NS, DEPTH>(buf[j], ro, f3(pd.x, pd.y, pd.z),
                                                                  f3(pr.x, pr.y, pr.z), s_val);
@@ -572,7 +610,7 @@ struct alignas(128) PairBwdSmem {
     float4 pdc[BLOCK];           // dL/dcolor, last contributor (as bits)
     float4 pdn[BLOCK];           // dL/dnormal
     float4 pgt[BLOCK];           // target colour (R-concentration term)
-    uint32_t mask[BLOCK][4];
+    alignas(16) uint32_t mask[BLOCK][4];
     float4 nrm[BATCH];
     PairBwdRes res[NWARP][32];   // a warp's window, or (CTA-wide) the CTA's window in thread order
     float red[NWARP];
@@ -819,7 +857,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
     const Ray ray = pixel_ray(view, px, py);
     const uint32_t pq = ray_octant(ray.rd);
     const float s_val = *s_ptr;
-    const int p_own = dy * TILE + dx;
+    const int p_own = pix_slot(dy * TILE + dx);
 
     // per-pixel adjoint state (backward.cu:156-216)
     const int64_t HW = (int64_t)W * H;
@@ -852,8 +890,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
     S.pdc[p_own] = make_float4(dpix.x, dpix.y, dpix.z, __uint_as_float(last_c));
     S.pdn[p_own] = make_float4(dN.x, dN.y, dN.z, 0.f);
     if (RCONC) S.pgt[p_own] = make_float4(gt.x, gt.y, gt.z, 0.f);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) S.mask[p_own][k] = 0u;
+    store_row(S.mask[p_own], make_uint4(0u, 0u, 0u, 0u));
 
     const uint32_t rg0 = ranges[tile].x;
     const uint32_t rg1 = tile_last[tile];
@@ -903,12 +940,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
         // ---------------------------------------------------------------- F: filter
         {
             const int r = tid >> 1, h = tid & 1;
-            bool big = false;
+            bool big = false, hit = false;
             int c0 = 0, c1 = -1, r0 = 0, r1 = -1;
             if (r < cnt) {
                 const Rec& rec = buf[r];
                 c0 = max((int)(rec.bbox0 >> 16) - tx0, 0);
-                c1 = min((int)(rec.bbox1 >> 16) - tx0, TILE - 1);
+                c1 = record_dead(rec, s_val) ? -1 : min((int)(rec.bbox1 >> 16) - tx0, TILE - 1);
                 r0 = max((int)(rec.bbox0 & 0xFFFFu) - ty0, 0);
                 r1 = min((int)(rec.bbox1 & 0xFFFFu) - ty0, TILE - 1);
                 const uint32_t q = rec.val >> 29;
@@ -920,18 +957,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
                 if (!big) {
                     for (int y = r0 + h; y <= r1; y += 2)
                         for (int x = c0; x <= c1; ++x) {
-                            const int p = y * TILE + x;
-                            if (rel < __float_as_uint(S.pdc[p].w) && filter_hit(S.pray[p], q, vc, vl, ro))
+                            const int p = pix_slot(y * TILE + x);
+                            if (rel < __float_as_uint(S.pdc[p].w) && filter_hit(S.pray[p], q, vc, vl, ro)) {
                                 atomicOr(&S.mask[p][r >> 5], 1u << (r & 31));
+                                hit = true;
+                            }
                         }
                 }
-                if (NORMAL && h == 0) {
-                    const float* g = rec.g;
-                    const float lin_nx = (g[4] + g[5] + g[6] + g[7]) - (g[0] + g[1] + g[2] + g[3]);
-                    const float lin_ny = (g[2] + g[3] + g[6] + g[7]) - (g[0] + g[1] + g[4] + g[5]);
-                    const float lin_nz = (g[1] + g[3] + g[5] + g[7]) - (g[0] + g[2] + g[4] + g[6]);
-                    S.nrm[r] = make_float4(lin_nx, lin_ny, lin_nz, safe_rnorm(lin_nx, lin_ny, lin_nz));
-                }
+            }
+            // the corner-difference normal, for records with a candidate pixel only
+            if (NORMAL) {
+                // every lane takes the shuffle (no short-circuit around a warp collective)
+                const bool pair_hit = __shfl_xor_sync(0xffffffffu, (int)hit, 1) != 0;
+                if (h == 0 && r < cnt && (hit || pair_hit || big)) S.nrm[r] = record_normal(buf[r]);
             }
             uint32_t bigm = __ballot_sync(0xffffffffu, big && h == 0);
             while (bigm) {
@@ -947,7 +985,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
                 const uint32_t rel = (uint32_t)(lo + rr);
                 const int wdt = bc1 - bc0 + 1, area = wdt * (br1 - br0 + 1);
                 for (int k = lane; k < area; k += 32) {
-                    const int p = (br0 + k / wdt) * TILE + bc0 + k % wdt;
+                    const int p = pix_slot((br0 + k / wdt) * TILE + bc0 + k % wdt);
                     if (rel < __float_as_uint(S.pdc[p].w) && filter_hit(S.pray[p], bq, bc, bl, ro))
                         atomicOr(&S.mask[p][rr >> 5], 1u << (rr & 31));
                 }
@@ -960,8 +998,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
             // front); per window of BLOCK pairs: A one pair per thread, B per pixel, C one pair
             // per thread
             uint32_t m[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) m[k] = S.mask[p_own][k];
+            {
+                const uint4 mv = load_row(S.mask[p_own]);
+                m[0] = mv.x; m[1] = mv.y; m[2] = mv.z; m[3] = mv.w;
+            }
             const int cnt_own = __popc(m[0]) + __popc(m[1]) + __popc(m[2]) + __popc(m[3]);
             int incl = cnt_own;
 #pragma unroll
@@ -989,8 +1029,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
                     cta_pair_owner(S.wcnt, S.ppre, i, t, k);
                     int odx, ody;
                     pair_pixel<LATTICE>(t >> 5, t & 31, odx, ody);
-                    p = ody * TILE + odx;
-                    const uint32_t om[4] = {S.mask[p][0], S.mask[p][1], S.mask[p][2], S.mask[p][3]};
+                    p = pix_slot(ody * TILE + odx);
+                    const uint4 omv = load_row(S.mask[p]);
+                    const uint32_t om[4] = {omv.x, omv.y, omv.z, omv.w};
                     j = kth_highest_bit(om, k);
                 }
                 PairBwdRes& R = RF[tid];
@@ -1004,8 +1045,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
                 __syncthreads();   // the next window overwrites RF
             }
             // every owner lookup of the slot is behind the last window's barriers
-#pragma unroll
-            for (int k = 0; k < 4; ++k) S.mask[p_own][k] = 0u;
+            store_row(S.mask[p_own], make_uint4(0u, 0u, 0u, 0u));
         } else {
             // ---------------------------------------------------------------- per warp
             uint32_t m[4];
@@ -1038,7 +1078,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
                 const int j = has ? kth_highest_bit(om, i - opre) : 0;
                 int odx, ody;
                 pair_pixel<LATTICE>(warp, ol, odx, ody);
-                const int p = ody * TILE + odx;
+                const int p = pix_slot(ody * TILE + odx);
                 PairBwdRes& R = S.res[warp][lane];
                 // ---------------------------------------------------------- A
                 if (has) bwd_pair_A<DEPTH, NORMAL>(R, S, buf, j, p, ro, s_val);

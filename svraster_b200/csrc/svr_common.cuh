@@ -40,8 +40,7 @@ struct __align__(16) Rec {
     float r, gr, b;             // colour
     uint32_t bbox0, bbox1;      // projected bbox (x<<16 | y) min / max
     uint32_t val;               // octant << 29 | voxel id
-    uint32_t view;              // view index of the record's tile
-    uint32_t pad;
+    float sdf_lo, sdf_hi;       // corner SDF bounds widened by the rounding margin (record_dead)
 };
 static_assert(sizeof(Rec) == 80, "record must stay 80 bytes");
 
