@@ -67,6 +67,12 @@ W, H = 800, 800          # mid-size view size
 OPS_PER_PAIR = {"fwd": {"eval": (269, 16), "acc": (53, 1)},
                 "bwd": {"eval": (157, 6), "acc": (527, 24)}}
 SMS, FP32_LANES, MUFU_LANES = 148, 128, 16
+# DRAM bytes per record (dram__bytes_read.sum + dram__bytes_write.sum of one launch over the
+# records it processes: R for the forward, R' for the adjoint), from the ncu capture of the
+# batched scene's first 8 views (36.3M records, 29.8M up to the tiles' last contributors):
+# forward 3.269 GB, adjoint 3.467 GB.  A full 64-view launch is too large to capture, so its
+# traffic is this figure times its record count (pixels and records grow together).
+TRAFFIC_PER_RECORD = {"render_fwd_kernel": 3.269e9 / 36327542, "render_bwd_kernel": 3.467e9 / 29848094}
 
 
 def rank_cameras(rank=0, n_views=None, config=DEFAULT_CONFIG):
@@ -278,9 +284,9 @@ def run_ours(args, rank, world, config):
     compute = compute_ceiling(step.state, step.s_val, kname, kms, clocks.get("sm_mhz"))
     roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak,
                 "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": None,
-                "traffic_note": "DRAM bytes per launch are taken by ncu outside the bench run (the ncu "
-                                "summaries of the render kernels); none is measured in this run",
+                "traffic": int(TRAFFIC_PER_RECORD[kname] * (R_prime if kname == "render_bwd_kernel" else R)),
+                "traffic_note": "DRAM bytes per record of an ncu capture of 8 views of the batched scene, "
+                                "times this launch's records (TRAFFIC_PER_RECORD)",
                 "algorithmic_bytes": int(kbytes), "launch_ms": round(kms, 4),
                 "launch_ms_source": "CUDA events around the kernel in eager steps, on its stream",
                 "compute": compute}
