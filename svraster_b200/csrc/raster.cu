@@ -656,15 +656,18 @@ extern "C" int svr_bin_tiles(const svr_view_t* views_host, int n_views, int N, i
     // about 8 CTAs per SM in all, split over the views (as preprocess)
     const int per_view = std::max(1, std::min((N + 255) / 256, (8 * 148 + n_views - 1) / n_views));
     dim3 grid(per_view, n_views);
+    // the count kernel's per-CTA histograms [per_view, T] go to the radix path's unsorted values
+    // (4R bytes, unused here) when they fit, and the scatter reads them instead of recounting
+    uint32_t* chist = (smem_hist && R > 0 && (int64_t)per_view * T <= R) ? (uint32_t*)(b + BL.vals_in) : nullptr;
     if (N > 0) {
         if (smem_hist) {
             static std::atomic<unsigned long long> d1{0}, d2{0};
             // the limit is raised once per device, to the largest histogram this path uses
             if ((rc = ensure_smem(tile_count_kernel<true>, 4 * MAX_HIST_TILES, d1))) return rc;
             if ((rc = ensure_smem(tile_scatter_kernel<true>, 4 * MAX_HIST_TILES, d2))) return rc;
-            tile_count_kernel<true><<<grid, 256, hist_bytes, st>>>(V, N, ndup, bbox, bits, tile_cnt);
+            tile_count_kernel<true><<<grid, 256, hist_bytes, st>>>(V, N, ndup, bbox, bits, tile_cnt, chist, T);
         } else {
-            tile_count_kernel<false><<<grid, 256, 0, st>>>(V, N, ndup, bbox, bits, tile_cnt);
+            tile_count_kernel<false><<<grid, 256, 0, st>>>(V, N, ndup, bbox, bits, tile_cnt, nullptr, T);
         }
         LAUNCH_CHECK();
     }
@@ -683,9 +686,10 @@ extern "C" int svr_bin_tiles(const svr_view_t* views_host, int n_views, int N, i
     uint32_t* tile_out = (uint32_t*)(b + BL.keys_out);
     if (smem_hist)
         tile_scatter_kernel<true><<<grid, 256, hist_bytes, st>>>(V, N, ndup, bbox, bits, pair_pos, cursor, R, pa,
-                                                                 status);
+                                                                 chist, T, status);
     else
-        tile_scatter_kernel<false><<<grid, 256, 0, st>>>(V, N, ndup, bbox, bits, pair_pos, cursor, R, pa, status);
+        tile_scatter_kernel<false><<<grid, 256, 0, st>>>(V, N, ndup, bbox, bits, pair_pos, cursor, R, pa, nullptr,
+                                                         T, status);
     LAUNCH_CHECK();
     static std::atomic<unsigned long long> d3{0};
     const int ts_smem = (int)sizeof(TileSortSmem);

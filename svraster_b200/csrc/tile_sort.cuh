@@ -436,11 +436,13 @@ __device__ __forceinline__ void load_items(int i0, int v1, int vi, int N, const 
 // Records per tile.  Grid (chunks, views): each CTA visits a range of the voxels of view
 // blockIdx.y, adds the octant count of every rendered item to each tile of its rectangle in
 // a shared-memory histogram of the view's tiles (SMEM; else straight to global memory), and
-// flushes the non-zero entries with one global atomic each.
+// flushes the non-zero entries with one global atomic each; with `chist` it also stores the
+// whole histogram (row blockIdx.x of a [gridDim.x, T] array), which the scatter then reads
+// instead of counting its records again.
 template <bool SMEM>
 __global__ void __launch_bounds__(256) tile_count_kernel(
     const __grid_constant__ Views V, int N, const uint32_t* __restrict__ ndup, const uint2* __restrict__ bboxes,
-    const uint32_t* __restrict__ bits, uint32_t* __restrict__ tile_cnt)
+    const uint32_t* __restrict__ bits, uint32_t* __restrict__ tile_cnt, uint32_t* __restrict__ chist, int T)
 {
     extern __shared__ __align__(16) uint32_t hist[];
     const int vi = blockIdx.y;
@@ -469,8 +471,13 @@ __global__ void __launch_bounds__(256) tile_count_kernel(
     }
     if (SMEM) {
         __syncthreads();
-        for (int i = threadIdx.x; i < nt; i += blockDim.x)
-            if (hist[i]) atomicAdd(&tile_cnt[view.tile_offset + i], hist[i]);
+        // chist (when given): the CTA's whole histogram, row blockIdx.x, for the scatter
+        uint32_t* row = chist ? chist + (size_t)blockIdx.x * T + view.tile_offset : nullptr;
+        for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+            const uint32_t c = hist[i];
+            if (c) atomicAdd(&tile_cnt[view.tile_offset + i], c);
+            if (row) row[i] = c;
+        }
     }
 }
 
@@ -625,7 +632,8 @@ __global__ void __launch_bounds__(256) tile_offsets_kernel(
 }
 
 // Scatter of the records into their tiles' ranges.  Same grid and histogram as
-// tile_count_kernel: the CTA counts its records per tile, reserves one contiguous run per
+// tile_count_kernel: the CTA takes its records per tile from the count kernel's stored
+// histogram (chist) or counts them again, reserves one contiguous run per
 // touched tile with a global atomic on the tile's cursor, then places every record inside
 // its run with a shared-memory atomic.  Key = the (voxel, octant) pair's position in the
 // reference order (pair-order table), value = octant << 29 | voxel id, stored together.
@@ -633,7 +641,7 @@ template <bool SMEM>
 __global__ void __launch_bounds__(256) tile_scatter_kernel(
     const __grid_constant__ Views V, int N, const uint32_t* __restrict__ ndup, const uint2* __restrict__ bboxes,
     const uint32_t* __restrict__ bits, const uint32_t* __restrict__ pair_pos, uint32_t* __restrict__ cursor,
-    int64_t cap, uint2* __restrict__ kv, unsigned* __restrict__ status)
+    int64_t cap, uint2* __restrict__ kv, const uint32_t* __restrict__ chist, int T, unsigned* __restrict__ status)
 {
     extern __shared__ __align__(16) uint32_t hist[];
     const int vi = blockIdx.y;
@@ -642,20 +650,26 @@ __global__ void __launch_bounds__(256) tile_scatter_kernel(
     const int per = (N + gridDim.x - 1) / gridDim.x;
     const int v0 = blockIdx.x * per, v1 = min(N, v0 + per);
     if (SMEM) {
-        for (int i = threadIdx.x; i < nt; i += blockDim.x) hist[i] = 0u;
-        __syncthreads();
-        for (int i0 = v0 + threadIdx.x; i0 < v1; i0 += ITEM_U * blockDim.x) {
-            uint32_t qb[ITEM_U];
-            uint2 bb[ITEM_U];
-            load_items(i0, v1, vi, N, ndup, bboxes, bits, qb, bb);
+        if (chist) {
+            // the count kernel's histogram of this CTA's records (same grid, same voxel range)
+            const uint32_t* row = chist + (size_t)blockIdx.x * T + view.tile_offset;
+            for (int i = threadIdx.x; i < nt; i += blockDim.x) hist[i] = row[i];
+        } else {
+            for (int i = threadIdx.x; i < nt; i += blockDim.x) hist[i] = 0u;
+            __syncthreads();
+            for (int i0 = v0 + threadIdx.x; i0 < v1; i0 += ITEM_U * blockDim.x) {
+                uint32_t qb[ITEM_U];
+                uint2 bb[ITEM_U];
+                load_items(i0, v1, vi, N, ndup, bboxes, bits, qb, bb);
 #pragma unroll
-            for (int u = 0; u < ITEM_U; ++u) {
-                if (!qb[u]) continue;
-                const uint32_t k = __popc(qb[u]);
-                int tx0, ty0, tx1, ty1;
-                item_rect(bb[u], gx, gy, tx0, ty0, tx1, ty1);
-                for (int y = ty0; y <= ty1; ++y)
-                    for (int x = tx0; x <= tx1; ++x) atomicAdd(&hist[y * gx + x], k);
+                for (int u = 0; u < ITEM_U; ++u) {
+                    if (!qb[u]) continue;
+                    const uint32_t k = __popc(qb[u]);
+                    int tx0, ty0, tx1, ty1;
+                    item_rect(bb[u], gx, gy, tx0, ty0, tx1, ty1);
+                    for (int y = ty0; y <= ty1; ++y)
+                        for (int x = tx0; x <= tx1; ++x) atomicAdd(&hist[y * gx + x], k);
+                }
             }
         }
         __syncthreads();
