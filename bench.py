@@ -1094,17 +1094,31 @@ def run_full(args):
     e[1].record()
     torch.cuda.synchronize()
     mc_ms = e[0].elapsed_time(e[1])
-    return {"metric": "fwd+bwd Mrays/s", "value": round(rays / ms / 1e3, 3), "unit": "Mrays/s",
+    n_faces, n_verts = int(faces.shape[0]), int(verts.shape[0])
+    fused = int((wacc > 0).sum().item())
+    del tsdf, wacc, sacc, verts, faces
+    torch.cuda.empty_cache()
+    # the reference's own extension per view on a sample of the training views (its whole
+    # step over all 128 views would take minutes): rays per second of its per-view step
+    ref = {"unavailable": "skipped (--no-per-view)"}
+    if not args.no_per_view:
+        ref = run_reference_cuda(scene, cams[:8], dev, steps=2, warmup=1)
+        if "value" in ref:
+            ref["sample"] = "the first 8 of the 128 training views"
+    out = {"metric": "fwd+bwd Mrays/s", "value": round(rays / ms / 1e3, 3), "unit": "Mrays/s",
             "ms_per_step": round(ms, 3), "iters_per_s": round(1e3 / ms, 3), "steps": args.steps,
             "config": {"workload": CONFIGS["full"]["workload"], "n_voxels": scene.n_vox, "n_grid_pts": M,
                        "views": len(cams), "view_chunk": args.view_chunk, "rays_per_step": rays,
                        "records_per_chunk": records, "scene_generation_s": round(gen_s, 1)},
             "stages_ms_eager": stages, "kernels_per_step": per_step, "clocks": clk.summary(),
             "extraction": {"views": len(tcams), "render_ms": round(render_ms, 3), "tsdf_fp64_ms": round(fuse_ms, 3),
-                           "fused_points": int((wacc > 0).sum().item()), "grid_points": M,
+                           "fused_points": fused, "grid_points": M,
                            "mc_level": int(scene.octlevel.max()), "mc_voxels": int(lv12.sum().item()),
-                           "mc_ms": round(mc_ms, 3), "mc_faces": int(faces.shape[0]),
-                           "mc_verts": int(verts.shape[0])}}
+                           "mc_ms": round(mc_ms, 3), "mc_faces": n_faces, "mc_verts": n_verts},
+           "reference_cuda": ref}
+    if "value" in ref:
+        out["vs_reference_cuda"] = {"value": round(out["value"] / ref["value"], 3)}
+    return out
 
 
 def sample_views(cams):
