@@ -10,13 +10,18 @@
 //    with a large rectangle are enumerated by a whole warp.  A record costs a handful of
 //    instructions unless it has candidates, where the warp-wide filter cost every warp of
 //    the tile a 32x32 bit transpose per 32 records;
-//  * P (pairs, per warp): the warp's candidate pairs are numbered (pixel-major, record
-//    order) and evaluated 32 at a time, one pair per lane, so the SDF / logistic-CDF
-//    arithmetic runs on full warps however unevenly the pixels' candidates are spread;
+//  * P (pairs): the candidate pairs are numbered (pixel-major, record order) and evaluated
+//    one pair per lane -- per warp, 32 at a time, or (CTAW, the default) over the whole CTA,
+//    a window of 256 pairs at a time -- so the SDF / logistic-CDF arithmetic runs on full
+//    warps however unevenly the pixels' candidates are spread;
 //  * C (compositing, per pixel): each pixel folds its own pairs in record order with the
 //    forward's expressions, so every output is bit-identical to render_fwd_kernel's.
-// Two CTA barriers per slot: when the slot has arrived (every warp is then through the previous
-// slot, which is refilled), and after F.
+// Per-warp variant: a CTA barrier when the slot has arrived (every warp is then through the
+// previous slot, which is refilled) and one after F.  CTA-wide variant: no barrier at the slot's
+// start -- the candidate masks alternate between two buffers by slot parity, the record normals
+// are computed where a pair uses them, and the refill of the previous slot waits for the
+// barrier after F -- so a warp filters slot b + 1 while others still composite slot b; then the
+// barrier of the pair numbering and one per window.
 #pragma once
 
 #include <climits>
@@ -34,17 +39,19 @@ struct alignas(128) PairFwdSmem {
     Rec buf[RING][BATCH];
     uint64_t full[RING];
     uint32_t armed[RING];
-    float4 pray[BLOCK];          // per tile pixel (row-major): rd_inv, octant | PIX_LIVE
+    float4 pray[BLOCK];          // per tile pixel slot: rd_inv, octant | PIX_LIVE
     float4 pdir[BLOCK];          // rd, 1 / |camera ray|
-    alignas(16) uint32_t mask[BLOCK][4];   // candidate records of the slot, per pixel
-    float4 nrm[BATCH];           // per record: corner-difference normal, its reciprocal norm
-    float2 res[NWARP][32];       // alpha and depth value of the pairs of a warp's window
+    // candidate records of a slot, per pixel; the CTA-wide kernel alternates the two buffers
+    // by slot parity, so that a warp can filter slot b + 1 while others still composite b
+    alignas(16) uint32_t mask[2][BLOCK][4];
+    union {
+        float2 res[NWARP][32];   // per-warp windows: alpha and depth value of a warp's pairs
+        float2 cres[2][BLOCK];   // CTA-wide windows: the pairs of a window (two buffers)
+    };
     uint32_t red[NWARP];
-    // CTA-wide pair windows: the pairs of a window (two buffers), each thread's pair offset
-    // within its warp, and the warps' pair counts
-    float2 cres[2][BLOCK];
-    int ppre[BLOCK];
-    int wcnt[NWARP];
+    int ppre[BLOCK];             // CTA-wide windows: each thread's pair offset within its warp
+    int wcnt[NWARP];             // and the warps' pair counts
+    int fail;                    // a wait of this CTA timed out
 };
 
 // Position of the k-th (from 0) set bit of w (k < popc(w)).
@@ -214,7 +221,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
     S.pray[p_own] = make_float4(ray.rd_inv.x, ray.rd_inv.y, ray.rd_inv.z,
                                 __uint_as_float(pq | (inside ? PIX_LIVE : 0u)));
     S.pdir[p_own] = make_float4(ray.rd.x, ray.rd.y, ray.rd.z, ray.rd_norm_inv);
-    store_row(S.mask[p_own], make_uint4(0u, 0u, 0u, 0u));
+    store_row(S.mask[0][p_own], make_uint4(0u, 0u, 0u, 0u));
+    store_row(S.mask[1][p_own], make_uint4(0u, 0u, 0u, 0u));
 
     const uint2 range = ranges[tile];
     const int n = (int)(range.y - range.x);
@@ -222,6 +230,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
     if (tid == 0) {
 #pragma unroll
         for (int k = 0; k < RING; ++k) { mbar_init(&S.full[k], 1); S.armed[k] = 0; }
+        S.fail = 0;
         fence_mbar_init();
     }
     __syncthreads();
@@ -249,21 +258,32 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
 
     for (int b = 0; b < nbatch; ++b) {
         const int slot = b % RING;
-        if (!mbar_wait(&S.full[slot], (parity >> slot) & 1)) failed = true;
-        // every thread must reach the barriers below: a timed-out wait is agreed on by all
-        if (__syncthreads_or(failed)) { failed = true; break; }
-        parity ^= 1u << slot;
-        // every warp is through the previous slot: refill it with the batch RING ahead
-        if (tid == 0 && b >= 1 && b - 1 + RING < nbatch) {
-            fence_proxy_async_smem();
-            issue(b - 1 + RING);
+        // the slot's candidate masks: the CTA-wide kernel alternates two buffers by parity
+        uint32_t (*M)[4] = S.mask[CTAW ? (b & 1) : 0];
+        if (CTAW) {
+            // no CTA barrier here: a warp starts filtering this slot as soon as its records
+            // have arrived, while other warps may still composite the previous one.  A timed-
+            // out wait is flagged in shared memory and agreed on at the filter's barrier (the
+            // filter only indexes inside the slot and the tile).
+            if (!mbar_wait(&S.full[slot], (parity >> slot) & 1)) { failed = true; S.fail = 1; }
+            parity ^= 1u << slot;
+        } else {
+            if (!mbar_wait(&S.full[slot], (parity >> slot) & 1)) failed = true;
+            // every thread must reach the barriers below: a timed-out wait is agreed on by all
+            if (__syncthreads_or(failed)) { failed = true; break; }
+            parity ^= 1u << slot;
+            // every warp is through the previous slot: refill it with the batch RING ahead
+            if (tid == 0 && b >= 1 && b - 1 + RING < nbatch) {
+                fence_proxy_async_smem();
+                issue(b - 1 + RING);
+            }
         }
         const int cnt = min(BATCH, n - b * BATCH);
         const Rec* buf = S.buf[slot];
         // ---------------------------------------------------------------- F: filter
         {
             const int r = tid >> 1, h = tid & 1;
-            bool big = false, hit = false;
+            bool big = false;
             int c0 = 0, c1 = -1, r0 = 0, r1 = -1;
             uint32_t q = 0;
             float3 vc = f3(0.f, 0.f, 0.f);
@@ -283,18 +303,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
                     for (int y = r0 + h; y <= r1; y += 2)
                         for (int x = c0; x <= c1; ++x) {
                             const int p = pix_slot(y * TILE + x);
-                            if (filter_hit(S.pray[p], q, vc, vl, ro)) {
-                                atomicOr(&S.mask[p][r >> 5], 1u << (r & 31));
-                                hit = true;
-                            }
+                            if (filter_hit(S.pray[p], q, vc, vl, ro)) atomicOr(&M[p][r >> 5], 1u << (r & 31));
                         }
                 }
-            }
-            // the corner-difference normal, for records with a candidate pixel only
-            if (NORMAL) {
-                // every lane takes the shuffle (no short-circuit around a warp collective)
-                const bool pair_hit = __shfl_xor_sync(0xffffffffu, (int)hit, 1) != 0;
-                if (h == 0 && r < cnt && (hit || pair_hit || big)) S.nrm[r] = record_normal(buf[r]);
             }
             // records with a large rectangle: the whole warp walks its pixels
             uint32_t bigm = __ballot_sync(0xffffffffu, big && h == 0);
@@ -311,19 +322,31 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
                 const int wdt = bc1 - bc0 + 1, area = wdt * (br1 - br0 + 1);
                 for (int k = lane; k < area; k += 32) {
                     const int p = pix_slot((br0 + k / wdt) * TILE + bc0 + k % wdt);
-                    if (filter_hit(S.pray[p], bq, bc, bl, ro)) atomicOr(&S.mask[p][rr >> 5], 1u << (rr & 31));
+                    if (filter_hit(S.pray[p], bq, bc, bl, ro)) atomicOr(&M[p][rr >> 5], 1u << (rr & 31));
                 }
             }
         }
         // the masks are complete; stop streaming once every pixel is done (as of the last slot)
-        if (__syncthreads_and(done)) break;
+        if constexpr (CTAW) {
+            const int n_done = __syncthreads_count(done);
+            if (S.fail) { failed = true; break; }
+            if (n_done == BLOCK) break;
+            // every warp is through the previous slot (its compositing ended before this
+            // barrier): refill it with the batch RING ahead
+            if (tid == 0 && b >= 1 && b - 1 + RING < nbatch) {
+                fence_proxy_async_smem();
+                issue(b - 1 + RING);
+            }
+        } else {
+            if (__syncthreads_and(done)) break;
+        }
         if constexpr (CTAW) {
             // ------------------------------------------------------------ P + C, CTA-wide
             // pairs numbered over the whole CTA (thread-major); each window of BLOCK pairs is
             // evaluated one pair per thread, then every pixel folds its pairs of the window
             uint32_t mc[4];
             {
-                const uint4 mv = load_row(S.mask[p_own]);
+                const uint4 mv = load_row(M[p_own]);
                 mc[0] = mv.x; mc[1] = mv.y; mc[2] = mv.z; mc[3] = mv.w;
             }
             const int cnt_own = __popc(mc[0]) + __popc(mc[1]) + __popc(mc[2]) + __popc(mc[3]);
@@ -352,7 +375,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
                     int odx, ody;
                     pair_pixel<LATTICE>(t >> 5, t & 31, odx, ody);
                     const int p = pix_slot(ody * TILE + odx);
-                    const uint4 omv = load_row(S.mask[p]);
+                    const uint4 omv = load_row(M[p]);
                     const uint32_t om0 = omv.x, om1 = omv.y, om2 = omv.z, om3 = omv.w;
                     int jb = 0;
                     uint32_t wsel = om0;
@@ -391,7 +414,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
                         if (T > 0.5f) { med_rec = (int64_t)range.x + (int64_t)b * BATCH + j2; med_T = T; }
                     }
                     if (NORMAL) {
-                        const float4 nv = S.nrm[j2];
+                        const float4 nv = record_normal(buf[j2]);
                         Nn = Nn + pt_w * nv.w * f3(nv.x, nv.y, nv.z);
                     }
                     T *= (1.f - alpha);
@@ -403,12 +426,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
                 }
             }
             // every owner lookup of the slot is behind the last window's barrier
-            store_row(S.mask[p_own], make_uint4(0u, 0u, 0u, 0u));
+            store_row(M[p_own], make_uint4(0u, 0u, 0u, 0u));
         } else {
             // ---------------------------------------------------------------- P + C, per warp
             uint32_t m[4], mc[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) { m[k] = mc[k] = S.mask[p_own][k]; S.mask[p_own][k] = 0u; }
+            for (int k = 0; k < 4; ++k) { m[k] = mc[k] = M[p_own][k]; M[p_own][k] = 0u; }
             const int cnt_own = __popc(m[0]) + __popc(m[1]) + __popc(m[2]) + __popc(m[3]);
             int incl = cnt_own;
 #pragma unroll
@@ -474,7 +497,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
                         if (T > 0.5f) { med_rec = (int64_t)range.x + (int64_t)b * BATCH + j2; med_T = T; }
                     }
                     if (NORMAL) {
-                        const float4 nv = S.nrm[j2];
+                        const float4 nv = record_normal(buf[j2]);
                         Nn = Nn + pt_w * nv.w * f3(nv.x, nv.y, nv.z);
                     }
                     T *= (1.f - alpha);
@@ -610,12 +633,14 @@ struct alignas(128) PairBwdSmem {
     float4 pdc[BLOCK];           // dL/dcolor, last contributor (as bits)
     float4 pdn[BLOCK];           // dL/dnormal
     float4 pgt[BLOCK];           // target colour (R-concentration term)
-    alignas(16) uint32_t mask[BLOCK][4];
-    float4 nrm[BATCH];
+    // candidate records of a slot, per pixel; the CTA-wide kernel alternates the two buffers
+    // by slot parity (a warp can filter slot b + 1 while others still finish slot b)
+    alignas(16) uint32_t mask[2][BLOCK][4];
     PairBwdRes res[NWARP][32];   // a warp's window, or (CTA-wide) the CTA's window in thread order
     float red[NWARP];
     int ppre[BLOCK];             // CTA-wide windows: each thread's pair offset within its warp
     int wcnt[NWARP];             // and the warps' pair counts
+    int fail;                    // a wait of this CTA timed out
 };
 
 // Position of the k-th (from 0) highest set bit of the 128-bit mask m[0..3].
@@ -669,7 +694,7 @@ __device__ __forceinline__ void bwd_pair_A(PairBwdRes& R, const SM& S, const Rec
         const float3 c3 = f3(r.r, r.gr, r.b);
         float dL_dpt_w = dot3(f3(pc.x, pc.y, pc.z), c3);
         if (NORMAL) {
-            const float4 nv = S.nrm[j];
+            const float4 nv = record_normal(buf[j]);
             const float3 surf_n = nv.w * f3(nv.x, nv.y, nv.z);
             const float4 pn = S.pdn[p];
             dL_dpt_w += dot3(f3(pn.x, pn.y, pn.z), surf_n);
@@ -771,7 +796,7 @@ __device__ __forceinline__ void bwd_pair_C(const PairBwdRes& R, const SM& S, con
     for (int q = 0; q < 8; ++q) dg[q] = 0.f;
     if (NORMAL) {
         // backward.cu:604-639
-        const float4 nv = S.nrm[j];
+        const float4 nv = record_normal(buf[j]);
         const float3 lin_n = f3(nv.x, nv.y, nv.z);
         const float r_lin = nv.w;
         const float3 surf_n = r_lin * lin_n;
@@ -890,7 +915,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
     S.pdc[p_own] = make_float4(dpix.x, dpix.y, dpix.z, __uint_as_float(last_c));
     S.pdn[p_own] = make_float4(dN.x, dN.y, dN.z, 0.f);
     if (RCONC) S.pgt[p_own] = make_float4(gt.x, gt.y, gt.z, 0.f);
-    store_row(S.mask[p_own], make_uint4(0u, 0u, 0u, 0u));
+    store_row(S.mask[0][p_own], make_uint4(0u, 0u, 0u, 0u));
+    store_row(S.mask[1][p_own], make_uint4(0u, 0u, 0u, 0u));
 
     const uint32_t rg0 = ranges[tile].x;
     const uint32_t rg1 = tile_last[tile];
@@ -899,6 +925,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
     if (tid == 0) {
 #pragma unroll
         for (int k = 0; k < RING; ++k) { mbar_init(&S.full[k], 1); S.armed[k] = 0; }
+        S.fail = 0;
         fence_mbar_init();
     }
     __syncthreads();
@@ -925,13 +952,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
 
     for (int b = 0; b < nbatch; ++b) {
         const int slot = b % RING;
-        if (!mbar_wait(&S.full[slot], (parity >> slot) & 1)) failed = true;
-        if (__syncthreads_or(failed)) { failed = true; break; }
-        parity ^= 1u << slot;
-        // every warp is through the previous slot: refill it with the batch RING ahead
-        if (tid == 0 && b >= 1 && b - 1 + RING < nbatch) {
-            fence_proxy_async_smem();
-            issue(b - 1 + RING);
+        uint32_t (*M)[4] = S.mask[CTAW ? (b & 1) : 0];   // the slot's candidate masks
+        if (CTAW) {
+            // no CTA barrier here (see render_fwd_pairs_kernel): a timed-out wait is flagged in
+            // shared memory and agreed on at the filter's barrier
+            if (!mbar_wait(&S.full[slot], (parity >> slot) & 1)) { failed = true; S.fail = 1; }
+            parity ^= 1u << slot;
+        } else {
+            if (!mbar_wait(&S.full[slot], (parity >> slot) & 1)) failed = true;
+            if (__syncthreads_or(failed)) { failed = true; break; }
+            parity ^= 1u << slot;
+            // every warp is through the previous slot: refill it with the batch RING ahead
+            if (tid == 0 && b >= 1 && b - 1 + RING < nbatch) {
+                fence_proxy_async_smem();
+                issue(b - 1 + RING);
+            }
         }
         const int hi = n - b * BATCH;
         const int cnt = min(BATCH, hi);
@@ -940,7 +975,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
         // ---------------------------------------------------------------- F: filter
         {
             const int r = tid >> 1, h = tid & 1;
-            bool big = false, hit = false;
+            bool big = false;
             int c0 = 0, c1 = -1, r0 = 0, r1 = -1;
             if (r < cnt) {
                 const Rec& rec = buf[r];
@@ -958,18 +993,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
                     for (int y = r0 + h; y <= r1; y += 2)
                         for (int x = c0; x <= c1; ++x) {
                             const int p = pix_slot(y * TILE + x);
-                            if (rel < __float_as_uint(S.pdc[p].w) && filter_hit(S.pray[p], q, vc, vl, ro)) {
-                                atomicOr(&S.mask[p][r >> 5], 1u << (r & 31));
-                                hit = true;
-                            }
+                            if (rel < __float_as_uint(S.pdc[p].w) && filter_hit(S.pray[p], q, vc, vl, ro))
+                                atomicOr(&M[p][r >> 5], 1u << (r & 31));
                         }
                 }
-            }
-            // the corner-difference normal, for records with a candidate pixel only
-            if (NORMAL) {
-                // every lane takes the shuffle (no short-circuit around a warp collective)
-                const bool pair_hit = __shfl_xor_sync(0xffffffffu, (int)hit, 1) != 0;
-                if (h == 0 && r < cnt && (hit || pair_hit || big)) S.nrm[r] = record_normal(buf[r]);
             }
             uint32_t bigm = __ballot_sync(0xffffffffu, big && h == 0);
             while (bigm) {
@@ -987,11 +1014,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
                 for (int k = lane; k < area; k += 32) {
                     const int p = pix_slot((br0 + k / wdt) * TILE + bc0 + k % wdt);
                     if (rel < __float_as_uint(S.pdc[p].w) && filter_hit(S.pray[p], bq, bc, bl, ro))
-                        atomicOr(&S.mask[p][rr >> 5], 1u << (rr & 31));
+                        atomicOr(&M[p][rr >> 5], 1u << (rr & 31));
                 }
             }
         }
         __syncthreads();
+        if constexpr (CTAW) {
+            if (S.fail) { failed = true; break; }
+            // every warp is through the previous slot: refill it with the batch RING ahead
+            if (tid == 0 && b >= 1 && b - 1 + RING < nbatch) {
+                fence_proxy_async_smem();
+                issue(b - 1 + RING);
+            }
+        }
         if constexpr (CTAW) {
             // ------------------------------------------------------------ CTA-wide windows
             // pairs numbered over the whole CTA (thread-major, each pixel's pairs back to
@@ -999,7 +1034,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
             // per thread
             uint32_t m[4];
             {
-                const uint4 mv = load_row(S.mask[p_own]);
+                const uint4 mv = load_row(M[p_own]);
                 m[0] = mv.x; m[1] = mv.y; m[2] = mv.z; m[3] = mv.w;
             }
             const int cnt_own = __popc(m[0]) + __popc(m[1]) + __popc(m[2]) + __popc(m[3]);
@@ -1030,7 +1065,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
                     int odx, ody;
                     pair_pixel<LATTICE>(t >> 5, t & 31, odx, ody);
                     p = pix_slot(ody * TILE + odx);
-                    const uint4 omv = load_row(S.mask[p]);
+                    const uint4 omv = load_row(M[p]);
                     const uint32_t om[4] = {omv.x, omv.y, omv.z, omv.w};
                     j = kth_highest_bit(om, k);
                 }
@@ -1045,12 +1080,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
                 __syncthreads();   // the next window overwrites RF
             }
             // every owner lookup of the slot is behind the last window's barriers
-            store_row(S.mask[p_own], make_uint4(0u, 0u, 0u, 0u));
+            store_row(M[p_own], make_uint4(0u, 0u, 0u, 0u));
         } else {
             // ---------------------------------------------------------------- per warp
             uint32_t m[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) { m[k] = S.mask[p_own][k]; S.mask[p_own][k] = 0u; }
+            for (int k = 0; k < 4; ++k) { m[k] = M[p_own][k]; M[p_own][k] = 0u; }
             const int cnt_own = __popc(m[0]) + __popc(m[1]) + __popc(m[2]) + __popc(m[3]);
             int incl = cnt_own;
 #pragma unroll
