@@ -9,10 +9,11 @@ precision (libsvr_oracle64, restricted to the sampled pixels).  The bf16 path is
 the FP64 oracle given the same bf16 values (arithmetic error) and given the f32 values
 (arithmetic + storage error).
 
-Default scale: the precision configuration (the mid-size procedure at levels 6-11, 7.9M
-voxels, 32 views of 1920x1080; about 3.4 s of oracle binning per view).  SVR_PRECISION_SMALL=1
-runs the mid-size scene with 4 views of 960x540 instead.  SVR_PRECISION_OUT=<path> writes the
-error table as JSON.
+Default scale: the precision configuration's scene (the mid-size procedure at levels 6-11,
+7.9M voxels) and resolution (1920x1080), on 8 of its 32 views (about 3.4 s of oracle binning
+per view); SVR_PRECISION_VIEWS=32 runs all of them.  SVR_PRECISION_SMALL=1 runs the mid-size
+scene with 4 views of 960x540 instead.  SVR_PRECISION_OUT=<path> writes the error table as
+JSON.
 """
 from __future__ import annotations
 
@@ -78,6 +79,7 @@ def workload():
     if FULL:
         sc = S.scene_precision(seed=0)
         cams = S.fibonacci_cameras(32, 3.0, 1920, 1080, fovx_deg=50.0)
+        cams = cams[:int(os.environ.get("SVR_PRECISION_VIEWS", "8"))]
     else:
         sc = S.scene_mid(seed=0)
         cams = S.fibonacci_cameras(4, 3.0, 960, 540, fovx_deg=50.0)
