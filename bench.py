@@ -14,6 +14,8 @@ torus, levels 6-10, 8 views of 800x800); the default line carries it as ``mid_si
           step's upstream gradient planes and target image copied from pinned host memory
           and the mean transmittance read back; ``e2e_per_view`` is the same through the
           per-view API
+  native_step : the same step issued and graph-captured by the library's own host code
+          (svr_step_*, the C entry a host without Python uses), inputs resident in HBM
   reference_cuda : the reference's own CUDA extension (built from its unmodified sources)
           on the same views, per view, timed after our timed regions (a baseline leg)
   roofline : the dominant kernel's algorithmic bytes / CUDA-event duration vs the measured
@@ -390,6 +392,38 @@ def run_e2e_batched(args, scene, cams, dev):
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4, "graph_status": list(status),
             "path": "svraster_b200.step.BatchedTrainStep (C ABI, forward / backward graphs), "
                     "upstream planes from pinned host memory every step, mean T read back"}
+
+
+def run_native_step(args, scene, cams, dev):
+    """The batched step issued by the library's own host code (svr_step_create / svr_step_capture
+    / svr_step_run through ``native_step.NativeStep``; what a host without Python runs): the
+    same launches as the headline's step, recorded by the library into two CUDA graphs and
+    launched on the caller's stream, inputs resident in HBM, same timing as ``value``."""
+    import torch
+    from svraster_b200.native_step import NativeStep
+    ns = NativeStep(scene, cams, device=dev)
+    g = torch.Generator(device=dev).manual_seed(0)
+    for name in ("dcolor", "ddepth", "dnormal"):
+        buf = ns.buffer(name)
+        buf.copy_(torch.randn(buf.numel(), device=dev, generator=g))
+    kernels = ns.capture()
+    for _ in range(args.warmup):
+        ns.run()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        ns.run()
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    info, status = ns.info(), ns.status()
+    ns.close()
+    del ns
+    torch.cuda.empty_cache()
+    return {"value": round(info["pixels"] / (ms * 1e-3) / 1e6, 3), "unit": "Mrays/s", "ms_per_step": round(ms, 3),
+            "kernels_per_step": int(kernels), "records": info["capacity"], "status": list(status),
+            "path": "svr_step_create / svr_step_capture / svr_step_run (C ABI, the library's own graphs)"}
 
 
 def run_per_view(args, scene, cams, dev, host_inputs, steps=None, warmup=None):
@@ -1236,6 +1270,7 @@ def main():
         torch.cuda.empty_cache()
         if not args.no_e2e:
             result["e2e"] = run_e2e_batched(args, scene, cams, dev)
+        result["native_step"] = run_native_step(args, scene, cams, dev)
         if not args.no_per_view:
             pv = run_per_view(args, scene, cams, dev, host_inputs=False, steps=args.per_view_steps)
             result["per_view"] = pv

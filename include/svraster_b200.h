@@ -536,6 +536,105 @@ SVR_API int svr_adam_step_at(int64_t numel, int biased, int sparse, float* param
                              uint32_t* status, void* stream);
 SVR_API int svr_counter_add(int64_t* counter, int64_t delta, void* stream);
 
+/* ---------------------------------------------------------------- batched training step
+ * The whole multi-view training step as one native object, for hosts that are not Python (no
+ * counterpart in the reference, which steps one view at a time from Python, train.py:324-709).
+ * One step: corner-SDF gather, SH colour of every view, preprocess, per-tile binning, render
+ * forward (three sub-samples, depth and normal), render adjoint, the fused Laplacian +
+ * grid-Eikonal adjoint (train.py:540-620), the corner-gradient scatter to the grid points, the
+ * SH adjoint, and Adam (unbiased, dense) on grid, sh0 and shs.  The upstream gradients
+ * dL/d(colour, depth, normal, T) (the photometric and normal-consistency losses run upstream of
+ * the rasterizer) are planes the step owns and the caller fills before each step.
+ *
+ * The caller owns the octree and the parameters (device memory that must outlive the step; Adam
+ * updates grid, sh0 and shs in place).  The step owns everything else, allocated once by
+ * svr_step_create: the record buffers (sized for the record count of the views, found by one
+ * counting pass, or for desc.record_capacity), the dense grid tables of the smoothness losses
+ * (built from the octree), Adam's moments and per-step coefficient table, and the output and
+ * upstream planes.  The views' matrices and backgrounds are copied, so the caller's may go.
+ * svr_step_create synchronises `stream`; a new octree or new views need a new step object. */
+typedef struct svr_step svr_step_t;
+
+typedef struct {
+    /* octree (device): N voxels */
+    int32_t n_vox;
+    int32_t sh_degree;              /* 0..3; sh0 f32/bf16[N,3], shs f32/bf16[N, (deg+1)^2 - 1, 3] */
+    int32_t sh_bf16;                /* 1: sh0 / shs hold bf16 (uint16) values, moments stay f32 */
+    int32_t grid_res_pow2;          /* dense grid of the smoothness losses: 2^p cells per side,
+                                       p in 1..10 (train.py:599 uses the finest voxel level) */
+    const int64_t* octpath;         /* [N] */
+    const float* centers;           /* [N,3] */
+    const float* lengths;           /* [N] */
+    const uint8_t* is_leaf;         /* [N] */
+    const int64_t* vox_key;         /* [N,8] grid point of each voxel corner */
+    /* parameters (device, updated in place) */
+    float* grid;                    /* [n_grid] corner SDF values */
+    void* sh0;
+    void* shs;
+    int64_t n_grid;
+    const float* s_val;             /* [1] SDF scale, read by the render kernels */
+    /* scene box of the dense grid (train.py:180-181) */
+    float scene_center[3];
+    float inside_extent;
+    /* losses and optimiser */
+    float lambda_ls, lambda_ge;     /* Laplacian / grid-Eikonal weights (0 skips one) */
+    float lambda_R_concen;          /* colour-concentration weight; >0 reads the SVR_STEP_GT plane */
+    double lr[3];                   /* grid, sh0, shs */
+    double beta1, beta2;
+    float eps;
+    int32_t seed;                   /* smoothness sampling seed; step t uses seed + t */
+    int32_t adam_rows;              /* steps the coefficient table covers (0: 2^20) */
+    int64_t record_capacity;        /* 0: the views' record count (counted at create) */
+} svr_step_desc_t;
+
+/* Buffers of a step object, for svr_step_buffer. */
+typedef enum {
+    SVR_STEP_COLOR = 0,     /* f32[3P] rendered colour (planar per view, as svr_render_fwd) */
+    SVR_STEP_DEPTH = 1,     /* f32[4P] */
+    SVR_STEP_NORMAL = 2,    /* f32[3P] */
+    SVR_STEP_T = 3,         /* f32[P] transmittance */
+    SVR_STEP_DCOLOR = 4,    /* f32[3P] upstream dL/dcolor (caller writes) */
+    SVR_STEP_DDEPTH = 5,    /* f32[4P] upstream dL/ddepth (caller writes) */
+    SVR_STEP_DNORMAL = 6,   /* f32[3P] upstream dL/dnormal (caller writes) */
+    SVR_STEP_DT = 7,        /* f32[P] upstream dL/dT (caller writes; zero at create) */
+    SVR_STEP_GT = 8,        /* f32[3P] ground-truth colour (only when lambda_R_concen > 0) */
+    SVR_STEP_GRAD_FLAT = 9, /* f32 all parameter gradients, one contiguous buffer (the one a
+                               data-parallel host all-reduces between the two phases) */
+    SVR_STEP_GRAD_GRID = 10,/* f32[n_grid], a 256-byte aligned view into GRAD_FLAT */
+    SVR_STEP_GRAD_SH0 = 11, /* f32[N*3] */
+    SVR_STEP_GRAD_SHS = 12, /* f32[N*(M-1)*3] */
+    SVR_STEP_DVOX = 13,     /* f32[N*12] per-voxel adjoint [8 corners | rgb | |dL/dalpha*alpha|] */
+    SVR_STEP_DS = 14,       /* f32[1] dL/ds */
+    SVR_STEP_STEP = 15,     /* int64[1] Adam steps taken (device counter) */
+    SVR_STEP_N_BUFFERS = 16
+} svr_step_buffer_t;
+
+/* Phases of svr_step_run: 1 = everything up to the gradients in GRAD_FLAT, 2 = Adam (and the
+ * step counter); 3 = both.  A data-parallel host runs 1, all-reduces GRAD_FLAT, runs 2. */
+#define SVR_STEP_GRADS 1
+#define SVR_STEP_ADAM 2
+
+SVR_API int svr_step_create(const svr_step_desc_t* desc, const svr_view_t* views_host, int n_views,
+                            void* stream, svr_step_t** out_host);
+SVR_API int svr_step_destroy(svr_step_t* step);
+/* Device pointer and element count of one buffer (svr_step_buffer_t). */
+SVR_API int svr_step_buffer(const svr_step_t* step, int which, void** ptr_host, int64_t* count_host);
+/* info_host[0..7] = total pixels P, record capacity, total tiles, dense-grid table rows G,
+ * GRAD_FLAT elements, views, kernels per step (phases 1+2), whether graphs are captured. */
+SVR_API int svr_step_info(const svr_step_t* step, int64_t* info_host);
+/* Run phases of one step on `stream` (asynchronous; after svr_step_capture by graph launch). */
+SVR_API int svr_step_run(svr_step_t* step, int phases, void* stream);
+/* Capture each phase into a CUDA graph, recorded on a stream of the step's own, so that any
+ * stream, the legacy default included, may be passed; later svr_step_run calls launch the
+ * graphs on their stream.  Runs phase 1 once eagerly on `stream` first (kernel attributes are
+ * set outside the capture); parameters and the step counter are left as they were.
+ * Synchronises `stream`. */
+SVR_API int svr_step_capture(svr_step_t* step, void* stream);
+/* Status words: the raster launches' (svr_read_status bits) and the smoothness / Adam kernels'
+ * (bit 2: an index out of range or a step outside the coefficient table).  Synchronises. */
+SVR_API int svr_step_status(const svr_step_t* step, uint32_t* raster_host, uint32_t* other_host,
+                            void* stream);
+
 #ifdef __cplusplus
 }
 #endif

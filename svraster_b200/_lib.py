@@ -31,6 +31,20 @@ class ViewDesc(C.Structure):
     ]
 
 
+class StepDesc(C.Structure):
+    """Mirror of ``svr_step_desc_t`` (natural alignment, as the C compiler lays it out)."""
+    _fields_ = [
+        ("n_vox", C.c_int32), ("sh_degree", C.c_int32), ("sh_bf16", C.c_int32), ("grid_res_pow2", C.c_int32),
+        ("octpath", C.c_void_p), ("centers", C.c_void_p), ("lengths", C.c_void_p), ("is_leaf", C.c_void_p),
+        ("vox_key", C.c_void_p), ("grid", C.c_void_p), ("sh0", C.c_void_p), ("shs", C.c_void_p),
+        ("n_grid", C.c_int64), ("s_val", C.c_void_p),
+        ("scene_center", C.c_float * 3), ("inside_extent", C.c_float),
+        ("lambda_ls", C.c_float), ("lambda_ge", C.c_float), ("lambda_R_concen", C.c_float),
+        ("lr", C.c_double * 3), ("beta1", C.c_double), ("beta2", C.c_double), ("eps", C.c_float),
+        ("seed", C.c_int32), ("adam_rows", C.c_int32), ("record_capacity", C.c_int64),
+    ]
+
+
 _P, _I, _I64, _U64, _F, _D, _SZ = C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.c_float, C.c_double, C.c_size_t
 
 _SIGS = {
@@ -118,6 +132,13 @@ _SIGS = {
     "svr_adam_step_bf16_at": (_I, [_I64, _I, _I, _P, _P, _P, _P, _P, _I64, _P, _D, _D, _F, _P, _P]),
     "svr_adam_step_at": (_I, [_I64, _I, _I, _P, _P, _P, _P, _P, _I64, _P, _D, _D, _F, _P, _P]),
     "svr_counter_add": (_I, [_P, _I64, _P]),
+    "svr_step_create": (_I, [_P, _P, _I, _P, C.POINTER(C.c_void_p)]),
+    "svr_step_destroy": (_I, [_P]),
+    "svr_step_buffer": (_I, [_P, _I, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]),
+    "svr_step_info": (_I, [_P, _P]),
+    "svr_step_run": (_I, [_P, _I, _P]),
+    "svr_step_capture": (_I, [_P, _P]),
+    "svr_step_status": (_I, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), _P]),
 }
 
 _lib = None
