@@ -107,6 +107,14 @@ SVR_API int svr_bin_and_sort(const svr_view_t* views_host, int n_views, int N, i
  * 16 flags a path with bits the trimmed key would drop).  svr_workspace_query returns the
  * geom, binning and image buffer sizes {sizes[0], sizes[1], sizes[2]} for a capacity. */
 SVR_API int svr_binning_count(const void* binning_buffer, int64_t* count_host, void* stream);
+/* Candidate rows (no counterpart in the reference): the CTA-wide forward (svr_render_set_impl 3,
+ * the default) stores, for every slot of 128 records it streams, each pixel's 128-bit mask of
+ * the records whose box its ray meets; the CTA-wide adjoint then reads these rows, limited to
+ * each pixel's last contributor, instead of testing the records again (the same masks, so the
+ * same gradients).  The rows are valid after such a forward and until the next binning or a
+ * forward of another kernel family (those repack the records without rows); otherwise the
+ * adjoint filters as before.  svr_binning_candidates_valid reads that state (synchronises). */
+SVR_API int svr_binning_candidates_valid(const void* binning_buffer, int* valid_host, void* stream);
 
 /* Dense ranks (no counterpart in the reference): svr_rank_table_build sorts the trimmed rank
  * (octpath ^ octant pattern, low groups dropped as for path_or) of every (voxel, octant) pair

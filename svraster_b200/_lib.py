@@ -72,6 +72,7 @@ _SIGS = {
     "svr_render_set_config": (_I, [_I, _I]),
     "svr_render_get_config": (_I, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "svr_binning_count": (_I, [_P, C.POINTER(C.c_int64), _P]),
+    "svr_binning_candidates_valid": (_I, [_P, C.POINTER(C.c_int), _P]),
     "svr_workspace_query": (_I, [_I, _I, _I64, _I64, _I, C.POINTER(C.c_size_t)]),
     "svr_binning_buffer_bytes": (_SZ, [_I64, _I]),
     "svr_image_buffer_bytes": (_SZ, [_I64, _I]),

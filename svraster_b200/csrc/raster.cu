@@ -95,13 +95,23 @@ struct BinMeta {
     int rank_bits;     // rank bits kept in the sort key (tile id sits above them)
     int key64;         // 1 when keys are 64-bit
     long long count;   // records binned: min(total from preprocess, capacity)
-    int pad[60];
+    int cand_ok;       // 1 when the candidate rows hold the masks of the last forward over these records
+    int pad[59];
 };
 static_assert(sizeof(BinMeta) == 256, "bin meta block");
 struct BinLayout {
-    size_t keys_in, keys_out, vals_in, vals_out, tmp, tmp_bytes, recs, pairs_b, total;
+    size_t keys_in, keys_out, vals_in, vals_out, tmp, tmp_bytes, recs, pairs_b, cand, total;
+    int64_t cand_slots;
 };
-static BinLayout bin_layout(int64_t R) {
+// Candidate rows: the forward's per-pixel candidate masks of every slot it streams (SVR_BATCH
+// records of a tile), one uint4 per pixel of the tile, 4 KB per slot; the adjoint reads them
+// instead of filtering again.  Slot s of the tile with records [r0, r1) is row block
+// r0 / SVR_BATCH + tile + s: distinct for every (tile, slot), below R / SVR_BATCH + T + 1.
+#ifndef SVR_BATCH
+#define SVR_BATCH 128
+#endif
+static int64_t cand_slot_count(int64_t R, int T) { return (R > 0 ? R : 0) / SVR_BATCH + (T > 0 ? T : 0) + 1; }
+static BinLayout bin_layout(int64_t R, int T) {
     BinLayout L{};
     const int n = (int)(R > 0 ? R : 1);
     size_t t64 = 0, t32 = 0;
@@ -117,6 +127,8 @@ static BinLayout bin_layout(int64_t R) {
     L.tmp = off; L.tmp_bytes = t64 > t32 ? t64 : t32; off = align_up(off + L.tmp_bytes, 256);
     L.recs = off; off = align_up(off + sizeof(Rec) * (size_t)n, 256);
     L.pairs_b = off; off = align_up(off + 8 * (size_t)n, 256);   // per-tile sort: second (key, value) array
+    L.cand_slots = cand_slot_count(R, T);
+    L.cand = off; off = align_up(off + (size_t)L.cand_slots * BLOCK * sizeof(uint4), 256);
     L.total = off;
     return L;
 }
@@ -153,7 +165,7 @@ static ImgLayout img_layout(int64_t P, int T) {
 }
 
 extern "C" size_t svr_geom_buffer_bytes(int64_t n_items) { return geom_layout(n_items).total; }
-extern "C" size_t svr_binning_buffer_bytes(int64_t R, int total_tiles) { (void)total_tiles; return bin_layout(R).total; }
+extern "C" size_t svr_binning_buffer_bytes(int64_t R, int total_tiles) { return bin_layout(R, total_tiles).total; }
 extern "C" size_t svr_image_buffer_bytes(int64_t P, int T) { return img_layout(P, T).total; }
 
 static int build_views(const svr_view_t* vh, int n, Views& V, int& total_tiles, int64_t& total_pix) {
@@ -550,12 +562,24 @@ extern "C" int svr_binning_count(const void* binning_buffer, int64_t* count_host
     return SVR_OK;
 }
 
+extern "C" int svr_binning_candidates_valid(const void* binning_buffer, int* valid_host, void* stream)
+{
+    if (!binning_buffer || !valid_host) return svr_fail(SVR_ERR_ARG, "candidates valid: null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    int v = 0;
+    CUDA_TRY(cudaMemcpyAsync(&v, (const char*)binning_buffer + offsetof(BinMeta, cand_ok), sizeof(int),
+                             cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    *valid_host = v;
+    return SVR_OK;
+}
+
 extern "C" int svr_workspace_query(int n_views, int N, int64_t capacity, int64_t total_pixels, int total_tiles,
                                    size_t* sizes_host)
 {
     if (!sizes_host || n_views <= 0 || N < 0 || capacity < 0) return svr_fail(SVR_ERR_ARG, "workspace query");
     sizes_host[0] = geom_layout((int64_t)N * n_views).total;
-    sizes_host[1] = bin_layout(capacity).total;
+    sizes_host[1] = bin_layout(capacity, total_tiles).total;
     sizes_host[2] = img_layout(total_pixels, total_tiles).total;
     return SVR_OK;
 }
@@ -572,7 +596,7 @@ static int bin_and_sort_impl(const svr_view_t* views_host, int n_views, int N, i
     cudaStream_t st = (cudaStream_t)stream;
     const int64_t M = (int64_t)N * n_views;
     GeomLayout GL = geom_layout(M);
-    BinLayout BL = bin_layout(R);
+    BinLayout BL = bin_layout(R, T);
     ImgLayout IL = img_layout(P, T);
     if (binning_bytes < BL.total) return svr_fail(SVR_ERR_CAPACITY, "binning buffer too small");
     char* g = (char*)geom_buffer;
@@ -581,6 +605,8 @@ static int bin_and_sort_impl(const svr_view_t* views_host, int n_views, int N, i
     unsigned* status = (unsigned*)(im + IL.status);
     CUDA_TRY(cudaMemsetAsync(im + IL.ranges, 0, 8 * (size_t)T, st));
     CUDA_TRY(cudaMemsetAsync(status, 0, 4, st));
+    // new records: no forward has written their candidate rows yet
+    CUDA_TRY(cudaMemsetAsync(b + offsetof(BinMeta, cand_ok), 0, sizeof(int), st));
     if (R == 0) return tile_launch_order(T, im, IL, st);
     KeyFmt kf = key_format(path_or, T);
     if (rank_table) {
@@ -632,7 +658,7 @@ extern "C" int svr_bin_tiles(const svr_view_t* views_host, int n_views, int N, i
     cudaStream_t st = (cudaStream_t)stream;
     const int64_t M = (int64_t)N * n_views;
     GeomLayout GL = geom_layout(M);
-    BinLayout BL = bin_layout(R);
+    BinLayout BL = bin_layout(R, T);
     ImgLayout IL = img_layout(P, T);
     if (binning_bytes < BL.total) return svr_fail(SVR_ERR_CAPACITY, "binning buffer too small");
     char* g = (char*)geom_buffer;
@@ -643,6 +669,7 @@ extern "C" int svr_bin_tiles(const svr_view_t* views_host, int n_views, int N, i
     uint32_t* tile_cnt = (uint32_t*)(im + IL.tile_cnt);
     uint32_t* cursor = (uint32_t*)(im + IL.cursor);
     CUDA_TRY(cudaMemsetAsync(status, 0, 4, st));
+    CUDA_TRY(cudaMemsetAsync(b + offsetof(BinMeta, cand_ok), 0, sizeof(int), st));   // new records
     CUDA_TRY(cudaMemsetAsync(tile_cnt, 0, 4 * (size_t)T, st));
     const uint32_t* ndup = (const uint32_t*)(g + GL.ndup);
     const uint2* bbox = (const uint2*)(g + GL.bbox);
@@ -832,7 +859,7 @@ extern "C" int svr_unpack_binning(const void* binning_buffer, int64_t R, int T, 
                                   uint32_t* n_contrib, void* stream)
 {
     cudaStream_t st = (cudaStream_t)stream;
-    BinLayout BL = bin_layout(R);
+    BinLayout BL = bin_layout(R, T);
     ImgLayout IL = img_layout(P, T);
     const char* b = (const char*)binning_buffer;
     const char* im = (const char*)image_buffer;
@@ -983,7 +1010,8 @@ template <bool DEPTH, bool NORMAL, bool RCONC, bool LATTICE = true, bool CTAW = 
 static int launch_bwd_pairs(int T, int N, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
                             const uint32_t* tl, const uint32_t* nc, const Rec* recs, const float* s_val,
                             const float* out_T, const float* dc, const float* dd, const float* dn, const float* dT,
-                            float lam, const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status)
+                            float lam, const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status,
+                            const uint4* cand, const int* cand_ok)
 {
     auto k = render_bwd_pairs_kernel<DEPTH, NORMAL, RCONC, RING, MINB, LATTICE, CTAW>;
     const int smem = (int)sizeof(PairBwdSmem<RING>);
@@ -991,10 +1019,13 @@ static int launch_bwd_pairs(int T, int N, cudaStream_t st, const Views& V, const
     int rc = ensure_smem(k, smem, done);
     if (rc) return rc;
     k<<<T, BLOCK, smem, st>>>(V, N, order, ranges, tl, nc, recs, s_val, out_T, dc, dd, dn, dT, lam, gt, dvox, drgbs, ds,
-                               status);
+                               status, CTAW ? cand : nullptr, cand_ok);
     LAUNCH_CHECK();
     return SVR_OK;
 }
+
+// Set by the forward launchers: whether the kernel just launched writes the candidate rows.
+static thread_local bool t_cand_written = false;
 
 #ifndef SVR_PFWD_RING
 #define SVR_PFWD_RING 3
@@ -1007,16 +1038,18 @@ template <int NS, bool DEPTH, bool NORMAL, bool MAXW, bool COUNT, bool LATTICE =
 static int launch_fwd_pairs(int T, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
                             const Rec* recs, const float* s_val, uint32_t* tile_last, uint32_t* n_contrib,
                             float* color, float* depth, float* normal, float* outT, float* max_w, int64_t mw_stride,
-                            unsigned* status, unsigned long long* pair_count)
+                            unsigned* status, unsigned long long* pair_count, uint4* cand)
 {
     auto k = render_fwd_pairs_kernel<NS, DEPTH, NORMAL, MAXW, RING, MINB, COUNT, LATTICE, CTAW>;
     const int smem = (int)sizeof(PairFwdSmem<RING>);
     static std::atomic<unsigned long long> done{0};
     int rc = ensure_smem(k, smem, done);
     if (rc) return rc;
+    if (!CTAW) cand = nullptr;
     k<<<T, BLOCK, smem, st>>>(V, order, ranges, recs, s_val, tile_last, n_contrib, color, depth, normal, outT, max_w,
-                              mw_stride, status, pair_count);
+                              mw_stride, status, pair_count, cand);
     LAUNCH_CHECK();
+    t_cand_written = cand != nullptr;
     return SVR_OK;
 }
 
@@ -1089,6 +1122,7 @@ static int launch_fwd_cfg(int T, cudaStream_t st, const Views& V, const uint32_t
     k<<<T, BLOCK, smem, st>>>(V, order, ranges, recs, s_val, tile_last, n_contrib, color,
                               depth, normal, outT, max_w, mw_stride, status, nullptr);
     LAUNCH_CHECK();
+    t_cand_written = false;
     return SVR_OK;
 }
 
@@ -1096,9 +1130,9 @@ template <int NS, bool DEPTH, bool NORMAL, bool MAXW>
 static int launch_fwd(int T, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
                       const Rec* recs,
                       const float* s_val, uint32_t* tile_last, uint32_t* n_contrib, float* color, float* depth,
-                      float* normal, float* outT, float* max_w, int64_t mw_stride, unsigned* status)
+                      float* normal, float* outT, float* max_w, int64_t mw_stride, unsigned* status, uint4* cand)
 {
-#define FWD_PAIR_ARGS T, st, V, order, ranges, recs, s_val, tile_last, n_contrib, color, depth, normal, outT, max_w, mw_stride, status, nullptr
+#define FWD_PAIR_ARGS T, st, V, order, ranges, recs, s_val, tile_last, n_contrib, color, depth, normal, outT, max_w, mw_stride, status, nullptr, cand
 #define FWD_CFG_ARGS T, st, V, order, ranges, recs, s_val, tile_last, n_contrib, color, depth, normal, outT, max_w, mw_stride, status
     if constexpr (NS == 3 && DEPTH && NORMAL && !MAXW) {
         switch (g_fwd_cfg.load()) {       // kFwdCfgs
@@ -1172,7 +1206,7 @@ static int render_fwd_impl(const svr_view_t* views_host, int n_views, int N, int
     cudaStream_t st = (cudaStream_t)stream;
     const int64_t M = (int64_t)N * n_views;
     GeomLayout GL = geom_layout(M);
-    BinLayout BL = bin_layout(R);
+    BinLayout BL = bin_layout(R, T);
     ImgLayout IL = img_layout(P, T);
     char* g = (char*)geom_buffer;
     char* b = (char*)binning_buffer;
@@ -1212,20 +1246,30 @@ static int render_fwd_impl(const svr_view_t* views_host, int n_views, int N, int
     const bool D = need_depth != 0, Nm = need_normal != 0, MW = max_w != nullptr;
 #define FWD_CASE(NS_)                                                                                   \
     if (n_samp == NS_) {                                                                                \
-        if (D && Nm && !MW) return launch_fwd<NS_, true, true, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status); \
-        if (D && Nm && MW) return launch_fwd<NS_, true, true, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status); \
-        if (D && !Nm && !MW) return launch_fwd<NS_, true, false, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status); \
-        if (D && !Nm && MW) return launch_fwd<NS_, true, false, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status); \
-        if (!D && Nm && !MW) return launch_fwd<NS_, false, true, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status); \
-        if (!D && Nm && MW) return launch_fwd<NS_, false, true, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status); \
-        if (!D && !Nm && !MW) return launch_fwd<NS_, false, false, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status); \
-        return launch_fwd<NS_, false, false, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status); \
+        if (D && Nm && !MW) return launch_fwd<NS_, true, true, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status, cand); \
+        if (D && Nm && MW) return launch_fwd<NS_, true, true, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status, cand); \
+        if (D && !Nm && !MW) return launch_fwd<NS_, true, false, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status, cand); \
+        if (D && !Nm && MW) return launch_fwd<NS_, true, false, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status, cand); \
+        if (!D && Nm && !MW) return launch_fwd<NS_, false, true, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status, cand); \
+        if (!D && Nm && MW) return launch_fwd<NS_, false, true, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status, cand); \
+        if (!D && !Nm && !MW) return launch_fwd<NS_, false, false, false>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status, cand); \
+        return launch_fwd<NS_, false, false, true>(T, st, V, order, ranges, recs, s_val, tl, nc, out_color, out_depth, out_normal, out_T, max_w, mw_stride, status, cand); \
     }
-    FWD_CASE(1)
-    FWD_CASE(2)
-    FWD_CASE(3)
+    uint4* cand = (uint4*)(b + BL.cand);
+    t_cand_written = false;
+    auto dispatch = [&]() -> int {
+        FWD_CASE(1)
+        FWD_CASE(2)
+        FWD_CASE(3)
+        return svr_fail(SVR_ERR_UNSUPPORTED, "n_samp");
+    };
 #undef FWD_CASE
-    return svr_fail(SVR_ERR_UNSUPPORTED, "n_samp");
+    rc = dispatch();
+    if (rc) return rc;
+    // the adjoint may read the candidate rows only when this forward wrote them: it packed the
+    // records they refer to
+    CUDA_TRY(cudaMemsetAsync(b + offsetof(BinMeta, cand_ok), t_cand_written ? 1 : 0, 1, st));
+    return SVR_OK;
 }
 
 // The pair-counting instance of the forward (three sub-samples, depth and normal on, the
@@ -1242,7 +1286,7 @@ extern "C" int svr_render_fwd_count_pairs(const svr_view_t* views_host, int n_vi
     if (!out_color || !out_depth || !out_normal || !out_T || !s_val || !pair_count)
         return svr_fail(SVR_ERR_ARG, "render_fwd_count_pairs: null argument");
     cudaStream_t st = (cudaStream_t)stream;
-    BinLayout BL = bin_layout(R);
+    BinLayout BL = bin_layout(R, T);
     ImgLayout IL = img_layout(P, T);
     char* b = (char*)binning_buffer;
     char* im = (char*)image_buffer;
@@ -1253,7 +1297,7 @@ extern "C" int svr_render_fwd_count_pairs(const svr_view_t* views_host, int n_vi
                                                             s_val, (uint32_t*)(im + IL.tile_last),
                                                             (uint32_t*)(im + IL.n_contrib), out_color, out_depth,
                                                             out_normal, out_T, nullptr, 0,
-                                                            (unsigned*)(im + IL.status), pair_count);
+                                                            (unsigned*)(im + IL.status), pair_count, nullptr);
     auto k = render_fwd_kernel<3, true, true, false, SVR_NSLOT, SVR_FWD_MINB, true>;
     const int smem = (int)sizeof(FwdSmem<SVR_NSLOT>);
     static std::atomic<unsigned long long> done{0};
@@ -1271,7 +1315,8 @@ template <bool DEPTH, bool NORMAL, bool RCONC, int RING, int MINB>
 static int launch_bwd_cfg(int T, int N, cudaStream_t st, const Views& V, const uint32_t* order, const uint2* ranges,
                           const uint32_t* tl, const uint32_t* nc, const Rec* recs, const float* s_val,
                           const float* out_T, const float* dc, const float* dd, const float* dn, const float* dT,
-                          float lam, const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status)
+                          float lam, const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status,
+                          const uint4*, const int*)
 {
     auto k = render_bwd_kernel<DEPTH, NORMAL, RCONC, RING, MINB>;
     const int smem = (int)sizeof(BwdSmem<RING>);
@@ -1289,9 +1334,10 @@ static int launch_bwd(int T, int N, cudaStream_t st, const Views& V, const uint3
                       const uint32_t* tl,
                       const uint32_t* nc, const Rec* recs, const float* s_val, const float* out_T,
                       const float* dc, const float* dd, const float* dn, const float* dT, float lam,
-                      const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status)
+                      const float* gt, float* dvox, float* drgbs, float* ds, unsigned* status, const uint4* cand,
+                      const int* cand_ok)
 {
-#define BWD_CFG_ARGS T, N, st, V, order, ranges, tl, nc, recs, s_val, out_T, dc, dd, dn, dT, lam, gt, dvox, drgbs, ds, status
+#define BWD_CFG_ARGS T, N, st, V, order, ranges, tl, nc, recs, s_val, out_T, dc, dd, dn, dT, lam, gt, dvox, drgbs, ds, status, cand, cand_ok
     if constexpr (DEPTH && NORMAL) {
         switch (g_bwd_cfg.load()) {       // kBwdCfgs
             case 1: return launch_bwd_pairs<DEPTH, NORMAL, RCONC, true, true, 3, 2>(BWD_CFG_ARGS);
@@ -1328,7 +1374,7 @@ extern "C" int svr_render_bwd(const svr_view_t* views_host, int n_views, int N, 
         (need_normal && !dL_dnormal) || (lambda_R_concen > 0 && !gt_color))
         return svr_fail(SVR_ERR_ARG, "render_bwd: null argument");
     cudaStream_t st = (cudaStream_t)stream;
-    BinLayout BL = bin_layout(R);
+    BinLayout BL = bin_layout(R, T);
     ImgLayout IL = img_layout(P, T);
     char* b = (char*)binning_buffer;
     char* im = (char*)image_buffer;
@@ -1338,7 +1384,9 @@ extern "C" int svr_render_bwd(const svr_view_t* views_host, int n_views, int N, 
     const uint32_t* nc = (const uint32_t*)(im + IL.n_contrib);
     const Rec* recs = (const Rec*)(b + BL.recs);
     const bool D = need_depth != 0, Nm = need_normal != 0, RC = lambda_R_concen > 0;
-#define BWD_ARGS T, N, st, V, (const uint32_t*)(im + IL.order), ranges, tl, nc, recs, s_val, out_T, dL_dcolor, dL_ddepth, dL_dnormal, dL_dT, lambda_R_concen, gt_color, dL_dvox, drgbs, dL_ds, status
+    const uint4* cand = (const uint4*)(b + BL.cand);
+    const int* cand_ok = (const int*)(b + offsetof(BinMeta, cand_ok));
+#define BWD_ARGS T, N, st, V, (const uint32_t*)(im + IL.order), ranges, tl, nc, recs, s_val, out_T, dL_dcolor, dL_ddepth, dL_dnormal, dL_dT, lambda_R_concen, gt_color, dL_dvox, drgbs, dL_ds, status, cand, cand_ok
     if (D && Nm && RC) return launch_bwd<true, true, true>(BWD_ARGS);
     if (D && Nm && !RC) return launch_bwd<true, true, false>(BWD_ARGS);
     if (D && !Nm && RC) return launch_bwd<true, false, true>(BWD_ARGS);

@@ -21,7 +21,8 @@
 // start -- the candidate masks alternate between two buffers by slot parity, the record normals
 // are computed where a pair uses them, and the refill of the previous slot waits for the
 // barrier after F -- so a warp filters slot b + 1 while others still composite slot b; then the
-// barrier of the pair numbering and one per window.
+// barrier of the pair numbering and one per window.  The CTA-wide variant also stores each
+// slot's masks (one 16-byte row per pixel, the candidate rows) for the adjoint.
 #pragma once
 
 #include <climits>
@@ -199,7 +200,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
     uint32_t* __restrict__ n_contrib,
     float* __restrict__ out_color, float* __restrict__ out_depth, float* __restrict__ out_normal,
     float* __restrict__ out_T, float* __restrict__ max_w, int64_t max_w_stride, unsigned* __restrict__ status,
-    unsigned long long* __restrict__ pair_count)
+    unsigned long long* __restrict__ pair_count, uint4* __restrict__ cand)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     PairFwdSmem<RING>& S = *reinterpret_cast<PairFwdSmem<RING>*>(smem_raw);
@@ -337,6 +338,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_fwd_pairs_kernel(
                 fence_proxy_async_smem();
                 issue(b - 1 + RING);
             }
+            // the slot's candidate row of this thread's pixel, for the adjoint (row block
+            // range.x / BATCH + tile + b; thread tid owns the same pixel there)
+            if (cand) cand[((size_t)(range.x / BATCH) + (size_t)tile + (size_t)b) * BLOCK + tid] = load_row(M[p_own]);
         } else {
             if (__syncthreads_and(done)) break;
         }
@@ -602,7 +606,11 @@ namespace svr {
 // The adjoint of render_bwd_kernel (cuda/src/backward.cu:41-851, SDF, three sub-samples) with
 // the same per-pair expressions, split so that the expensive per-pair arithmetic runs on full
 // warps.  Per ring slot (records back to front):
-//  * F: as the forward's filter, with each pixel's limit of its last contributor;
+//  * F: as the forward's filter, with each pixel's limit of its last contributor -- or, when
+//    the last forward over these records was the CTA-wide one, that forward's candidate row of
+//    the pixel read back (one 16-byte load, issued a slot ahead) and cut at the same limit,
+//    which gives the same masks without testing a record again.  Slots are the forward's:
+//    records [s * BATCH, (s + 1) * BATCH) of the tile, taken from the last one down;
 //  * per warp, pairs numbered pixel-major and, within a pixel, in descending record order;
 //    for every window of 32 pairs:
 //    A (one pair per lane): alpha, dL/d(point weight) and the alpha, logistic-CDF and depth
@@ -864,7 +872,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
     const float* __restrict__ out_T, const float* __restrict__ dL_dcolor, const float* __restrict__ dL_ddepth,
     const float* __restrict__ dL_dnormal, const float* __restrict__ dL_dT, float lambda_R,
     const float* __restrict__ gt_color, float* __restrict__ dL_dvox, float* __restrict__ drgbs,
-    float* __restrict__ dL_ds, unsigned* __restrict__ status)
+    float* __restrict__ dL_ds, unsigned* __restrict__ status, const uint4* __restrict__ cand,
+    const int* __restrict__ cand_ok)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     PairBwdSmem<RING>& S = *reinterpret_cast<PairBwdSmem<RING>*>(smem_raw);
@@ -929,15 +938,16 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
         fence_mbar_init();
     }
     __syncthreads();
-    // batch b covers relative records [hi - c, hi) with hi = n - b*BATCH (back to front)
+    // batch b (back to front) is the forward's slot nbatch - 1 - b: relative records
+    // [lo, lo + c) with lo = (nbatch - 1 - b) * BATCH, c = min(BATCH, n - lo)
     auto issue = [&](int b) {
         const int slot = b % RING;
-        const int hi = n - b * BATCH;
-        const int c = min(BATCH, hi);
+        const int lo = (nbatch - 1 - b) * BATCH;
+        const int c = min(BATCH, n - lo);
         const uint32_t bytes = (uint32_t)c * (uint32_t)sizeof(Rec);
         ++S.armed[slot];
         mbar_arrive_tx(&S.full[slot], bytes);
-        bulk_g2s(S.buf[slot], recs + rg0 + (hi - c), bytes, &S.full[slot]);
+        bulk_g2s(S.buf[slot], recs + rg0 + lo, bytes, &S.full[slot]);
     };
     if (tid == 0)
         for (int b = 0; b < min(RING, nbatch); ++b) issue(b);
@@ -949,6 +959,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
     uint32_t parity = 0;
     bool failed = false;
     const int tx0 = tx * TILE, ty0 = ty * TILE;
+    // the forward's candidate rows of this tile, when the last forward over these records wrote
+    // them: the filter is then one row read per slot (prefetched a slot ahead), limited to the
+    // pixel's last contributor -- the same masks the filter below computes
+    const bool use_cand = CTAW && cand != nullptr && *cand_ok != 0;
+    const size_t cand0 = (size_t)(rg0 / BATCH) + (size_t)tile;
+    uint4 crow = make_uint4(0u, 0u, 0u, 0u);
+    if (use_cand && nbatch > 0) crow = cand[(cand0 + (size_t)(nbatch - 1)) * BLOCK + tid];
 
     for (int b = 0; b < nbatch; ++b) {
         const int slot = b % RING;
@@ -968,12 +985,20 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
                 issue(b - 1 + RING);
             }
         }
-        const int hi = n - b * BATCH;
-        const int cnt = min(BATCH, hi);
-        const int lo = hi - cnt;                      // relative index of slot entry 0
+        const int lo = (nbatch - 1 - b) * BATCH;      // relative index of slot entry 0
+        const int cnt = min(BATCH, n - lo);
         const Rec* buf = S.buf[slot];
         // ---------------------------------------------------------------- F: filter
-        {
+        if (use_cand) {
+            // bits r of the forward's row with lo + r below the pixel's last contributor count
+            const uint4 row = crow;
+            if (b + 1 < nbatch) crow = cand[(cand0 + (size_t)(nbatch - 2 - b)) * BLOCK + tid];
+            const int k = min(max((int)last_c - lo, 0), BATCH);
+            const uint32_t k0 = (uint32_t)min(k, 32), k1 = (uint32_t)min(max(k - 32, 0), 32);
+            const uint32_t k2 = (uint32_t)min(max(k - 64, 0), 32), k3 = (uint32_t)min(max(k - 96, 0), 32);
+            auto low = [](uint32_t c) { return c >= 32u ? 0xffffffffu : (1u << c) - 1u; };
+            store_row(M[p_own], make_uint4(row.x & low(k0), row.y & low(k1), row.z & low(k2), row.w & low(k3)));
+        } else {
             const int r = tid >> 1, h = tid & 1;
             bool big = false;
             int c0 = 0, c1 = -1, r0 = 0, r1 = -1;

@@ -150,6 +150,14 @@ class RasterState:
               "svr_binning_count")
         return int(n.value)
 
+    def candidates_valid(self):
+        """Whether the adjoint will read the forward's candidate rows (svr_binning_candidates_valid);
+        synchronises."""
+        v = C.c_int(0)
+        check(_lib.load().svr_binning_candidates_valid(ptr(self.binning), C.byref(v), stream_ptr(self.device)),
+              "svr_binning_candidates_valid")
+        return bool(v.value)
+
     # -------------------------------------------------------------- introspection (tests)
     def status(self):
         st = C.c_uint32(0)
