@@ -72,9 +72,11 @@ SMS, FP32_LANES, MUFU_LANES = 148, 128, 16
 # DRAM bytes per record (dram__bytes_read.sum + dram__bytes_write.sum of one launch over the
 # records it processes: R for the forward, R' for the adjoint), from the ncu capture of the
 # batched scene's first 8 views (36.3M records, 29.8M up to the tiles' last contributors):
-# forward 3.269 GB, adjoint 3.467 GB.  A full 64-view launch is too large to capture, so its
-# traffic is this figure times its record count (pixels and records grow together).
-TRAFFIC_PER_RECORD = {"render_fwd_kernel": 3.269e9 / 36327542, "render_bwd_kernel": 3.467e9 / 29848094}
+# forward 4.461 GB (1.17 GB of it the candidate rows it writes for the adjoint), adjoint
+# 4.406 GB (0.94 GB of it those rows read back).  A full 64-view launch is too large to
+# capture, so its traffic is this figure times its record count (pixels and records grow
+# together).
+TRAFFIC_PER_RECORD = {"render_fwd_kernel": 4.461e9 / 36327542, "render_bwd_kernel": 4.406e9 / 29848094}
 
 
 def rank_cameras(rank=0, n_views=None, config=DEFAULT_CONFIG):

@@ -57,3 +57,11 @@ def test_null_arguments_are_rejected_before_any_cuda_call():
     assert lib.svr_laplacian_bw_noalloc(*args) == -1
     args[5] = 256                      # above the static index: capacity
     assert lib.svr_laplacian_bw_noalloc(*args) == -3
+
+
+def test_candidate_row_query_rejects_null_arguments():
+    import ctypes as C
+    lib = _lib.load()
+    v = C.c_int(7)
+    assert lib.svr_binning_candidates_valid(None, C.byref(v), None) == -1
+    assert v.value == 7
