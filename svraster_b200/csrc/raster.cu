@@ -3,13 +3,16 @@
 // Behaviour follows the reference's SDF path (cuda/src/preprocess.cu, forward.cu,
 // backward.cu); the organisation is ours:
 //  * all stages take a batch of views (one launch per stage for the whole batch);
-//  * binning sorts a key trimmed to the octree levels in use (order-equivalent to the
-//    reference's 64-bit [tile | rank] key), then gathers each sorted record into an
-//    80-byte AoS stream so a tile's records reach shared memory with one bulk copy;
-//  * the render kernels double-buffer those copies on mbarriers, pre-filter records per
-//    warp (8x4 pixel footprint + octant set) once per record instead of once per pixel,
-//    and the adjoint accumulates per-record gradients in shared memory so each record
-//    reaches global memory with one vector atomic per CTA instead of one per pixel.
+//  * binning gives the reference's record order either by a radix sort of a key trimmed to
+//    the octree levels in use (order-equivalent to its 64-bit [tile | rank] key) or, in the
+//    training step, by per-tile counting, scatter and a one-CTA-per-tile sort over a
+//    pair-order table (tile_sort.cuh); each sorted record is then packed into an 80-byte
+//    AoS stream so a tile's records reach shared memory with one bulk copy per slot;
+//  * the render kernels (render_pairs.cuh) stream 128-record slots through an mbarrier
+//    ring, filter each slot's records once for the whole tile, and evaluate the candidate
+//    (pixel, record) pairs on full warps; the forward stores each slot's candidate masks,
+//    which the adjoint reads back instead of filtering again, and the adjoint sends each
+//    pair's gradients with vector reductions.
 #include <algorithm>
 #include <atomic>
 #include <cstddef>

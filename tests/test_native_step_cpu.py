@@ -71,3 +71,25 @@ def test_null_handles():
     assert L.svr_step_info(None, (C.c_int64 * 8)()) == -1
     assert L.svr_step_status(None, C.byref(r), C.byref(o), None) == -1
     assert L.svr_step_destroy(None) == 0
+
+
+def test_python_buffer_names_match_the_header_enum():
+    import os
+    import re
+    from svraster_b200 import native_step
+    hdr = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                            "svraster_b200.h")).read()
+    enum = {m.group(1).lower(): int(m.group(2)) for m in re.finditer(r"SVR_STEP_([A-Z0-9_]+) = (\d+)", hdr)}
+    n = enum.pop("n_buffers")
+    assert len(native_step.BUFFERS) == n == len(enum)
+    assert {k.lower(): v for k, v in native_step.BUFFERS.items()} == enum
+    assert (native_step.GRADS, native_step.ADAM) == (1, 2)
+
+
+def test_binning_buffer_holds_a_candidate_row_block_per_tile_and_per_slot():
+    """svr_binning_buffer_bytes(R, T) includes the candidate rows: 4 KB per slot of 128
+    records plus 4 KB per tile (a tile's partial slot)."""
+    lib = _lib.load()
+    R = 1_000_000
+    assert lib.svr_binning_buffer_bytes(R, 101) - lib.svr_binning_buffer_bytes(R, 100) == 4096
+    assert lib.svr_binning_buffer_bytes(R + 128 * 10, 100) - lib.svr_binning_buffer_bytes(R, 100) >= 10 * 4096
