@@ -1043,13 +1043,17 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
                 }
             }
         }
-        __syncthreads();
+        // with candidate rows each thread has written only its own row: the numbering barrier
+        // below is the slot's first, and the timeout check and the refill follow it there
+        if (!use_cand) __syncthreads();
         if constexpr (CTAW) {
-            if (S.fail) { failed = true; break; }
-            // every warp is through the previous slot: refill it with the batch RING ahead
-            if (tid == 0 && b >= 1 && b - 1 + RING < nbatch) {
-                fence_proxy_async_smem();
-                issue(b - 1 + RING);
+            if (!use_cand) {
+                if (S.fail) { failed = true; break; }
+                // every warp is through the previous slot: refill it with the batch RING ahead
+                if (tid == 0 && b >= 1 && b - 1 + RING < nbatch) {
+                    fence_proxy_async_smem();
+                    issue(b - 1 + RING);
+                }
             }
         }
         if constexpr (CTAW) {
@@ -1072,6 +1076,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) render_bwd_pairs_kernel(
             S.ppre[tid] = incl - cnt_own;
             if (lane == 31) S.wcnt[warp] = incl;
             __syncthreads();
+            if (use_cand) {
+                if (S.fail) { failed = true; break; }
+                // every warp is through the previous slot: refill it with the batch RING ahead
+                if (tid == 0 && b >= 1 && b - 1 + RING < nbatch) {
+                    fence_proxy_async_smem();
+                    issue(b - 1 + RING);
+                }
+            }
             int pre = incl - cnt_own, total = 0;
 #pragma unroll
             for (int q = 0; q < NWARP; ++q) {
