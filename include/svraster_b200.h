@@ -639,7 +639,8 @@ SVR_API int svr_step_run(svr_step_t* step, int phases, void* stream);
  * Synchronises `stream`. */
 SVR_API int svr_step_capture(svr_step_t* step, void* stream);
 /* Status words: the raster launches' (svr_read_status bits) and the smoothness / Adam kernels'
- * (bit 2: an index out of range or a step outside the coefficient table).  Synchronises. */
+ * (bit 2: an index out of range or a step outside the coefficient table).  The second word
+ * keeps its bits for the life of the step object.  Synchronises. */
 SVR_API int svr_step_status(const svr_step_t* step, uint32_t* raster_host, uint32_t* other_host,
                             void* stream);
 
