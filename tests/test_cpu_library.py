@@ -65,3 +65,17 @@ def test_candidate_row_query_rejects_null_arguments():
     v = C.c_int(7)
     assert lib.svr_binning_candidates_valid(None, C.byref(v), None) == -1
     assert v.value == 7
+
+
+def test_binding_argument_counts_match_the_header():
+    """Every ctypes signature in _lib has as many arguments as the header's prototype."""
+    src = open(os.path.join(ROOT, "include", "svraster_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    protos = {}
+    for m in re.finditer(r"SVR_API\s+[\w\s\*]+?\b(svr_\w+)\s*\(([^;]*?)\)\s*;", src, flags=re.S):
+        params = m.group(2).strip()
+        protos[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    assert set(protos) == set(declared_symbols())
+    for name, n in protos.items():
+        assert name in _lib._SIGS, f"{name} has no ctypes signature"
+        assert len(_lib._SIGS[name][1]) == n, f"{name}: header has {n} arguments, binding {len(_lib._SIGS[name][1])}"
