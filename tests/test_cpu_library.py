@@ -79,3 +79,29 @@ def test_binding_argument_counts_match_the_header():
     for name, n in protos.items():
         assert name in _lib._SIGS, f"{name} has no ctypes signature"
         assert len(_lib._SIGS[name][1]) == n, f"{name}: header has {n} arguments, binding {len(_lib._SIGS[name][1])}"
+
+
+def test_binding_argument_types_match_the_header():
+    """Scalar arguments have the header's width (int / int64_t / size_t / float / double /
+    uint64_t), pointers are bound as pointers."""
+    import ctypes as C
+    src = open(os.path.join(ROOT, "include", "svraster_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    scalar = {"int": C.c_int, "int32_t": C.c_int, "int64_t": C.c_int64, "uint64_t": C.c_uint64,
+              "size_t": C.c_size_t, "float": C.c_float, "double": C.c_double, "uint32_t": C.c_uint32}
+    for m in re.finditer(r"SVR_API\s+[\w\s\*]+?\b(svr_\w+)\s*\(([^;]*?)\)\s*;", src, flags=re.S):
+        name, params = m.group(1), m.group(2).strip()
+        if params in ("", "void"):
+            continue
+        bound = _lib._SIGS[name][1]
+        for i, (param, ct) in enumerate(zip(params.split(","), bound)):
+            p = " ".join(param.replace("const", " ").split())
+            if "*" in p:
+                assert ct in (C.c_void_p, C.c_char_p) or hasattr(ct, "_type_") and ct.__name__.startswith("LP_"), \
+                    f"{name} argument {i} ({param.strip()}) is a pointer, bound as {ct}"
+            else:
+                base = p.split()[0]
+                assert base in scalar, f"{name} argument {i}: unknown type {param.strip()}"
+                assert C.sizeof(ct) == C.sizeof(scalar[base]) and \
+                    (ct in (C.c_float, C.c_double)) == (scalar[base] in (C.c_float, C.c_double)), \
+                    f"{name} argument {i} ({param.strip()}) bound as {ct}"
