@@ -624,6 +624,8 @@ typedef enum {
 
 SVR_API int svr_step_create(const svr_step_desc_t* desc, const svr_view_t* views_host, int n_views,
                             void* stream, svr_step_t** out_host);
+/* Waits for the device (the step's work may still be queued on the caller's streams), then
+ * frees everything the step owns. */
 SVR_API int svr_step_destroy(svr_step_t* step);
 /* Device pointer and element count of one buffer (svr_step_buffer_t). */
 SVR_API int svr_step_buffer(const svr_step_t* step, int which, void** ptr_host, int64_t* count_host);

@@ -389,8 +389,9 @@ static void drop_graphs(svr_step* h)
 extern "C" int svr_step_destroy(svr_step_t* h)
 {
     if (!h) return SVR_OK;
+    // the caller's streams may still run this step's graphs or launches: wait for the device
+    cudaDeviceSynchronize();
     drop_graphs(h);
-    if (h->cap) cudaStreamSynchronize(h->cap);
     for (void* p : h->allocs) cudaFree(p);
     if (h->cap) cudaStreamDestroy(h->cap);
     delete h;
